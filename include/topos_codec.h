@@ -1,0 +1,274 @@
+/* topos_codec.h - public C ABI of the B200 Topos Codec intra frame library.
+ *
+ * This header declares the drop-in subset of the Topos Codec C ABI that the
+ * GPU library implements, with struct layouts identical to the reference ABI
+ * version 2 (reference: native/include/topos_codec.h). Every declaration cites
+ * the reference declaration it replaces. Callers built against the reference
+ * header can link against this library unchanged for the frame path.
+ *
+ * Conventions (same as the reference ABI):
+ *  - Every public struct starts with struct_size then abi_version. Callers
+ *    zero-initialise; 0 in either field means "current". The library writes
+ *    struct_size = sizeof on structs it fills.
+ *  - Status codes are frozen; negative = error, TC_WARN_CONCEALED = +1.
+ *  - Returned const char* strings are library-owned (static or thread-local).
+ *  - All frame functions are re-entrant: state is caller-owned, errors are
+ *    thread-local, device work is issued on per-call stream leases.
+ *
+ * The tcg_* functions at the end are extensions that do not exist in the
+ * reference ABI (batched encode, device-resident buffers, serving loop); they
+ * change no reference symbol's behaviour.
+ */
+#ifndef TOPOS_CODEC_H
+#define TOPOS_CODEC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* reference: native/include/topos_codec.h:31 */
+#define TOPOS_CODEC_ABI_VERSION 2
+
+/* Status codes. reference: native/include/topos_codec.h:34-56 */
+enum {
+    TC_OK                           =   0,
+    TC_WARN_CONCEALED               =   1,
+    TC_ERR_INVALID_ARGUMENT         =  -1,
+    TC_ERR_OUT_OF_MEMORY            =  -2,
+    TC_ERR_UNSUPPORTED_VERSION      =  -3,
+    TC_ERR_UNSUPPORTED_PROFILE      =  -4,
+    TC_ERR_UNSUPPORTED_PIXEL_FORMAT =  -5,
+    TC_ERR_UNSUPPORTED_MATRIX       =  -6,
+    TC_ERR_UNSUPPORTED_ALPHA_MODE   =  -7,
+    TC_ERR_LIMIT_EXCEEDED           =  -8,
+    TC_ERR_MALFORMED                =  -9,
+    TC_ERR_TRUNCATED                = -10,
+    TC_ERR_CHECKSUM_MISMATCH        = -11,
+    TC_ERR_STATE                    = -12,
+    TC_ERR_CANCELLED                = -13,
+    TC_ERR_IO                       = -14,
+    TC_ERR_BUFFER_TOO_SMALL         = -15,
+    TC_ERR_NOT_IMPLEMENTED          = -16,
+    TC_ERR_REFERENCE_INVALID        = -17
+};
+
+/* reference: native/include/topos_codec.h:58-67 */
+typedef struct topos_version_info {
+    uint32_t    struct_size;
+    uint32_t    abi_version;
+    uint32_t    version_major;
+    uint32_t    version_minor;
+    uint32_t    version_patch;
+    const char* git_commit;
+    const char* build_target;
+    uint32_t    reserved[4];
+} topos_version_info;
+
+/* reference: native/include/topos_codec.h:70-80 */
+#define TOPOS_CPU_X86_AVX2    (1u << 0)
+#define TOPOS_CPU_X86_AVX512F (1u << 1)
+#define TOPOS_CPU_ARM_NEON    (1u << 2)
+#define TOPOS_CPU_X86_FMA     (1u << 3)
+
+typedef struct topos_cpu_features {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t flags;
+    uint32_t reserved[5];
+} topos_cpu_features;
+
+/* reference: native/include/topos_codec.h:84-104 */
+#define TC_CODEC_CAP_FULL_DECODE               (1u << 0)
+#define TC_CODEC_CAP_FIXED_REDUCED_DECODE      (1u << 1)
+#define TC_CODEC_CAP_AUTO_2K_DECODE            (1u << 2)
+#define TC_CODEC_CAP_CPU_SURFACE_OUTPUT        (1u << 3)
+#define TC_CODEC_CAP_HOST_VISIBLE_GPU_SURFACE  (1u << 4)
+#define TC_CODEC_CAP_V7A_BAND_DECODE           (1u << 5)
+#define TC_CODEC_CAP_V7B_SCALABLE_BASE         (1u << 6)
+#define TC_CODEC_CAP_DECODE_DROP_ALPHA         (1u << 7)
+
+#define TC_CODEC_MAX_DIM 16384u
+#define TC_CODEC_AUTO_2K_MAX_DIM 2048u
+
+typedef struct topos_codec_capabilities {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t flags;
+    uint32_t max_width;
+    uint32_t max_height;
+    uint32_t auto2k_max_dim;
+    uint32_t reserved[4];
+} topos_codec_capabilities;
+
+/* reference: native/include/topos_codec.h:125 */
+int32_t tc_abi_version(void);
+/* reference: native/include/topos_codec.h:128 */
+int32_t tc_version(topos_version_info* out);
+/* reference: native/include/topos_codec.h:131 */
+int32_t tc_query_cpu_features(topos_cpu_features* out);
+/* reference: native/include/topos_codec.h:135. This library advertises
+ * FULL_DECODE | CPU_SURFACE_OUTPUT (the paths it implements). */
+int32_t tc_query_capabilities(topos_codec_capabilities* out);
+/* reference: native/include/topos_codec.h:142 */
+int32_t tc_query_support(uint32_t profile, uint32_t pixel_format, uint32_t bit_depth,
+                         uint32_t alpha_mode);
+/* reference: native/include/topos_codec.h:146 */
+const char* tc_status_message(int32_t status);
+/* reference: native/include/topos_codec.h:150 */
+const char* tc_last_error(void);
+
+/* ============================ frame coding ============================ */
+
+/* reference: native/include/topos_codec.h:168-173 */
+#define TC_FRAME_MAX_PLANES 4
+#define TC_FRAME_DEFAULT_SLICE_ROWS 16u
+
+/* reference: native/include/topos_codec.h:177-224. reserved[0] low byte selects
+ * the coding generation; this library encodes 8 (V7-R2 rANS2 intra) and
+ * reserved[5] carries the V7-R2 output features (bit0 DEBLOCK, bit1 QPT2). */
+typedef struct topos_frame_config {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint16_t visible_width;
+    uint16_t visible_height;
+    uint8_t profile;
+    uint8_t pixel_format;     /* 0 YUV 4:2:2, 1 YUV 4:4:4, 2 GBR, 3 CFA */
+    uint8_t bit_depth;
+    uint8_t qmatrix_id;
+    uint8_t qp_base;
+    int8_t qp_delta_luma;
+    int8_t qp_delta_chroma;
+    uint8_t slice_rows;       /* block rows per slice; 0 = 16 */
+    uint8_t alpha_mode;       /* 0 none, 1 lossless, 2 near-lossless */
+    uint8_t alpha_bit_depth;
+    uint8_t alpha_premultiplied;
+    uint8_t color_range;
+    uint8_t color_primaries;
+    uint8_t color_transfer;
+    uint8_t color_matrix;
+    uint8_t chroma_siting;
+    uint16_t sar_num;
+    uint16_t sar_den;
+    uint32_t reserved[8];
+} topos_frame_config;
+
+/* reference: native/include/topos_codec.h:231-237. Strides are in uint16
+ * elements; 0 = tight. */
+typedef struct topos_frame_input {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    const uint16_t* planes[TC_FRAME_MAX_PLANES];
+    size_t strides[TC_FRAME_MAX_PLANES];
+    uint32_t reserved[8];
+} topos_frame_input;
+
+/* reference: native/include/topos_codec.h:240-254 */
+typedef struct topos_frame_stats {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t packet_size;
+    uint32_t color_payload_bytes;
+    uint32_t alpha_payload_bytes;
+    uint32_t color_header_bytes;
+    uint32_t alpha_header_bytes;
+    uint16_t slice_count;
+    uint8_t qp_base;
+    uint8_t reserved8;
+    uint16_t alpha_max_abs_error;
+    uint16_t reserved16;
+    uint32_t reserved[8];
+} topos_frame_stats;
+
+/* reference: native/include/topos_codec.h:257-285 */
+#define TC_FRAME_SLICE_OK 0u
+#define TC_FRAME_SLICE_CONCEALED 1u
+#define TC_MAX_SLICES 512
+
+typedef struct topos_frame_output {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint16_t visible_width;
+    uint16_t visible_height;
+    uint16_t coded_width;
+    uint16_t coded_height;
+    uint8_t plane_count;
+    uint8_t bit_depth;
+    uint8_t profile;
+    uint8_t pixel_format;
+    uint8_t alpha_mode;
+    uint8_t alpha_bit_depth;
+    uint8_t color_range;
+    uint8_t color_primaries;
+    uint8_t color_transfer;
+    uint8_t color_matrix;
+    uint8_t chroma_siting;
+    uint16_t concealed_slices;
+    uint16_t slice_count;
+    uint16_t sar_num;
+    uint16_t sar_den;
+    uint8_t slice_status[TC_MAX_SLICES];
+    uint32_t reserved[8];
+} topos_frame_output;
+
+/* reference: native/include/topos_codec.h:288 (rules: native/src/codec/codec.c:426-605) */
+int32_t tc_frame_config_validate(const topos_frame_config* cfg);
+
+/* reference: native/include/topos_codec.h:292 (native/src/codec/codec.c:607-647) */
+size_t tc_frame_packet_bound(const topos_frame_config* cfg);
+
+/* reference: native/include/topos_codec.h:296 (native/src/codec/codec.c:5970-6018).
+ * Fixed-QP V7-R2 encode on the GPU. out is written only on success;
+ * out == NULL with out_cap == 0 is a size probe (BUFFER_TOO_SMALL + stats). */
+int32_t tc_frame_encode(const topos_frame_config* cfg, const topos_frame_input* input,
+                        uint8_t* out, size_t out_cap, topos_frame_stats* stats);
+
+/* reference: native/include/topos_codec.h:336 (native/src/codec/codec.c:9005-9098).
+ * planes_out == NULL = query mode (geometry only). Damaged slices are
+ * concealed and the call returns TC_WARN_CONCEALED. */
+int32_t tc_frame_decode(const uint8_t* data, size_t size,
+                        uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
+                        const size_t strides[TC_FRAME_MAX_PLANES],
+                        topos_frame_output* out_info);
+
+/* reference: native/include/topos_codec.h:387-390 */
+typedef struct topos_batch_packet {
+    const uint8_t* data;
+    size_t size;
+} topos_batch_packet;
+
+/* reference: native/include/topos_codec.h:398 (native/src/codec/codec.c:9639-9805).
+ * planes_out is count x TC_FRAME_MAX_PLANES (row = frame); strides same shape
+ * or NULL. All frames' slices are decoded in one device launch sequence. */
+int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint32_t count,
+                              uint16_t* const* planes_out, const size_t* strides,
+                              topos_frame_output* infos);
+
+/* reference: native/include/topos_codec.h:410 (native/src/codec/codec.c:9807-9831) */
+int32_t tc_frame_plane_geometry(const topos_frame_output* info, uint32_t plane,
+                                uint32_t* width, uint32_t* height);
+
+/* ==================== extensions (no reference counterpart) ==================== */
+
+/* Batched encode: count frames (any mix of geometries and configs) coded in one
+ * device launch sequence. outs[i]/out_caps[i] receive frame i's packet; stats[i]
+ * (array of count, may be NULL) receives its stats; rcs[i] its status. Returns
+ * the first non-OK frame status (frame order), TC_OK otherwise. Each frame's
+ * packet is byte-identical to tc_frame_encode of that frame alone. */
+int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
+                               const topos_frame_input* inputs, uint32_t count,
+                               uint8_t* const* outs, const size_t* out_caps,
+                               topos_frame_stats* stats, int32_t* rcs);
+
+/* Device selection and teardown for the calling process. tcg_device_init is
+ * implicit on first use (device 0 or the current CUDA device). */
+int32_t tcg_device_init(int32_t device);
+void tcg_device_release(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOPOS_CODEC_H */
