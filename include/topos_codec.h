@@ -267,6 +267,10 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
 int32_t tcg_device_init(int32_t device);
 void tcg_device_release(void);
 
+/* Number of device kernel launches issued by this library in this process
+ * (diagnostics for benchmarks). */
+uint64_t tcg_kernel_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

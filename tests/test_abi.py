@@ -1,0 +1,144 @@
+"""The C-ABI boundary, checked without a GPU: the library loads and exports
+every symbol the public header declares, struct layouts match the reference
+ABI, and the host-side rules (config validation, packet bound, structural
+packet parse) agree with the oracle status for status."""
+import ctypes
+import os
+import random
+import re
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+from topos_codec_b200 import binding as B
+
+HEADER = os.path.join(ROOT, "include", "topos_codec.h")
+REF_HEADER = "/root/reference/native/include/topos_codec.h"
+
+
+def _declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b((?:tc|tcg)_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_every_declared_symbol_is_exported(built):
+    out = subprocess.run(["nm", "-D", "--defined-only", B.PRODUCT_LIBRARY], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if " T " in l)
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    missing = [f for f in declared if f not in exported]
+    assert not missing, missing
+    # nothing internal leaks out of the library
+    extra = [s for s in exported if not (s.startswith("tc_") or s.startswith("tcg_"))]
+    assert not extra, extra
+
+
+def test_library_loads_and_answers_queries(product):
+    L = product._lib
+    assert L.tc_abi_version() == 2
+    caps = (ctypes.c_uint32 * 10)()
+    assert L.tc_query_capabilities(caps) == 0
+    assert caps[0] == 40 and caps[3] == 16384 and (caps[2] & 1) == 1
+    L.tc_status_message.restype = ctypes.c_char_p
+    assert L.tc_status_message(ctypes.c_int32(1)).startswith(b"concealment")
+    assert L.tc_status_message(ctypes.c_int32(-99)) == b"unknown status"
+    assert L.tc_query_support(3, 0, 10, 0) == 0
+    assert L.tc_query_support(7, 0, 12, 0) == -5
+    assert L.tc_query_support(4, 0, 10, 0) == -4
+    assert L.tc_query_support(3, 0, 10, 3) == -7
+
+
+LAYOUT_PROBE = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "topos_codec.h"
+#define P(T, F) printf(#T "." #F " %zu\n", offsetof(T, F))
+int main(void) {
+  printf("cfg %zu in %zu st %zu out %zu bp %zu ver %zu caps %zu\n", sizeof(topos_frame_config),
+         sizeof(topos_frame_input), sizeof(topos_frame_stats), sizeof(topos_frame_output),
+         sizeof(topos_batch_packet), sizeof(topos_version_info), sizeof(topos_codec_capabilities));
+  P(topos_frame_config, qp_base); P(topos_frame_config, sar_num); P(topos_frame_config, reserved);
+  P(topos_frame_input, strides); P(topos_frame_stats, slice_count); P(topos_frame_stats, alpha_max_abs_error);
+  P(topos_frame_output, concealed_slices); P(topos_frame_output, slice_status); P(topos_frame_output, reserved);
+  return 0;
+}
+"""
+
+
+def _layout(include_dir, tmp_path, tag):
+    src = tmp_path / f"probe_{tag}.c"
+    exe = tmp_path / f"probe_{tag}"
+    src.write_text(LAYOUT_PROBE)
+    subprocess.run(["gcc", "-std=c11", f"-I{include_dir}", str(src), "-o", str(exe)], check=True)
+    return subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+
+
+def test_struct_layouts(tmp_path):
+    mine = _layout(os.path.dirname(HEADER), tmp_path, "mine")
+    sizes = dict(zip(mine.split()[0:14:2], map(int, mine.split()[1:14:2])))
+    assert sizes["cfg"] == ctypes.sizeof(B.FrameConfig)
+    assert sizes["in"] == ctypes.sizeof(B.FrameInput)
+    assert sizes["st"] == ctypes.sizeof(B.FrameStats)
+    assert sizes["out"] == ctypes.sizeof(B.FrameOutput)
+    if os.path.exists(REF_HEADER):
+        assert mine == _layout(os.path.dirname(REF_HEADER), tmp_path, "ref")
+
+
+def _rand_cfg(rng):
+    c = B.make_config(rng.choice([0, 1, 7, 64, 1920, 16384, 16385]), rng.choice([0, 1, 9, 1080, 16384]),
+                      qp=rng.choice([0, 8, 63, 64, 95, 96]), qmatrix_id=rng.choice([0, 1, 2, 3, 4, 5]),
+                      pixel_format=rng.choice([0, 0, 1, 2, 3, 4]), bit_depth=rng.choice([0, 10, 12, 16, 8]),
+                      profile=rng.choice([0, 3, 3, 5, 6, 7, 2]), slice_rows=rng.choice([0, 1, 2, 16, 255]),
+                      alpha_mode=rng.choice([0, 0, 1, 2, 3]), alpha_bit_depth=rng.choice([0, 8, 10, 16]),
+                      features=rng.choice([0, 1, 2, 3, 4]), color_matrix=rng.choice([0, 1, 5, 2]),
+                      color_range=rng.choice([0, 1, 2]), chroma_siting=rng.choice([0, 1, 3]),
+                      coding=rng.choice([8, 8, 8, 0, 1, 3, 9, 10, 12]))
+    c.reserved[1] = rng.choice([0, 0, 0, 1, 2])
+    c.reserved[3] = rng.choice([0, 0, 0, 1])
+    c.struct_size = rng.choice([ctypes.sizeof(B.FrameConfig)] * 8 + [0, 12])
+    return c
+
+
+def test_config_validation_matches_oracle(product, oracle):
+    rng = random.Random(11)
+    seen = set()
+    for _ in range(3000):
+        c = _rand_cfg(rng)
+        a, b = product.validate(c), oracle.validate(c)
+        assert a == b, bytes(c)
+        assert product.packet_bound(c) == oracle.packet_bound(c)
+        seen.add(a)
+    assert len(seen) >= 5
+
+
+def test_structural_parse_matches_oracle(product, oracle):
+    """Query-mode decode (header + slice map rules) on damaged headers."""
+    rng = random.Random(5)
+    names = [f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz")]
+    for name in sorted(names):
+        pkt = bytes(np.load(os.path.join(GOLDEN, name + ".npz"))["packet"])
+        for trial in range(60):
+            p = bytearray(pkt)
+            mode = trial % 4
+            if mode == 0:      # header field with a fixed-up CRC
+                i = rng.randrange(4, 49)
+                p[i] = rng.randrange(256)
+                crc = __import__("zlib").crc32(bytes(p[:49])) & 0xFFFFFFFF
+                p[49:53] = struct.pack(">I", crc)
+            elif mode == 1:    # any header byte
+                p[rng.randrange(53)] ^= 1 << rng.randrange(8)
+            elif mode == 2:    # slice header bytes
+                if len(p) > 70:
+                    p[53 + rng.randrange(17)] = rng.randrange(256)
+            else:              # truncation / extension
+                p = p[: rng.randrange(len(p) + 1)] if rng.random() < 0.7 else p + b"\0" * rng.randint(1, 9)
+            p = bytes(p)
+            ra, ia = product.query(p)
+            rb, ib = oracle.query(p)
+            assert ra == rb, (name, trial)
+            if ra == 0:
+                assert bytes(ia) == bytes(ib)

@@ -1,0 +1,161 @@
+"""GPU parity through the C-ABI: packets byte-identical to the oracle and to the
+reference fixtures, decoded pixels and per-slice concealment identical."""
+import json
+import os
+import random
+import struct
+import zlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from test_oracle import _random_config
+from topos_codec_b200 import binding as B, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    with open(os.path.join(GOLDEN, "index.json")) as f:
+        return json.load(f)
+
+
+@pytest.mark.parametrize("case", [c["name"] for c in _cases()])
+def test_fixture_encode_decode(product, case):
+    meta = next(c for c in _cases() if c["name"] == case)
+    z = np.load(os.path.join(GOLDEN, f"{case}.npz"))
+    planes = [z[f"in{p}"] for p in range(meta["planes"])]
+    cfg = B.make_config(meta["width"], meta["height"], **meta["config"])
+    pkt, stats = product.encode_frame(cfg, planes)
+    assert pkt == z["packet"].tobytes()
+    assert stats == meta["stats"]
+    dec = product.decode(z["packet"].tobytes())
+    assert dec.status == 0
+    for p, a in enumerate(dec.planes):
+        assert np.array_equal(a, z[f"dec{p}"]), p
+    bad = product.decode_status(z["damaged"].tobytes(), fill=0)
+    assert bad.status == meta["damaged_rc"]
+    assert bad.slice_status == list(z["bad_status"])
+    for p, a in enumerate(bad.planes):
+        assert np.array_equal(a, z[f"bad{p}"]), p
+
+
+def test_random_configs_vs_oracle(product, oracle):
+    rng = random.Random(99)
+    for i in range(60):
+        w, h, kw, ck = _random_config(rng)
+        planes = synth.make_frame_np(w, h, seed=500 + i, **kw)
+        cfg = B.make_config(w, h, **ck)
+        ra, pa, sa = oracle.encode_status(cfg, planes)
+        rb, pb, sb = product.encode_status(cfg, planes)
+        assert ra == rb, (i, w, h, ck, product.last_error())
+        if ra != 0:
+            continue
+        assert pa == pb, (i, w, h, ck)
+        assert sa.as_dict() == sb.as_dict()
+        da, db = oracle.decode(pa), product.decode(pa)
+        assert da.status == db.status
+        for x, y in zip(da.planes, db.planes):
+            assert np.array_equal(x, y), (i, w, h, ck)
+
+
+def _spans(pkt):
+    off, out = 53, []
+    while off < len(pkt):
+        size = struct.unpack(">I", pkt[off:off + 4])[0]
+        out.append((off, off + 17, size))
+        off += 17 + size
+    return out
+
+
+def test_damaged_packets_vs_oracle(product, oracle):
+    rng = random.Random(3)
+    for case in range(2):
+        if case == 0:
+            w, h = 160, 96
+            planes = synth.make_frame_np(w, h, seed=31, bit_depth=12, pixel_format=2, limited=False, alpha=True, sigma=12)
+            cfg = B.make_config(w, h, qp=2, bit_depth=12, pixel_format=2, profile=5, alpha_mode=1, alpha_bit_depth=16,
+                                color_range=1, slice_rows=2)
+        else:
+            w, h = 256, 128
+            planes = synth.make_frame_np(w, h, seed=32)
+            cfg = B.make_config(w, h, qp=8, qmatrix_id=4, features=1, slice_rows=2)
+        pkt = oracle.encode(cfg, planes)
+        spans = _spans(pkt)
+        for trial in range(80):
+            p = bytearray(pkt)
+            ho, po, size = spans[rng.randrange(len(spans))]
+            for _ in range(rng.randint(1, 3)):
+                p[po + rng.randrange(size)] = rng.randrange(256)
+            if trial % 2 == 0:
+                p[ho + 13:ho + 17] = struct.pack(">I", zlib.crc32(bytes(p[po:po + size])) & 0xFFFFFFFF)
+            p = bytes(p)
+            da, db = oracle.decode_status(p), product.decode_status(p)
+            assert da.status == db.status, trial
+            assert da.slice_status == db.slice_status, trial
+            for x, y in zip(da.planes, db.planes):
+                assert np.array_equal(x, y), trial
+
+
+def test_1080p_422_deblock_roundtrip(product, oracle):
+    """1920x1080 10-bit 4:2:2, qp 8, edge-balanced matrix, deblock."""
+    planes = synth.make_frame_np(1920, 1080, seed=0)
+    cfg = B.make_config(1920, 1080, qp=8, qmatrix_id=4, features=1)
+    pa = oracle.encode(cfg, planes)
+    pb = product.encode(cfg, planes)
+    assert pa == pb
+    da, db = oracle.decode(pa), product.decode(pa)
+    for x, y in zip(da.planes, db.planes):
+        assert np.array_equal(x, y)
+
+
+def test_4k_422_hq_full_size(product, oracle):
+    """3840x2160 10-bit 4:2:2 HQ (qp 4, flat matrix, deblock + refined table)."""
+    planes = synth.make_frame_np(3840, 2160, seed=1, frame=7)
+    cfg = B.make_config(3840, 2160, qp=4, qmatrix_id=0, features=3)
+    pa = oracle.encode(cfg, planes)
+    pb = product.encode(cfg, planes)
+    assert pa == pb
+    da, db = oracle.decode(pa), product.decode(pa)
+    for x, y in zip(da.planes, db.planes):
+        assert np.array_equal(x, y)
+
+
+def test_batch_encode_equals_single(product):
+    sizes = [(1280, 720), (64, 48), (1920, 1080), (333, 77)]
+    cfgs, frames = [], []
+    for i, (w, h) in enumerate(sizes):
+        frames.append(synth.make_frame_np(w, h, seed=60 + i))
+        cfgs.append(B.make_config(w, h, qp=2 + 4 * i, qmatrix_id=4 if i % 2 else 0, features=1 + (i % 2)))
+    rc, pkts, rcs, stats = product.encode_batch(cfgs, frames)
+    assert rc == 0 and rcs == [0] * len(sizes)
+    for c, f, p in zip(cfgs, frames, pkts):
+        assert p == product.encode(c, f)
+
+
+def test_batch_decode_equals_single(product):
+    pkts = []
+    for i, (w, h) in enumerate([(640, 360), (96, 64), (1920, 1080)]):
+        pkts.append(product.encode(B.make_config(w, h, qp=6, qmatrix_id=4, features=1), synth.make_frame_np(w, h, seed=70 + i)))
+    rc, frames = product.decode_batch(pkts)
+    assert rc == 0
+    for p, f in zip(pkts, frames):
+        d = product.decode(p)
+        for x, y in zip(d.planes, f.planes):
+            assert np.array_equal(x, y)
+
+
+def test_strided_io_and_buffer_too_small(product):
+    w, h = 200, 120
+    planes = synth.make_frame_np(w, h, seed=5)
+    cfg = B.make_config(w, h, qp=8, qmatrix_id=4, features=1)
+    tight = product.encode(cfg, planes)
+    padded = []
+    for a in planes:
+        big = np.full((a.shape[0], a.shape[1] + 37), 7, dtype=np.uint16)
+        big[:, : a.shape[1]] = a
+        padded.append(big[:, : a.shape[1]])
+    assert product.encode(cfg, padded) == tight
+    rc, pkt, st = product.encode_status(cfg, planes, out_cap=len(tight) - 1)
+    assert rc == B.TC_ERR_BUFFER_TOO_SMALL and st.packet_size == len(tight)

@@ -1,0 +1,767 @@
+// tcg_decode.cu - V7-R2 intra decode on the GPU (any batch of frames).
+//
+// Pipeline (one stream):
+//   k_dcrc      per slice: CRC-32 of the payload vs the slice header
+//                                               (reference codec.c:8204-8225)
+//   k_dtables   per colour slice: flags/rows prefix -> rANS models, symbol
+//               lookup tables, quantiser steps    (slice_codec.c:554-625)
+//   k_dchain    per colour slice: serial forward rANS2 decode -> natural-order
+//               coefficients, DC reconstruction, domain checks
+//                                               (slice_codec.c:626-736)
+//   k_didct     per block: dequantise, exact inverse transform, clamp, crop
+//                                               (color_store.h:529-711)
+//   k_dalpha    per alpha slice: Rice run/level decode -> residuals
+//                                               (block_coding.c:529-560)
+//   k_dalpha_med per alpha slice: MED reconstruction as an anti-diagonal
+//               wavefront; near-lossless multiple check (codec.c:7919-7972)
+//   k_dconceal  damaged slices: neutral fill of the visible band rows
+//                                               (codec.c:7975-7985)
+//   k_deblock_v / k_deblock_h  frame-level output filter (deblock.c:71-341)
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "tcg_common.cuh"
+#include "tcg_runtime.h"
+
+namespace tcg {
+
+constexpr uint32_t CTX_BYTES = 4096u + 128u + 128u;  // lut[4096] u8, freq[64] u16, cum[64] u16
+constexpr uint32_t MAX_CTX = 11u;                    // dc 5 + run 1 + lvl 5
+constexpr uint32_t DTAB_BYTES = MAX_CTX * CTX_BYTES + 256u + 16u;  // + Q[64] u32 + header
+
+struct DPlane {
+    uint64_t out_off;   // element offset in the device output buffer (tight rows)
+    uint32_t vis_w, vis_h, coded_w, cols, rows;
+    uint32_t bd, kind, alpha_shift, refined;
+    uint32_t blk0;
+    uint32_t frame;
+    uint16_t qm[64];
+};
+
+struct DSlice {
+    uint32_t frame, plane, pidx, kind;
+    uint32_t y0, bh, cols;
+    uint32_t blk0, nblk;
+    uint32_t size, crc, qp;
+    uint32_t k1, k2;
+    uint64_t pay;       // payload offset in the device packet buffer
+    uint64_t res_off;   // alpha: residual offset (int32 units)
+};
+
+struct DFrame {
+    uint32_t plane0, planes, bd, deblock, refined, qp_base;
+};
+
+// ------------------------------------------------------------------ CRC
+
+__global__ void __launch_bounds__(256) k_dcrc(const DSlice* __restrict__ slices, const uint8_t* __restrict__ pkt,
+                                              const uint32_t* __restrict__ crctab, int32_t* __restrict__ status)
+{
+    __shared__ uint32_t t[8 * 256];
+    __shared__ uint32_t scratch[512];
+    for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
+    __syncthreads();
+    const DSlice& S = slices[blockIdx.x];
+    const uint32_t c = crc32_block(pkt + S.pay, S.size, t, scratch);
+    if (threadIdx.x == 0) { status[blockIdx.x] = c == S.crc ? 0 : TCG_ERR_CHECKSUM_MISMATCH; }
+}
+
+// ------------------------------------------------------------------ tables
+
+__global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                                const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
+                                                const uint32_t* __restrict__ qscale, uint8_t* __restrict__ tabs,
+                                                int32_t* __restrict__ status)
+{
+    __shared__ int32_t bad;
+    __shared__ uint32_t meta[3];
+    const uint32_t si = cslices[blockIdx.x];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint8_t* pay = pkt + S.pay;
+    uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        bad = 0;
+        if (S.size < 1u + 121u + 4u) {
+            bad = TCG_ERR_TRUNCATED;
+        } else {
+            const uint32_t fl = pay[0], lm = fl & 3u, dm = (fl >> 2) & 1u;
+            if ((fl & 0xF8u) != 0u || lm > 2u) { bad = TCG_ERR_MALFORMED; }
+            const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u, nd = dm ? DCP_CTX : 1u;
+            const uint32_t plen = 1u + nd * DC_SYMS + RUN_SYMS + nl * LVL_SYMS;
+            if (bad == 0 && S.size < plen + 4u) { bad = TCG_ERR_TRUNCATED; }
+            meta[0] = lm; meta[1] = dm; meta[2] = plen;
+        }
+    }
+    __syncwarp();
+    if (bad != 0) {
+        if (t == 0) { status[si] = bad; }
+        return;
+    }
+    const uint32_t lm = meta[0], dm = meta[1];
+    const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+    // context c: 0..nd-1 dc rows, 5 run, 6..6+nl-1 lvl rows
+    const uint32_t nrows = nd + 1u + nl;
+    bool ok = true;
+    if (t < nrows) {
+        uint32_t ctx, off, n;
+        if (t < nd) { ctx = t; off = 1u + t * DC_SYMS; n = DC_SYMS; }
+        else if (t == nd) { ctx = 5u; off = 1u + nd * DC_SYMS; n = RUN_SYMS; }
+        else { ctx = 6u + (t - nd - 1u); off = 1u + nd * DC_SYMS + RUN_SYMS + (t - nd - 1u) * LVL_SYMS; n = LVL_SYMS; }
+        uint8_t* c = tb + (size_t)ctx * CTX_BYTES;
+        uint16_t* fr = reinterpret_cast<uint16_t*>(c + 4096u);
+        uint16_t* cu = fr + 64;
+        uint8_t bytes[64];
+        for (uint32_t s = 0; s < n; ++s) { bytes[s] = pay[off + s]; }
+        ok = model_from_bytes(bytes, n, fr, cu);
+        if (ok) {
+            for (uint32_t s = 0; s < n; ++s) {
+                for (uint32_t k = cu[s]; k < (uint32_t)cu[s] + fr[s]; ++k) { c[k] = (uint8_t)s; }
+            }
+        }
+    }
+    if (__any_sync(0xFFFFFFFFu, !ok)) {
+        if (t == 0) { status[si] = TCG_ERR_MALFORMED; }
+        return;
+    }
+    // quantiser steps for this slice's effective qp
+    uint32_t* Q = reinterpret_cast<uint32_t*>(tb + MAX_CTX * CTX_BYTES);
+    const uint32_t sc = qscale[(P.refined ? 96u : 0u) + S.qp];
+    for (uint32_t i = t; i < 64u; i += 32u) {
+        const uint32_t q = (uint32_t)((((uint64_t)P.qm[i] * sc) + 128u) >> 8);
+        Q[i] = q == 0u ? 1u : q;
+    }
+    if (t == 0) {
+        uint32_t* hdr = Q + 64;
+        hdr[0] = lm; hdr[1] = dm; hdr[2] = meta[2];
+    }
+}
+
+// ------------------------------------------------------------------ chain
+
+struct RDec {
+    uint32_t x;
+    uint32_t pos;
+    uint32_t n;
+    const uint8_t* b;
+};
+
+__device__ __forceinline__ int32_t rd_renorm(RDec& d)
+{
+    while (d.x < RANS_L) {
+        if (d.pos >= d.n) { return TCG_ERR_TRUNCATED; }
+        d.x = (d.x << 8) | __ldg(d.b + d.pos);
+        d.pos++;
+    }
+    return 0;
+}
+
+__device__ __forceinline__ int32_t rd_sym(RDec& d, const uint8_t* ctx, uint32_t& sym)
+{
+    const uint32_t slot = d.x & 4095u;
+    const uint32_t s = ctx[slot];
+    const uint16_t* fr = reinterpret_cast<const uint16_t*>(ctx + 4096u);
+    d.x = (uint32_t)fr[s] * (d.x >> 12) + slot - fr[64 + s];
+    sym = s;
+    return rd_renorm(d);
+}
+
+__device__ __forceinline__ int32_t rd_chunk(RDec& d, uint32_t w, uint32_t& c)
+{
+    c = d.x & ((1u << w) - 1u);
+    d.x >>= w;
+    return rd_renorm(d);
+}
+
+__device__ __forceinline__ int32_t rd_suffix(RDec& d, uint32_t cat, uint32_t& m)
+{
+    uint32_t v = 0;
+    int32_t rc;
+    if (cat > 1u) {
+        const uint32_t b = cat - 1u;
+        if (b > 23u) {
+            uint32_t lo, hi;
+            if ((rc = rd_chunk(d, 16u, lo)) != 0) { return rc; }
+            if ((rc = rd_chunk(d, b - 16u, hi)) != 0) { return rc; }
+            v = (hi << 16) | lo;
+        } else if ((rc = rd_chunk(d, b, v)) != 0) {
+            return rc;
+        }
+    }
+    m = cat == 0u ? 0u : (1u << (cat - 1u)) | v;
+    return 0;
+}
+
+// One 32-thread block per colour slice; the block stages the slice's lookup
+// tables in shared memory and lane 0 runs the symbol chain.
+__global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                               const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
+                                               const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
+                                               int32_t* __restrict__ status)
+{
+    extern __shared__ __align__(16) uint8_t sm[];
+    const uint32_t si = cslices[blockIdx.x];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + MAX_CTX * CTX_BYTES) + 64;
+    const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
+    // stage the context tables that this slice uses
+    for (uint32_t i = threadIdx.x * 16u; i < MAX_CTX * CTX_BYTES; i += blockDim.x * 16u) {
+        const uint32_t ctx = i / CTX_BYTES;
+        const bool used = ctx < (dm ? 5u : 1u) || ctx == 5u || (ctx >= 6u && ctx < 6u + (lm == 1u ? 4u : lm == 2u ? 5u : 1u));
+        if (used) { *reinterpret_cast<uint4*>(sm + i) = *reinterpret_cast<const uint4*>(tb + i); }
+    }
+    int32_t* rows = reinterpret_cast<int32_t*>(sm + MAX_CTX * CTX_BYTES);
+    int32_t* prow = rows;
+    int32_t* crow = rows + S.cols;
+    for (uint32_t i = threadIdx.x; i < 2u * S.cols; i += blockDim.x) { rows[i] = 0; }
+    __syncthreads();
+    if (threadIdx.x != 0) { return; }
+    const uint8_t* pay = pkt + S.pay;
+    RDec d;
+    d.b = pay + plen;
+    d.n = S.size - plen;
+    d.x = ((uint32_t)d.b[0] << 24) | ((uint32_t)d.b[1] << 16) | ((uint32_t)d.b[2] << 8) | d.b[3];
+    d.pos = 4u;
+    int32_t rc = d.x < RANS_L ? TCG_ERR_MALFORMED : 0;
+    const bool wide = P.bd > 12u;
+    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
+    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
+    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
+    const uint8_t* run_t = sm + 5u * CTX_BYTES;
+    uint32_t prev_dcc = 0;
+    bool first = true;
+    for (uint32_t by = 0; by < S.bh && rc == 0; ++by) {
+        for (uint32_t bx = 0; bx < S.cols; ++bx) {
+            int32_t* blk = coef + (size_t)(S.blk0 + by * S.cols + bx) * 64u;
+            const uint32_t dctx = dm ? (first ? 0u : dcp_ctx(prev_dcc, true)) : 0u;
+            uint32_t cat, m;
+            if ((rc = rd_sym(d, sm + dctx * CTX_BYTES, cat)) != 0) { break; }
+            if ((rc = rd_suffix(d, cat, m)) != 0) { break; }
+            if (m > mdc) { rc = TCG_ERR_MALFORMED; break; }
+            const int32_t pred = dc_pred(bx != 0u, bx != 0u ? crow[bx - 1u] : 0, by != 0u, prow[bx]);
+            const int64_t dcv = (int64_t)pred + unmap_s(m);
+            if (dcv > dlim || dcv < -dlim) { rc = TCG_ERR_MALFORMED; break; }
+            blk[0] = (int32_t)dcv;
+            crow[bx] = (int32_t)dcv;
+            prev_dcc = cat;
+            first = false;
+            uint32_t pos = 1, pcat = 0;
+            bool has = false;
+            for (;;) {
+                uint32_t r;
+                if ((rc = rd_sym(d, run_t, r)) != 0) { break; }
+                if (r == 63u) { break; }
+                const uint32_t idx = pos + r;
+                if (idx > 63u) { rc = TCG_ERR_MALFORMED; break; }
+                const uint32_t lc = lm == 1u ? pos_ctx(idx) : lm == 2u ? prev_ctx(pcat, has) : 0u;
+                if ((rc = rd_sym(d, sm + (6u + lc) * CTX_BYTES, cat)) != 0) { break; }
+                if ((rc = rd_suffix(d, cat, m)) != 0) { break; }
+                if (m > mlv) { rc = TCG_ERR_MALFORMED; break; }
+                blk[c_zigzag[idx]] = unmap_s(m);
+                pcat = cat;
+                has = true;
+                pos = idx + 1u;
+            }
+            if (rc != 0) { break; }
+        }
+        int32_t* sw = prow; prow = crow; crow = sw;
+    }
+    if (rc == 0 && d.pos != d.n) { rc = TCG_ERR_MALFORMED; }
+    status[si] = rc;
+}
+
+// ------------------------------------------------------------------ reconstruction
+
+__global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ blk_slice,
+                                               const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
+                                               const uint8_t* __restrict__ tabs, const int32_t* __restrict__ coef,
+                                               const int32_t* __restrict__ status, uint32_t total,
+                                               uint16_t* __restrict__ out)
+{
+    const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gb >= total) { return; }
+    const uint32_t si = blk_slice[gb];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint32_t* Q = reinterpret_cast<const uint32_t*>(tabs + (size_t)slice_tab[si] * DTAB_BYTES + MAX_CTX * CTX_BYTES);
+    const uint32_t lb = gb - S.blk0;
+    const uint32_t bx = lb % S.cols, by = S.y0 + lb / S.cols;
+    const int64_t fc = P.bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (P.bd - 1u)) - 1u)) / 2047;
+    int32_t c[64], xh[64];
+    const int4* src = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int4 v = src[i];
+        const int32_t vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int64_t f = (int64_t)vv[j] * __ldg(Q + i * 4 + j);
+            f = f > fc ? fc : (f < -fc ? -fc : f);
+            c[i * 4 + j] = (int32_t)f;
+        }
+    }
+    idct8x8(c, xh);
+    const int32_t mid = 1 << (P.bd - 1u), maxv = (1 << P.bd) - 1;
+    const uint32_t px = bx * 8u, py = by * 8u;
+    const uint32_t cw = min(8u, P.vis_w - px), ch = min(8u, P.vis_h - py);
+    uint16_t* dst = out + P.out_off + (size_t)py * P.vis_w + px;
+    for (uint32_t y = 0; y < ch; ++y) {
+        for (uint32_t x = 0; x < cw; ++x) {
+            int32_t v = xh[y * 8 + x] + mid;
+            v = v < 0 ? 0 : (v > maxv ? maxv : v);
+            dst[(size_t)y * P.vis_w + x] = (uint16_t)v;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ alpha
+
+struct BitR {
+    const uint8_t* d;
+    uint64_t nbits, pos;
+};
+
+__device__ __forceinline__ bool br_bit(BitR& r, uint32_t& b)
+{
+    if (r.pos >= r.nbits) { return false; }
+    b = (__ldg(r.d + (r.pos >> 3)) >> (7u - (uint32_t)(r.pos & 7u))) & 1u;
+    r.pos++;
+    return true;
+}
+
+__device__ inline int32_t rice_get(BitR& r, uint32_t k, uint32_t mmax, uint32_t& m)
+{
+    uint32_t q = 0, b = 0;
+    while (q < 31u) {
+        if (!br_bit(r, b)) { return TCG_ERR_TRUNCATED; }
+        if (b == 0u) { break; }
+        ++q;
+    }
+    uint64_t v;
+    if (q == 31u) {
+        if (r.nbits - r.pos < 32u) { return TCG_ERR_TRUNCATED; }
+        uint32_t lit = 0;
+        for (int i = 0; i < 32; ++i) { br_bit(r, b); lit = (lit << 1) | b; }
+        v = lit;
+    } else {
+        if (r.nbits - r.pos < k) { return TCG_ERR_TRUNCATED; }
+        uint32_t rem = 0;
+        for (uint32_t i = 0; i < k; ++i) { br_bit(r, b); rem = (rem << 1) | b; }
+        v = ((uint64_t)q << k) | rem;
+    }
+    if (v > mmax) { return TCG_ERR_MALFORMED; }
+    m = (uint32_t)v;
+    return 0;
+}
+
+__global__ void k_dalpha(const DSlice* __restrict__ slices, const uint32_t* __restrict__ aslices, uint32_t na,
+                         const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt, int32_t* __restrict__ res,
+                         int32_t* __restrict__ status)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= na) { return; }
+    const uint32_t si = aslices[i];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint64_t count = (uint64_t)P.coded_w * S.bh * 8u;
+    int32_t* rr = res + S.res_off;
+    BitR r = {pkt + S.pay, (uint64_t)S.size * 8u, 0};
+    int32_t rc = 0;
+    uint64_t pos = 0;
+    while (pos < count) {
+        const uint64_t remaining = count - pos;
+        uint32_t run, lv;
+        if ((rc = rice_get(r, S.k2, (uint32_t)remaining, run)) != 0) { break; }
+        if ((rc = rice_get(r, S.k1, 0x00020000u, lv)) != 0) { break; }
+        if (lv == 0u) {
+            if ((uint64_t)run != remaining) { rc = TCG_ERR_MALFORMED; }
+            break;
+        }
+        if ((uint64_t)run + 1u > remaining) { rc = TCG_ERR_MALFORMED; break; }
+        rr[pos + run] = unmap_s(lv);
+        pos += (uint64_t)run + 1u;
+    }
+    if (rc == 0) {
+        const uint64_t p = (r.pos + 7u) & ~(uint64_t)7u;
+        if (p > r.nbits) { rc = TCG_ERR_TRUNCATED; }
+        else if (p != r.nbits) { rc = TCG_ERR_MALFORMED; }
+    }
+    status[si] = rc;
+}
+
+// Anti-diagonal wavefront over one band, in groups of 128 rows: thread t owns
+// group row t and at step d reconstructs column x = d - t from its left value,
+// the row above (shared memory, double buffered) and the above-left value kept
+// from the previous step. The first row of a group reads the previous group's
+// last row from `edge` (dynamic shared memory, coded_w entries), which the
+// group's last row overwrites 127 columns behind the readers.
+__global__ void __launch_bounds__(128) k_dalpha_med(const DSlice* __restrict__ slices, const uint32_t* __restrict__ aslices,
+                                                    const DPlane* __restrict__ planes, const int32_t* __restrict__ res,
+                                                    int32_t* __restrict__ status, uint16_t* __restrict__ out)
+{
+    extern __shared__ int32_t edge[];
+    __shared__ int32_t line[2][128];
+    __shared__ int32_t bad;
+    const uint32_t si = aslices[blockIdx.x];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint32_t H = S.bh * 8u, W = P.coded_w;
+    const uint32_t t = threadIdx.x;
+    const uint32_t mask = P.alpha_shift ? ((1u << P.alpha_shift) - 1u) : 0u;
+    const int32_t* rr = res + S.res_off;
+    if (t == 0) { bad = 0; }
+    __syncthreads();
+    for (uint32_t g0 = 0; g0 < H; g0 += 128u) {
+        const uint32_t gh = min(128u, H - g0);
+        const uint32_t y = g0 + t;          // band row
+        const uint32_t gy = S.y0 * 8u + y;  // plane row
+        int32_t left = 0, upleft = 0;
+        for (uint32_t d = 0; d < W + gh - 1u; ++d) {
+            const uint32_t b = d & 1u;
+            if (t < gh && d >= t && d - t < W) {
+                const uint32_t x = d - t;
+                int32_t up = 0;
+                if (y > 0u) { up = t > 0u ? line[b ^ 1u][t - 1u] : edge[x]; }
+                int32_t pred;
+                if (y == 0u) { pred = x == 0u ? 0 : left; }
+                else if (x == 0u) { pred = up; }
+                else if (upleft >= left && upleft >= up) { pred = left < up ? left : up; }
+                else if (upleft <= left && upleft <= up) { pred = left < up ? up : left; }
+                else { pred = left + up - upleft; }
+                int32_t v = pred + rr[(size_t)y * W + x];
+                v = v < 0 ? 0 : (v > 65535 ? 65535 : v);
+                if (mask != 0u && ((uint32_t)v & mask) != 0u) { bad = 1; }
+                if (gy < P.vis_h && x < P.vis_w) { out[P.out_off + (size_t)gy * P.vis_w + x] = (uint16_t)v; }
+                line[b][t] = v;
+                if (t == gh - 1u) { edge[x] = v; }
+                left = v;
+                upleft = up;
+            }
+            __syncthreads();
+        }
+    }
+    if (t == 0 && bad) { status[si] = TCG_ERR_MALFORMED; }
+}
+
+// ------------------------------------------------------------------ concealment
+
+__global__ void __launch_bounds__(256) k_dconceal(const DSlice* __restrict__ slices, const DPlane* __restrict__ planes,
+                                                  const int32_t* __restrict__ status, uint16_t* __restrict__ out)
+{
+    const uint32_t si = blockIdx.x;
+    if (status[si] == 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint16_t fill = P.kind == TCG_PLANE_ALPHA ? 0xFFFFu : (uint16_t)(1u << (P.bd - 1u));
+    const uint32_t y0 = S.y0 * 8u;
+    const uint32_t rows = min(S.bh * 8u, P.vis_h - y0);
+    const uint64_t n = (uint64_t)rows * P.vis_w;
+    uint16_t* dst = out + P.out_off + (size_t)y0 * P.vis_w;
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) { dst[i] = fill; }
+}
+
+// ------------------------------------------------------------------ deblock
+
+struct DbPlane {
+    uint64_t off;
+    uint32_t w, h, alpha, beta, clip, maxv;
+};
+
+__device__ __forceinline__ bool db_gate(int32_t p1, int32_t p0, int32_t q0, int32_t q1, int32_t a, int32_t b)
+{
+    return (uint32_t)abs(q0 - p0) < (uint32_t)a && (uint32_t)abs(p1 - p0) < (uint32_t)b && (uint32_t)abs(q1 - q0) < (uint32_t)b;
+}
+
+__device__ __forceinline__ int32_t db_delta(int32_t p1, int32_t p0, int32_t q0, int32_t q1, int32_t clip)
+{
+    int32_t d = (12 * (q0 - p0) + 4 * (p1 - q1) + 8) >> 4;
+    const int32_t dl = q0 - p0;
+    const int32_t half = dl >= 0 ? (dl >> 1) : -((-dl) >> 1);
+    if (half >= 0) { d = d > half ? half : d; d = d < 0 ? 0 : d; }
+    else { d = d < half ? half : d; d = d > 0 ? 0 : d; }
+    return d < -clip ? -clip : (d > clip ? clip : d);
+}
+
+__device__ __forceinline__ void db_apply(uint16_t* a, uint16_t* b, uint16_t* c, uint16_t* e, int32_t p1, int32_t p0,
+                                         int32_t q0, int32_t q1, int32_t d, int32_t maxv)
+{
+    auto cl = [maxv](int32_t v) { return (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v)); };
+    *b = cl(p0 + d);
+    *c = cl(q0 - d);
+    *a = cl(p1 + (d >> 1));
+    *e = cl(q1 - (d >> 1));
+}
+
+// vertical edges: one thread per (row, edge)
+__global__ void k_deblock_v(const DbPlane* __restrict__ dp, uint32_t np, uint16_t* __restrict__ out)
+{
+    const DbPlane P = dp[blockIdx.y];
+    const uint32_t edges = P.w / 8u - 1u;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)edges * P.h) { return; }
+    const uint32_t y = (uint32_t)(i / edges), x0 = 8u * (uint32_t)(i % edges + 1u);
+    uint16_t* r = out + P.off + (size_t)y * P.w;
+    const int32_t p1 = r[x0 - 2], p0 = r[x0 - 1], q0 = r[x0], q1 = r[x0 + 1];
+    if (db_gate(p1, p0, q0, q1, (int32_t)P.alpha, (int32_t)P.beta)) {
+        db_apply(r + x0 - 2, r + x0 - 1, r + x0, r + x0 + 1, p1, p0, q0, q1, db_delta(p1, p0, q0, q1, (int32_t)P.clip),
+                 (int32_t)P.maxv);
+    }
+    (void)np;
+}
+
+// horizontal edges: one thread per (edge row, column)
+__global__ void k_deblock_h(const DbPlane* __restrict__ dp, uint32_t np, uint16_t* __restrict__ out)
+{
+    const DbPlane P = dp[blockIdx.y];
+    const uint32_t edges = P.h / 8u - 1u;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)edges * P.w) { return; }
+    const uint32_t r = (uint32_t)(i / P.w) + 1u, x = (uint32_t)(i % P.w);
+    const uint32_t y0 = 8u * r;
+    uint16_t* b = out + P.off + x;
+    uint16_t* a2 = b + (size_t)(y0 - 2u) * P.w;
+    uint16_t* a1 = b + (size_t)(y0 - 1u) * P.w;
+    uint16_t* b0 = b + (size_t)y0 * P.w;
+    uint16_t* b1 = b + (size_t)(y0 + 1u) * P.w;
+    const int32_t p1 = *a2, p0 = *a1, q0 = *b0, q1 = *b1;
+    if (db_gate(p1, p0, q0, q1, (int32_t)P.alpha, (int32_t)P.beta)) {
+        db_apply(a2, a1, b0, b1, p1, p0, q0, q1, db_delta(p1, p0, q0, q1, (int32_t)P.clip), (int32_t)P.maxv);
+    }
+    (void)np;
+}
+
+// ------------------------------------------------------------------ driver
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1u) / a * a; }
+
+static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
+{
+    static const uint32_t s[64] = {
+        1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5, 6, 7, 8, 10, 11, 13, 16, 19, 23, 27, 32, 38, 45, 54, 64, 76, 91, 108,
+        128, 152, 181, 215, 256, 304, 362, 431, 512, 609, 724, 861, 1024, 1218, 1448, 1722,
+        2048, 2435, 2896, 3444, 4096, 4871, 5793, 6889, 8192, 9742, 11585, 13777, 16384, 19484, 23170, 27555};
+    static const uint32_t hi[2][32] = {
+        {32768, 38968, 46341, 55109, 65536, 77936, 92682, 110218, 131072, 155872, 185364, 220436, 262144, 311744, 370728,
+         440872, 524288, 623487, 741455, 881744, 1048576, 1246974, 1482910, 1763488, 2097152, 2493948, 2965821, 3526975,
+         4194304, 4987896, 5931642, 7053950},
+        {32768, 36781, 41285, 46341, 52016, 58386, 65536, 73562, 82570, 92682, 104032, 116772, 131072, 147123, 165140,
+         185364, 208064, 233544, 262144, 294247, 330281, 370728, 416128, 467088, 524288, 588493, 660561, 741455, 832255,
+         934175, 1048576, 1176987}};
+    return qp < 64u ? s[qp] : hi[refined ? 1 : 0][qp - 64u];
+}
+
+static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
+{
+    std::vector<DPlane> planes;
+    std::vector<DSlice> slices;
+    std::vector<uint32_t> cslices, aslices, slice_tab, blk_slice;
+    std::vector<DbPlane> dbp;
+    std::vector<uint64_t> pkt_off(count, 0);
+    std::vector<uint32_t> frame_slice0(count, 0);
+    uint64_t out_elems = 0, pkt_bytes = 0, nblk = 0, alpha_res = 0;
+    uint32_t max_cols = 1;
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_dec_frame& F = frames[f];
+        frame_slice0[f] = (uint32_t)slices.size();
+        if (F.skip) { continue; }
+        pkt_off[f] = pkt_bytes;
+        pkt_bytes = align_up(pkt_bytes + F.size, 256);
+        const uint32_t pg0 = (uint32_t)planes.size();
+        for (uint32_t p = 0; p < F.planes; ++p) {
+            DPlane P;
+            memset(&P, 0, sizeof(P));
+            P.out_off = out_elems;
+            out_elems = align_up(out_elems + (uint64_t)F.vis_w[p] * F.vis_h[p], 64);
+            P.vis_w = F.vis_w[p]; P.vis_h = F.vis_h[p]; P.coded_w = F.coded_w[p];
+            P.cols = F.cols[p]; P.rows = F.rows[p];
+            P.bd = F.bit_depth;
+            P.kind = (p == 3u && F.alpha_mode != 0u) ? TCG_PLANE_ALPHA : TCG_PLANE_COLOR;
+            P.alpha_shift = P.kind == TCG_PLANE_ALPHA ? F.alpha_shift : 0u;
+            P.refined = F.refined;
+            P.blk0 = (uint32_t)nblk;
+            P.frame = f;
+            memcpy(P.qm, F.qm[p], sizeof(P.qm));
+            if (P.kind == TCG_PLANE_COLOR) { nblk += (uint64_t)P.cols * P.rows; }
+            max_cols = P.cols > max_cols ? P.cols : max_cols;
+            planes.push_back(P);
+            if (F.deblock && p < 3u) {
+                const uint32_t w = P.vis_w, h = P.vis_h;
+                if (w >= 16u && h >= 16u && (w % 8u) == 0u && (h % 8u) == 0u && F.qp_base <= 95u) {
+                    const uint32_t sc = host_qp_scale(F.refined, F.qp_base);
+                    uint32_t step = (sc * 3u + 173056u / 2u) / 173056u;
+                    step = step < 1u ? 1u : step;
+                    uint32_t a = step * 2u;
+                    a = a < 3u ? 3u : (a > 48u ? 48u : a);
+                    DbPlane d = {P.out_off, w, h, a, a / 2u + 2u, a >> 1, (1u << F.bit_depth) - 1u};
+                    dbp.push_back(d);
+                }
+            }
+        }
+        for (uint32_t i = 0; i < F.slices; ++i) {
+            const tcg_dec_slice& I = F.slice[i];
+            DSlice S;
+            memset(&S, 0, sizeof(S));
+            const DPlane& P = planes[pg0 + I.plane];
+            S.frame = f; S.plane = pg0 + I.plane; S.pidx = I.plane; S.kind = P.kind;
+            S.y0 = I.y0; S.bh = I.bh; S.cols = P.cols;
+            S.size = I.size; S.crc = I.crc; S.qp = I.qp; S.k1 = I.k1; S.k2 = I.k2;
+            S.pay = pkt_off[f] + I.off;
+            const uint32_t si = (uint32_t)slices.size();
+            if (S.kind == TCG_PLANE_COLOR) {
+                S.blk0 = P.blk0 + I.y0 * P.cols;
+                S.nblk = I.bh * P.cols;
+                slice_tab.push_back((uint32_t)cslices.size());
+                cslices.push_back(si);
+            } else {
+                S.res_off = alpha_res;
+                alpha_res += (uint64_t)P.coded_w * I.bh * 8u;
+                slice_tab.push_back(0u);
+                aslices.push_back(si);
+            }
+            slices.push_back(S);
+        }
+    }
+    blk_slice.resize(nblk);
+    for (uint32_t si : cslices) {
+        for (uint32_t k = 0; k < slices[si].nblk; ++k) { blk_slice[slices[si].blk0 + k] = si; }
+    }
+    const uint32_t ns = (uint32_t)slices.size(), nc = (uint32_t)cslices.size(), na = (uint32_t)aslices.size();
+    const size_t desc = align_up(planes.size() * sizeof(DPlane), 256) + align_up(ns * sizeof(DSlice), 256) +
+                        align_up((size_t)(nc + na) * 4u + 16, 256) + align_up((size_t)ns * 4u + 16, 256) +
+                        align_up((size_t)nblk * 4u + 16, 256) + align_up(dbp.size() * sizeof(DbPlane) + 16, 256);
+    if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_DEC_TAB, (size_t)nc * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
+        !dreserve(C, B_DEC_RES, (size_t)ns * 4u + 256) || !dreserve(C, B_ALPHA, alpha_res * 4u + 256) ||
+        !dreserve(C, B_DESC, desc + 256) || !hreserve(C, 0, desc + 256) || !hreserve(C, 1, (size_t)ns * 4u + 256)) {
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    cudaStream_t st = C->stream;
+    uint8_t* hd = (uint8_t*)C->h[0].p;
+    uint8_t* dd = dptr<uint8_t>(C, B_DESC);
+    size_t o = 0;
+    auto put = [&](const void* src, size_t n) -> size_t {
+        const size_t at = o;
+        if (n) { memcpy(hd + o, src, n); }
+        o = align_up(o + n, 256);
+        return at;
+    };
+    std::vector<uint32_t> cs_as(cslices);
+    cs_as.insert(cs_as.end(), aslices.begin(), aslices.end());
+    const size_t o_pl = put(planes.data(), planes.size() * sizeof(DPlane));
+    const size_t o_sl = put(slices.data(), ns * sizeof(DSlice));
+    const size_t o_ca = put(cs_as.data(), cs_as.size() * 4u);
+    const size_t o_st = put(slice_tab.data(), slice_tab.size() * 4u);
+    const size_t o_bs = put(blk_slice.data(), blk_slice.size() * 4u);
+    const size_t o_db = put(dbp.data(), dbp.size() * sizeof(DbPlane));
+    TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
+    const DPlane* d_pl = (const DPlane*)(dd + o_pl);
+    const DSlice* d_sl = (const DSlice*)(dd + o_sl);
+    const uint32_t* d_cs = (const uint32_t*)(dd + o_ca);
+    const uint32_t* d_as = d_cs + nc;
+    const uint32_t* d_st = (const uint32_t*)(dd + o_st);
+    const uint32_t* d_bs = (const uint32_t*)(dd + o_bs);
+    const DbPlane* d_db = (const DbPlane*)(dd + o_db);
+    uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
+    for (uint32_t f = 0; f < count; ++f) {
+        if (frames[f].skip) { continue; }
+        TCG_CHECK(cudaMemcpyAsync(d_pkt + pkt_off[f], frames[f].packet, frames[f].size, cudaMemcpyDefault, st));
+    }
+    int32_t* d_status = dptr<int32_t>(C, B_DEC_RES);
+    int32_t* d_coef = dptr<int32_t>(C, B_DEC_COEF);
+    uint8_t* d_tab = dptr<uint8_t>(C, B_DEC_TAB);
+    uint16_t* d_out = dptr<uint16_t>(C, B_DEC_OUT);
+    int32_t* d_ares = dptr<int32_t>(C, B_ALPHA);
+    const DevTables& T = tables();
+    uint32_t launches = 0;
+    if (ns > 0) {
+        TCG_CHECK(cudaMemsetAsync(d_status, 0, (size_t)ns * 4u, st));
+        k_dcrc<<<ns, 256, 0, st>>>(d_sl, d_pkt, T.crc, d_status);
+        launches++;
+    }
+    if (nc > 0) {
+        TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+        k_dtables<<<nc, 32, 0, st>>>(d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
+        const size_t smem = MAX_CTX * CTX_BYTES + (size_t)max_cols * 8u;
+        static size_t attr = 0;
+        if (smem > attr) {
+            cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            attr = smem;
+        }
+        k_dchain<<<nc, 32, smem, st>>>(d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
+        k_didct<<<(uint32_t)((nblk + 127u) / 128u), 128, 0, st>>>(d_sl, d_bs, d_st, d_pl, d_tab, d_coef, d_status,
+                                                                 (uint32_t)nblk, d_out);
+        launches += 3;
+    }
+    if (na > 0) {
+        TCG_CHECK(cudaMemsetAsync(d_ares, 0, alpha_res * 4u, st));
+        k_dalpha<<<(na + 63u) / 64u, 64, 0, st>>>(d_sl, d_as, na, d_pl, d_pkt, d_ares, d_status);
+        uint32_t max_w = 8;
+        for (uint32_t a : aslices) { max_w = std::max(max_w, planes[slices[a].plane].coded_w); }
+        const size_t esmem = (size_t)max_w * 4u;
+        static size_t eattr = 0;
+        if (esmem > eattr) {
+            cudaFuncSetAttribute(k_dalpha_med, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
+            eattr = esmem;
+        }
+        k_dalpha_med<<<na, 128, esmem, st>>>(d_sl, d_as, d_pl, d_ares, d_status, d_out);
+        launches += 2;
+    }
+    if (ns > 0) {
+        k_dconceal<<<ns, 256, 0, st>>>(d_sl, d_pl, d_status, d_out);
+        launches++;
+    }
+    if (!dbp.empty()) {
+        uint64_t mv = 0, mh = 0;
+        for (const DbPlane& d : dbp) {
+            mv = std::max<uint64_t>(mv, (uint64_t)(d.w / 8u - 1u) * d.h);
+            mh = std::max<uint64_t>(mh, (uint64_t)(d.h / 8u - 1u) * d.w);
+        }
+        k_deblock_v<<<dim3((uint32_t)((mv + 255u) / 256u), (uint32_t)dbp.size()), 256, 0, st>>>(d_db, (uint32_t)dbp.size(), d_out);
+        k_deblock_h<<<dim3((uint32_t)((mh + 255u) / 256u), (uint32_t)dbp.size()), 256, 0, st>>>(d_db, (uint32_t)dbp.size(), d_out);
+        launches += 2;
+    }
+    note_launch(launches);
+    TCG_CHECK(cudaGetLastError());
+    // outputs to the caller's planes
+    uint32_t pg = 0;
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_dec_frame& F = frames[f];
+        if (F.skip) { continue; }
+        for (uint32_t p = 0; p < F.planes; ++p, ++pg) {
+            const DPlane& P = planes[pg];
+            const size_t pitch = (F.dst_stride[p] ? F.dst_stride[p] : P.vis_w) * 2u;
+            TCG_CHECK(cudaMemcpy2DAsync(F.dst[p], pitch, d_out + P.out_off, (size_t)P.vis_w * 2u, (size_t)P.vis_w * 2u,
+                                        P.vis_h, cudaMemcpyDefault, st));
+        }
+    }
+    int32_t* hs = (int32_t*)C->h[1].p;
+    if (ns > 0) { TCG_CHECK(cudaMemcpyAsync(hs, d_status, (size_t)ns * 4u, cudaMemcpyDeviceToHost, st)); }
+    TCG_CHECK(cudaStreamSynchronize(st));
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_dec_frame& F = frames[f];
+        if (F.skip) { continue; }
+        for (uint32_t i = 0; i < F.slices; ++i) { F.slice_status[i] = hs[frame_slice0[f] + i] != 0 ? 1u : 0u; }
+    }
+    return 0;
+}
+
+}  // namespace tcg
+
+extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
+{
+    tcg::Ctx* c = tcg::ctx_acquire();
+    if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
+    const int32_t rc = tcg::decode_impl(c, frames, count);
+    tcg::ctx_release(c);
+    return rc;
+}

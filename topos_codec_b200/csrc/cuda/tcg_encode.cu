@@ -1,0 +1,1027 @@
+// tcg_encode.cu - V7-R2 intra encode on the GPU (any batch of frames).
+//
+// Pipeline (one stream, no host round trip until the packets are complete):
+//   k_fdct      8x8 blocks: edge-replicated load, level shift, exact integer
+//               forward DCT, dead-zone quantisation -> zigzag coefficients +
+//               non-zero mask                       (reference codec.c:1702-1848)
+//   k_tokens    DC residuals, run/level categories, per-slice histograms and
+//               joint context histograms, op counts  (codec.c:1702-1848, 2116-2151)
+//   k_select    per slice: exact double-precision model cost, model choice,
+//               row tables, coding tables             (codec.c:2159-2388, rans.c)
+//   k_opscan    per slice: reverse exclusive scan of op counts
+//   k_opgen     per block: the block's rANS operations in coding order
+//   k_chain     one lane per slice: the serial backward rANS state chain
+//               with byte renormalisation                (codec.c:2188-2265, 2410-2509)
+//   k_alpha     alpha bands: MED residuals + Rice run/level bit packing
+//               (codec.c:2969-3010, block_coding.c:456-481)
+//   k_pack_*    payload sizes, prefix sums into packet offsets, payload copy,
+//               slice CRC-32 + 17-byte headers, frame header size + CRC
+//               (codec.c:5203-5225, 5660-5693; frame_header.c:590-631)
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "tcg_common.cuh"
+#include "tcg_runtime.h"
+
+namespace tcg {
+
+struct EPlane {
+    uint64_t pix_off;    // element offset in the device sample buffer
+    uint32_t vis_w, vis_h, coded_w, coded_h, cols, rows;
+    uint32_t kind, alpha_shift, bd, q_is_one;
+    uint32_t blk0;       // first global colour block
+    uint32_t Q[64];
+    int64_t fclamp;
+};
+
+struct ESlice {
+    uint32_t frame, plane, kind;
+    uint32_t y0, bh, cols;
+    uint32_t blk0, nblk;
+    uint32_t qdb;
+    uint32_t pidx;        // plane index within the frame (slice header field)
+    uint64_t op_base;     // u32 units
+    uint64_t stage_base;  // bytes
+    uint64_t stage_cap;
+};
+
+struct ESliceRes {
+    uint32_t nops, nbytes, xfin, plen;
+    uint32_t payload, crc, err, pad;
+    uint64_t pkt_off;     // slice header offset within the frame packet
+};
+
+struct EFrame {
+    uint32_t slice0, nslices;
+    uint64_t pkt_base;
+    uint8_t hdr[56];
+};
+
+struct EFrameRes {
+    uint32_t size, color_payload, alpha_payload, err;
+    uint32_t alpha_err, color_slices, alpha_slices, pad;
+};
+
+struct EWork {  // token-pass work item: a run of blocks of one colour slice
+    uint32_t slice, lb0, n, pad;
+};
+
+// ============================== forward DCT ==============================
+
+__global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes, const uint32_t* __restrict__ cplanes,
+                                              uint32_t ncp, uint32_t total, const uint16_t* __restrict__ pix,
+                                              int32_t* __restrict__ coef, uint64_t* __restrict__ mask)
+{
+    const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gb >= total) { return; }
+    int lo = 0, hi = (int)ncp - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (planes[cplanes[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1; }
+    }
+    const EPlane& P = planes[cplanes[lo]];
+    const uint32_t lb = gb - P.blk0;
+    const uint32_t bx = lb % P.cols, by = lb / P.cols;
+    const uint16_t* src = pix + P.pix_off;
+    const int32_t mid = 1 << (P.bd - 1u);
+    const bool wide = P.bd > 12u;
+    int32_t x[64], F[64];
+#pragma unroll
+    for (int y = 0; y < 8; ++y) {
+        const uint32_t sy = min(by * 8u + (uint32_t)y, P.vis_h - 1u);
+        const uint16_t* row = src + (size_t)sy * P.vis_w;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t sx = min(bx * 8u + (uint32_t)k, P.vis_w - 1u);
+            const int32_t d = (int32_t)__ldg(row + sx) - mid;
+            x[y * 8 + k] = wide ? d : (int32_t)(int16_t)d;
+        }
+    }
+    if (!wide) { fdct8x8_i32(x, F); } else { fdct8x8_wide(x, F); }
+    // dead-zone quantisation (quant.c:310-346): q = sign*((|F|+Q/2-dz)/Q), dz = Q/4 (AC)
+    int32_t q[64];
+    const int64_t fc = P.fclamp;
+#pragma unroll
+    for (int i = 0; i < 64; ++i) {
+        int64_t v = F[i];
+        v = v > fc ? fc : (v < -fc ? -fc : v);
+        const uint32_t mag = (uint32_t)(v < 0 ? -v : v);
+        uint32_t qm;
+        if (P.q_is_one) {
+            qm = mag;
+        } else {
+            const uint32_t Q = P.Q[i];
+            const uint32_t dz = i == 0 ? 0u : Q >> 2;
+            const uint32_t num = mag + (Q >> 1);
+            qm = num > dz ? (num - dz) / Q : 0u;
+        }
+        q[i] = v < 0 ? -(int32_t)qm : (int32_t)qm;
+    }
+    uint64_t m = 0;
+    int4* out = reinterpret_cast<int4*>(coef + (size_t)gb * 64u);
+#pragma unroll
+    for (int p = 0; p < 64; p += 4) {
+        int4 v;
+        v.x = q[c_zigzag[p]]; v.y = q[c_zigzag[p + 1]]; v.z = q[c_zigzag[p + 2]]; v.w = q[c_zigzag[p + 3]];
+        m |= (uint64_t)(v.x != 0) << p | (uint64_t)(v.y != 0) << (p + 1) | (uint64_t)(v.z != 0) << (p + 2) |
+             (uint64_t)(v.w != 0) << (p + 3);
+        out[p >> 2] = v;
+    }
+    mask[gb] = m & ~(uint64_t)1;
+}
+
+// ======================= tokens + histograms + op counts =======================
+
+__device__ __forceinline__ uint32_t block_dcm(const int32_t* coef, uint32_t gb, uint32_t lb, uint32_t cols, bool* viol)
+{
+    const uint32_t bx = lb % cols, by = lb / cols;
+    const int32_t q0 = coef[(size_t)gb * 64u];
+    const int32_t l = bx > 0u ? coef[(size_t)(gb - 1u) * 64u] : 0;
+    const int32_t t = by > 0u ? coef[(size_t)(gb - cols) * 64u] : 0;
+    uint32_t dcm = map_s(q0 - dc_pred(bx > 0u, l, by > 0u, t));
+    if (dcm > 0x0FFFFFFFu) { dcm = 0x0FFFFFFFu; *viol = true; }
+    return dcm;
+}
+
+__global__ void __launch_bounds__(256) k_tokens(const EWork* __restrict__ work, const ESlice* __restrict__ slices,
+                                                const int32_t* __restrict__ coef, const uint64_t* __restrict__ mask,
+                                                uint32_t* __restrict__ dcm_out, uint32_t* __restrict__ nops_out,
+                                                uint32_t* __restrict__ hist, ESliceRes* __restrict__ sres)
+{
+    extern __shared__ uint32_t sh[];  // [H_BINS][32] lane-replicated counters
+    const EWork w = work[blockIdx.x];
+    const ESlice& S = slices[w.slice];
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = threadIdx.x; i < H_BINS * 32u; i += blockDim.x) { sh[i] = 0u; }
+    __syncthreads();
+    bool viol = false;
+    if (threadIdx.x < w.n) {
+        const uint32_t lb = w.lb0 + threadIdx.x;
+        const uint32_t gb = S.blk0 + lb;
+        const uint32_t dcm = block_dcm(coef, gb, lb, S.cols, &viol);
+        const uint32_t dcc = bitlen32(dcm);
+        uint32_t ctx = 0u;
+        if (lb > 0u) {
+            bool dummy = false;
+            ctx = dcp_ctx(bitlen32(block_dcm(coef, gb - 1u, lb - 1u, S.cols, &dummy)), true);
+        }
+        atomicAdd(&sh[(H_DC + dcc) * 32u + lane], 1u);
+        atomicAdd(&sh[(H_JDC + ctx * DC_SYMS + dcc) * 32u + lane], 1u);
+        uint32_t nops = 2u + suffix_chunks(dcc);  // EOB + DC symbol + DC suffix
+        uint64_t m = mask[gb];
+        uint32_t prev = 0u, pcat = 0u;
+        bool has = false;
+        const int32_t* c = coef + (size_t)gb * 64u;
+        while (m != 0u) {
+            const uint32_t p = (uint32_t)__ffsll((long long)m) - 1u;
+            m &= m - 1u;
+            uint32_t lm = map_s(c[p]);
+            if (lm > 0x07FFFFFFu) { lm = 0x07FFFFFFu; viol = true; }
+            const uint32_t cat = bitlen32(lm);
+            const uint32_t run = p - prev - 1u;
+            atomicAdd(&sh[(H_RUN + run) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_LVL + cat) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_JPOS + pos_ctx(p) * LVL_SYMS + cat) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_JPREV + prev_ctx(pcat, has) * LVL_SYMS + cat) * 32u + lane], 1u);
+            nops += 2u + suffix_chunks(cat);
+            prev = p;
+            pcat = cat;
+            has = true;
+        }
+        atomicAdd(&sh[(H_RUN + 63u) * 32u + lane], 1u);
+        dcm_out[gb] = dcm;
+        nops_out[gb] = nops;
+    }
+    if (__syncthreads_or(viol) && threadIdx.x == 0) { atomicOr(&sres[w.slice].err, 1u); }
+    uint32_t* g = hist + (size_t)w.slice * H_BINS;
+    for (uint32_t b = threadIdx.x; b < H_BINS; b += blockDim.x) {
+        uint32_t s = 0;
+#pragma unroll 8
+        for (uint32_t r = 0; r < 32u; ++r) { s += sh[b * 32u + ((r + b) & 31u)]; }
+        if (s != 0u) { atomicAdd(&g[b], s); }
+    }
+}
+
+// ============================ per-slice model choice ============================
+
+// One 32-thread block per colour slice. Row models are normalised in parallel
+// (one row per lane); the five candidate costs are then accumulated each by a
+// single lane in the reference order with separately rounded double ops.
+__global__ void __launch_bounds__(32) k_select(const ESlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                               const uint32_t* __restrict__ hist, const double* __restrict__ log2t,
+                                               uint32_t* __restrict__ stab, uint8_t* __restrict__ prefix,
+                                               ESliceRes* __restrict__ sres)
+{
+    __shared__ uint32_t h[H_BINS];
+    __shared__ uint8_t rb[17][64];
+    __shared__ uint16_t rf[17][64];
+    __shared__ uint16_t rc[17][64];
+    __shared__ double cost[5];
+    __shared__ uint32_t sel[2];
+    const uint32_t si = cslices[blockIdx.x];
+    const uint32_t t = threadIdx.x;
+    for (uint32_t i = t; i < H_BINS; i += 32u) { h[i] = hist[(size_t)si * H_BINS + i]; }
+    __syncwarp();
+    // rows: 0 lvl, 1-4 jpos, 5-9 jprev, 10 dc, 11-15 jdc, 16 run
+    if (t < 17u) {
+        const uint32_t* cnt;
+        uint32_t n;
+        if (t == 0u) { cnt = h + H_LVL; n = LVL_SYMS; }
+        else if (t <= 4u) { cnt = h + H_JPOS + (t - 1u) * LVL_SYMS; n = LVL_SYMS; }
+        else if (t <= 9u) { cnt = h + H_JPREV + (t - 5u) * LVL_SYMS; n = LVL_SYMS; }
+        else if (t == 10u) { cnt = h + H_DC; n = DC_SYMS; }
+        else if (t <= 15u) { cnt = h + H_JDC + (t - 11u) * DC_SYMS; n = DC_SYMS; }
+        else { cnt = h + H_RUN; n = RUN_SYMS; }
+        row_encode(rb[t], n, cnt);
+        model_from_bytes(rb[t], n, rf[t], rc[t]);
+    }
+    __syncwarp();
+    if (t < 5u) {
+        uint32_t r0, nr, n, base, stride;
+        double extra;
+        if (t == 0u) { r0 = 0; nr = 1; n = LVL_SYMS; base = H_LVL; stride = LVL_SYMS; extra = 8.0 * 28.0; }
+        else if (t == 1u) { r0 = 1; nr = 4; n = LVL_SYMS; base = H_JPOS; stride = LVL_SYMS; extra = 8.0 * 112.0; }
+        else if (t == 2u) { r0 = 5; nr = 5; n = LVL_SYMS; base = H_JPREV; stride = LVL_SYMS; extra = 8.0 * 140.0; }
+        else if (t == 3u) { r0 = 10; nr = 1; n = DC_SYMS; base = H_DC; stride = DC_SYMS; extra = 8.0 * 29.0; }
+        else { r0 = 11; nr = 5; n = DC_SYMS; base = H_JDC; stride = DC_SYMS; extra = 8.0 * 145.0; }
+        double bits = 0.0;
+        for (uint32_t r = 0; r < nr; ++r) {
+            for (uint32_t s = 0; s < n; ++s) {
+                const uint32_t c = h[base + r * stride + s];
+                if (c != 0u) {
+                    bits = __dadd_rn(bits, __dmul_rn((double)c, __dsub_rn(12.0, log2t[rf[r0 + r][s]])));
+                }
+            }
+        }
+        cost[t] = __dadd_rn(bits, extra);
+    }
+    __syncwarp();
+    if (t == 0u) {
+        uint32_t lm = 0;
+        double best = cost[0];
+        if (cost[1] < best) { best = cost[1]; lm = 1; }
+        if (cost[2] < best) { lm = 2; }
+        sel[0] = lm;
+        sel[1] = cost[4] < cost[3] ? 1u : 0u;
+    }
+    __syncwarp();
+    const uint32_t lm = sel[0], dm = sel[1];
+    const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+    const uint32_t dr0 = dm ? 11u : 10u, lr0 = lm == 1u ? 1u : lm == 2u ? 5u : 0u;
+    uint8_t* pre = prefix + (size_t)si * PREFIX_MAX;
+    const uint32_t plen = 1u + nd * DC_SYMS + RUN_SYMS + nl * LVL_SYMS;
+    for (uint32_t i = t; i < plen; i += 32u) {
+        uint8_t v;
+        if (i == 0u) { v = (uint8_t)(lm | (dm << 2)); }
+        else if (i < 1u + nd * DC_SYMS) { const uint32_t j = i - 1u; v = rb[dr0 + j / DC_SYMS][j % DC_SYMS]; }
+        else if (i < 1u + nd * DC_SYMS + RUN_SYMS) { v = rb[16][i - 1u - nd * DC_SYMS]; }
+        else { const uint32_t j = i - 1u - nd * DC_SYMS - RUN_SYMS; v = rb[lr0 + j / LVL_SYMS][j % LVL_SYMS]; }
+        pre[i] = v;
+    }
+    uint32_t* tb = stab + (size_t)si * T_SIZE;
+    for (uint32_t i = t; i < T_SIZE; i += 32u) {
+        uint32_t r, s;
+        if (i < T_RUN) { r = dr0 + (i / DC_SYMS < nd ? i / DC_SYMS : 0u); s = i % DC_SYMS; }
+        else if (i < T_LVL) { r = 16u; s = i - T_RUN; }
+        else { const uint32_t j = i - T_LVL; r = lr0 + (j / LVL_SYMS < nl ? j / LVL_SYMS : 0u); s = j % LVL_SYMS; }
+        tb[i] = ((uint32_t)rf[r][s] << 12) | rc[r][s];
+    }
+    if (t == 0u) { sres[si].plen = plen | (lm << 16) | (dm << 20); }
+}
+
+// ======================= op counts -> offsets (reverse scan) =======================
+
+__global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                                 const uint32_t* __restrict__ nops, uint32_t* __restrict__ opoff,
+                                                 ESliceRes* __restrict__ sres)
+{
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t carry;
+    const uint32_t si = cslices[blockIdx.x];
+    const ESlice& S = slices[si];
+    const uint32_t n = S.nblk;
+    if (threadIdx.x == 0) { carry = 0u; }
+    __syncthreads();
+    // position r counts blocks from the end of the slice (coding order)
+    for (uint32_t base = 0; base < n; base += blockDim.x) {
+        const uint32_t r = base + threadIdx.x;
+        const uint32_t v = r < n ? nops[S.blk0 + (n - 1u - r)] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+            if ((threadIdx.x & 31u) >= (uint32_t)d) { x += y; }
+        }
+        if ((threadIdx.x & 31u) == 31u) { wsum[threadIdx.x >> 5] = x; }
+        __syncthreads();
+        if (threadIdx.x < 32u) {
+            uint32_t s = threadIdx.x < (blockDim.x >> 5) ? wsum[threadIdx.x] : 0u;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, d);
+                if (threadIdx.x >= (uint32_t)d) { s += y; }
+            }
+            wsum[threadIdx.x] = s;
+        }
+        __syncthreads();
+        const uint32_t wpre = (threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1u] : 0u;
+        if (r < n) { opoff[S.blk0 + (n - 1u - r)] = carry + wpre + x - v; }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1u) { carry += wpre + x; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { sres[si].nops = carry; }
+}
+
+// ============================== op generation ==============================
+// op word: bit31 = 0 symbol (bits 12..24 freq, 0..11 cum); 1 raw chunk
+// (bits 23..27 width w, 0..22 value).
+
+__device__ __forceinline__ uint32_t op_chunk(uint32_t w, uint32_t v) { return 0x80000000u | (w << 23) | (v & ((1u << w) - 1u)); }
+
+__device__ __forceinline__ void put_suffix_ops(uint32_t*& o, uint32_t cat, uint32_t m)
+{
+    if (cat <= 1u) { return; }
+    uint32_t b = cat - 1u;
+    if (b > 23u) { *o++ = op_chunk(b - 16u, m >> 16); b = 16u; }
+    *o++ = op_chunk(b, m);
+}
+
+__global__ void __launch_bounds__(256) k_opgen(const EWork* __restrict__ work, const ESlice* __restrict__ slices,
+                                               const int32_t* __restrict__ coef, const uint64_t* __restrict__ mask,
+                                               const uint32_t* __restrict__ dcm, const uint32_t* __restrict__ opoff,
+                                               const uint32_t* __restrict__ stab, const ESliceRes* __restrict__ sres,
+                                               uint32_t* __restrict__ ops)
+{
+    const EWork w = work[blockIdx.x];
+    if (threadIdx.x >= w.n) { return; }
+    const ESlice& S = slices[w.slice];
+    const uint32_t lb = w.lb0 + threadIdx.x;
+    const uint32_t gb = S.blk0 + lb;
+    const uint32_t* tb = stab + (size_t)w.slice * T_SIZE;
+    const uint32_t pl = sres[w.slice].plen;
+    const uint32_t lmod = (pl >> 16) & 3u, dmod = (pl >> 20) & 1u;
+    uint32_t* o = ops + S.op_base + opoff[gb];
+    const int32_t* c = coef + (size_t)gb * 64u;
+    *o++ = __ldg(tb + T_RUN + 63u);  // EOB
+    uint64_t m = mask[gb];
+    // walk non-zero positions from the highest down; the forward-order
+    // neighbour of position p is the next lower set bit (or the DC at 0)
+    while (m != 0u) {
+        const uint32_t p = 63u - (uint32_t)__clzll((long long)m);
+        m &= ~((uint64_t)1 << p);
+        const uint32_t below = m != 0u ? 63u - (uint32_t)__clzll((long long)m) : 0u;
+        const uint32_t lv = map_s(c[p]);
+        const uint32_t lmv = lv > 0x07FFFFFFu ? 0x07FFFFFFu : lv;
+        const uint32_t cat = bitlen32(lmv);
+        put_suffix_ops(o, cat, lmv);
+        uint32_t ctx = 0u;
+        if (lmod == 1u) {
+            ctx = pos_ctx(p);
+        } else if (lmod == 2u) {
+            uint32_t pc = 0u;
+            if (m != 0u) {
+                const uint32_t pv = map_s(c[below]);
+                pc = bitlen32(pv > 0x07FFFFFFu ? 0x07FFFFFFu : pv);
+            }
+            ctx = prev_ctx(pc, m != 0u);
+        }
+        *o++ = __ldg(tb + T_LVL + ctx * LVL_SYMS + cat);
+        *o++ = __ldg(tb + T_RUN + (p - below - 1u));
+    }
+    const uint32_t dm = dcm[gb];
+    const uint32_t ds = bitlen32(dm);
+    put_suffix_ops(o, ds, dm);
+    const uint32_t dctx = dmod ? dcp_ctx(lb > 0u ? bitlen32(dcm[gb - 1u]) : 0u, lb > 0u) : 0u;
+    *o++ = __ldg(tb + T_DC + dctx * DC_SYMS + ds);
+}
+
+// =============================== rANS chains ===============================
+
+// One lane per colour slice; the lane walks its slice's operations in coding
+// order and writes renormalisation bytes backwards from the end of its
+// staging window, so the stream reads forwards when the chain finishes.
+__global__ void __launch_bounds__(32) k_chain(const ESlice* __restrict__ slices, const uint32_t* __restrict__ order,
+                                              uint32_t n, const uint32_t* __restrict__ ops,
+                                              const uint32_t* __restrict__ div_m, const uint8_t* __restrict__ div_l,
+                                              uint8_t* __restrict__ stage, ESliceRes* __restrict__ sres)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    const uint32_t si = order[i];
+    const ESlice& S = slices[si];
+    const uint32_t nops = sres[si].nops;
+    const uint32_t* op = ops + S.op_base;
+    uint8_t* end = stage + S.stage_base + S.stage_cap;  // byte k goes to end[-1-k]
+    uint32_t x = RANS_L;
+    uint32_t pos = 0;
+    uint32_t cur = nops > 0u ? __ldg(op) : 0u;
+    for (uint32_t k = 0; k < nops; ++k) {
+        const uint32_t nxt = k + 1u < nops ? __ldg(op + k + 1u) : 0u;
+        if ((int32_t)cur < 0) {
+            const uint32_t w = (cur >> 23) & 31u;
+            const uint32_t thr = 1u << (31u - w);
+            while (x >= thr) { end[-1 - (int64_t)pos] = (uint8_t)x; ++pos; x >>= 8; }
+            x = (x << w) | (cur & 0x7FFFFFu);
+        } else {
+            const uint32_t f = (cur >> 12) & 0x1FFFu;
+            const uint32_t cum = cur & 0xFFFu;
+            const uint32_t mg = __ldg(div_m + f);
+            const uint32_t sh = __ldg(div_l + f);
+            const uint32_t xmax = f << 19;
+            while (x >= xmax) { end[-1 - (int64_t)pos] = (uint8_t)x; ++pos; x >>= 8; }
+            const uint32_t q = __umulhi(x << 1, mg) >> sh;
+            x = x + q * (4096u - f) + cum;
+        }
+        cur = nxt;
+    }
+    sres[si].nbytes = pos;
+    sres[si].xfin = x;
+}
+
+// ================================ alpha bands ================================
+
+__device__ __forceinline__ uint32_t rice_len(uint32_t k, uint32_t m)
+{
+    const uint32_t q = m >> k;
+    return q <= 30u ? q + 1u + k : 63u;
+}
+
+// OR an n-bit field (n <= 32, MSB first) into a zeroed byte stream at bit o.
+__device__ __forceinline__ void put_bits_or(uint8_t* base, uint64_t o, uint32_t n, uint32_t v)
+{
+    while (n > 0u) {
+        const uint32_t room = 8u - (uint32_t)(o & 7u);
+        const uint32_t take = n < room ? n : room;
+        const uint32_t piece = (v >> (n - take)) & ((1u << take) - 1u);
+        const uint8_t b = (uint8_t)(piece << (room - take));
+        uint8_t* p = base + (o >> 3);
+        uint32_t* wd = reinterpret_cast<uint32_t*>((uintptr_t)p & ~(uintptr_t)3);
+        atomicOr(wd, (uint32_t)b << (8u * ((uintptr_t)p & 3u)));
+        o += take;
+        n -= take;
+    }
+}
+
+__device__ __forceinline__ void put_rice(uint8_t* base, uint64_t o, uint32_t k, uint32_t m)
+{
+    const uint32_t q = m >> k;
+    if (q <= 30u) {
+        const uint32_t ones = q == 0u ? 0u : (0xFFFFFFFFu >> (32u - q));
+        put_bits_or(base, o, q + 1u, ones << 1);  // q ones then a zero
+        if (k > 0u) { put_bits_or(base, o + q + 1u, k, m & ((1u << k) - 1u)); }
+    } else {
+        put_bits_or(base, o, 31u, 0x7FFFFFFFu);
+        put_bits_or(base, o + 31u, 32u, m);
+    }
+}
+
+__device__ __forceinline__ uint32_t alpha_sample(const uint16_t* src, const EPlane& P, uint32_t x, uint32_t y)
+{
+    const uint32_t sx = min(x, P.vis_w - 1u), sy = min(y, P.vis_h - 1u);
+    uint32_t v = __ldg(src + (size_t)sy * P.vis_w + sx);
+    if (P.alpha_shift != 0u) {
+        const uint32_t s = P.alpha_shift, top = (0xFFFFu >> s) << s;
+        v = ((v + (1u << (s - 1u))) >> s) << s;
+        v = v > top ? top : v;
+    }
+    return v;
+}
+
+__device__ __forceinline__ int32_t alpha_residual(const uint16_t* src, const EPlane& P, uint32_t py0, uint32_t idx)
+{
+    const uint32_t w = P.coded_w;
+    const uint32_t y = idx / w, x = idx % w;
+    const int32_t a = (int32_t)alpha_sample(src, P, x, py0 + y);
+    int32_t pred;
+    if (y == 0u) {
+        pred = x == 0u ? 0 : (int32_t)alpha_sample(src, P, x - 1u, py0);
+    } else if (x == 0u) {
+        pred = (int32_t)alpha_sample(src, P, 0u, py0 + y - 1u);
+    } else {
+        const int32_t l = (int32_t)alpha_sample(src, P, x - 1u, py0 + y);
+        const int32_t u = (int32_t)alpha_sample(src, P, x, py0 + y - 1u);
+        const int32_t ul = (int32_t)alpha_sample(src, P, x - 1u, py0 + y - 1u);
+        if (ul >= l && ul >= u) { pred = l < u ? l : u; }
+        else if (ul <= l && ul <= u) { pred = l < u ? u : l; }
+        else { pred = l + u - ul; }
+    }
+    return a - pred;
+}
+
+// Block-wide exclusive scan (sum) of one value per thread; returns the
+// exclusive prefix and writes the block total to *total.
+template <typename T>
+__device__ inline T block_exscan(T v, T* total, T* sm)
+{
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const T y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= (uint32_t)d) { x += y; }
+    }
+    if (lane == 31u) { sm[wid] = x; }
+    __syncthreads();
+    if (wid == 0) {
+        T s = lane < (blockDim.x >> 5) ? sm[lane] : (T)0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const T y = __shfl_up_sync(0xFFFFFFFFu, s, d);
+            if (lane >= (uint32_t)d) { s += y; }
+        }
+        sm[lane] = s;
+    }
+    __syncthreads();
+    const T pre = (wid ? sm[wid - 1u] : (T)0) + x - v;
+    *total = sm[(blockDim.x >> 5) - 1u];
+    __syncthreads();
+    return pre;
+}
+
+// One block per alpha band. Pass 1 computes the Rice parameters from the
+// residual statistics, pass 2 emits (run, level) pairs and the trailing
+// (run, 0) terminator with every code placed by a prefix sum of code lengths.
+__global__ void __launch_bounds__(256) k_alpha(const ESlice* __restrict__ slices, const uint32_t* __restrict__ aslices,
+                                               const EPlane* __restrict__ planes, const uint16_t* __restrict__ pix,
+                                               uint8_t* __restrict__ stage, ESliceRes* __restrict__ sres,
+                                               uint32_t* __restrict__ alpha_err)
+{
+    __shared__ unsigned long long sm64[32];
+    __shared__ int32_t last_nz;
+    __shared__ uint32_t kk[2];
+    const uint32_t si = aslices[blockIdx.x];
+    const ESlice& S = slices[si];
+    const EPlane& P = planes[S.plane];
+    const uint16_t* src = pix + P.pix_off;
+    const uint32_t w = P.coded_w;
+    const uint32_t py0 = S.y0 * 8u;
+    const uint32_t count = w * S.bh * 8u;
+    uint8_t* out = stage + S.stage_base;
+    // max |source - near-lossless value| over the band (coded geometry)
+    if (P.alpha_shift != 0u) {
+        uint32_t me = 0;
+        for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) {
+            const uint32_t x = i % w, y = i / w;
+            const uint32_t sx = min(x, P.vis_w - 1u), sy = min(py0 + y, P.vis_h - 1u);
+            const uint32_t v = __ldg(src + (size_t)sy * P.vis_w + sx);
+            const uint32_t q = alpha_sample(src, P, x, py0 + y);
+            me = max(me, v > q ? v - q : q - v);
+        }
+        atomicMax(alpha_err + S.frame, me);
+    }
+    // pass 1: statistics
+    unsigned long long s_lvl = 0, c_lvl = 0, s_run = 0, c_run = 0;
+    if (threadIdx.x == 0) { last_nz = -1; }
+    __syncthreads();
+    for (uint32_t base = 0; base < count; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const int32_t r = i < count ? alpha_residual(src, P, py0, i) : 0;
+        const bool nz = r != 0;
+        // previous non-zero index: max over earlier non-zero lanes of this tile or the carry
+        int32_t mine = nz ? (int32_t)i : -1;
+        int32_t run_max = mine;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int32_t y = __shfl_up_sync(0xFFFFFFFFu, run_max, d);
+            if ((threadIdx.x & 31u) >= (uint32_t)d) { run_max = max(run_max, y); }
+        }
+        __shared__ int32_t wmax[8];
+        if ((threadIdx.x & 31u) == 31u) { wmax[threadIdx.x >> 5] = run_max; }
+        __syncthreads();
+        int32_t before = last_nz;
+        for (uint32_t q = 0; q < (threadIdx.x >> 5); ++q) { before = max(before, wmax[q]); }
+        const int32_t incl_prev = __shfl_up_sync(0xFFFFFFFFu, run_max, 1);
+        if ((threadIdx.x & 31u) > 0u) { before = max(before, incl_prev); }
+        if (nz) {
+            s_run += (unsigned long long)((int32_t)i - before - 1);
+            c_run++;
+            s_lvl += map_s(r);
+            c_lvl++;
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1u) {
+            int32_t m = last_nz;
+            for (uint32_t q = 0; q < (blockDim.x >> 5); ++q) { m = max(m, wmax[q]); }
+            last_nz = m;
+        }
+        __syncthreads();
+    }
+    unsigned long long tot;
+    s_lvl = block_exscan<unsigned long long>(s_lvl, &tot, sm64); s_lvl = tot;
+    c_lvl = block_exscan<unsigned long long>(c_lvl, &tot, sm64); c_lvl = tot;
+    s_run = block_exscan<unsigned long long>(s_run, &tot, sm64); s_run = tot;
+    c_run = block_exscan<unsigned long long>(c_run, &tot, sm64); c_run = tot;
+    if (threadIdx.x == 0) {
+        const int32_t tail = (int32_t)count - 1 - last_nz;
+        if (tail > 0) { s_run += (unsigned long long)tail; c_run++; }
+        uint32_t k1 = 0, k2 = 0;
+        if (c_lvl != 0u && s_lvl != 0u) { const unsigned long long mn = s_lvl / c_lvl; while (k1 < 14u && (mn >> (k1 + 1u)) != 0u) { ++k1; } }
+        if (c_run != 0u && s_run != 0u) { const unsigned long long mn = s_run / c_run; while (k2 < 14u && (mn >> (k2 + 1u)) != 0u) { ++k2; } }
+        kk[0] = k1;
+        kk[1] = k2;
+        last_nz = -1;
+    }
+    __syncthreads();
+    const uint32_t k1 = kk[0], k2 = kk[1];
+    // pass 2: codes
+    unsigned long long bitpos = 0;
+    __shared__ unsigned long long carry_bits;
+    if (threadIdx.x == 0) { carry_bits = 0; }
+    __syncthreads();
+    for (uint32_t base = 0; base < count; base += blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const int32_t r = i < count ? alpha_residual(src, P, py0, i) : 0;
+        const bool nz = r != 0;
+        int32_t run_max = nz ? (int32_t)i : -1;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int32_t y = __shfl_up_sync(0xFFFFFFFFu, run_max, d);
+            if ((threadIdx.x & 31u) >= (uint32_t)d) { run_max = max(run_max, y); }
+        }
+        __shared__ int32_t wmax2[8];
+        if ((threadIdx.x & 31u) == 31u) { wmax2[threadIdx.x >> 5] = run_max; }
+        __syncthreads();
+        int32_t before = last_nz;
+        for (uint32_t q = 0; q < (threadIdx.x >> 5); ++q) { before = max(before, wmax2[q]); }
+        const int32_t incl_prev = __shfl_up_sync(0xFFFFFFFFu, run_max, 1);
+        if ((threadIdx.x & 31u) > 0u) { before = max(before, incl_prev); }
+        const uint32_t run = nz ? (uint32_t)((int32_t)i - before - 1) : 0u;
+        const uint32_t lm = nz ? map_s(r) : 0u;
+        const unsigned long long len = nz ? (unsigned long long)(rice_len(k2, run) + rice_len(k1, lm)) : 0ull;
+        unsigned long long tile_total;
+        const unsigned long long pre = block_exscan<unsigned long long>(len, &tile_total, sm64);
+        if (nz) {
+            const unsigned long long o = carry_bits + pre;
+            put_rice(out, o, k2, run);
+            put_rice(out, o + rice_len(k2, run), k1, lm);
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1u) {
+            int32_t m = last_nz;
+            for (uint32_t q = 0; q < (blockDim.x >> 5); ++q) { m = max(m, wmax2[q]); }
+            last_nz = m;
+            carry_bits += tile_total;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        bitpos = carry_bits;
+        const int32_t tail = (int32_t)count - 1 - last_nz;
+        if (tail > 0) {
+            put_rice(out, bitpos, k2, (uint32_t)tail);
+            bitpos += rice_len(k2, (uint32_t)tail);
+            put_rice(out, bitpos, k1, 0u);
+            bitpos += rice_len(k1, 0u);
+        }
+        sres[si].nbytes = (uint32_t)((bitpos + 7u) >> 3);
+        sres[si].plen = 0u;
+        sres[si].xfin = (k1 << 8) | k2;  // alpha: Rice parameters for the slice header
+    }
+}
+
+// ============================== packet assembly ==============================
+
+__device__ __forceinline__ uint32_t payload_size(const ESlice& S, const ESliceRes& R)
+{
+    return S.kind == TCG_PLANE_COLOR ? (R.plen & 0xFFFFu) + 4u + R.nbytes : R.nbytes;
+}
+
+// one thread per frame: payload sizes, packet offsets, totals
+__global__ void k_pack_sizes(const EFrame* __restrict__ frames, uint32_t nf, const ESlice* __restrict__ slices,
+                             ESliceRes* __restrict__ sres, EFrameRes* __restrict__ fres)
+{
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) { return; }
+    const EFrame& F = frames[f];
+    uint64_t off = 53u;
+    uint32_t cp = 0, ap = 0, cs = 0, as = 0, err = 0;
+    for (uint32_t i = 0; i < F.nslices; ++i) {
+        const uint32_t si = F.slice0 + i;
+        ESliceRes& R = sres[si];
+        const uint32_t pay = payload_size(slices[si], R);
+        R.payload = pay;
+        R.pkt_off = off;
+        off += 17u + pay;
+        if (slices[si].kind == TCG_PLANE_COLOR) { cp += pay; cs++; } else { ap += pay; as++; }
+        err |= R.err;
+    }
+    fres[f].size = off > 268435456ull ? 0xFFFFFFFFu : (uint32_t)off;
+    fres[f].color_payload = cp;
+    fres[f].alpha_payload = ap;
+    fres[f].color_slices = cs;
+    fres[f].alpha_slices = as;
+    fres[f].err = err;
+}
+
+// grid (slice, part): copy prefix | state | stream (or the alpha bytes) into the packet
+__global__ void __launch_bounds__(256) k_pack_copy(const EFrame* __restrict__ frames, const ESlice* __restrict__ slices,
+                                                   const ESliceRes* __restrict__ sres, const uint8_t* __restrict__ prefix,
+                                                   const uint8_t* __restrict__ stage, uint8_t* __restrict__ pkt,
+                                                   uint32_t cap_frames)
+{
+    const uint32_t si = blockIdx.x;
+    const ESlice& S = slices[si];
+    const ESliceRes& R = sres[si];
+    const EFrame& F = frames[S.frame];
+    uint8_t* dst = pkt + F.pkt_base + R.pkt_off + 17u;
+    const uint32_t plen = S.kind == TCG_PLANE_COLOR ? (R.plen & 0xFFFFu) : 0u;
+    const uint32_t head = S.kind == TCG_PLANE_COLOR ? plen + 4u : 0u;
+    const uint8_t* stream = S.kind == TCG_PLANE_COLOR ? stage + S.stage_base + S.stage_cap - R.nbytes
+                                                      : stage + S.stage_base;
+    const uint32_t total = R.payload;
+    const uint32_t stride = gridDim.y * blockDim.x;
+    for (uint32_t i = blockIdx.y * blockDim.x + threadIdx.x; i < total; i += stride) {
+        uint8_t v;
+        if (i < plen) { v = prefix[(size_t)si * PREFIX_MAX + i]; }
+        else if (i < head) { v = (uint8_t)(R.xfin >> (8u * (3u - (i - plen)))); }
+        else { v = stream[i - head]; }
+        dst[i] = v;
+    }
+    (void)cap_frames;
+}
+
+// one block per slice: payload CRC-32 and the 17-byte slice header
+__global__ void __launch_bounds__(256) k_pack_crc(const EFrame* __restrict__ frames, const ESlice* __restrict__ slices,
+                                                  ESliceRes* __restrict__ sres, const uint32_t* __restrict__ crctab,
+                                                  uint8_t* __restrict__ pkt)
+{
+    __shared__ uint32_t t[8 * 256];
+    __shared__ uint32_t scratch[512];
+    for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
+    __syncthreads();
+    const uint32_t si = blockIdx.x;
+    const ESlice& S = slices[si];
+    ESliceRes& R = sres[si];
+    uint8_t* h = pkt + frames[S.frame].pkt_base + R.pkt_off;
+    const uint32_t crc = crc32_block(h + 17u, R.payload, t, scratch);
+    if (threadIdx.x == 0) {
+        R.crc = crc;
+        const uint32_t k1 = S.kind == TCG_PLANE_COLOR ? 0u : (R.xfin >> 8) & 0xFFu;
+        const uint32_t k2 = S.kind == TCG_PLANE_COLOR ? 0u : R.xfin & 0xFFu;
+        // 17-byte slice header (slice_map.c:7-20), big-endian
+        h[0] = (uint8_t)(R.payload >> 24); h[1] = (uint8_t)(R.payload >> 16);
+        h[2] = (uint8_t)(R.payload >> 8); h[3] = (uint8_t)R.payload;
+        h[4] = (uint8_t)S.pidx;
+        h[5] = (uint8_t)(S.y0 >> 8); h[6] = (uint8_t)S.y0;
+        h[7] = (uint8_t)(S.bh >> 8); h[8] = (uint8_t)S.bh;
+        h[9] = (uint8_t)S.qdb;
+        h[10] = (uint8_t)k1; h[11] = (uint8_t)k2; h[12] = 0u;
+        h[13] = (uint8_t)(crc >> 24); h[14] = (uint8_t)(crc >> 16);
+        h[15] = (uint8_t)(crc >> 8); h[16] = (uint8_t)crc;
+    }
+}
+
+// one thread per frame: header with the packet size, then CRC over bytes 0..48
+__global__ void k_pack_header(const EFrame* __restrict__ frames, uint32_t nf, const EFrameRes* __restrict__ fres,
+                              const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
+{
+    const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) { return; }
+    uint8_t* h = pkt + frames[f].pkt_base;
+    const uint32_t size = fres[f].size;
+    for (int i = 0; i < 53; ++i) { h[i] = frames[f].hdr[i]; }
+    h[41] = (uint8_t)(size >> 24); h[42] = (uint8_t)(size >> 16); h[43] = (uint8_t)(size >> 8); h[44] = (uint8_t)size;
+    uint32_t c = 0xFFFFFFFFu;
+    for (int i = 0; i < 49; ++i) { c = crctab[(c ^ h[i]) & 0xFFu] ^ (c >> 8); }
+    c ^= 0xFFFFFFFFu;
+    h[49] = (uint8_t)(c >> 24); h[50] = (uint8_t)(c >> 16); h[51] = (uint8_t)(c >> 8); h[52] = (uint8_t)c;
+}
+
+// ================================== driver ==================================
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1u) / a * a; }
+
+static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs,
+                           const size_t* caps, tcg_enc_result* res)
+{
+    // ---------------- host planning ----------------
+    std::vector<EPlane> planes;
+    std::vector<ESlice> slices;
+    std::vector<EFrame> ef(count);
+    std::vector<uint32_t> cplanes, cslices, aslices;
+    std::vector<EWork> work;
+    uint64_t pix_elems = 0, nblk = 0, ops_words = 0, stage_bytes = 0, pkt_bytes = 0;
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_enc_frame& F = frames[f];
+        ef[f].slice0 = (uint32_t)slices.size();
+        ef[f].nslices = 0;
+        memset(ef[f].hdr, 0, sizeof(ef[f].hdr));
+        memcpy(ef[f].hdr, F.header, 53);
+        uint64_t fbound = 53;
+        for (uint32_t p = 0; p < F.planes; ++p) {
+            const tcg_enc_plane& I = F.plane[p];
+            EPlane P;
+            memset(&P, 0, sizeof(P));
+            P.pix_off = pix_elems;
+            pix_elems += (uint64_t)I.vis_w * I.vis_h;
+            pix_elems = align_up(pix_elems, 64);
+            P.vis_w = I.vis_w; P.vis_h = I.vis_h; P.coded_w = I.coded_w; P.coded_h = I.coded_h;
+            P.cols = I.cols; P.rows = I.rows; P.kind = I.kind; P.alpha_shift = I.alpha_shift;
+            P.bd = F.bit_depth;
+            P.blk0 = (uint32_t)nblk;
+            P.fclamp = I.fclamp;
+            P.q_is_one = 1u;
+            for (int i = 0; i < 64; ++i) { P.Q[i] = I.Q[i]; if (I.Q[i] != 1u) { P.q_is_one = 0u; } }
+            const uint32_t pg = (uint32_t)planes.size();
+            if (I.kind == TCG_PLANE_COLOR) {
+                cplanes.push_back(pg);
+                nblk += (uint64_t)I.cols * I.rows;
+            }
+            for (uint32_t y0 = 0; y0 < I.rows; y0 += F.slice_rows) {
+                ESlice S;
+                memset(&S, 0, sizeof(S));
+                S.frame = f; S.plane = pg; S.kind = I.kind; S.pidx = p;
+                S.y0 = y0; S.bh = std::min(F.slice_rows, I.rows - y0); S.cols = I.cols;
+                S.qdb = I.qdb;
+                uint64_t pay;
+                if (I.kind == TCG_PLANE_COLOR) {
+                    S.blk0 = P.blk0 + y0 * I.cols;
+                    S.nblk = S.bh * I.cols;
+                    S.op_base = ops_words;
+                    ops_words += (uint64_t)S.nblk * 256u;
+                    S.stage_cap = (uint64_t)S.nblk * 512u + 64u;
+                    pay = PREFIX_MAX + 4u + S.stage_cap;
+                    const uint32_t si = (uint32_t)slices.size();
+                    cslices.push_back(si);
+                    for (uint32_t lb = 0; lb < S.nblk; lb += 256u) {
+                        EWork w = {si, lb, std::min(256u, S.nblk - lb), 0u};
+                        work.push_back(w);
+                    }
+                } else {
+                    S.stage_cap = (uint64_t)I.coded_w * S.bh * 8u * 16u + 64u;
+                    pay = S.stage_cap;
+                    aslices.push_back((uint32_t)slices.size());
+                }
+                S.stage_base = stage_bytes;
+                stage_bytes = align_up(stage_bytes + S.stage_cap, 256);
+                fbound += 17u + pay;
+                slices.push_back(S);
+                ef[f].nslices++;
+            }
+            planes.push_back(P);
+        }
+        ef[f].pkt_base = pkt_bytes;
+        pkt_bytes = align_up(pkt_bytes + fbound, 256);
+    }
+    const uint32_t ns = (uint32_t)slices.size(), nc = (uint32_t)cslices.size();
+    // chain lanes: largest slices first so each warp holds similar chain lengths
+    std::vector<uint32_t> order = cslices;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return slices[a].nblk > slices[b].nblk; });
+
+    // ---------------- device buffers ----------------
+    const size_t desc_bytes = align_up(planes.size() * sizeof(EPlane), 256) + align_up(ns * sizeof(ESlice), 256) +
+                              align_up(count * sizeof(EFrame), 256) + align_up(work.size() * sizeof(EWork), 256) +
+                              align_up((cplanes.size() + cslices.size() + aslices.size() + order.size()) * 4u + 16u, 256);
+    if (!dreserve(C, B_PIX, pix_elems * 2u + 256) || !dreserve(C, B_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_MASK, nblk * 8u + 256) || !dreserve(C, B_DCM, nblk * 4u + 256) ||
+        !dreserve(C, B_NOPS, nblk * 4u + 256) || !dreserve(C, B_OPOFF, nblk * 4u + 256) ||
+        !dreserve(C, B_HIST, (size_t)ns * H_BINS * 4u + 256) || !dreserve(C, B_STAB, (size_t)ns * T_SIZE * 4u + 256) ||
+        !dreserve(C, B_TMP0, (size_t)ns * PREFIX_MAX + 256) || !dreserve(C, B_OPS, ops_words * 4u + 256) ||
+        !dreserve(C, B_STAGE, stage_bytes + 256) || !dreserve(C, B_SRES, (size_t)ns * sizeof(ESliceRes) + 256) ||
+        !dreserve(C, B_FRES, (size_t)count * (sizeof(EFrameRes) + 4u) + 256) || !dreserve(C, B_PKT, pkt_bytes + 256) ||
+        !dreserve(C, B_DESC, desc_bytes) || !hreserve(C, 0, desc_bytes) ||
+        !hreserve(C, 1, (size_t)count * sizeof(EFrameRes) + 4096)) {
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    cudaStream_t st = C->stream;
+    // descriptors through pinned staging
+    uint8_t* hd = (uint8_t*)C->h[0].p;
+    uint8_t* dd = dptr<uint8_t>(C, B_DESC);
+    size_t o = 0;
+    auto put = [&](const void* src, size_t n) -> size_t {
+        const size_t at = o;
+        if (n) { memcpy(hd + o, src, n); }
+        o = align_up(o + n, 256);
+        return at;
+    };
+    const size_t o_pl = put(planes.data(), planes.size() * sizeof(EPlane));
+    const size_t o_sl = put(slices.data(), ns * sizeof(ESlice));
+    const size_t o_fr = put(ef.data(), count * sizeof(EFrame));
+    const size_t o_wk = put(work.data(), work.size() * sizeof(EWork));
+    const size_t o_cp = put(cplanes.data(), cplanes.size() * 4u);
+    const size_t o_cs = put(cslices.data(), cslices.size() * 4u);
+    const size_t o_as = put(aslices.data(), aslices.size() * 4u);
+    const size_t o_or = put(order.data(), order.size() * 4u);
+    TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
+    const EPlane* d_pl = (const EPlane*)(dd + o_pl);
+    const ESlice* d_sl = (const ESlice*)(dd + o_sl);
+    const EFrame* d_fr = (const EFrame*)(dd + o_fr);
+    const EWork* d_wk = (const EWork*)(dd + o_wk);
+    const uint32_t* d_cp = (const uint32_t*)(dd + o_cp);
+    const uint32_t* d_cs = (const uint32_t*)(dd + o_cs);
+    const uint32_t* d_as = (const uint32_t*)(dd + o_as);
+    const uint32_t* d_or = (const uint32_t*)(dd + o_or);
+
+    // samples: one 2-D copy per plane (host or device source, caller stride)
+    uint16_t* d_pix = dptr<uint16_t>(C, B_PIX);
+    {
+        uint32_t pg = 0;
+        for (uint32_t f = 0; f < count; ++f) {
+            for (uint32_t p = 0; p < frames[f].planes; ++p, ++pg) {
+                const tcg_enc_plane& I = frames[f].plane[p];
+                TCG_CHECK(cudaMemcpy2DAsync(d_pix + planes[pg].pix_off, (size_t)I.vis_w * 2u, I.src, I.stride * 2u,
+                                            (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, st));
+            }
+        }
+    }
+    ESliceRes* d_sres = dptr<ESliceRes>(C, B_SRES);
+    EFrameRes* d_fres = dptr<EFrameRes>(C, B_FRES);
+    uint32_t* d_aerr = reinterpret_cast<uint32_t*>(dptr<uint8_t>(C, B_FRES) + align_up(count * sizeof(EFrameRes), 16));
+    TCG_CHECK(cudaMemsetAsync(d_sres, 0, (size_t)ns * sizeof(ESliceRes), st));
+    TCG_CHECK(cudaMemsetAsync(d_aerr, 0, (size_t)count * 4u, st));
+    TCG_CHECK(cudaMemsetAsync(dptr<uint32_t>(C, B_HIST), 0, (size_t)ns * H_BINS * 4u, st));
+    const DevTables& T = tables();
+    int32_t* d_coef = dptr<int32_t>(C, B_COEF);
+    uint64_t* d_mask = dptr<uint64_t>(C, B_MASK);
+    uint32_t* d_dcm = dptr<uint32_t>(C, B_DCM);
+    uint32_t* d_nops = dptr<uint32_t>(C, B_NOPS);
+    uint32_t* d_opoff = dptr<uint32_t>(C, B_OPOFF);
+    uint32_t* d_hist = dptr<uint32_t>(C, B_HIST);
+    uint32_t* d_stab = dptr<uint32_t>(C, B_STAB);
+    uint8_t* d_prefix = dptr<uint8_t>(C, B_TMP0);
+    uint32_t* d_ops = dptr<uint32_t>(C, B_OPS);
+    uint8_t* d_stage = dptr<uint8_t>(C, B_STAGE);
+    uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
+
+    uint32_t launches = 0;
+    if (nblk > 0) {
+        k_fdct<<<(uint32_t)((nblk + 127u) / 128u), 128, 0, st>>>(d_pl, d_cp, (uint32_t)cplanes.size(), (uint32_t)nblk,
+                                                                d_pix, d_coef, d_mask);
+        const size_t tok_smem = H_BINS * 32u * 4u;
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(k_tokens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tok_smem);
+            attr_set = true;
+        }
+        k_tokens<<<(uint32_t)work.size(), 256, tok_smem, st>>>(d_wk, d_sl, d_coef, d_mask, d_dcm, d_nops, d_hist, d_sres);
+        k_select<<<nc, 32, 0, st>>>(d_sl, d_cs, d_hist, T.log2, d_stab, d_prefix, d_sres);
+        k_opscan<<<nc, 1024, 0, st>>>(d_sl, d_cs, d_nops, d_opoff, d_sres);
+        k_opgen<<<(uint32_t)work.size(), 256, 0, st>>>(d_wk, d_sl, d_coef, d_mask, d_dcm, d_opoff, d_stab, d_sres, d_ops);
+        k_chain<<<(nc + 31u) / 32u, 32, 0, st>>>(d_sl, d_or, nc, d_ops, T.div_m, T.div_l, d_stage, d_sres);
+        launches += 6;
+    }
+    if (!aslices.empty()) {
+        for (uint32_t a : aslices) {
+            TCG_CHECK(cudaMemsetAsync(d_stage + slices[a].stage_base, 0, slices[a].stage_cap, st));
+        }
+        k_alpha<<<(uint32_t)aslices.size(), 256, 0, st>>>(d_sl, d_as, d_pl, d_pix, d_stage, d_sres, d_aerr);
+        launches += 1;
+    }
+    k_pack_sizes<<<(count + 127u) / 128u, 128, 0, st>>>(d_fr, count, d_sl, d_sres, d_fres);
+    k_pack_copy<<<dim3(ns, 8), 256, 0, st>>>(d_fr, d_sl, d_sres, d_prefix, d_stage, d_pkt, count);
+    k_pack_crc<<<ns, 256, 0, st>>>(d_fr, d_sl, d_sres, T.crc, d_pkt);
+    k_pack_header<<<(count + 127u) / 128u, 128, 0, st>>>(d_fr, count, d_fres, T.crc, d_pkt);
+    launches += 4;
+    note_launch(launches);
+    TCG_CHECK(cudaGetLastError());
+
+    // ---------------- results ----------------
+    EFrameRes* hf = (EFrameRes*)C->h[1].p;
+    uint32_t* ha = (uint32_t*)((uint8_t*)C->h[1].p + align_up(count * sizeof(EFrameRes), 16));
+    TCG_CHECK(cudaMemcpyAsync(hf, d_fres, count * sizeof(EFrameRes), cudaMemcpyDeviceToHost, st));
+    TCG_CHECK(cudaMemcpyAsync(ha, d_aerr, count * 4u, cudaMemcpyDeviceToHost, st));
+    TCG_CHECK(cudaStreamSynchronize(st));
+    for (uint32_t f = 0; f < count; ++f) {
+        tcg_enc_result& r = res[f];
+        memset(&r, 0, sizeof(r));
+        r.alpha_max_err = ha[f];
+        if (hf[f].err != 0u) {
+            r.rc = TCG_ERR_INVALID_ARGUMENT;
+            continue;
+        }
+        if (hf[f].size == 0xFFFFFFFFu) {
+            r.rc = TCG_ERR_LIMIT_EXCEEDED;
+            continue;
+        }
+        r.packet_size = hf[f].size;
+        r.color_payload = hf[f].color_payload;
+        r.alpha_payload = hf[f].alpha_payload;
+        r.color_slices = hf[f].color_slices;
+        r.alpha_slices = hf[f].alpha_slices;
+        if ((size_t)r.packet_size > caps[f]) {
+            r.rc = TCG_ERR_BUFFER_TOO_SMALL;
+            continue;
+        }
+        if (outs[f] != nullptr) {
+            TCG_CHECK(cudaMemcpyAsync(outs[f], d_pkt + ef[f].pkt_base, r.packet_size, cudaMemcpyDefault, st));
+        }
+        r.rc = 0;
+    }
+    TCG_CHECK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+}  // namespace tcg
+
+extern "C" int32_t tcg_encode(const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs, const size_t* caps,
+                              tcg_enc_result* res)
+{
+    tcg::Ctx* c = tcg::ctx_acquire();
+    if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
+    const int32_t rc = tcg::encode_impl(c, frames, count, outs, caps, res);
+    tcg::ctx_release(c);
+    return rc;
+}

@@ -1,0 +1,239 @@
+// tcg_runtime.cu - device init, context leases, frozen tables.
+#include <stdio.h>
+#include <string.h>
+
+#include <mutex>
+
+#include "tcg_runtime.h"
+
+namespace tcg {
+
+static std::mutex g_mu;
+static Ctx* g_free = nullptr;
+static bool g_init = false;
+static int g_device = -1;
+static DevTables g_tab;
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int32_t cuda_fail(cudaError_t e, const char* what)
+{
+    char buf[200];
+    snprintf(buf, sizeof(buf), "CUDA error %s in %s", cudaGetErrorString(e), what);
+    const int32_t st = (e == cudaErrorMemoryAllocation) ? TCG_ERR_OUT_OF_MEMORY : TCG_ERR_INVALID_ARGUMENT;
+    tcg_host_set_error(st, buf);
+    return st;
+}
+
+// rANS division magic: q = umulhi(2x, m) >> l equals floor(x / f) for every
+// x < 2^31 and 1 <= f <= 4096, with l = ceil(log2 f), m = ceil(2^(31+l) / f)
+// (m < 2^32 for all such f; proof in the DESIGN notes and an exhaustive host test).
+static void build_div(uint32_t* m, uint8_t* l)
+{
+    m[0] = 0; l[0] = 0;
+    for (uint32_t f = 1; f <= 4096u; ++f) {
+        uint32_t s = 0;
+        while ((1u << s) < f) { ++s; }
+        const uint64_t num = (uint64_t)1 << (31u + s);
+        m[f] = (uint32_t)((num + f - 1u) / f);
+        l[f] = (uint8_t)s;
+    }
+}
+
+static void build_crc(uint32_t* t)
+{
+    for (uint32_t i = 0; i < 256u; ++i) {
+        uint32_t c = i;
+        for (int k = 0; k < 8; ++k) { c = (c & 1u) ? 0xEDB88320u ^ (c >> 1) : c >> 1; }
+        t[i] = c;
+    }
+    for (uint32_t i = 0; i < 256u; ++i) {
+        for (int s = 1; s < 8; ++s) { t[s * 256 + i] = (t[(s - 1) * 256 + i] >> 8) ^ t[t[(s - 1) * 256 + i] & 0xFFu]; }
+    }
+}
+
+// qp scale tables (bitstream constants; classic and refined variants)
+static const uint32_t k_scale[96] = {
+    1, 1, 1, 1, 1, 1, 1, 2, 2, 2, 3, 3, 4, 5, 6, 7,
+    8, 10, 11, 13, 16, 19, 23, 27, 32, 38, 45, 54, 64, 76, 91, 108,
+    128, 152, 181, 215, 256, 304, 362, 431, 512, 609, 724, 861, 1024, 1218, 1448, 1722,
+    2048, 2435, 2896, 3444, 4096, 4871, 5793, 6889, 8192, 9742, 11585, 13777, 16384, 19484, 23170, 27555,
+    32768, 38968, 46341, 55109, 65536, 77936, 92682, 110218,
+    131072, 155872, 185364, 220436, 262144, 311744, 370728, 440872,
+    524288, 623487, 741455, 881744, 1048576, 1246974, 1482910, 1763488,
+    2097152, 2493948, 2965821, 3526975, 4194304, 4987896, 5931642, 7053950};
+static const uint32_t k_scale_refined_hi[32] = {
+    32768, 36781, 41285, 46341, 52016, 58386, 65536, 73562,
+    82570, 92682, 104032, 116772, 131072, 147123, 165140, 185364,
+    208064, 233544, 262144, 294247, 330281, 370728, 416128, 467088,
+    524288, 588493, 660561, 741455, 832255, 934175, 1048576, 1176987};
+
+static bool init_locked(int device)
+{
+    if (g_init) { return true; }
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        tcg_host_set_error(TCG_ERR_NOT_IMPLEMENTED, "no CUDA device available: the GPU library has no CPU path");
+        return false;
+    }
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) { device = 0; }
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        tcg_host_set_error(TCG_ERR_INVALID_ARGUMENT, "cudaSetDevice failed");
+        return false;
+    }
+    g_device = device;
+    const size_t bytes = 4097 * 4 + 4097 + 7 + 4097 * 8 + 8 * 256 * 4 + 2 * 96 * 4;
+    uint8_t* h = (uint8_t*)malloc(bytes);
+    uint8_t* d = nullptr;
+    if (h == nullptr || cudaMalloc(&d, bytes) != cudaSuccess) {
+        free(h);
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "device table allocation failed");
+        return false;
+    }
+    size_t o = 0;
+    uint32_t* m = (uint32_t*)(h + o); const size_t om = o; o += 4097 * 4;
+    uint8_t* l = h + o; const size_t ol = o; o += 4097 + 7;
+    double* lg = (double*)(h + o); const size_t olg = o; o += 4097 * 8;
+    uint32_t* crc = (uint32_t*)(h + o); const size_t oc = o; o += 8 * 256 * 4;
+    uint32_t* qs = (uint32_t*)(h + o); const size_t oq = o; o += 2 * 96 * 4;
+    build_div(m, l);
+    memcpy(lg, tc_log2_table(), 4097 * sizeof(double));
+    build_crc(crc);
+    for (int q = 0; q < 96; ++q) {
+        qs[q] = k_scale[q];
+        qs[96 + q] = q >= 64 ? k_scale_refined_hi[q - 64] : k_scale[q];
+    }
+    e = cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice);
+    free(h);
+    if (e != cudaSuccess) {
+        cuda_fail(e, "table upload");
+        return false;
+    }
+    g_tab.div_m = (const uint32_t*)(d + om);
+    g_tab.div_l = d + ol;
+    g_tab.log2 = (const double*)(d + olg);
+    g_tab.crc = (const uint32_t*)(d + oc);
+    g_tab.qscale = (const uint32_t*)(d + oq);
+    g_init = true;
+    return true;
+}
+
+bool ensure_init()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!init_locked(-1)) { return false; }
+    // Device selection is per host thread in the CUDA runtime.
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != g_device) { cudaSetDevice(g_device); }
+    return true;
+}
+
+const DevTables& tables() { return g_tab; }
+
+Ctx* ctx_acquire()
+{
+    if (!ensure_init()) { return nullptr; }
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        if (g_free != nullptr) {
+            Ctx* c = g_free;
+            g_free = c->next;
+            c->next = nullptr;
+            return c;
+        }
+    }
+    Ctx* c = new Ctx();
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) != cudaSuccess) {
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "stream creation failed");
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+void ctx_release(Ctx* c)
+{
+    if (c == nullptr) { return; }
+    std::lock_guard<std::mutex> lk(g_mu);
+    c->next = g_free;
+    g_free = c;
+}
+
+bool dreserve(Ctx* c, BufId id, size_t bytes)
+{
+    DBuf& b = c->d[id];
+    if (bytes <= b.cap) { return true; }
+    if (b.p != nullptr) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    size_t want = bytes + bytes / 8 + 4096;
+    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        char msg[128];
+        snprintf(msg, sizeof(msg), "device allocation of %zu bytes failed", want);
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, msg);
+        return false;
+    }
+    b.cap = want;
+    return true;
+}
+
+bool hreserve(Ctx* c, int id, size_t bytes)
+{
+    HBuf& b = c->h[id];
+    if (bytes <= b.cap) { return true; }
+    if (b.p != nullptr) {
+        cudaStreamSynchronize(c->stream);
+        cudaFreeHost(b.p);
+        b.p = nullptr;
+        b.cap = 0;
+    }
+    size_t want = bytes + bytes / 8 + 4096;
+    if (cudaMallocHost(&b.p, want) != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "pinned host allocation failed");
+        return false;
+    }
+    b.cap = want;
+    return true;
+}
+
+}  // namespace tcg
+
+extern "C" int32_t tcg_init(int32_t device)
+{
+    std::lock_guard<std::mutex> lk(tcg::g_mu);
+    return tcg::init_locked(device) ? 0 : TCG_ERR_INVALID_ARGUMENT;
+}
+
+extern "C" void tcg_shutdown(void)
+{
+    std::lock_guard<std::mutex> lk(tcg::g_mu);
+    tcg::Ctx* c = tcg::g_free;
+    while (c != nullptr) {
+        tcg::Ctx* n = c->next;
+        cudaStreamSynchronize(c->stream);
+        for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
+        for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
+        cudaEventDestroy(c->ev);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        c = n;
+    }
+    tcg::g_free = nullptr;
+}
+
+extern "C" uint64_t tcg_launch_count(void)
+{
+    return tcg::g_launches.load(std::memory_order_relaxed);
+}

@@ -1,0 +1,88 @@
+// tcg_runtime.h - CUDA-side runtime shared by the encode and decode drivers:
+// device selection, context leases (one stream + grow-only device/pinned
+// buffers per concurrent caller), frozen device tables, error plumbing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <atomic>
+
+#include "../tcg_device.h"
+
+#define TCG_OK 0
+#define TCG_ERR_INVALID_ARGUMENT (-1)
+#define TCG_ERR_OUT_OF_MEMORY (-2)
+#define TCG_ERR_LIMIT_EXCEEDED (-8)
+#define TCG_ERR_MALFORMED (-9)
+#define TCG_ERR_TRUNCATED (-10)
+#define TCG_ERR_CHECKSUM_MISMATCH (-11)
+#define TCG_ERR_BUFFER_TOO_SMALL (-15)
+#define TCG_ERR_NOT_IMPLEMENTED (-16)
+
+namespace tcg {
+
+// Grow-only device buffer.
+struct DBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+// Grow-only pinned host buffer.
+struct HBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+
+enum BufId {
+    B_PIX, B_COEF, B_MASK, B_DCM, B_NOPS, B_OPOFF, B_HIST, B_STAB, B_OPS, B_STAGE,
+    B_SRES, B_PKT, B_DESC, B_FRES, B_ALPHA, B_DEC_COEF, B_DEC_TAB, B_DEC_OUT, B_DEC_PKT,
+    B_DEC_RES, B_TMP0, B_TMP1, B_COUNT
+};
+
+struct Ctx {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    DBuf d[B_COUNT];
+    HBuf h[4];
+    Ctx* next = nullptr;
+};
+
+// Lease a context (creates one when none is free). Thread-safe.
+Ctx* ctx_acquire();
+void ctx_release(Ctx* c);
+
+// Ensure device buffer capacity; returns false (and sets the error) on failure.
+bool dreserve(Ctx* c, BufId id, size_t bytes);
+bool hreserve(Ctx* c, int id, size_t bytes);
+
+template <typename T>
+T* dptr(Ctx* c, BufId id) { return static_cast<T*>(c->d[id].p); }
+
+// Device-global frozen tables (defined in tcg_runtime.cu, uploaded by init).
+struct DevTables {
+    const uint32_t* div_m;   // [4097] rANS division magic (index = freq)
+    const uint8_t* div_l;    // [4097] shift
+    const double* log2;      // [4097] exact log2 series values
+    const uint32_t* crc;     // [8][256] slicing-by-8 CRC-32 tables
+    const uint32_t* qscale;  // [2][96] classic / refined qp scale
+};
+const DevTables& tables();
+
+bool ensure_init();
+void note_launch(uint32_t n = 1);
+
+// CUDA error -> host status + thread-local detail.
+int32_t cuda_fail(cudaError_t e, const char* what);
+
+// Host-side helpers for CRC combination (GF(2) polynomial arithmetic).
+uint32_t crc_shift_op(uint64_t len_bytes);
+
+}  // namespace tcg
+
+#define TCG_CHECK(call)                                           \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) { return tcg::cuda_fail(e_, #call); } \
+    } while (0)

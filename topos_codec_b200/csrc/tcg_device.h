@@ -1,0 +1,108 @@
+/* tcg_device.h - internal C ABI between the C11 host library and the CUDA layer.
+ *
+ * The host library validates configurations, parses packet structure and
+ * plans slices; it hands the CUDA layer fully resolved job descriptors made of
+ * plain integers and pointers. The CUDA layer owns device memory, streams and
+ * kernels, and returns per-frame results. Nothing here is public API.
+ */
+#ifndef TCG_DEVICE_H
+#define TCG_DEVICE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* --------------------------------- encode --------------------------------- */
+
+enum { TCG_PLANE_COLOR = 0, TCG_PLANE_ALPHA = 1 };
+
+typedef struct tcg_enc_plane {
+    const uint16_t* src;    /* caller samples (host or device memory), visible area */
+    size_t stride;          /* uint16 elements between rows */
+    uint32_t vis_w, vis_h;  /* visible plane size */
+    uint32_t coded_w, coded_h;
+    uint32_t cols, rows;    /* 8x8 blocks */
+    uint32_t kind;          /* TCG_PLANE_COLOR / TCG_PLANE_ALPHA */
+    uint32_t alpha_shift;   /* near-lossless alpha: 16 - alpha_bit_depth, else 0 */
+    uint32_t qdb;           /* slice-header qp_delta_biased for this plane */
+    uint32_t Q[64];         /* colour: quantiser steps, natural order */
+    int64_t fclamp;         /* colour: coefficient clamp */
+} tcg_enc_plane;
+
+typedef struct tcg_enc_frame {
+    uint32_t planes;
+    uint32_t bit_depth;
+    uint32_t slice_rows;
+    uint32_t slices;        /* total slices (all planes) */
+    tcg_enc_plane plane[4];
+    uint8_t header[53];     /* frame header; packet size and header CRC are patched on the device */
+} tcg_enc_frame;
+
+typedef struct tcg_enc_result {
+    int32_t rc;             /* TC_OK or the frame's error status */
+    uint32_t packet_size;
+    uint32_t color_payload, alpha_payload;
+    uint32_t color_slices, alpha_slices;
+    uint32_t alpha_max_err;
+} tcg_enc_result;
+
+/* Encodes count frames in one device launch sequence. For each frame whose
+ * packet fits caps[i], the packet is copied to outs[i] (host or device memory).
+ * Returns TC_OK when the device work ran (per-frame status in res[i].rc), or a
+ * call-level error (out of device memory, CUDA failure). */
+int32_t tcg_encode(const tcg_enc_frame* frames, uint32_t count,
+                   uint8_t* const* outs, const size_t* caps, tcg_enc_result* res);
+
+/* --------------------------------- decode --------------------------------- */
+
+typedef struct tcg_dec_slice {
+    uint32_t off;           /* payload offset within the packet */
+    uint32_t size;          /* payload bytes */
+    uint32_t crc;           /* slice-header CRC-32 of the payload */
+    uint16_t plane, y0, bh;
+    uint16_t qp;            /* effective qp of the slice */
+    uint16_t k1, k2;        /* alpha Rice parameters */
+} tcg_dec_slice;
+
+typedef struct tcg_dec_frame {
+    const uint8_t* packet;  /* host or device memory */
+    size_t size;
+    uint32_t planes, bit_depth, alpha_mode, alpha_shift;
+    uint32_t vis_w[4], vis_h[4], coded_w[4], cols[4], rows[4];
+    uint16_t qm[4][64];     /* per-plane quantisation matrix (natural order) */
+    uint32_t refined;       /* refined qp scale table (header flags bit 3) */
+    uint32_t deblock;       /* header flags bit 2 */
+    uint32_t qp_base;
+    uint32_t slices;
+    const tcg_dec_slice* slice;
+    uint16_t* dst[4];       /* caller planes (host or device memory) */
+    size_t dst_stride[4];   /* uint16 elements */
+    uint8_t* slice_status;  /* out: TC_FRAME_SLICE_* per slice (host memory) */
+    int32_t skip;           /* in: nonzero = frame already rejected by the host */
+} tcg_dec_frame;
+
+/* Decodes count frames in one device launch sequence; per-slice status is
+ * written to each frame's slice_status. Returns TC_OK when the device work ran,
+ * or a call-level error. */
+int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count);
+
+/* ---------------------------------- device --------------------------------- */
+
+int32_t tcg_init(int32_t device);
+void tcg_shutdown(void);
+/* number of kernel launches issued by this process (all streams) */
+uint64_t tcg_launch_count(void);
+
+/* provided by the host library: thread-local error detail */
+void tcg_host_set_error(int32_t status, const char* text);
+/* provided by the host library: exact log2 table (4097 doubles, index = freq) */
+const double* tc_log2_table(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCG_DEVICE_H */
