@@ -86,20 +86,22 @@ static bool init_locked(int device)
         return false;
     }
     g_device = device;
-    const size_t bytes = 4097 * 4 + 4097 + 7 + 4097 * 8 + 8 * 256 * 4 + 2 * 96 * 4;
-    uint8_t* h = (uint8_t*)malloc(bytes);
+    // every section starts on a 16-byte boundary (the log2 table holds doubles)
+    auto a16 = [](size_t v) { return (v + 15u) & ~(size_t)15u; };
+    const size_t om = 0, ol = a16(om + 4097 * 4), olg = a16(ol + 4097), oc = a16(olg + 4097 * 8),
+                 oq = a16(oc + 8 * 256 * 4), bytes = a16(oq + 2 * 96 * 4);
+    uint8_t* h = (uint8_t*)calloc(1, bytes);
     uint8_t* d = nullptr;
     if (h == nullptr || cudaMalloc(&d, bytes) != cudaSuccess) {
         free(h);
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "device table allocation failed");
         return false;
     }
-    size_t o = 0;
-    uint32_t* m = (uint32_t*)(h + o); const size_t om = o; o += 4097 * 4;
-    uint8_t* l = h + o; const size_t ol = o; o += 4097 + 7;
-    double* lg = (double*)(h + o); const size_t olg = o; o += 4097 * 8;
-    uint32_t* crc = (uint32_t*)(h + o); const size_t oc = o; o += 8 * 256 * 4;
-    uint32_t* qs = (uint32_t*)(h + o); const size_t oq = o; o += 2 * 96 * 4;
+    uint32_t* m = (uint32_t*)(h + om);
+    uint8_t* l = h + ol;
+    double* lg = (double*)(h + olg);
+    uint32_t* crc = (uint32_t*)(h + oc);
+    uint32_t* qs = (uint32_t*)(h + oq);
     build_div(m, l);
     memcpy(lg, tc_log2_table(), 4097 * sizeof(double));
     build_crc(crc);
