@@ -1,0 +1,419 @@
+"""Benchmark: 4K 10-bit 4:2:2 HQ intra encode + decode of a 60-frame batch.
+
+Workload: 3840x2160 10-bit YUV 4:2:2 limited range, fixed QP 4, HQ tier mapping
+(flat quantisation matrix, DEBLOCK + refined qp table), default slice layout
+(16 block rows), 60 synthetic frames (seeded sinusoids + rectangles + Gaussian
+noise, per-frame phase drift). One step = batched GPU encode of the 60 frames
+followed by batched GPU decode of the 60 packets (the round trip). The metric
+is round-trip frames/s; encode and decode rates are reported beside it, with
+the plain per-frame GPU path on the same frames for comparison.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun every rank codes its own 60-frame batch (weak scaling, no
+collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, FRAMES = 3840, 2160, 60
+CFG = dict(qp=4, qmatrix_id=0, features=3, profile=3)
+METRIC = "4K 422 HQ enc/dec frames/s (batched vs plain GPU, bit-exact); served p50/p99 ms"
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libtopos_codec_ref.so")
+ORACLE_LIB = os.path.join(ROOT, "oracle", "liboracle_tc.so")
+
+
+def plane_bytes(w=W, h=H):
+    return w * h * 2 + 2 * ((w + 1) // 2) * h * 2
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference CPU path
+
+def reference_rate(frames_np, cfg, budget_s=10.0, threads=None):
+    """Round-trip frames/s of the reference CPU library (built from its own
+    sources into oracle/_ref) on the host cores: frame-parallel, one frame per
+    worker thread, the reference's slice pool at one thread per call."""
+    os.environ["TOPOS_SLICE_THREADS"] = "1"
+    from topos_codec_b200 import binding as B
+    ref = B.ToposCodec(REF_LIB)
+    cores = threads or (os.cpu_count() or 1)
+    n = len(frames_np)
+    done, lock = [0], threading.Lock()
+    t_end = [0.0]
+
+    def work(i0):
+        k = i0
+        while True:
+            with lock:
+                if time.perf_counter() > t_end[0] and done[0] >= cores:
+                    return
+                done[0] += 1
+            f = frames_np[k % n]
+            pkt = ref.encode(cfg, f)
+            ref.decode(pkt)
+            k += cores
+
+    t0 = time.perf_counter()
+    t_end[0] = t0 + budget_s
+    th = [threading.Thread(target=work, args=(i,)) for i in range(cores)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    el = time.perf_counter() - t0
+    return done[0] / el, cores, done[0], el
+
+
+# ------------------------------------------------------------------ GPU path
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=FRAMES)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    from topos_codec_b200 import binding as B, synth
+
+    cfg = B.make_config(W, H, **CFG)
+    config_desc = {"workload": f"3840x2160 10-bit 4:2:2 HQ qp4 x{args.frames} frames (round trip)",
+                   "frames_per_rank": args.frames, "width": W, "height": H, "qp": 4, "qmatrix_id": 0,
+                   "features": "DEBLOCK|QPT2", "slice_rows": 16, "l2": "inputs larger than L2 (>=2 GB per step)",
+                   "parallelism": f"frame-sharded x{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        if not os.path.exists(REF_LIB):
+            print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/_ref)"}))
+            return
+        frames = [synth.make_frame_np(W, H, seed=0, frame=i) for i in range(4)]
+        for _ in range(args.warmup):
+            reference_rate(frames[:1], cfg, budget_s=0.0, threads=1)
+        rates = []
+        for _ in range(args.steps):
+            r, cores, n, el = reference_rate(frames, cfg, budget_s=10.0)
+            rates.append(r)
+        value = statistics.median(rates)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.frames / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/int32",
+            "data": "synthetic", "config": config_desc,
+            "cpu_baseline": {"value": value, "unit": "frames/s", "cores": cores, "kind": "reference",
+                             "sample": f"each step: frame-parallel encode+decode on {cores} threads for ~10 s"},
+            "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+
+    gpu = B.ToposCodec(B.PRODUCT_LIBRARY)
+    L = gpu._lib
+    L.tcg_last_device_ms.restype = ctypes.c_double
+    L.tcg_kernel_launches.restype = ctypes.c_uint64
+    L.tcg_profile_read.restype = ctypes.c_int32
+    L.tcg_profile_read.argtypes = [ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_uint64)]
+    L.tcg_device_init(local)
+
+    nf = args.frames
+    dev = torch.device("cuda", local)
+    # inputs resident in HBM: uint16 planes
+    frames_d = []
+    for i in range(nf):
+        ps = synth.make_frame(W, H, seed=rank, frame=i, device=dev)
+        frames_d.append([p.to(torch.uint16) for p in ps])
+    torch.cuda.synchronize()
+    in_bytes = plane_bytes() * nf
+    cap = plane_bytes() * 2 + (1 << 20)
+    out_d = [torch.empty(cap, dtype=torch.uint8, device=dev) for _ in range(nf)]
+    dec_d = [[torch.empty((H, w), dtype=torch.uint16, device=dev) for w in (W, W // 2, W // 2)] for _ in range(nf)]
+
+    cfgs = (B.FrameConfig * nf)(*[cfg] * nf)
+
+    def inputs_for(planes_list):
+        arr = (B.FrameInput * nf)()
+        for i, planes in enumerate(planes_list):
+            arr[i].struct_size = ctypes.sizeof(B.FrameInput)
+            arr[i].abi_version = 2
+            for p, t in enumerate(planes):
+                arr[i].planes[p] = t.data_ptr()
+                arr[i].strides[p] = t.shape[1]
+        return arr
+
+    in_d = inputs_for(frames_d)
+    outs_d = (ctypes.c_void_p * nf)(*[t.data_ptr() for t in out_d])
+    caps = (ctypes.c_size_t * nf)(*[cap] * nf)
+    stats = (B.FrameStats * nf)()
+    rcs = (ctypes.c_int32 * nf)()
+    dec_ptrs = (ctypes.c_void_p * (4 * nf))()
+    for i in range(nf):
+        for p in range(3):
+            dec_ptrs[4 * i + p] = dec_d[i][p].data_ptr()
+    infos = (B.FrameOutput * nf)()
+
+    def encode_batch(inputs, outs):
+        rc = L.tcg_frame_encode_batch(cfgs, inputs, nf, outs, caps, stats, rcs)
+        if rc != 0:
+            raise RuntimeError(f"encode batch failed [{rc}]: {gpu.last_error()}")
+        return L.tcg_last_device_ms()
+
+    def decode_batch(pkts, ptrs):
+        arr = (B.BatchPacket * nf)()
+        for i in range(nf):
+            arr[i].data = pkts[i]
+            arr[i].size = stats[i].packet_size
+        rc = L.tc_frame_decode_batch(arr, nf, ptrs, None, infos)
+        if rc != 0:
+            raise RuntimeError(f"decode batch failed [{rc}]: {gpu.last_error()}")
+        return L.tcg_last_device_ms()
+
+    pkt_ptrs_d = [t.data_ptr() for t in out_d]
+
+    def step():
+        te = encode_batch(in_d, outs_d)
+        td = decode_batch(pkt_ptrs_d, dec_ptrs)
+        return te, td
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    pkt_bytes = sum(stats[i].packet_size for i in range(nf))
+
+    # ---------------- timed region: device-resident batched round trip ----------------
+    L.tcg_profile_reset()
+    L.tcg_profile_enable(1)
+    launches0 = L.tcg_kernel_launches()
+    enc_ms, dec_ms = [], []
+    with ClockSampler(local) as clk:
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            te, td = step()
+            enc_ms.append(te)
+            dec_ms.append(td)
+        barrier()
+        wall = time.perf_counter() - t0
+    L.tcg_profile_enable(0)
+    launches = L.tcg_kernel_launches() - launches0
+    step_ms = (sum(enc_ms) + sum(dec_ms)) / args.steps
+    if world > 1:
+        t = torch.tensor([step_ms, sum(enc_ms) / args.steps, sum(dec_ms) / args.steps], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms, enc_avg, dec_avg = t.tolist()
+    else:
+        enc_avg, dec_avg = sum(enc_ms) / args.steps, sum(dec_ms) / args.steps
+    value = nf * world / (step_ms / 1000.0)
+
+    # per-kernel timings over the timed region
+    kern = {}
+    for k in range(64):
+        name, ms, n = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_uint64()
+        if L.tcg_profile_read(k, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(n)) != 0:
+            break
+        if n.value:
+            kern[name.value.decode()] = {"ms": ms.value, "launches": n.value}
+
+    # ---------------- bit-exactness: batched vs plain per-frame vs oracle ----------------
+    batched_pkts = [out_d[i][: stats[i].packet_size].cpu().numpy().tobytes() for i in range(nf)]
+    plain_enc_ms, plain_dec_ms, exact = 0.0, 0.0, True
+    one_out = torch.empty(cap, dtype=torch.uint8, device=dev)
+    st1 = B.FrameStats()
+    for i in range(nf):
+        rc = L.tc_frame_encode(ctypes.byref(cfg), ctypes.byref(in_d[i]), ctypes.c_void_p(one_out.data_ptr()), cap,
+                               ctypes.byref(st1))
+        plain_enc_ms += L.tcg_last_device_ms()
+        if rc != 0 or one_out[: st1.packet_size].cpu().numpy().tobytes() != batched_pkts[i]:
+            exact = False
+        info = B.FrameOutput()
+        plain_out = [torch.empty_like(dec_d[i][p]) for p in range(3)]
+        ptrs1 = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in plain_out], None)
+        rc = L.tc_frame_decode(ctypes.c_void_p(out_d[i].data_ptr()), stats[i].packet_size, ptrs1, None, ctypes.byref(info))
+        plain_dec_ms += L.tcg_last_device_ms()
+        if rc != 0 or not all(torch.equal(a.view(torch.int16), b.view(torch.int16)) for a, b in zip(plain_out, dec_d[i])):
+            exact = False
+    oracle_ok = None
+    if rank == 0 and os.path.exists(ORACLE_LIB):
+        orc = B.ToposCodec(ORACLE_LIB)
+        f0 = [p.cpu().numpy() for p in frames_d[0]]
+        oracle_ok = orc.encode(cfg, f0) == batched_pkts[0]
+        d0 = orc.decode(batched_pkts[0])
+        oracle_ok = oracle_ok and all(np.array_equal(a, b.cpu().numpy()) for a, b in zip(d0.planes, dec_d[0]))
+        exact = exact and oracle_ok
+
+    # ---------------- e2e: host (pinned) buffers through the public API ----------------
+    frames_h = [[p.cpu().pin_memory() for p in fr] for fr in frames_d]
+    in_h = inputs_for(frames_h)
+    out_h = [torch.empty(cap, dtype=torch.uint8).pin_memory() for _ in range(nf)]
+    outs_h = (ctypes.c_void_p * nf)(*[t.data_ptr() for t in out_h])
+    dec_h = [[torch.empty((H, w), dtype=torch.uint16).pin_memory() for w in (W, W // 2, W // 2)] for _ in range(nf)]
+    dec_ptrs_h = (ctypes.c_void_p * (4 * nf))()
+    for i in range(nf):
+        for p in range(3):
+            dec_ptrs_h[4 * i + p] = dec_h[i][p].data_ptr()
+    pkt_ptrs_h = [t.data_ptr() for t in out_h]
+    encode_batch(in_h, outs_h)
+    decode_batch(pkt_ptrs_h, dec_ptrs_h)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        encode_batch(in_h, outs_h)
+        decode_batch(pkt_ptrs_h, dec_ptrs_h)
+    barrier()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e_exact = all(out_h[i][: stats[i].packet_size].numpy().tobytes() == batched_pkts[i] for i in range(nf))
+    exact = exact and e2e_exact
+
+    # ---------------- roofline of the dominant kernel ----------------
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak, peak_src = json.load(open(peaks_path))["hbm_gbs"], "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    top = max(kern.items(), key=lambda kv: kv[1]["ms"]) if kern else (None, None)
+    roof = None
+    if top[0] is not None:
+        per_launch_ms = top[1]["ms"] / top[1]["launches"]
+        # algorithmic bytes per launch: one launch codes the whole batch
+        dec_side = top[0].startswith("k_d") or top[0].startswith("k_deblock")
+        out_side = plane_bytes() * nf if dec_side else pkt_bytes
+        algo = (pkt_bytes + plane_bytes() * nf) if dec_side else (in_bytes + pkt_bytes)
+        achieved = algo / (per_launch_ms / 1000.0) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.txt")
+        if os.path.exists(tp):
+            for line in open(tp):
+                if line.startswith(top[0] + " "):
+                    try:
+                        traffic = float(line.split()[1]) * nf
+                    except ValueError:
+                        pass
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                "algorithmic_bytes_per_launch": algo, "launch_ms": per_launch_ms,
+                "note": "serial rANS state chains bound this kernel by dependent-op latency, not HBM"}
+        _ = out_side
+
+    # ---------------- CPU baseline (rank 0, N=1 only) ----------------
+    cpu = None
+    if rank == 0 and world == 1 and os.path.exists(REF_LIB):
+        f_np = [[p.cpu().numpy() for p in frames_d[i]] for i in range(min(nf, 8))]
+        r, cores, n, el = reference_rate(f_np, cfg, budget_s=12.0)
+        cpu = {"value": r, "unit": "frames/s", "cores": cores, "kind": "reference",
+               "sample": f"{n} frames encoded+decoded frame-parallel in {el:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16/int32", "data": "synthetic", "config": config_desc,
+            "encode_fps": nf * world / (enc_avg / 1000.0), "decode_fps": nf * world / (dec_avg / 1000.0),
+            "plain_encode_fps": nf / (plain_enc_ms / 1000.0), "plain_decode_fps": nf / (plain_dec_ms / 1000.0),
+            "batched_vs_plain": (plain_enc_ms + plain_dec_ms) / step_ms,
+            "bit_exact": exact, "oracle_frame0_exact": oracle_ok,
+            "pixel_gbs": (in_bytes * 2) * world / (step_ms / 1000.0) / 1e9,
+            "wall_s_timed": wall,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+            "kernels_ms": {k: round(v["ms"] / args.steps, 3) for k, v in kern.items()},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": nf * world / e2e_s, "unit": "frames/s",
+                    "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes)},
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -271,6 +271,19 @@ void tcg_device_release(void);
  * (diagnostics for benchmarks). */
 uint64_t tcg_kernel_launches(void);
 
+/* Device time in milliseconds of the calling thread's last frame call,
+ * measured with CUDA events on the stream the call's kernels ran on (from the
+ * first upload to the last download). */
+double tcg_last_device_ms(void);
+
+/* Optional per-kernel timing: when enabled, every kernel launch is bracketed
+ * by CUDA events and the durations are summed per kernel for the process.
+ * tcg_profile_read(id) returns TC_OK with the kernel's name, total ms and
+ * launch count, or a negative value past the last kernel id. */
+void tcg_profile_enable(int32_t on);
+void tcg_profile_reset(void);
+int32_t tcg_profile_read(uint32_t id, const char** name, double* total_ms, uint64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

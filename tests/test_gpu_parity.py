@@ -146,6 +146,42 @@ def test_batch_decode_equals_single(product):
             assert np.array_equal(x, y)
 
 
+def test_device_resident_encode_decode(product):
+    """Device pointers for samples, packets and output planes (no host staging):
+    same packet and pixels as the host-memory path, including a damaged packet
+    parsed from its device-walked headers."""
+    import ctypes
+
+    import torch
+    w, h = 640, 360
+    planes = synth.make_frame_np(w, h, seed=9)
+    cfg = B.make_config(w, h, qp=6, qmatrix_id=4, features=1)
+    host_pkt = product.encode(cfg, planes)
+    dev = [torch.from_numpy(p.astype(np.int32)).cuda().to(torch.uint16) for p in planes]
+    fi = B.FrameInput()
+    fi.struct_size, fi.abi_version = ctypes.sizeof(B.FrameInput), 2
+    for i, t in enumerate(dev):
+        fi.planes[i], fi.strides[i] = t.data_ptr(), t.shape[1]
+    out = torch.zeros(2 * len(host_pkt), dtype=torch.uint8, device="cuda")
+    st = B.FrameStats()
+    rc = product._lib.tc_frame_encode(ctypes.byref(cfg), ctypes.byref(fi), ctypes.c_void_p(out.data_ptr()),
+                                      out.numel(), ctypes.byref(st))
+    assert rc == 0 and out[: st.packet_size].cpu().numpy().tobytes() == host_pkt
+    ref = product.decode(host_pkt)
+    for pkt_bytes, want_status in ((host_pkt, 0), (host_pkt[:-1], B.TC_ERR_MALFORMED)):
+        dpkt = torch.from_numpy(np.frombuffer(pkt_bytes, dtype=np.uint8).copy()).cuda()
+        outs = [torch.zeros(p.shape, dtype=torch.uint16, device="cuda") for p in ref.planes]
+        ptrs = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in outs], None)
+        info = B.FrameOutput()
+        rc = product._lib.tc_frame_decode(ctypes.c_void_p(dpkt.data_ptr()), len(pkt_bytes), ptrs, None,
+                                          ctypes.byref(info))
+        hrc, _ = product.query(pkt_bytes)
+        assert rc == (0 if hrc == 0 else hrc)
+        if want_status == 0:
+            for a, b in zip(outs, ref.planes):
+                assert np.array_equal(a.cpu().numpy(), b)
+
+
 def test_strided_io_and_buffer_too_small(product):
     w, h = 200, 120
     planes = synth.make_frame_np(w, h, seed=5)

@@ -672,6 +672,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const uint32_t* d_bs = (const uint32_t*)(dd + o_bs);
     const DbPlane* d_db = (const DbPlane*)(dd + o_db);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
+    call_begin(C);
     for (uint32_t f = 0; f < count; ++f) {
         if (frames[f].skip) { continue; }
         TCG_CHECK(cudaMemcpyAsync(d_pkt + pkt_off[f], frames[f].packet, frames[f].size, cudaMemcpyDefault, st));
@@ -682,29 +683,26 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     uint16_t* d_out = dptr<uint16_t>(C, B_DEC_OUT);
     int32_t* d_ares = dptr<int32_t>(C, B_ALPHA);
     const DevTables& T = tables();
-    uint32_t launches = 0;
     if (ns > 0) {
         TCG_CHECK(cudaMemsetAsync(d_status, 0, (size_t)ns * 4u, st));
-        k_dcrc<<<ns, 256, 0, st>>>(d_sl, d_pkt, T.crc, d_status);
-        launches++;
+        TCG_LAUNCH(C, K_DCRC, k_dcrc, ns, 256, 0, d_sl, d_pkt, T.crc, d_status);
     }
     if (nc > 0) {
         TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-        k_dtables<<<nc, 32, 0, st>>>(d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
+        TCG_LAUNCH(C, K_DTABLES, k_dtables, nc, 32, 0, d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
         const size_t smem = MAX_CTX * CTX_BYTES + (size_t)max_cols * 8u;
         static size_t attr = 0;
         if (smem > attr) {
             cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             attr = smem;
         }
-        k_dchain<<<nc, 32, smem, st>>>(d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
-        k_didct<<<(uint32_t)((nblk + 127u) / 128u), 128, 0, st>>>(d_sl, d_bs, d_st, d_pl, d_tab, d_coef, d_status,
-                                                                 (uint32_t)nblk, d_out);
-        launches += 3;
+        TCG_LAUNCH(C, K_DCHAIN, k_dchain, nc, 32, smem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
+        TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_bs, d_st, d_pl, d_tab, d_coef,
+                   d_status, (uint32_t)nblk, d_out);
     }
     if (na > 0) {
         TCG_CHECK(cudaMemsetAsync(d_ares, 0, alpha_res * 4u, st));
-        k_dalpha<<<(na + 63u) / 64u, 64, 0, st>>>(d_sl, d_as, na, d_pl, d_pkt, d_ares, d_status);
+        TCG_LAUNCH(C, K_DALPHA, k_dalpha, (na + 63u) / 64u, 64, 0, d_sl, d_as, na, d_pl, d_pkt, d_ares, d_status);
         uint32_t max_w = 8;
         for (uint32_t a : aslices) { max_w = std::max(max_w, planes[slices[a].plane].coded_w); }
         const size_t esmem = (size_t)max_w * 4u;
@@ -713,12 +711,10 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             cudaFuncSetAttribute(k_dalpha_med, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
             eattr = esmem;
         }
-        k_dalpha_med<<<na, 128, esmem, st>>>(d_sl, d_as, d_pl, d_ares, d_status, d_out);
-        launches += 2;
+        TCG_LAUNCH(C, K_DALPHA_MED, k_dalpha_med, na, 128, esmem, d_sl, d_as, d_pl, d_ares, d_status, d_out);
     }
     if (ns > 0) {
-        k_dconceal<<<ns, 256, 0, st>>>(d_sl, d_pl, d_status, d_out);
-        launches++;
+        TCG_LAUNCH(C, K_DCONCEAL, k_dconceal, ns, 256, 0, d_sl, d_pl, d_status, d_out);
     }
     if (!dbp.empty()) {
         uint64_t mv = 0, mh = 0;
@@ -726,11 +722,11 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             mv = std::max<uint64_t>(mv, (uint64_t)(d.w / 8u - 1u) * d.h);
             mh = std::max<uint64_t>(mh, (uint64_t)(d.h / 8u - 1u) * d.w);
         }
-        k_deblock_v<<<dim3((uint32_t)((mv + 255u) / 256u), (uint32_t)dbp.size()), 256, 0, st>>>(d_db, (uint32_t)dbp.size(), d_out);
-        k_deblock_h<<<dim3((uint32_t)((mh + 255u) / 256u), (uint32_t)dbp.size()), 256, 0, st>>>(d_db, (uint32_t)dbp.size(), d_out);
-        launches += 2;
+        TCG_LAUNCH(C, K_DEBLOCK_V, k_deblock_v, dim3((uint32_t)((mv + 255u) / 256u), (uint32_t)dbp.size()), 256, 0,
+                   d_db, (uint32_t)dbp.size(), d_out);
+        TCG_LAUNCH(C, K_DEBLOCK_H, k_deblock_h, dim3((uint32_t)((mh + 255u) / 256u), (uint32_t)dbp.size()), 256, 0,
+                   d_db, (uint32_t)dbp.size(), d_out);
     }
-    note_launch(launches);
     TCG_CHECK(cudaGetLastError());
     // outputs to the caller's planes
     uint32_t pg = 0;
@@ -747,11 +743,73 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     int32_t* hs = (int32_t*)C->h[1].p;
     if (ns > 0) { TCG_CHECK(cudaMemcpyAsync(hs, d_status, (size_t)ns * 4u, cudaMemcpyDeviceToHost, st)); }
     TCG_CHECK(cudaStreamSynchronize(st));
+    call_end(C);
     for (uint32_t f = 0; f < count; ++f) {
         const tcg_dec_frame& F = frames[f];
         if (F.skip) { continue; }
         for (uint32_t i = 0; i < F.slices; ++i) { F.slice_status[i] = hs[frame_slice0[f] + i] != 0 ? 1u : 0u; }
     }
+    return 0;
+}
+
+// ------------------------------------------------------------------ packet walk
+
+// One thread per packet: copy the first 61 packet bytes (frame header plus the
+// bytes a generation probe inspects) and every slice header reachable inside
+// the packet (at most 512), stopping exactly where a host structural parse
+// would stop for lack of bytes. Record layout (TCG_WALK_REC in tcg_device.h):
+// [64: packet bytes 0..60, zero beyond the packet][u32 walked][u32 end offset]
+// [8 pad][512 x 17 slice headers].
+constexpr size_t WALK_REC = TCG_WALK_REC;
+
+__global__ void k_walk(const uint8_t* const* __restrict__ pkts, const uint64_t* __restrict__ sizes, uint32_t n,
+                       uint8_t* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) { return; }
+    const uint8_t* p = pkts[i];
+    const uint64_t sz = sizes[i];
+    uint8_t* r = out + (size_t)i * WALK_REC;
+    for (uint32_t k = 0; k < 64u; ++k) { r[k] = (k < 61u && k < sz) ? p[k] : 0u; }
+    uint32_t walked = 0;
+    uint64_t off = 53u;
+    if (sz >= 53u) {
+        uint32_t ns = ((uint32_t)p[30] << 8) | p[31];
+        ns = ns > 512u ? 512u : ns;
+        for (uint32_t s = 0; s < ns; ++s) {
+            if (off > sz || sz - off < 17u) { break; }
+            const uint8_t* h = p + off;
+            for (uint32_t k = 0; k < 17u; ++k) { r[80u + s * 17u + k] = h[k]; }
+            walked = s + 1u;
+            off += 17u;
+            const uint32_t pay = ((uint32_t)h[0] << 24) | ((uint32_t)h[1] << 16) | ((uint32_t)h[2] << 8) | h[3];
+            if (sz - off < pay) { break; }
+            off += pay;
+        }
+    }
+    *reinterpret_cast<uint32_t*>(r + 64) = walked;
+    *reinterpret_cast<uint32_t*>(r + 68) = (uint32_t)off;
+}
+
+static int32_t walk_impl(Ctx* C, const uint8_t* const* pkts, const size_t* sizes, uint32_t n, uint8_t* host_out)
+{
+    const size_t ptr_bytes = align_up((size_t)n * 8u, 256);
+    if (!dreserve(C, B_TMP1, ptr_bytes * 2u + (size_t)n * WALK_REC + 256) || !hreserve(C, 2, ptr_bytes * 2u) ||
+        !hreserve(C, 3, (size_t)n * WALK_REC)) {
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    uint8_t* hb = (uint8_t*)C->h[2].p;
+    memcpy(hb, pkts, (size_t)n * 8u);
+    for (uint32_t i = 0; i < n; ++i) { reinterpret_cast<uint64_t*>(hb + ptr_bytes)[i] = sizes[i]; }
+    uint8_t* db = dptr<uint8_t>(C, B_TMP1);
+    call_begin(C);
+    TCG_CHECK(cudaMemcpyAsync(db, hb, ptr_bytes * 2u, cudaMemcpyHostToDevice, C->stream));
+    TCG_LAUNCH(C, K_WALK, k_walk, (n + 63u) / 64u, 64, 0, (const uint8_t* const*)db, (const uint64_t*)(db + ptr_bytes),
+               n, db + 2u * ptr_bytes);
+    TCG_CHECK(cudaMemcpyAsync(C->h[3].p, db + 2u * ptr_bytes, (size_t)n * WALK_REC, cudaMemcpyDeviceToHost, C->stream));
+    TCG_CHECK(cudaStreamSynchronize(C->stream));
+    call_end(C);
+    memcpy(host_out, C->h[3].p, (size_t)n * WALK_REC);
     return 0;
 }
 
@@ -762,6 +820,15 @@ extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
     tcg::Ctx* c = tcg::ctx_acquire();
     if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
     const int32_t rc = tcg::decode_impl(c, frames, count);
+    tcg::ctx_release(c);
+    return rc;
+}
+
+extern "C" int32_t tcg_walk_packets(const uint8_t* const* pkts, const size_t* sizes, uint32_t n, uint8_t* host_out)
+{
+    tcg::Ctx* c = tcg::ctx_acquire();
+    if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
+    const int32_t rc = tcg::walk_impl(c, pkts, sizes, n, host_out);
     tcg::ctx_release(c);
     return rc;
 }

@@ -905,6 +905,7 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
     const size_t o_cs = put(cslices.data(), cslices.size() * 4u);
     const size_t o_as = put(aslices.data(), aslices.size() * 4u);
     const size_t o_or = put(order.data(), order.size() * 4u);
+    call_begin(C);
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
     const EPlane* d_pl = (const EPlane*)(dd + o_pl);
     const ESlice* d_sl = (const ESlice*)(dd + o_sl);
@@ -946,36 +947,33 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
     uint8_t* d_stage = dptr<uint8_t>(C, B_STAGE);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
 
-    uint32_t launches = 0;
     if (nblk > 0) {
-        k_fdct<<<(uint32_t)((nblk + 127u) / 128u), 128, 0, st>>>(d_pl, d_cp, (uint32_t)cplanes.size(), (uint32_t)nblk,
-                                                                d_pix, d_coef, d_mask);
+        TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)cplanes.size(),
+                   (uint32_t)nblk, d_pix, d_coef, d_mask);
         const size_t tok_smem = H_BINS * 32u * 4u;
         static bool attr_set = false;
         if (!attr_set) {
             cudaFuncSetAttribute(k_tokens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tok_smem);
             attr_set = true;
         }
-        k_tokens<<<(uint32_t)work.size(), 256, tok_smem, st>>>(d_wk, d_sl, d_coef, d_mask, d_dcm, d_nops, d_hist, d_sres);
-        k_select<<<nc, 32, 0, st>>>(d_sl, d_cs, d_hist, T.log2, d_stab, d_prefix, d_sres);
-        k_opscan<<<nc, 1024, 0, st>>>(d_sl, d_cs, d_nops, d_opoff, d_sres);
-        k_opgen<<<(uint32_t)work.size(), 256, 0, st>>>(d_wk, d_sl, d_coef, d_mask, d_dcm, d_opoff, d_stab, d_sres, d_ops);
-        k_chain<<<(nc + 31u) / 32u, 32, 0, st>>>(d_sl, d_or, nc, d_ops, T.div_m, T.div_l, d_stage, d_sres);
-        launches += 6;
+        TCG_LAUNCH(C, K_TOKENS, k_tokens, (uint32_t)work.size(), 256, tok_smem, d_wk, d_sl, d_coef, d_mask, d_dcm, d_nops,
+                   d_hist, d_sres);
+        TCG_LAUNCH(C, K_SELECT, k_select, nc, 32, 0, d_sl, d_cs, d_hist, T.log2, d_stab, d_prefix, d_sres);
+        TCG_LAUNCH(C, K_OPSCAN, k_opscan, nc, 1024, 0, d_sl, d_cs, d_nops, d_opoff, d_sres);
+        TCG_LAUNCH(C, K_OPGEN, k_opgen, (uint32_t)work.size(), 256, 0, d_wk, d_sl, d_coef, d_mask, d_dcm, d_opoff, d_stab,
+                   d_sres, d_ops);
+        TCG_LAUNCH(C, K_CHAIN, k_chain, (nc + 31u) / 32u, 32, 0, d_sl, d_or, nc, d_ops, T.div_m, T.div_l, d_stage, d_sres);
     }
     if (!aslices.empty()) {
         for (uint32_t a : aslices) {
             TCG_CHECK(cudaMemsetAsync(d_stage + slices[a].stage_base, 0, slices[a].stage_cap, st));
         }
-        k_alpha<<<(uint32_t)aslices.size(), 256, 0, st>>>(d_sl, d_as, d_pl, d_pix, d_stage, d_sres, d_aerr);
-        launches += 1;
+        TCG_LAUNCH(C, K_ALPHA, k_alpha, (uint32_t)aslices.size(), 256, 0, d_sl, d_as, d_pl, d_pix, d_stage, d_sres, d_aerr);
     }
-    k_pack_sizes<<<(count + 127u) / 128u, 128, 0, st>>>(d_fr, count, d_sl, d_sres, d_fres);
-    k_pack_copy<<<dim3(ns, 8), 256, 0, st>>>(d_fr, d_sl, d_sres, d_prefix, d_stage, d_pkt, count);
-    k_pack_crc<<<ns, 256, 0, st>>>(d_fr, d_sl, d_sres, T.crc, d_pkt);
-    k_pack_header<<<(count + 127u) / 128u, 128, 0, st>>>(d_fr, count, d_fres, T.crc, d_pkt);
-    launches += 4;
-    note_launch(launches);
+    TCG_LAUNCH(C, K_PACK_SIZES, k_pack_sizes, (count + 127u) / 128u, 128, 0, d_fr, count, d_sl, d_sres, d_fres);
+    TCG_LAUNCH(C, K_PACK_COPY, k_pack_copy, dim3(ns, 8), 256, 0, d_fr, d_sl, d_sres, d_prefix, d_stage, d_pkt, count);
+    TCG_LAUNCH(C, K_PACK_CRC, k_pack_crc, ns, 256, 0, d_fr, d_sl, d_sres, T.crc, d_pkt);
+    TCG_LAUNCH(C, K_PACK_HEADER, k_pack_header, (count + 127u) / 128u, 128, 0, d_fr, count, d_fres, T.crc, d_pkt);
     TCG_CHECK(cudaGetLastError());
 
     // ---------------- results ----------------
@@ -1011,6 +1009,7 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
         r.rc = 0;
     }
     TCG_CHECK(cudaStreamSynchronize(st));
+    call_end(C);
     return 0;
 }
 

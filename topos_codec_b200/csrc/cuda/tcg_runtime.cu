@@ -14,8 +14,56 @@ static bool g_init = false;
 static int g_device = -1;
 static DevTables g_tab;
 static std::atomic<uint64_t> g_launches{0};
+static std::atomic<int> g_prof_on{0};
+static double g_prof_ms[K_COUNT];
+static uint64_t g_prof_n[K_COUNT];
+static thread_local double t_last_ms = 0.0;
+static const char* k_names[K_COUNT] = {
+    "k_fdct", "k_tokens", "k_select", "k_opscan", "k_opgen", "k_chain", "k_alpha", "k_pack_sizes", "k_pack_copy",
+    "k_pack_crc", "k_pack_header", "k_dcrc", "k_dtables", "k_dchain", "k_didct", "k_dalpha", "k_dalpha_med",
+    "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk"};
 
 void note_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void call_begin(Ctx* c)
+{
+    c->prof = g_prof_on.load(std::memory_order_relaxed) != 0;
+    c->kn = 0;
+    cudaEventRecord(c->t0, c->stream);
+}
+
+void kern_begin(Ctx* c, int id)
+{
+    if (!c->prof || c->kn >= MAX_PROF) { return; }
+    c->kid[c->kn] = id;
+    cudaEventRecord(c->kev[2 * c->kn], c->stream);
+}
+
+void kern_end(Ctx* c)
+{
+    if (!c->prof || c->kn >= MAX_PROF) { return; }
+    cudaEventRecord(c->kev[2 * c->kn + 1], c->stream);
+    c->kn++;
+}
+
+void call_end(Ctx* c)
+{
+    cudaEventRecord(c->t1, c->stream);
+    cudaEventSynchronize(c->t1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->t0, c->t1);
+    t_last_ms = ms;
+    if (c->prof && c->kn > 0) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (int i = 0; i < c->kn; ++i) {
+            float k = 0.f;
+            cudaEventElapsedTime(&k, c->kev[2 * i], c->kev[2 * i + 1]);
+            g_prof_ms[c->kid[i]] += k;
+            g_prof_n[c->kid[i]] += 1;
+        }
+    }
+    c->kn = 0;
+}
 
 int32_t cuda_fail(cudaError_t e, const char* what)
 {
@@ -149,8 +197,11 @@ Ctx* ctx_acquire()
         }
     }
     Ctx* c = new Ctx();
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
+    for (int i = 0; ok && i < 2 * MAX_PROF; ++i) { ok = cudaEventCreate(&c->kev[i]) == cudaSuccess; }
+    if (!ok) {
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "stream creation failed");
         delete c;
         return nullptr;
@@ -238,4 +289,35 @@ extern "C" void tcg_shutdown(void)
 extern "C" uint64_t tcg_launch_count(void)
 {
     return tcg::g_launches.load(std::memory_order_relaxed);
+}
+
+extern "C" double tcg_last_ms(void) { return tcg::t_last_ms; }
+
+extern "C" void tcg_prof_enable(int32_t on) { tcg::g_prof_on.store(on != 0 ? 1 : 0); }
+
+extern "C" void tcg_prof_reset(void)
+{
+    std::lock_guard<std::mutex> lk(tcg::g_mu);
+    for (int i = 0; i < tcg::K_COUNT; ++i) { tcg::g_prof_ms[i] = 0.0; tcg::g_prof_n[i] = 0; }
+}
+
+extern "C" int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uint64_t* launches)
+{
+    if (id >= (uint32_t)tcg::K_COUNT) { return -1; }
+    std::lock_guard<std::mutex> lk(tcg::g_mu);
+    if (name) { *name = tcg::k_names[id]; }
+    if (ms) { *ms = tcg::g_prof_ms[id]; }
+    if (launches) { *launches = tcg::g_prof_n[id]; }
+    return 0;
+}
+
+extern "C" int32_t tcg_is_device_ptr(const void* p)
+{
+    if (p == nullptr) { return 0; }
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }

@@ -41,13 +41,42 @@ enum BufId {
     B_DEC_RES, B_TMP0, B_TMP1, B_COUNT
 };
 
+// Kernel identities for optional per-kernel event timing.
+enum KernelId {
+    K_FDCT, K_TOKENS, K_SELECT, K_OPSCAN, K_OPGEN, K_CHAIN, K_ALPHA, K_PACK_SIZES, K_PACK_COPY, K_PACK_CRC,
+    K_PACK_HEADER, K_DCRC, K_DTABLES, K_DCHAIN, K_DIDCT, K_DALPHA, K_DALPHA_MED, K_DCONCEAL, K_DEBLOCK_V,
+    K_DEBLOCK_H, K_WALK, K_COUNT
+};
+
+constexpr int MAX_PROF = 64;
+
 struct Ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;    // whole-call device time
+    cudaEvent_t kev[2 * MAX_PROF] = {};        // per-kernel timing (profiling on)
+    int kid[MAX_PROF] = {};
+    int kn = 0;
+    bool prof = false;
     DBuf d[B_COUNT];
     HBuf h[4];
     Ctx* next = nullptr;
 };
+
+// Call bracketing: records the device start/end events and, with profiling
+// enabled, folds the per-kernel event pairs into the process totals.
+void call_begin(Ctx* c);
+void call_end(Ctx* c);  // after the stream was synchronised
+void kern_begin(Ctx* c, int id);
+void kern_end(Ctx* c);
+
+#define TCG_LAUNCH(C, id, kern, grid, block, smem, ...)                 \
+    do {                                                                 \
+        tcg::kern_begin((C), (id));                                      \
+        kern<<<(grid), (block), (smem), (C)->stream>>>(__VA_ARGS__);     \
+        tcg::kern_end((C));                                              \
+        tcg::note_launch(1);                                             \
+    } while (0)
 
 // Lease a context (creates one when none is free). Thread-safe.
 Ctx* ctx_acquire();

@@ -371,6 +371,53 @@ TC_EXPORT int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs, const t
 
 /* ============================== decode ============================== */
 
+/* Generation probe + structural parse of n packets. Packets in host memory are
+ * parsed in place; packets in device memory are walked on the GPU (one launch
+ * for all of them) and parsed from the compact header records, so a
+ * device-resident decode never copies whole packets back to the host. */
+static int32_t parse_packets(const topos_batch_packet* pk, uint32_t n, tc_view* v)
+{
+    uint32_t ndev = 0;
+    for (uint32_t i = 0; i < n; ++i) { ndev += tcg_is_device_ptr(pk[i].data) ? 1u : 0u; }
+    uint8_t* rec = NULL;
+    uint32_t* slot = NULL;
+    if (ndev > 0u) {
+        const uint8_t** ptrs = (const uint8_t**)malloc(sizeof(uint8_t*) * ndev);
+        size_t* sizes = (size_t*)malloc(sizeof(size_t) * ndev);
+        rec = (uint8_t*)malloc((size_t)ndev * TCG_WALK_REC);
+        slot = (uint32_t*)malloc(sizeof(uint32_t) * n);
+        if (ptrs == NULL || sizes == NULL || rec == NULL || slot == NULL) {
+            free(ptrs); free(sizes); free(rec); free(slot);
+            return tc_fail(TC_ERR_OUT_OF_MEMORY, "packet walk staging");
+        }
+        uint32_t k = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            slot[i] = UINT32_MAX;
+            if (tcg_is_device_ptr(pk[i].data)) {
+                ptrs[k] = pk[i].data;
+                sizes[k] = pk[i].size;
+                slot[i] = k++;
+            }
+        }
+        const int32_t rc = tcg_walk_packets(ptrs, sizes, ndev, rec);
+        free(ptrs);
+        free(sizes);
+        if (rc != TC_OK) { free(rec); free(slot); return rc; }
+    }
+    int32_t rc = TC_OK;
+    for (uint32_t i = 0; i < n && rc == TC_OK; ++i) {
+        const uint8_t* head = (slot != NULL && slot[i] != UINT32_MAX) ? rec + (size_t)slot[i] * TCG_WALK_REC : pk[i].data;
+        rc = tc_probe_generation(head, pk[i].size);
+        if (rc == 0) {
+            rc = (slot != NULL && slot[i] != UINT32_MAX) ? tc_parse_compact(head, pk[i].size, &v[i])
+                                                         : tc_parse_structure(pk[i].data, pk[i].size, &v[i]);
+        }
+    }
+    free(rec);
+    free(slot);
+    return rc;
+}
+
 static int32_t build_decode(const tc_view* v, const uint8_t* data, uint16_t* const* planes_out, const size_t* strides,
                             tcg_dec_frame* jf, tcg_dec_slice* sl, topos_frame_output* o)
 {
@@ -437,11 +484,10 @@ TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* co
     o->struct_size = (uint32_t)sizeof(topos_frame_output);
     o->abi_version = TOPOS_CODEC_ABI_VERSION;
     if (data == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "data == NULL"); }
-    int32_t rc = tc_probe_generation(data, size);
-    if (rc != 0) { return rc; }
     tc_view* v = (tc_view*)malloc(sizeof(tc_view));
     if (v == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "decode view"); }
-    rc = tc_parse_structure(data, size, v);
+    const topos_batch_packet one = {data, size};
+    int32_t rc = parse_packets(&one, 1u, v);
     if (rc != TC_OK) { free(v); return rc; }
     tc_fill_info(&v->h, o);
     if (planes_out == NULL) { free(v); return TC_OK; }
@@ -475,9 +521,8 @@ TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint3
     }
     tc_view* v = (tc_view*)malloc(sizeof(tc_view) * count);
     if (v == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "decode batch context"); }
-    for (uint32_t i = 0; i < count; ++i) {
-        int32_t rc = tc_probe_generation(packets[i].data, packets[i].size);
-        if (rc == 0) { rc = tc_parse_structure(packets[i].data, packets[i].size, &v[i]); }
+    {
+        const int32_t rc = parse_packets(packets, count, v);
         if (rc != TC_OK) { free(v); return rc; }
     }
     int32_t* frc = (int32_t*)calloc(count, sizeof(int32_t));
@@ -536,3 +581,10 @@ TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint3
 TC_EXPORT int32_t tcg_device_init(int32_t device) { return tcg_init(device); }
 TC_EXPORT void tcg_device_release(void) { tcg_shutdown(); }
 TC_EXPORT uint64_t tcg_kernel_launches(void) { return tcg_launch_count(); }
+TC_EXPORT double tcg_last_device_ms(void) { return tcg_last_ms(); }
+TC_EXPORT void tcg_profile_enable(int32_t on) { tcg_prof_enable(on); }
+TC_EXPORT void tcg_profile_reset(void) { tcg_prof_reset(); }
+TC_EXPORT int32_t tcg_profile_read(uint32_t id, const char** name, double* ms, uint64_t* launches)
+{
+    return tcg_prof_read(id, name, ms, launches);
+}

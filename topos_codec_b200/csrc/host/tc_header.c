@@ -369,10 +369,13 @@ static int32_t map_validate(const tc_hdr* h, const tc_shdr* s, uint32_t n)
     return TC_OK;
 }
 
-int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v)
+/* Structural parse from either the whole packet (full != NULL) or from a
+ * compact record of its frame header and slice headers (see tcg_device.h,
+ * TCG_WALK_REC); both forms apply the same checks in the same order. */
+static int32_t parse_impl(const uint8_t* full, const uint8_t* hdr53, const uint8_t* shdrs, size_t n, tc_view* v)
 {
     memset(&v->h, 0, sizeof(v->h));
-    int32_t rc = hdr_decode(d, n, &v->h);
+    int32_t rc = hdr_decode(full != NULL ? full : hdr53, n, &v->h);
     if (rc != TC_OK) { return rc; }
     if (v->h.major == 8u || v->h.major == 9u) {
         return tc_fail(TC_ERR_UNSUPPORTED_VERSION, "v8/v9 packet in the V7 scanner");
@@ -381,7 +384,7 @@ int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v)
     size_t off = TC_HDR_SIZE;
     for (uint32_t i = 0; i < v->h.slices; ++i) {
         if (off > n || n - off < TC_SH_SIZE) { return tc_fail(TC_ERR_TRUNCATED, "slice %u header out of packet at offset %zu", i, off); }
-        const uint8_t* q = d + off;
+        const uint8_t* q = full != NULL ? full + off : shdrs + (size_t)i * TC_SH_SIZE;
         tc_shdr* s = &v->s[i];
         s->size = ld32(q); s->plane = q[4]; s->y0 = (uint16_t)ld16(q + 5); s->bh = (uint16_t)ld16(q + 7);
         s->qdb = q[9]; s->k1 = q[10]; s->k2 = q[11]; s->k3 = q[12]; s->crc = ld32(q + 13);
@@ -393,6 +396,16 @@ int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v)
     }
     if (off != n) { return tc_fail(TC_ERR_MALFORMED, "packet has %zu trailing bytes after last slice", n - off); }
     return map_validate(&v->h, v->s, v->h.slices);
+}
+
+int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v)
+{
+    return parse_impl(d, NULL, NULL, n, v);
+}
+
+int32_t tc_parse_compact(const uint8_t* rec, size_t n, tc_view* v)
+{
+    return parse_impl(NULL, rec, rec + 80, n, v);
 }
 
 void tc_fill_info(const tc_hdr* h, topos_frame_output* o)

@@ -85,6 +85,8 @@ int32_t tc_band_plan(const tc_hdr* h, uint32_t rows_per, uint32_t* total);
 /* generation probe ahead of the structural parse; 0 = continue */
 int32_t tc_probe_generation(const uint8_t* d, size_t n);
 int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v);
+/* same checks from a device walk record (tcg_device.h TCG_WALK_REC layout) */
+int32_t tc_parse_compact(const uint8_t* rec, size_t n, tc_view* v);
 void tc_fill_info(const tc_hdr* h, topos_frame_output* o);
 
 #endif /* TC_INTERNAL_H */

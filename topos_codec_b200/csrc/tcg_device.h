@@ -95,6 +95,22 @@ int32_t tcg_init(int32_t device);
 void tcg_shutdown(void);
 /* number of kernel launches issued by this process (all streams) */
 uint64_t tcg_launch_count(void);
+/* device time (ms, CUDA events on the library stream) of this thread's last call */
+double tcg_last_ms(void);
+/* optional per-kernel event timing (process totals) */
+void tcg_prof_enable(int32_t on);
+void tcg_prof_reset(void);
+int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uint64_t* launches);
+/* nonzero when p is device (or managed) memory */
+int32_t tcg_is_device_ptr(const void* p);
+
+/* Structural walk of packets that live in device memory: per packet a record of
+ * TCG_WALK_REC bytes = [64: packet bytes 0..60, zero beyond the packet]
+ * [u32 slice headers walked][u32 end offset][8 pad][512 x 17-byte slice
+ * headers], written to host_out. The walk stops exactly where a host parse of
+ * the same bytes would run out of packet. */
+#define TCG_WALK_REC (80u + 512u * 17u)
+int32_t tcg_walk_packets(const uint8_t* const* pkts, const size_t* sizes, uint32_t n, uint8_t* host_out);
 
 /* provided by the host library: thread-local error detail */
 void tcg_host_set_error(int32_t status, const char* text);
