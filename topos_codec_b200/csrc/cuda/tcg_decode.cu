@@ -5,7 +5,8 @@
 //                                               (reference codec.c:8204-8225)
 //   k_dtables   per colour slice: flags/rows prefix -> rANS models, symbol
 //               lookup tables, quantiser steps    (slice_codec.c:554-625)
-//   k_dchain    per colour slice: serial forward rANS2 decode -> natural-order
+//   k_dchain    one warp per colour slice: serial forward rANS2 decode with
+//               the symbol search spread over the lanes -> natural-order
 //               coefficients, DC reconstruction, domain checks
 //                                               (slice_codec.c:626-736)
 //   k_didct     per block: dequantise, exact inverse transform, clamp, crop
@@ -27,7 +28,7 @@
 
 namespace tcg {
 
-constexpr uint32_t CTX_BYTES = 4096u + 128u + 128u;  // lut[4096] u8, freq[64] u16, cum[64] u16
+constexpr uint32_t CTX_BYTES = 128u + 128u;  // freq[64] u16, cum[64] u16 (zero past the alphabet)
 constexpr uint32_t MAX_CTX = 11u;                    // dc 5 + run 1 + lvl 5
 constexpr uint32_t DTAB_BYTES = MAX_CTX * CTX_BYTES + 256u + 16u;  // + Q[64] u32 + header
 
@@ -112,17 +113,12 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
         if (t < nd) { ctx = t; off = 1u + t * DC_SYMS; n = DC_SYMS; }
         else if (t == nd) { ctx = 5u; off = 1u + nd * DC_SYMS; n = RUN_SYMS; }
         else { ctx = 6u + (t - nd - 1u); off = 1u + nd * DC_SYMS + RUN_SYMS + (t - nd - 1u) * LVL_SYMS; n = LVL_SYMS; }
-        uint8_t* c = tb + (size_t)ctx * CTX_BYTES;
-        uint16_t* fr = reinterpret_cast<uint16_t*>(c + 4096u);
+        uint16_t* fr = reinterpret_cast<uint16_t*>(tb + (size_t)ctx * CTX_BYTES);
         uint16_t* cu = fr + 64;
         uint8_t bytes[64];
         for (uint32_t s = 0; s < n; ++s) { bytes[s] = pay[off + s]; }
         ok = model_from_bytes(bytes, n, fr, cu);
-        if (ok) {
-            for (uint32_t s = 0; s < n; ++s) {
-                for (uint32_t k = cu[s]; k < (uint32_t)cu[s] + fr[s]; ++k) { c[k] = (uint8_t)s; }
-            }
-        }
+        for (uint32_t s = n; s < 64u; ++s) { fr[s] = 0u; cu[s] = 0u; }
     }
     if (__any_sync(0xFFFFFFFFu, !ok)) {
         if (t == 0) { status[si] = TCG_ERR_MALFORMED; }
@@ -142,68 +138,259 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
 }
 
 // ------------------------------------------------------------------ chain
+//
+// One warp decodes one slice. The coder state is warp-uniform; lane j holds the
+// frequency and cumulative start of symbol j (and j+32 for the 64-symbol run
+// alphabet) of every context the slice uses, so a symbol search is one compare
+// per lane and the matching lane's next state is broadcast with a warp OR
+// reduction (exactly one lane matches: the alphabet partitions 0..4095).
+// Stream bytes come through a 64-bit bit window refilled one word at a time
+// from 128-byte chunks that the lanes load one chunk ahead. Error conditions
+// accumulate in a flag and end the slice at the next block boundary: any
+// error conceals the slice, so only whether one occurred matters, and reading
+// past the payload is harmless because it can only add to a consumed-byte
+// count that must end equal to the payload size.
 
-struct RDec {
-    uint32_t x;
-    uint32_t pos;
-    uint32_t n;
-    const uint8_t* b;
+#define FULL_MASK 0xFFFFFFFFu
+
+struct Win {
+    uint32_t x;            // coder state
+    uint32_t whi, wlo;     // upcoming stream bits, first bit in the MSB of whi
+    uint32_t wbits;        // valid bits in whi:wlo
+    uint32_t cb;           // stream bytes moved into the state
+    uint32_t cur, nxt;     // lane j: word j of the current / next 128-byte chunk (big-endian)
+    uint32_t k;            // next word of the current chunk
+    const uint32_t* cp;    // aligned start of the chunk after the next one
+    const uint32_t* lim;   // one past the last word that overlaps the payload
 };
 
-__device__ __forceinline__ int32_t rd_renorm(RDec& d)
+__device__ __forceinline__ uint32_t win_load(const uint32_t* p, const uint32_t* lim)
 {
-    while (d.x < RANS_L) {
-        if (d.pos >= d.n) { return TCG_ERR_TRUNCATED; }
-        d.x = (d.x << 8) | __ldg(d.b + d.pos);
-        d.pos++;
+    return p < lim ? __byte_perm(__ldg(p), 0u, 0x0123u) : 0u;
+}
+
+__device__ __forceinline__ uint32_t win_take(Win& w, uint32_t lane)
+{
+    const uint32_t word = __shfl_sync(FULL_MASK, w.cur, w.k);
+    w.k += 1u;
+    if (w.k == 32u) {
+        w.k = 0u;
+        w.cur = w.nxt;
+        w.nxt = win_load(w.cp + lane, w.lim);
+        w.cp += 32;
     }
-    return 0;
+    return word;
 }
 
-__device__ __forceinline__ int32_t rd_sym(RDec& d, const uint8_t* ctx, uint32_t& sym)
+// keep at least 32 bits in the window (called after every renormalisation,
+// which consumes at most 24)
+__device__ __forceinline__ void win_refill(Win& w, uint32_t lane)
 {
-    const uint32_t slot = d.x & 4095u;
-    const uint32_t s = ctx[slot];
-    const uint16_t* fr = reinterpret_cast<const uint16_t*>(ctx + 4096u);
-    d.x = (uint32_t)fr[s] * (d.x >> 12) + slot - fr[64 + s];
-    sym = s;
-    return rd_renorm(d);
+    if (w.wbits < 32u) {
+        const uint32_t word = win_take(w, lane);
+        w.whi |= word >> w.wbits;
+        w.wlo |= word << (32u - w.wbits);
+        w.wbits += 32u;
+    }
 }
 
-__device__ __forceinline__ int32_t rd_chunk(RDec& d, uint32_t w, uint32_t& c)
+// state <- xn followed by as many stream bytes as bring it to [2^23, ...)
+__device__ __forceinline__ void win_renorm(Win& w, uint32_t xn, uint32_t lane)
 {
-    c = d.x & ((1u << w) - 1u);
-    d.x >>= w;
-    return rd_renorm(d);
+    const bool c1 = xn < RANS_L, c2 = xn < (RANS_L >> 8), c3 = xn < (RANS_L >> 16);
+    const uint32_t x8 = __funnelshift_l(w.whi, xn, 8);
+    const uint32_t x16 = __funnelshift_l(w.whi, xn, 16);
+    const uint32_t x24 = __funnelshift_l(w.whi, xn, 24);
+    w.x = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : xn);
+    const uint32_t n8 = c2 ? (c3 ? 24u : 16u) : (c1 ? 8u : 0u);
+    w.whi = __funnelshift_l(w.wlo, w.whi, n8);
+    w.wlo <<= n8;
+    w.wbits -= n8;
+    w.cb += n8 >> 3;
+    win_refill(w, lane);
 }
 
-__device__ __forceinline__ int32_t rd_suffix(RDec& d, uint32_t cat, uint32_t& m)
+__device__ __forceinline__ void win_init(Win& w, const uint8_t* b, uint32_t n, uint32_t lane)
 {
-    uint32_t v = 0;
-    int32_t rc;
-    if (cat > 1u) {
-        const uint32_t b = cat - 1u;
-        if (b > 23u) {
-            uint32_t lo, hi;
-            if ((rc = rd_chunk(d, 16u, lo)) != 0) { return rc; }
-            if ((rc = rd_chunk(d, b - 16u, hi)) != 0) { return rc; }
-            v = (hi << 16) | lo;
-        } else if ((rc = rd_chunk(d, b, v)) != 0) {
-            return rc;
+    const uintptr_t a = (uintptr_t)b;
+    const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)127);
+    w.lim = reinterpret_cast<const uint32_t*>((a + n + 3u) & ~(uintptr_t)3);
+    w.cur = win_load(base + lane, w.lim);
+    w.nxt = win_load(base + 32 + lane, w.lim);
+    w.cp = base + 64;
+    const uint32_t off = (uint32_t)(a & 127u);
+    w.k = off >> 2;
+    const uint32_t a8 = (off & 3u) * 8u;
+    const uint32_t w0 = win_take(w, lane);
+    const uint32_t w1 = win_take(w, lane);
+    w.x = __funnelshift_l(w1, w0, a8);  // first four payload bytes, big-endian
+    w.whi = w1 << a8;
+    w.wlo = 0u;
+    w.wbits = 32u - a8;
+    w.cb = 4u;
+    win_refill(w, lane);
+}
+
+// one symbol of an alphabet of at most 32 (lane j holds symbol j)
+__device__ __forceinline__ uint32_t dec_sym32(Win& w, uint32_t f, uint32_t c, uint32_t lane)
+{
+    const uint32_t x = w.x;
+    const uint32_t d = (x & 4095u) - c;
+    const bool in = d < f;
+    const uint32_t xn = f * (x >> 12) + d;
+    const uint32_t xv = __reduce_or_sync(FULL_MASK, in ? xn : 0u);
+    const uint32_t s = __reduce_or_sync(FULL_MASK, in ? lane : 0u);
+    win_renorm(w, xv, lane);
+    return s;
+}
+
+// one symbol of a 64-symbol alphabet (lane j holds symbols j and j+32)
+__device__ __forceinline__ uint32_t dec_sym64(Win& w, uint32_t fa, uint32_t ca, uint32_t fb, uint32_t cb,
+                                              uint32_t lane)
+{
+    const uint32_t x = w.x;
+    const uint32_t slot = x & 4095u, xs = x >> 12;
+    const uint32_t da = slot - ca, db = slot - cb;
+    const bool ia = da < fa, ib = db < fb;
+    const uint32_t v = ia ? fa * xs + da : (ib ? fb * xs + db : 0u);
+    const uint32_t xv = __reduce_or_sync(FULL_MASK, v);
+    const uint32_t s = __reduce_or_sync(FULL_MASK, ia ? lane : (ib ? lane + 32u : 0u));
+    win_renorm(w, xv, lane);
+    return s;
+}
+
+// raw chunk of wd bits (wd <= 23)
+__device__ __forceinline__ uint32_t dec_chunk(Win& w, uint32_t wd, uint32_t lane)
+{
+    const uint32_t v = w.x & ~(0xFFFFFFFFu << wd);
+    win_renorm(w, w.x >> wd, lane);
+    return v;
+}
+
+// category suffix: m = 2^(cat-1) | (cat-1 raw bits), split 16 + rest above 23
+__device__ __forceinline__ uint32_t dec_suffix(Win& w, uint32_t cat, uint32_t lane)
+{
+    const uint32_t b = cat > 1u ? cat - 1u : 0u;
+    uint32_t v;
+    if (b <= 23u) {
+        v = dec_chunk(w, b, lane);
+    } else {
+        const uint32_t lo = dec_chunk(w, 16u, lane);
+        v = (dec_chunk(w, b - 16u, lane) << 16) | lo;
+    }
+    return cat == 0u ? 0u : (1u << (cat - 1u)) | v;
+}
+
+template <uint32_t LM, uint32_t DM>
+__device__ __forceinline__ int32_t dchain_slice(const DSlice& S, const DPlane& P, const uint8_t* __restrict__ tb,
+                                                const uint8_t* __restrict__ stream, uint32_t nbytes,
+                                                int32_t* __restrict__ coef, int32_t* __restrict__ rows)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    // per-lane model entries
+    constexpr uint32_t ND = DM ? 5u : 1u;
+    constexpr uint32_t NL = LM == 1u ? 4u : (LM == 2u ? 5u : 1u);
+    uint32_t dcf[ND], dcc[ND], lvf[NL], lvc[NL];
+    auto ent = [&](uint32_t ctx, uint32_t s, uint32_t& f, uint32_t& c) {
+        const uint16_t* fr = reinterpret_cast<const uint16_t*>(tb + (size_t)ctx * CTX_BYTES);
+        f = fr[s];
+        c = fr[64 + s];
+    };
+#pragma unroll
+    for (uint32_t i = 0; i < ND; ++i) { ent(i, lane, dcf[i], dcc[i]); }
+#pragma unroll
+    for (uint32_t i = 0; i < NL; ++i) { ent(6u + i, lane, lvf[i], lvc[i]); }
+    uint32_t rfa, rca, rfb, rcb;
+    ent(5u, lane, rfa, rca);
+    ent(5u, lane + 32u, rfb, rcb);
+
+    Win w;
+    win_init(w, stream, nbytes, lane);
+    uint32_t err = w.x < RANS_L ? 1u : 0u;
+    const bool wide = P.bd > 12u;
+    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
+    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
+    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
+    int32_t* prow = rows;
+    int32_t* crow = rows + S.cols;
+    uint32_t prev_dcc = 0;
+    bool first = true;
+    for (uint32_t by = 0; by < S.bh && err == 0u; ++by) {
+        int32_t left = 0;
+        for (uint32_t bx = 0; bx < S.cols; ++bx) {
+            // DC
+            uint32_t f0 = dcf[0], c0 = dcc[0];
+            if (DM) {
+                const uint32_t dctx = first ? 0u : dcp_ctx(prev_dcc, true);
+#pragma unroll
+                for (uint32_t i = 1; i < ND; ++i) {
+                    f0 = dctx == i ? dcf[i] : f0;
+                    c0 = dctx == i ? dcc[i] : c0;
+                }
+            }
+            const int32_t top = by != 0u ? prow[bx] : 0;
+            const uint32_t dcat = dec_sym32(w, f0, c0, lane);
+            const uint32_t dmv = dec_suffix(w, dcat, lane);
+            err |= dmv > mdc ? 1u : 0u;
+            const int32_t pred = dc_pred(bx != 0u, left, by != 0u, top);
+            const int64_t dcv = (int64_t)pred + unmap_s(dmv);
+            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+            left = (int32_t)dcv;
+            if (lane == 0u) { crow[bx] = left; }
+            prev_dcc = dcat;
+            first = false;
+            int32_t clo = lane == 0u ? left : 0, chi = 0;
+            // AC: (run, level, suffix) until the end-of-block run symbol
+            uint32_t pos = 1u, pcat = 0u;
+            bool has = false;
+            for (;;) {
+                const uint32_t r = dec_sym64(w, rfa, rca, rfb, rcb, lane);
+                const uint32_t idx = pos + r;
+                if (r == 63u || idx > 63u) {
+                    err |= r != 63u ? 1u : 0u;
+                    break;
+                }
+                uint32_t fl = lvf[0], cl = lvc[0];
+                if (LM != 0u) {
+                    const uint32_t lc = LM == 1u ? pos_ctx(idx) : prev_ctx(pcat, has);
+#pragma unroll
+                    for (uint32_t i = 1; i < NL; ++i) {
+                        fl = lc == i ? lvf[i] : fl;
+                        cl = lc == i ? lvc[i] : cl;
+                    }
+                }
+                const uint32_t cat = dec_sym32(w, fl, cl, lane);
+                const uint32_t m = dec_suffix(w, cat, lane);
+                err |= m > mlv ? 1u : 0u;
+                const uint32_t nat = c_zigzag[idx];
+                const int32_t v = unmap_s(m);
+                if ((nat & 31u) == lane) {
+                    if (nat & 32u) { chi = v; } else { clo = v; }
+                }
+                pcat = cat;
+                has = true;
+                pos = idx + 1u;
+            }
+            int32_t* blk = coef + (size_t)(S.blk0 + by * S.cols + bx) * 64u;
+            blk[lane] = clo;
+            blk[32u + lane] = chi;
+            if (err != 0u) { break; }
         }
+        __syncwarp();
+        int32_t* sw = prow; prow = crow; crow = sw;
     }
-    m = cat == 0u ? 0u : (1u << (cat - 1u)) | v;
-    return 0;
+    if (err == 0u && w.cb != nbytes) { err = 1u; }
+    return err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
-// One 32-thread block per colour slice; the block stages the slice's lookup
-// tables in shared memory and lane 0 runs the symbol chain.
+// One warp per colour slice (one warp per block, so every slice of a batch is
+// resident at once); dynamic shared memory holds two DC rows of the slice.
 __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
                                                const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
                                                const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
                                                int32_t* __restrict__ status)
 {
-    extern __shared__ __align__(16) uint8_t sm[];
+    extern __shared__ __align__(16) int32_t rows[];
     const uint32_t si = cslices[blockIdx.x];
     if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
@@ -211,70 +398,18 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     const uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
     const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + MAX_CTX * CTX_BYTES) + 64;
     const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
-    // stage the context tables that this slice uses
-    for (uint32_t i = threadIdx.x * 16u; i < MAX_CTX * CTX_BYTES; i += blockDim.x * 16u) {
-        const uint32_t ctx = i / CTX_BYTES;
-        const bool used = ctx < (dm ? 5u : 1u) || ctx == 5u || (ctx >= 6u && ctx < 6u + (lm == 1u ? 4u : lm == 2u ? 5u : 1u));
-        if (used) { *reinterpret_cast<uint4*>(sm + i) = *reinterpret_cast<const uint4*>(tb + i); }
+    const uint8_t* stream = pkt + S.pay + plen;
+    const uint32_t nb = S.size - plen;
+    int32_t rc;
+    switch (lm * 2u + dm) {
+    case 0: rc = dchain_slice<0, 0>(S, P, tb, stream, nb, coef, rows); break;
+    case 1: rc = dchain_slice<0, 1>(S, P, tb, stream, nb, coef, rows); break;
+    case 2: rc = dchain_slice<1, 0>(S, P, tb, stream, nb, coef, rows); break;
+    case 3: rc = dchain_slice<1, 1>(S, P, tb, stream, nb, coef, rows); break;
+    case 4: rc = dchain_slice<2, 0>(S, P, tb, stream, nb, coef, rows); break;
+    default: rc = dchain_slice<2, 1>(S, P, tb, stream, nb, coef, rows); break;
     }
-    int32_t* rows = reinterpret_cast<int32_t*>(sm + MAX_CTX * CTX_BYTES);
-    int32_t* prow = rows;
-    int32_t* crow = rows + S.cols;
-    for (uint32_t i = threadIdx.x; i < 2u * S.cols; i += blockDim.x) { rows[i] = 0; }
-    __syncthreads();
-    if (threadIdx.x != 0) { return; }
-    const uint8_t* pay = pkt + S.pay;
-    RDec d;
-    d.b = pay + plen;
-    d.n = S.size - plen;
-    d.x = ((uint32_t)d.b[0] << 24) | ((uint32_t)d.b[1] << 16) | ((uint32_t)d.b[2] << 8) | d.b[3];
-    d.pos = 4u;
-    int32_t rc = d.x < RANS_L ? TCG_ERR_MALFORMED : 0;
-    const bool wide = P.bd > 12u;
-    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
-    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
-    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
-    const uint8_t* run_t = sm + 5u * CTX_BYTES;
-    uint32_t prev_dcc = 0;
-    bool first = true;
-    for (uint32_t by = 0; by < S.bh && rc == 0; ++by) {
-        for (uint32_t bx = 0; bx < S.cols; ++bx) {
-            int32_t* blk = coef + (size_t)(S.blk0 + by * S.cols + bx) * 64u;
-            const uint32_t dctx = dm ? (first ? 0u : dcp_ctx(prev_dcc, true)) : 0u;
-            uint32_t cat, m;
-            if ((rc = rd_sym(d, sm + dctx * CTX_BYTES, cat)) != 0) { break; }
-            if ((rc = rd_suffix(d, cat, m)) != 0) { break; }
-            if (m > mdc) { rc = TCG_ERR_MALFORMED; break; }
-            const int32_t pred = dc_pred(bx != 0u, bx != 0u ? crow[bx - 1u] : 0, by != 0u, prow[bx]);
-            const int64_t dcv = (int64_t)pred + unmap_s(m);
-            if (dcv > dlim || dcv < -dlim) { rc = TCG_ERR_MALFORMED; break; }
-            blk[0] = (int32_t)dcv;
-            crow[bx] = (int32_t)dcv;
-            prev_dcc = cat;
-            first = false;
-            uint32_t pos = 1, pcat = 0;
-            bool has = false;
-            for (;;) {
-                uint32_t r;
-                if ((rc = rd_sym(d, run_t, r)) != 0) { break; }
-                if (r == 63u) { break; }
-                const uint32_t idx = pos + r;
-                if (idx > 63u) { rc = TCG_ERR_MALFORMED; break; }
-                const uint32_t lc = lm == 1u ? pos_ctx(idx) : lm == 2u ? prev_ctx(pcat, has) : 0u;
-                if ((rc = rd_sym(d, sm + (6u + lc) * CTX_BYTES, cat)) != 0) { break; }
-                if ((rc = rd_suffix(d, cat, m)) != 0) { break; }
-                if (m > mlv) { rc = TCG_ERR_MALFORMED; break; }
-                blk[c_zigzag[idx]] = unmap_s(m);
-                pcat = cat;
-                has = true;
-                pos = idx + 1u;
-            }
-            if (rc != 0) { break; }
-        }
-        int32_t* sw = prow; prow = crow; crow = sw;
-    }
-    if (rc == 0 && d.pos != d.n) { rc = TCG_ERR_MALFORMED; }
-    status[si] = rc;
+    if (threadIdx.x == 0) { status[si] = rc; }
 }
 
 // ------------------------------------------------------------------ reconstruction
@@ -688,9 +823,8 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         TCG_LAUNCH(C, K_DCRC, k_dcrc, ns, 256, 0, d_sl, d_pkt, T.crc, d_status);
     }
     if (nc > 0) {
-        TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
         TCG_LAUNCH(C, K_DTABLES, k_dtables, nc, 32, 0, d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
-        const size_t smem = MAX_CTX * CTX_BYTES + (size_t)max_cols * 8u;
+        const size_t smem = (size_t)max_cols * 8u;
         static size_t attr = 0;
         if (smem > attr) {
             cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -336,10 +336,16 @@ __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slic
 }
 
 // ============================== op generation ==============================
-// op word: bit31 = 0 symbol (bits 12..24 freq, 0..11 cum); 1 raw chunk
-// (bits 23..27 width w, 0..22 value).
+// op word: bits 23..31 index into the slice's coding table, bits 0..22 a raw
+// value. Index 0..23 is a raw chunk of that many bits (0 = identity); index
+// 24 + t is the symbol whose frequency/cumulative word sits at t in the
+// slice's symbol table (T_DC / T_RUN / T_LVL layout).
 
-__device__ __forceinline__ uint32_t op_chunk(uint32_t w, uint32_t v) { return 0x80000000u | (w << 23) | (v & ((1u << w) - 1u)); }
+constexpr uint32_t OP_CHUNKS = 24u;
+constexpr uint32_t OP_ENTRIES = OP_CHUNKS + T_SIZE;
+
+__device__ __forceinline__ uint32_t op_chunk(uint32_t w, uint32_t v) { return (w << 23) | (v & ((1u << w) - 1u)); }
+__device__ __forceinline__ uint32_t op_sym(uint32_t t) { return (OP_CHUNKS + t) << 23; }
 
 __device__ __forceinline__ void put_suffix_ops(uint32_t*& o, uint32_t cat, uint32_t m)
 {
@@ -360,12 +366,11 @@ __global__ void __launch_bounds__(256) k_opgen(const EWork* __restrict__ work, c
     const ESlice& S = slices[w.slice];
     const uint32_t lb = w.lb0 + threadIdx.x;
     const uint32_t gb = S.blk0 + lb;
-    const uint32_t* tb = stab + (size_t)w.slice * T_SIZE;
     const uint32_t pl = sres[w.slice].plen;
     const uint32_t lmod = (pl >> 16) & 3u, dmod = (pl >> 20) & 1u;
     uint32_t* o = ops + S.op_base + opoff[gb];
     const int32_t* c = coef + (size_t)gb * 64u;
-    *o++ = __ldg(tb + T_RUN + 63u);  // EOB
+    *o++ = op_sym(T_RUN + 63u);  // EOB
     uint64_t m = mask[gb];
     // walk non-zero positions from the highest down; the forward-order
     // neighbour of position p is the next lower set bit (or the DC at 0)
@@ -388,56 +393,123 @@ __global__ void __launch_bounds__(256) k_opgen(const EWork* __restrict__ work, c
             }
             ctx = prev_ctx(pc, m != 0u);
         }
-        *o++ = __ldg(tb + T_LVL + ctx * LVL_SYMS + cat);
-        *o++ = __ldg(tb + T_RUN + (p - below - 1u));
+        *o++ = op_sym(T_LVL + ctx * LVL_SYMS + cat);
+        *o++ = op_sym(T_RUN + (p - below - 1u));
     }
     const uint32_t dm = dcm[gb];
     const uint32_t ds = bitlen32(dm);
     put_suffix_ops(o, ds, dm);
     const uint32_t dctx = dmod ? dcp_ctx(lb > 0u ? bitlen32(dcm[gb - 1u]) : 0u, lb > 0u) : 0u;
-    *o++ = __ldg(tb + T_DC + dctx * DC_SYMS + ds);
+    *o++ = op_sym(T_DC + dctx * DC_SYMS + ds);
 }
 
 // =============================== rANS chains ===============================
 
-// One lane per colour slice; the lane walks its slice's operations in coding
-// order and writes renormalisation bytes backwards from the end of its
-// staging window, so the stream reads forwards when the chain finishes.
-__global__ void __launch_bounds__(32) k_chain(const ESlice* __restrict__ slices, const uint32_t* __restrict__ order,
-                                              uint32_t n, const uint32_t* __restrict__ ops,
-                                              const uint32_t* __restrict__ div_m, const uint8_t* __restrict__ div_l,
-                                              uint8_t* __restrict__ stage, ESliceRes* __restrict__ sres)
+// Coding-table entry of one operation: renormalisation threshold, division
+// magic m and shift l (q = umulhi(2x, m) >> l = x / f for x < 2^31), additive
+// term, and multiplier B | l << 24. Every operation is then
+//   x <- q * B + x + add  after renormalisation against lim:
+// a symbol of frequency f has B = 4096 - f, add = cum (x/f*4096 + x%f + cum);
+// a raw chunk of w bits has f = 1 (q = x), B = 2^w - 1, add = the value
+// (x * 2^w + value); the 0-bit chunk is the identity.
+__device__ __forceinline__ uint4 chunk_entry(uint32_t w)
 {
+    return make_uint4(1u << (31u - w), 0x80000000u, 0u, (1u << w) - 1u);
+}
+
+__device__ __forceinline__ uint4 symbol_entry(uint32_t word, const uint32_t* __restrict__ div_m,
+                                              const uint8_t* __restrict__ div_l)
+{
+    const uint32_t f = word >> 12;
+    if (f == 0u) { return chunk_entry(0u); }  // symbol absent from the model: never coded
+    return make_uint4(f << 19, __ldg(div_m + f), word & 0xFFFu, (4096u - f) | ((uint32_t)__ldg(div_l + f) << 24));
+}
+
+// One coding operation, branch-free; emitted bytes (0..3, least significant
+// first) are stored downwards from p.
+__device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, const uint4* __restrict__ tab)
+{
+    const uint4 e = tab[o >> 23];
+    const uint32_t v = o & 0x7FFFFFu;
+    const uint32_t x8 = x >> 8, x16 = x >> 16, x24 = x >> 24;
+    const bool c1 = x >= e.x, c2 = x8 >= e.x, c3 = x16 >= e.x;
+    const uint32_t xr = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : x);
+    const uint32_t q = __umulhi(xr << 1, e.y) >> (e.w >> 24);
+    const uint32_t xn = q * (e.w & 0xFFFFFFu) + (xr + e.z + v);
+    if (c1) { p[-1] = (uint8_t)x; }
+    if (c2) { p[-2] = (uint8_t)x8; }
+    if (c3) { p[-3] = (uint8_t)x16; }
+    p -= c2 ? (c3 ? 3 : 2) : (c1 ? 1 : 0);
+    x = xn;
+}
+
+// Four consecutive operations of a slice (group g); positions at or past the
+// slice's operation count read as identities, and groups wholly past it are
+// not loaded.
+__device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t nops)
+{
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (4u * g < nops) { v = __ldg(op4 + g); }
+    const uint32_t k = 4u * g;
+    v.x = k < nops ? v.x : 0u;
+    v.y = k + 1u < nops ? v.y : 0u;
+    v.z = k + 2u < nops ? v.z : 0u;
+    v.w = k + 3u < nops ? v.w : 0u;
+    return v;
+}
+
+#define ENC_GROUP(v)                  \
+    do {                              \
+        enc_step(x, p, (v).x, tab);   \
+        enc_step(x, p, (v).y, tab);   \
+        enc_step(x, p, (v).z, tab);   \
+        enc_step(x, p, (v).w, tab);   \
+    } while (0)
+
+constexpr uint32_t CHAIN_LANES = 32u;
+constexpr size_t CHAIN_SMEM = (size_t)CHAIN_LANES * OP_ENTRIES * sizeof(uint4);
+
+// One lane per colour slice. The lane expands its slice's symbol table into
+// per-operation coding entries in shared memory, then walks the operations in
+// coding order, sixteen per iteration with the operation words loaded sixteen
+// ahead of their use. Bytes go downwards from the end of the lane's staging
+// window, so the stream reads forwards.
+__global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict__ slices,
+                                                       const uint32_t* __restrict__ order, uint32_t n,
+                                                       const uint32_t* __restrict__ ops,
+                                                       const uint32_t* __restrict__ stab,
+                                                       const uint32_t* __restrict__ div_m,
+                                                       const uint8_t* __restrict__ div_l, uint8_t* __restrict__ stage,
+                                                       ESliceRes* __restrict__ sres)
+{
+    extern __shared__ uint4 chain_tab[];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) { return; }
     const uint32_t si = order[i];
+    uint4* tab = chain_tab + (size_t)threadIdx.x * OP_ENTRIES;
+    for (uint32_t w = 0; w < OP_CHUNKS; ++w) { tab[w] = chunk_entry(w); }
+    const uint32_t* st = stab + (size_t)si * T_SIZE;
+    for (uint32_t t = 0; t < T_SIZE; ++t) { tab[OP_CHUNKS + t] = symbol_entry(__ldg(st + t), div_m, div_l); }
     const ESlice& S = slices[si];
     const uint32_t nops = sres[si].nops;
-    const uint32_t* op = ops + S.op_base;
-    uint8_t* end = stage + S.stage_base + S.stage_cap;  // byte k goes to end[-1-k]
+    // op windows start on 1 KiB boundaries (256 words per block) and hold whole groups
+    const uint4* op4 = reinterpret_cast<const uint4*>(ops + S.op_base);
+    uint8_t* const end = stage + S.stage_base + S.stage_cap;  // emitted byte k lives at end[-1-k]
+    uint8_t* p = end;
     uint32_t x = RANS_L;
-    uint32_t pos = 0;
-    uint32_t cur = nops > 0u ? __ldg(op) : 0u;
-    for (uint32_t k = 0; k < nops; ++k) {
-        const uint32_t nxt = k + 1u < nops ? __ldg(op + k + 1u) : 0u;
-        if ((int32_t)cur < 0) {
-            const uint32_t w = (cur >> 23) & 31u;
-            const uint32_t thr = 1u << (31u - w);
-            while (x >= thr) { end[-1 - (int64_t)pos] = (uint8_t)x; ++pos; x >>= 8; }
-            x = (x << w) | (cur & 0x7FFFFFu);
-        } else {
-            const uint32_t f = (cur >> 12) & 0x1FFFu;
-            const uint32_t cum = cur & 0xFFFu;
-            const uint32_t mg = __ldg(div_m + f);
-            const uint32_t sh = __ldg(div_l + f);
-            const uint32_t xmax = f << 19;
-            while (x >= xmax) { end[-1 - (int64_t)pos] = (uint8_t)x; ++pos; x >>= 8; }
-            const uint32_t q = __umulhi(x << 1, mg) >> sh;
-            x = x + q * (4096u - f) + cum;
-        }
-        cur = nxt;
+    uint4 a = op_group(op4, 0u, nops), b = op_group(op4, 1u, nops);
+    uint4 c = op_group(op4, 2u, nops), d = op_group(op4, 3u, nops);
+    for (uint32_t g = 0; 4u * g < nops; g += 4u) {
+        ENC_GROUP(a);
+        a = op_group(op4, g + 4u, nops);
+        ENC_GROUP(b);
+        b = op_group(op4, g + 5u, nops);
+        ENC_GROUP(c);
+        c = op_group(op4, g + 6u, nops);
+        ENC_GROUP(d);
+        d = op_group(op4, g + 7u, nops);
     }
-    sres[si].nbytes = pos;
+    sres[si].nbytes = (uint32_t)(end - p);
     sres[si].xfin = x;
 }
 
@@ -962,7 +1034,13 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
         TCG_LAUNCH(C, K_OPSCAN, k_opscan, nc, 1024, 0, d_sl, d_cs, d_nops, d_opoff, d_sres);
         TCG_LAUNCH(C, K_OPGEN, k_opgen, (uint32_t)work.size(), 256, 0, d_wk, d_sl, d_coef, d_mask, d_dcm, d_opoff, d_stab,
                    d_sres, d_ops);
-        TCG_LAUNCH(C, K_CHAIN, k_chain, (nc + 31u) / 32u, 32, 0, d_sl, d_or, nc, d_ops, T.div_m, T.div_l, d_stage, d_sres);
+        static bool chain_attr = false;
+        if (!chain_attr) {
+            cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHAIN_SMEM);
+            chain_attr = true;
+        }
+        TCG_LAUNCH(C, K_CHAIN, k_chain, (nc + CHAIN_LANES - 1u) / CHAIN_LANES, CHAIN_LANES, CHAIN_SMEM, d_sl, d_or, nc,
+                   d_ops, d_stab, T.div_m, T.div_l, d_stage, d_sres);
     }
     if (!aslices.empty()) {
         for (uint32_t a : aslices) {
