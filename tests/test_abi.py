@@ -16,11 +16,12 @@ from conftest import GOLDEN, ROOT
 from topos_codec_b200 import binding as B
 
 HEADER = os.path.join(ROOT, "include", "topos_codec.h")
+HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include"))) if f.endswith(".h")]
 REF_HEADER = "/root/reference/native/include/topos_codec.h"
 
 
 def _declared_functions():
-    text = open(HEADER).read()
+    text = "\n".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b((?:tc|tcg)_[a-z0-9_]+)\s*\(", text)))
 
@@ -142,3 +143,36 @@ def test_structural_parse_matches_oracle(product, oracle):
             assert ra == rb, (name, trial)
             if ra == 0:
                 assert bytes(ia) == bytes(ib)
+
+
+REF_PY = "/root/reference/python"
+
+
+def test_reference_python_binding_loads_this_library(built):
+    """The reference's own Python binding binds every symbol it needs from this
+    library (hot path for real, the rest as NOT_IMPLEMENTED exports) and its
+    host-side answers match ours. Runs only where the reference is checked out."""
+    import importlib
+    import sys
+    if not os.path.isdir(REF_PY):
+        pytest.skip("reference Python package not present")
+    sys.path.insert(0, REF_PY)
+    try:
+        tb = importlib.import_module("topos_codec.topos_binding")
+    finally:
+        sys.path.remove(REF_PY)
+    codec = tb.ToposCodec(library=ctypes.CDLL(B.PRODUCT_LIBRARY))
+    assert codec.abi_version == 2
+    ours = B.ToposCodec(B.PRODUCT_LIBRARY)
+    for w, h, kw in [(1920, 1080, dict(qp=8, qmatrix_id=4, features=1)), (3840, 2160, dict(qp=4, features=3)),
+                     (4096, 2160, dict(qp=2, bit_depth=12, pixel_format=2, profile=5, alpha_mode=1,
+                                       alpha_bit_depth=16, color_range=1))]:
+        mine = B.make_config(w, h, **kw)
+        theirs = tb._CFrameConfig.from_buffer_copy(bytes(mine))
+        assert codec.config_validate(theirs) == ours.validate(mine) == 0
+        assert codec.packet_bound(theirs) == ours.packet_bound(mine)
+    lib = codec._lib
+    lib.tc_frame_encode_sized.restype = ctypes.c_int32
+    assert lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == B.TC_ERR_NOT_IMPLEMENTED
+    lib.tc_scalable_status_name.restype = ctypes.c_char_p
+    assert lib.tc_scalable_status_name(1) == b"reference" and lib.tc_scalable_status_name(9) == b"unknown"

@@ -28,7 +28,8 @@ def _sources():
 
 
 def _headers():
-    out = [os.path.join(ROOT, "include", "topos_codec.h"), os.path.join(CSRC, "tcg_device.h")]
+    out = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
+    out.append(os.path.join(CSRC, "tcg_device.h"))
     for sub in ("host", "cuda"):
         d = os.path.join(CSRC, sub)
         out += [os.path.join(d, f) for f in os.listdir(d) if f.endswith((".h", ".cuh"))]
