@@ -262,6 +262,34 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
                                uint8_t* const* outs, const size_t* out_caps,
                                topos_frame_stats* stats, int32_t* rcs);
 
+/* Allocation-free packet query. No counterpart in the reference: it exists for
+ * callers that must not allocate device memory while they run - a serving
+ * process whose GPU memory is handed out up front by its own pool (a stray
+ * cudaMalloc can fail there once the pool holds the free memory, and it breaks
+ * the pool's accounting), and latency-critical threads, because cudaMalloc and
+ * cudaFree may synchronise the whole device and stall the work of others.
+ *
+ * Returns, for count packets, the same frame information (and the same status)
+ * as tc_frame_decode_batch(packets, count, NULL, NULL, infos). Packets may sit
+ * in device memory (their headers are walked on the GPU) or in host memory.
+ * The call allocates nothing, in device or host memory: its device scratch
+ * (~550 KB) is a static array of the library that every GPU loading the
+ * library holds until the process exits. Limits and rules:
+ *  - at most TCG_NOALLOC_MAX_PACKETS packets per call; more is rejected with
+ *    TC_ERR_LIMIT_EXCEEDED before any device work;
+ *  - the first call on a device looks up the scratch address on that device
+ *    (which may load the library's device code there); make that first call
+ *    before any CUDA stream capture is in progress;
+ *  - the scratch is shared by every call on a device and keeps the last call's
+ *    records; each call clears the records it uses before writing them, but
+ *    calls that overlap on the GPU (from several host threads at once) race on
+ *    it, so serialise them;
+ *  - the call runs on the default stream and returns when its device work has
+ *    finished. */
+#define TCG_NOALLOC_MAX_PACKETS 64u
+int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
+                                      topos_frame_output* infos);
+
 /* Device selection and teardown for the calling process. tcg_device_init is
  * implicit on first use (device 0 or the current CUDA device). */
 int32_t tcg_device_init(int32_t device);

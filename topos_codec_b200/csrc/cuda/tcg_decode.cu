@@ -21,6 +21,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "tcg_common.cuh"
@@ -947,6 +948,40 @@ static int32_t walk_impl(Ctx* C, const uint8_t* const* pkts, const size_t* sizes
     return 0;
 }
 
+// ------------------------------------------------ allocation-free packet walk
+//
+// Scratch of tcg_walk_packets_noalloc: the packet pointer and size tables and
+// one walk record per packet, for at most TCG_NOALLOC_MAX_PACKETS packets. It
+// lives in the library's static device data (every GPU that loads the library
+// holds these ~550 KB until exit); no call allocates device memory. Host code
+// reaches it through the address that cudaGetSymbolAddress reports for the
+// current device, looked up on the first call on each device.
+constexpr size_t NA_TABLE = (size_t)TCG_NOALLOC_MAX_PACKETS * 8u;
+constexpr size_t NA_BYTES = 2u * NA_TABLE + (size_t)TCG_NOALLOC_MAX_PACKETS * WALK_REC;
+static __device__ __align__(256) uint8_t g_walk_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+static std::mutex g_na_mu;
+static uint8_t* g_na_base[NA_MAX_DEVICES];
+
+static int32_t noalloc_base(uint8_t** base)
+{
+    int dev = 0;
+    TCG_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) {
+        tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: device ordinal beyond 63");
+        return TCG_ERR_LIMIT_EXCEEDED;
+    }
+    std::lock_guard<std::mutex> g(g_na_mu);
+    if (g_na_base[dev] == nullptr) {
+        void* p = nullptr;
+        TCG_CHECK(cudaGetSymbolAddress(&p, g_walk_scratch));
+        g_na_base[dev] = static_cast<uint8_t*>(p);
+    }
+    *base = g_na_base[dev];
+    return 0;
+}
+
 }  // namespace tcg
 
 extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
@@ -965,4 +1000,45 @@ extern "C" int32_t tcg_walk_packets(const uint8_t* const* pkts, const size_t* si
     const int32_t rc = tcg::walk_impl(c, pkts, sizes, n, host_out);
     tcg::ctx_release(c);
     return rc;
+}
+
+extern "C" int32_t tcg_walk_packets_noalloc(const uint8_t* const* pkts, const size_t* sizes, uint32_t n)
+{
+    if (n == 0u) { return 0; }
+    if (n > TCG_NOALLOC_MAX_PACKETS) {
+        tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: more than 64 packets in one call");
+        return TCG_ERR_LIMIT_EXCEEDED;
+    }
+    uint8_t* base = nullptr;
+    const int32_t rc = tcg::noalloc_base(&base);
+    if (rc != 0) { return rc; }
+    uint64_t tab[2u * TCG_NOALLOC_MAX_PACKETS];
+    for (uint32_t i = 0; i < n; ++i) {
+        tab[i] = (uint64_t)(uintptr_t)pkts[i];
+        tab[TCG_NOALLOC_MAX_PACKETS + i] = sizes[i];
+    }
+    uint8_t* recs = base + 2u * tcg::NA_TABLE;
+    TCG_CHECK(cudaMemcpyAsync(base, tab, sizeof(tab), cudaMemcpyHostToDevice, 0));
+    // the records of this call start from zero, so nothing an earlier call left is read back
+    TCG_CHECK(cudaMemsetAsync(recs, 0, (size_t)n * tcg::WALK_REC, 0));
+    tcg::k_walk<<<(n + 63u) / 64u, 64, 0, 0>>>(reinterpret_cast<const uint8_t* const*>(base),
+                                                reinterpret_cast<const uint64_t*>(base + tcg::NA_TABLE), n, recs);
+    tcg::note_launch(1);
+    TCG_CHECK(cudaGetLastError());
+    TCG_CHECK(cudaStreamSynchronize(0));
+    return 0;
+}
+
+extern "C" int32_t tcg_walk_record_noalloc(uint32_t i, uint8_t* host_rec)
+{
+    if (i >= TCG_NOALLOC_MAX_PACKETS) {
+        tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: record index beyond 63");
+        return TCG_ERR_LIMIT_EXCEEDED;
+    }
+    uint8_t* base = nullptr;
+    const int32_t rc = tcg::noalloc_base(&base);
+    if (rc != 0) { return rc; }
+    TCG_CHECK(cudaMemcpy(host_rec, base + 2u * tcg::NA_TABLE + (size_t)i * tcg::WALK_REC, tcg::WALK_REC,
+                         cudaMemcpyDeviceToHost));
+    return 0;
 }

@@ -508,6 +508,66 @@ TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* co
     return rc;
 }
 
+/* Allocation-free form of tc_frame_decode_batch's query mode (no reference
+ * counterpart). Every buffer is on the stack or in the device library's static
+ * scratch; packets in device memory are walked with the static-scratch walk
+ * and parsed from their records one at a time. The packets are parsed twice -
+ * once to find the first failing status, then to fill infos - so that, like
+ * the batch query, infos is left untouched when any packet fails. */
+TC_EXPORT int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
+                                                topos_frame_output* infos)
+{
+    if (count == 0u) { return TC_OK; }
+    if (count > TCG_NOALLOC_MAX_PACKETS) {
+        return tc_fail(TC_ERR_LIMIT_EXCEEDED, "allocation-free query: count %u > %u", count,
+                       (unsigned)TCG_NOALLOC_MAX_PACKETS);
+    }
+    if (infos == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "infos == NULL"); }
+    if (packets == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "batch packets == NULL"); }
+    const uint8_t* dptrs[TCG_NOALLOC_MAX_PACKETS];
+    size_t dsizes[TCG_NOALLOC_MAX_PACKETS];
+    uint32_t slot[TCG_NOALLOC_MAX_PACKETS];
+    uint32_t ndev = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (packets[i].data == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "packets[%u].data == NULL", i); }
+        slot[i] = UINT32_MAX;
+        if (tcg_is_device_ptr(packets[i].data)) {
+            dptrs[ndev] = packets[i].data;
+            dsizes[ndev] = packets[i].size;
+            slot[i] = ndev++;
+        }
+    }
+    if (ndev > 0u) {
+        const int32_t rc = tcg_walk_packets_noalloc(dptrs, dsizes, ndev);
+        if (rc != TC_OK) { return rc; }
+    }
+    uint8_t rec[TCG_WALK_REC];
+    tc_view v;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (uint32_t i = 0; i < count; ++i) {
+            const int dev = slot[i] != UINT32_MAX;
+            if (dev) {
+                const int32_t rc = tcg_walk_record_noalloc(slot[i], rec);
+                if (rc != TC_OK) { return rc; }
+            }
+            const uint8_t* head = dev ? rec : packets[i].data;
+            int32_t rc = tc_probe_generation(head, packets[i].size);
+            if (rc == 0) {
+                rc = dev ? tc_parse_compact(head, packets[i].size, &v) : tc_parse_structure(packets[i].data, packets[i].size, &v);
+            }
+            if (rc != TC_OK) { return rc; }
+            if (pass == 1) {
+                topos_frame_output* o = &infos[i];
+                memset(o, 0, sizeof(*o));
+                o->struct_size = (uint32_t)sizeof(topos_frame_output);
+                o->abi_version = TOPOS_CODEC_ABI_VERSION;
+                tc_fill_info(&v.h, o);
+            }
+        }
+    }
+    return TC_OK;
+}
+
 /* reference: native/src/codec/codec.c:9639-9805 */
 TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
                                         const size_t* strides, topos_frame_output* infos)

@@ -112,6 +112,16 @@ int32_t tcg_is_device_ptr(const void* p);
 #define TCG_WALK_REC (80u + 512u * 17u)
 int32_t tcg_walk_packets(const uint8_t* const* pkts, const size_t* sizes, uint32_t n, uint8_t* host_out);
 
+/* identical to the public definition in topos_codec.h */
+#define TCG_NOALLOC_MAX_PACKETS 64u
+
+/* The same walk for at most TCG_NOALLOC_MAX_PACKETS packets, with its tables
+ * and records in the library's static device scratch instead of allocated
+ * buffers (nothing is allocated). tcg_walk_record_noalloc copies record i of
+ * the last walk on the current device to host_rec (TCG_WALK_REC bytes). */
+int32_t tcg_walk_packets_noalloc(const uint8_t* const* pkts, const size_t* sizes, uint32_t n);
+int32_t tcg_walk_record_noalloc(uint32_t i, uint8_t* host_rec);
+
 /* provided by the host library: thread-local error detail */
 void tcg_host_set_error(int32_t status, const char* text);
 /* provided by the host library: exact log2 table (4097 doubles, index = freq) */
