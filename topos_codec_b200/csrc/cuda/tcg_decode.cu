@@ -29,9 +29,23 @@
 
 namespace tcg {
 
-constexpr uint32_t CTX_BYTES = 128u + 128u;  // freq[64] u16, cum[64] u16 (zero past the alphabet)
-constexpr uint32_t MAX_CTX = 11u;                    // dc 5 + run 1 + lvl 5
-constexpr uint32_t DTAB_BYTES = MAX_CTX * CTX_BYTES + 256u + 16u;  // + Q[64] u32 + header
+// Per colour slice decode tables (global, built by k_dtables):
+//   LUT  11 x 256 u32  per context, bucket b of 16 slots: symbol s0 holding
+//                      slot 16b | cum[s0] << 6 | cum[s0+1] << 18
+//   CUM  11 x 66 u16   per context: cum[0..nsym], then 4096 up to index 65
+//   Q    64 u32        quantiser steps of the slice's effective qp
+//   HDR  4 u32         level model, dc model, prefix length
+// Context ids: 0..4 DC (by previous DC category), 5 run, 6..10 level.
+constexpr uint32_t MAX_CTX = 11u;
+constexpr uint32_t LUT_BUCKETS = 256u;
+constexpr uint32_t LUT_BYTES = LUT_BUCKETS * 4u;
+constexpr uint32_t CUM_LEN = 66u;
+constexpr uint32_t CUM_BYTES = CUM_LEN * 2u;
+constexpr uint32_t TAB_LUT = 0u;
+constexpr uint32_t TAB_CUM = MAX_CTX * LUT_BYTES;
+constexpr uint32_t TAB_Q = (TAB_CUM + MAX_CTX * CUM_BYTES + 15u) & ~15u;
+constexpr uint32_t TAB_HDR = TAB_Q + 256u;
+constexpr uint32_t DTAB_BYTES = TAB_HDR + 16u;
 
 struct DPlane {
     uint64_t out_off;   // element offset in the device output buffer (tight rows)
@@ -106,7 +120,8 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
     }
     const uint32_t lm = meta[0], dm = meta[1];
     const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
-    // context c: 0..nd-1 dc rows, 5 run, 6..6+nl-1 lvl rows
+    // one thread per model row, in prefix order: dc rows (contexts 0..nd-1),
+    // run (5), level rows (6..6+nl-1)
     const uint32_t nrows = nd + 1u + nl;
     bool ok = true;
     if (t < nrows) {
@@ -114,303 +129,282 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
         if (t < nd) { ctx = t; off = 1u + t * DC_SYMS; n = DC_SYMS; }
         else if (t == nd) { ctx = 5u; off = 1u + nd * DC_SYMS; n = RUN_SYMS; }
         else { ctx = 6u + (t - nd - 1u); off = 1u + nd * DC_SYMS + RUN_SYMS + (t - nd - 1u) * LVL_SYMS; n = LVL_SYMS; }
-        uint16_t* fr = reinterpret_cast<uint16_t*>(tb + (size_t)ctx * CTX_BYTES);
-        uint16_t* cu = fr + 64;
         uint8_t bytes[64];
-        for (uint32_t s = 0; s < n; ++s) { bytes[s] = pay[off + s]; }
+        for (uint32_t k = 0; k < n; ++k) { bytes[k] = pay[off + k]; }
+        uint16_t fr[64], cu[64];
         ok = model_from_bytes(bytes, n, fr, cu);
-        for (uint32_t s = n; s < 64u; ++s) { fr[s] = 0u; cu[s] = 0u; }
+        if (ok) {
+            uint16_t* cd = reinterpret_cast<uint16_t*>(tb + TAB_CUM + (size_t)ctx * CUM_BYTES);
+            for (uint32_t k = 0; k < CUM_LEN; ++k) { cd[k] = k < n ? cu[k] : (uint16_t)4096u; }
+            // bucket b (slots 16b..16b+15) records the symbol holding slot 16b
+            uint32_t* lut = reinterpret_cast<uint32_t*>(tb + TAB_LUT + (size_t)ctx * LUT_BYTES);
+            for (uint32_t sy = 0; sy < n; ++sy) {
+                const uint32_t c0 = cu[sy], c1 = c0 + fr[sy];
+                for (uint32_t bk = (c0 + 15u) >> 4; bk < LUT_BUCKETS && (bk << 4) < c1; ++bk) {
+                    lut[bk] = sy | (c0 << 6) | (c1 << 18);
+                }
+            }
+        }
     }
     if (__any_sync(0xFFFFFFFFu, !ok)) {
         if (t == 0) { status[si] = TCG_ERR_MALFORMED; }
         return;
     }
     // quantiser steps for this slice's effective qp
-    uint32_t* Q = reinterpret_cast<uint32_t*>(tb + MAX_CTX * CTX_BYTES);
+    uint32_t* Q = reinterpret_cast<uint32_t*>(tb + TAB_Q);
     const uint32_t sc = qscale[(P.refined ? 96u : 0u) + S.qp];
     for (uint32_t i = t; i < 64u; i += 32u) {
         const uint32_t q = (uint32_t)((((uint64_t)P.qm[i] * sc) + 128u) >> 8);
         Q[i] = q == 0u ? 1u : q;
     }
     if (t == 0) {
-        uint32_t* hdr = Q + 64;
+        uint32_t* hdr = reinterpret_cast<uint32_t*>(tb + TAB_HDR);
         hdr[0] = lm; hdr[1] = dm; hdr[2] = meta[2];
     }
 }
 
 // ------------------------------------------------------------------ chain
 //
-// One warp decodes one slice. The coder state is warp-uniform; lane j holds the
-// frequency and cumulative start of symbol j (and j+32 for the 64-symbol run
-// alphabet) of every context the slice uses, so a symbol search is one compare
-// per lane and the matching lane's next state is broadcast with a warp OR
-// reduction (exactly one lane matches: the alphabet partitions 0..4095).
-// Stream bytes come through a 64-bit bit window refilled one word at a time
-// from 128-byte chunks that the lanes load one chunk ahead. Error conditions
-// accumulate in a flag and end the slice at the next block boundary: any
-// error conceals the slice, so only whether one occurred matters, and reading
-// past the payload is harmless because it can only add to a consumed-byte
-// count that must end equal to the payload size.
+// One lane per colour slice; a block holds DCH_LANES slices and copies their
+// lookup tables into shared memory. A lane's loop iteration decodes one run
+// symbol, then either a level (run < 63) or, after an end-of-block run, the
+// next block's DC category, and that category's raw suffix: every lane runs
+// the same instruction sequence whatever its slice is doing. Symbol lookup is
+// one shared-memory read of the bucket holding the slot (16 slots per bucket);
+// a slot past the bucket's first symbol walks the cumulative table. Stream
+// bytes arrive through a per-lane 64-bit bit window refilled one aligned word
+// at a time. Error conditions accumulate in a flag that ends the slice: any
+// error conceals it, so only whether one occurred matters, and reading past
+// the payload only grows a consumed-byte count that must end equal to the
+// payload size.
 
-#define FULL_MASK 0xFFFFFFFFu
+constexpr uint32_t DCH_LANES = 8u;      // slices per block
+constexpr uint32_t DCH_LUT_SLOTS = 7u;  // shared-memory bucket tables per slice
+constexpr uint32_t DCH_CUM_BYTES = (MAX_CTX * CUM_BYTES + 15u) & ~15u;
+constexpr uint32_t DCH_LANE_BYTES = DCH_LUT_SLOTS * LUT_BYTES + DCH_CUM_BYTES;
+constexpr uint32_t DCH_SMEM = 64u + DCH_LANES * DCH_LANE_BYTES;
 
-struct Win {
-    uint32_t x;            // coder state
-    uint32_t whi, wlo;     // upcoming stream bits, first bit in the MSB of whi
-    uint32_t wbits;        // valid bits in whi:wlo
-    uint32_t cb;           // stream bytes moved into the state
-    uint32_t cur, nxt;     // lane j: word j of the current / next 128-byte chunk (big-endian)
-    uint32_t k;            // next word of the current chunk
-    const uint32_t* cp;    // aligned start of the chunk after the next one
-    const uint32_t* lim;   // one past the last word that overlaps the payload
+struct DLane {
+    uint32_t x;           // coder state
+    uint32_t whi, wlo;    // upcoming stream bits, first bit in the MSB of whi
+    uint32_t wbits;       // valid bits in whi:wlo
+    uint32_t nxt;         // next stream word (memory byte order)
+    uint32_t cb;          // stream bytes moved into the state
+    const uint32_t* wp;   // address of nxt
+    const uint32_t* wlim; // one past the last word that overlaps the payload
 };
 
-__device__ __forceinline__ uint32_t win_load(const uint32_t* p, const uint32_t* lim)
+// keep at least 32 bits in the window (branch-free: every lane runs the same
+// instructions; only the loads are predicated). Entering a new 128-byte line
+// of the stream prefetches the line 256 bytes ahead into L1, so word loads
+// hit L1 instead of stalling the warp on DRAM.
+__device__ __forceinline__ void dl_refill(DLane& L)
 {
-    return p < lim ? __byte_perm(__ldg(p), 0u, 0x0123u) : 0u;
+    const bool need = L.wbits < 32u;
+    const uint32_t w = __byte_perm(L.nxt, 0u, 0x0123u);
+    const uint32_t sh = L.wbits & 31u;
+    L.whi |= need ? (w >> sh) : 0u;
+    L.wlo |= need ? (w << ((32u - sh) & 31u)) : 0u;
+    L.wbits += need ? 32u : 0u;
+    L.wp += need ? 1 : 0;
+    const bool ld = need && L.wp < L.wlim;
+    uint32_t v = L.nxt;
+    if (ld) { v = __ldg(L.wp); }
+    L.nxt = v;
+    const uint32_t pf = (uint32_t)(ld && (((uintptr_t)L.wp & 127u) == 0u) && (L.wp + 64 < L.wlim));
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
+                 :: "l"(L.wp + 64), "r"(pf));
 }
 
-__device__ __forceinline__ uint32_t win_take(Win& w, uint32_t lane)
-{
-    const uint32_t word = __shfl_sync(FULL_MASK, w.cur, w.k);
-    w.k += 1u;
-    if (w.k == 32u) {
-        w.k = 0u;
-        w.cur = w.nxt;
-        w.nxt = win_load(w.cp + lane, w.lim);
-        w.cp += 32;
-    }
-    return word;
-}
-
-// keep at least 32 bits in the window (called after every renormalisation,
-// which consumes at most 24)
-__device__ __forceinline__ void win_refill(Win& w, uint32_t lane)
-{
-    if (w.wbits < 32u) {
-        const uint32_t word = win_take(w, lane);
-        w.whi |= word >> w.wbits;
-        w.wlo |= word << (32u - w.wbits);
-        w.wbits += 32u;
-    }
-}
-
-// state <- xn followed by as many stream bytes as bring it to [2^23, ...)
-__device__ __forceinline__ void win_renorm(Win& w, uint32_t xn, uint32_t lane)
+__device__ __forceinline__ void dl_renorm(DLane& L, uint32_t xn)
 {
     const bool c1 = xn < RANS_L, c2 = xn < (RANS_L >> 8), c3 = xn < (RANS_L >> 16);
-    const uint32_t x8 = __funnelshift_l(w.whi, xn, 8);
-    const uint32_t x16 = __funnelshift_l(w.whi, xn, 16);
-    const uint32_t x24 = __funnelshift_l(w.whi, xn, 24);
-    w.x = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : xn);
+    const uint32_t x8 = __funnelshift_l(L.whi, xn, 8);
+    const uint32_t x16 = __funnelshift_l(L.whi, xn, 16);
+    const uint32_t x24 = __funnelshift_l(L.whi, xn, 24);
+    L.x = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : xn);
     const uint32_t n8 = c2 ? (c3 ? 24u : 16u) : (c1 ? 8u : 0u);
-    w.whi = __funnelshift_l(w.wlo, w.whi, n8);
-    w.wlo <<= n8;
-    w.wbits -= n8;
-    w.cb += n8 >> 3;
-    win_refill(w, lane);
+    L.whi = __funnelshift_l(L.wlo, L.whi, n8);
+    L.wlo <<= n8;
+    L.wbits -= n8;
+    L.cb += n8 >> 3;
+    dl_refill(L);
 }
 
-__device__ __forceinline__ void win_init(Win& w, const uint8_t* b, uint32_t n, uint32_t lane)
+__device__ __forceinline__ void dl_init(DLane& L, const uint8_t* b, uint32_t n)
 {
     const uintptr_t a = (uintptr_t)b;
-    const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)127);
-    w.lim = reinterpret_cast<const uint32_t*>((a + n + 3u) & ~(uintptr_t)3);
-    w.cur = win_load(base + lane, w.lim);
-    w.nxt = win_load(base + 32 + lane, w.lim);
-    w.cp = base + 64;
-    const uint32_t off = (uint32_t)(a & 127u);
-    w.k = off >> 2;
-    const uint32_t a8 = (off & 3u) * 8u;
-    const uint32_t w0 = win_take(w, lane);
-    const uint32_t w1 = win_take(w, lane);
-    w.x = __funnelshift_l(w1, w0, a8);  // first four payload bytes, big-endian
-    w.whi = w1 << a8;
-    w.wlo = 0u;
-    w.wbits = 32u - a8;
-    w.cb = 4u;
-    win_refill(w, lane);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)3);
+    L.wlim = reinterpret_cast<const uint32_t*>((a + n + 3u) & ~(uintptr_t)3);
+    const uint32_t a8 = (uint32_t)(a & 3u) * 8u;
+    const uint32_t w0 = __byte_perm(__ldg(w), 0u, 0x0123u);
+    const uint32_t w1 = w + 1 < L.wlim ? __byte_perm(__ldg(w + 1), 0u, 0x0123u) : 0u;
+    L.x = __funnelshift_l(w1, w0, a8);  // first four payload bytes, big-endian
+    L.whi = w1 << a8;
+    L.wlo = 0u;
+    L.wbits = 32u - a8;
+    L.cb = 4u;
+    L.wp = w + 2;
+    L.nxt = L.wp < L.wlim ? __ldg(L.wp) : 0u;
+    dl_refill(L);
 }
 
-// one symbol of an alphabet of at most 32 (lane j holds symbol j)
-__device__ __forceinline__ uint32_t dec_sym32(Win& w, uint32_t f, uint32_t c, uint32_t lane)
+// One symbol: through the bucket table when use_lut, otherwise by walking the
+// cumulative table from symbol 0. Both pointers always address valid tables.
+__device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool use_lut, const uint16_t* cum)
 {
-    const uint32_t x = w.x;
-    const uint32_t d = (x & 4095u) - c;
-    const bool in = d < f;
-    const uint32_t xn = f * (x >> 12) + d;
-    const uint32_t xv = __reduce_or_sync(FULL_MASK, in ? xn : 0u);
-    const uint32_t s = __reduce_or_sync(FULL_MASK, in ? lane : 0u);
-    win_renorm(w, xv, lane);
+    const uint32_t x = L.x, slot = x & 4095u;
+    const uint32_t e = use_lut ? lut[slot >> 4] : ((uint32_t)cum[1] << 18);
+    uint32_t s = e & 63u, c0 = (e >> 6) & 0xFFFu, c1 = e >> 18;
+    while (slot >= c1 && s < CUM_LEN - 2u) {
+        ++s;
+        c0 = c1;
+        c1 = cum[s + 1u];
+    }
+    dl_renorm(L, (c1 - c0) * (x >> 12) + slot - c0);
     return s;
 }
 
-// one symbol of a 64-symbol alphabet (lane j holds symbols j and j+32)
-__device__ __forceinline__ uint32_t dec_sym64(Win& w, uint32_t fa, uint32_t ca, uint32_t fb, uint32_t cb,
-                                              uint32_t lane)
+// raw chunk of w bits (w <= 23; 0 leaves the state unchanged)
+__device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
 {
-    const uint32_t x = w.x;
-    const uint32_t slot = x & 4095u, xs = x >> 12;
-    const uint32_t da = slot - ca, db = slot - cb;
-    const bool ia = da < fa, ib = db < fb;
-    const uint32_t v = ia ? fa * xs + da : (ib ? fb * xs + db : 0u);
-    const uint32_t xv = __reduce_or_sync(FULL_MASK, v);
-    const uint32_t s = __reduce_or_sync(FULL_MASK, ia ? lane : (ib ? lane + 32u : 0u));
-    win_renorm(w, xv, lane);
-    return s;
-}
-
-// raw chunk of wd bits (wd <= 23)
-__device__ __forceinline__ uint32_t dec_chunk(Win& w, uint32_t wd, uint32_t lane)
-{
-    const uint32_t v = w.x & ~(0xFFFFFFFFu << wd);
-    win_renorm(w, w.x >> wd, lane);
+    const uint32_t v = L.x & ~(0xFFFFFFFFu << w);
+    dl_renorm(L, L.x >> w);
     return v;
 }
 
 // category suffix: m = 2^(cat-1) | (cat-1 raw bits), split 16 + rest above 23
-__device__ __forceinline__ uint32_t dec_suffix(Win& w, uint32_t cat, uint32_t lane)
+__device__ __forceinline__ uint32_t dl_suffix(DLane& L, uint32_t cat)
 {
     const uint32_t b = cat > 1u ? cat - 1u : 0u;
     uint32_t v;
     if (b <= 23u) {
-        v = dec_chunk(w, b, lane);
+        v = dl_chunk(L, b);
     } else {
-        const uint32_t lo = dec_chunk(w, 16u, lane);
-        v = (dec_chunk(w, b - 16u, lane) << 16) | lo;
+        const uint32_t lo = dl_chunk(L, 16u);
+        const uint32_t w2 = b - 16u;
+        v = (dl_chunk(L, w2 <= 23u ? w2 : 23u) << 16) | lo;
     }
-    return cat == 0u ? 0u : (1u << (cat - 1u)) | v;
+    return cat == 0u ? 0u : (1u << ((cat - 1u) & 31u)) | v;
 }
 
-template <uint32_t LM, uint32_t DM>
-__device__ __forceinline__ int32_t dchain_slice(const DSlice& S, const DPlane& P, const uint8_t* __restrict__ tb,
-                                                const uint8_t* __restrict__ stream, uint32_t nbytes,
-                                                int32_t* __restrict__ coef, int32_t* __restrict__ rows)
-{
-    const uint32_t lane = threadIdx.x & 31u;
-    // per-lane model entries
-    constexpr uint32_t ND = DM ? 5u : 1u;
-    constexpr uint32_t NL = LM == 1u ? 4u : (LM == 2u ? 5u : 1u);
-    uint32_t dcf[ND], dcc[ND], lvf[NL], lvc[NL];
-    auto ent = [&](uint32_t ctx, uint32_t s, uint32_t& f, uint32_t& c) {
-        const uint16_t* fr = reinterpret_cast<const uint16_t*>(tb + (size_t)ctx * CTX_BYTES);
-        f = fr[s];
-        c = fr[64 + s];
-    };
-#pragma unroll
-    for (uint32_t i = 0; i < ND; ++i) { ent(i, lane, dcf[i], dcc[i]); }
-#pragma unroll
-    for (uint32_t i = 0; i < NL; ++i) { ent(6u + i, lane, lvf[i], lvc[i]); }
-    uint32_t rfa, rca, rfb, rcb;
-    ent(5u, lane, rfa, rca);
-    ent(5u, lane + 32u, rfb, rcb);
-
-    Win w;
-    win_init(w, stream, nbytes, lane);
-    uint32_t err = w.x < RANS_L ? 1u : 0u;
-    const bool wide = P.bd > 12u;
-    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
-    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
-    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
-    int32_t* prow = rows;
-    int32_t* crow = rows + S.cols;
-    uint32_t prev_dcc = 0;
-    bool first = true;
-    for (uint32_t by = 0; by < S.bh && err == 0u; ++by) {
-        int32_t left = 0;
-        for (uint32_t bx = 0; bx < S.cols; ++bx) {
-            // DC
-            uint32_t f0 = dcf[0], c0 = dcc[0];
-            if (DM) {
-                const uint32_t dctx = first ? 0u : dcp_ctx(prev_dcc, true);
-#pragma unroll
-                for (uint32_t i = 1; i < ND; ++i) {
-                    f0 = dctx == i ? dcf[i] : f0;
-                    c0 = dctx == i ? dcc[i] : c0;
-                }
-            }
-            const int32_t top = by != 0u ? prow[bx] : 0;
-            const uint32_t dcat = dec_sym32(w, f0, c0, lane);
-            const uint32_t dmv = dec_suffix(w, dcat, lane);
-            err |= dmv > mdc ? 1u : 0u;
-            const int32_t pred = dc_pred(bx != 0u, left, by != 0u, top);
-            const int64_t dcv = (int64_t)pred + unmap_s(dmv);
-            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
-            left = (int32_t)dcv;
-            if (lane == 0u) { crow[bx] = left; }
-            prev_dcc = dcat;
-            first = false;
-            int32_t clo = lane == 0u ? left : 0, chi = 0;
-            // AC: (run, level, suffix) until the end-of-block run symbol
-            uint32_t pos = 1u, pcat = 0u;
-            bool has = false;
-            for (;;) {
-                const uint32_t r = dec_sym64(w, rfa, rca, rfb, rcb, lane);
-                const uint32_t idx = pos + r;
-                if (r == 63u || idx > 63u) {
-                    err |= r != 63u ? 1u : 0u;
-                    break;
-                }
-                uint32_t fl = lvf[0], cl = lvc[0];
-                if (LM != 0u) {
-                    const uint32_t lc = LM == 1u ? pos_ctx(idx) : prev_ctx(pcat, has);
-#pragma unroll
-                    for (uint32_t i = 1; i < NL; ++i) {
-                        fl = lc == i ? lvf[i] : fl;
-                        cl = lc == i ? lvc[i] : cl;
-                    }
-                }
-                const uint32_t cat = dec_sym32(w, fl, cl, lane);
-                const uint32_t m = dec_suffix(w, cat, lane);
-                err |= m > mlv ? 1u : 0u;
-                const uint32_t nat = c_zigzag[idx];
-                const int32_t v = unmap_s(m);
-                if ((nat & 31u) == lane) {
-                    if (nat & 32u) { chi = v; } else { clo = v; }
-                }
-                pcat = cat;
-                has = true;
-                pos = idx + 1u;
-            }
-            int32_t* blk = coef + (size_t)(S.blk0 + by * S.cols + bx) * 64u;
-            blk[lane] = clo;
-            blk[32u + lane] = chi;
-            if (err != 0u) { break; }
-        }
-        __syncwarp();
-        int32_t* sw = prow; prow = crow; crow = sw;
-    }
-    if (err == 0u && w.cb != nbytes) { err = 1u; }
-    return err != 0u ? TCG_ERR_MALFORMED : 0;
-}
-
-// One warp per colour slice (one warp per block, so every slice of a batch is
-// resident at once); dynamic shared memory holds two DC rows of the slice.
-__global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+__global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices, const uint32_t* __restrict__ order,
+                                               uint32_t nc, const uint32_t* __restrict__ slice_tab,
                                                const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
                                                const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
                                                int32_t* __restrict__ status)
 {
-    extern __shared__ __align__(16) int32_t rows[];
-    const uint32_t si = cslices[blockIdx.x];
+    extern __shared__ __align__(16) uint8_t dsm[];
+    uint8_t* zz = dsm;  // zigzag order, shared by the lanes
+    const uint32_t t = threadIdx.x;
+    zz[t] = c_zigzag[t];
+    zz[t + 32u] = c_zigzag[t + 32u];
+    // stage every lane's tables: run and level contexts always, DC contexts when they fit
+    const uint32_t i0 = blockIdx.x * DCH_LANES;
+    for (uint32_t l = 0; l < DCH_LANES && i0 + l < nc; ++l) {
+        const uint32_t sl = order[i0 + l];
+        if (status[sl] != 0) { continue; }
+        const uint8_t* tb = tabs + (size_t)slice_tab[sl] * DTAB_BYTES;
+        const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
+        const uint32_t lm = hdr[0], dm = hdr[1];
+        const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u, nd = dm ? DCP_CTX : 1u;
+        const uint32_t ndl = 1u + nl + nd <= DCH_LUT_SLOTS ? nd : 0u;
+        uint8_t* ls = dsm + 64u + (size_t)l * DCH_LANE_BYTES;
+        const uint32_t nlut = 1u + nl + ndl;
+        for (uint32_t k = t; k < nlut * (LUT_BYTES / 16u); k += 32u) {
+            const uint32_t slot = k / (LUT_BYTES / 16u), part = k % (LUT_BYTES / 16u);
+            const uint32_t ctx = slot == 0u ? 5u : (slot <= nl ? 6u + (slot - 1u) : slot - 1u - nl);
+            reinterpret_cast<uint4*>(ls + (size_t)slot * LUT_BYTES)[part] =
+                reinterpret_cast<const uint4*>(tb + TAB_LUT + (size_t)ctx * LUT_BYTES)[part];
+        }
+        for (uint32_t k = t; k < DCH_CUM_BYTES / 16u; k += 32u) {
+            reinterpret_cast<uint4*>(ls + DCH_LUT_SLOTS * LUT_BYTES)[k] = reinterpret_cast<const uint4*>(tb + TAB_CUM)[k];
+        }
+    }
+    __syncthreads();
+    if (t >= DCH_LANES || i0 + t >= nc) { return; }
+    const uint32_t si = order[i0 + t];
     if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
-    const uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
-    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + MAX_CTX * CTX_BYTES) + 64;
+    const uint8_t* tb = tabs + (size_t)slice_tab[si] * DTAB_BYTES;
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
     const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
-    const uint8_t* stream = pkt + S.pay + plen;
-    const uint32_t nb = S.size - plen;
-    int32_t rc;
-    switch (lm * 2u + dm) {
-    case 0: rc = dchain_slice<0, 0>(S, P, tb, stream, nb, coef, rows); break;
-    case 1: rc = dchain_slice<0, 1>(S, P, tb, stream, nb, coef, rows); break;
-    case 2: rc = dchain_slice<1, 0>(S, P, tb, stream, nb, coef, rows); break;
-    case 3: rc = dchain_slice<1, 1>(S, P, tb, stream, nb, coef, rows); break;
-    case 4: rc = dchain_slice<2, 0>(S, P, tb, stream, nb, coef, rows); break;
-    default: rc = dchain_slice<2, 1>(S, P, tb, stream, nb, coef, rows); break;
+    const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u, nd = dm ? DCP_CTX : 1u;
+    const bool dc_lut = 1u + nl + nd <= DCH_LUT_SLOTS;
+    const uint8_t* ls = dsm + 64u + (size_t)t * DCH_LANE_BYTES;
+    const uint32_t* lut_run = reinterpret_cast<const uint32_t*>(ls);
+    const uint32_t* lut_lvl = lut_run + LUT_BUCKETS;                               // + ctx * LUT_BUCKETS
+    const uint32_t* lut_dc = dc_lut ? lut_lvl + nl * LUT_BUCKETS : lut_run;      // + ctx * LUT_BUCKETS when dc_lut
+    const uint16_t* cums = reinterpret_cast<const uint16_t*>(ls + DCH_LUT_SLOTS * LUT_BYTES);
+    const uint16_t* cum_run = cums + 5u * CUM_LEN;
+    const uint16_t* cum_lvl = cums + 6u * CUM_LEN;
+    const uint16_t* cum_dc = cums;
+
+    const uint32_t nbytes = S.size - plen;
+    DLane L;
+    dl_init(L, pkt + S.pay + plen, nbytes);
+    uint32_t err = L.x < RANS_L ? 1u : 0u;
+    const bool wide = P.bd > 12u;
+    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
+    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
+    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
+    const uint32_t cols = S.cols, nblk = S.nblk;
+    int32_t* blk = coef + (size_t)S.blk0 * 64u;
+
+    // first block's DC (no left, no top, context 0)
+    uint32_t dcat = dl_sym(L, lut_dc, dc_lut, cum_dc);
+    uint32_t m = dl_suffix(L, dcat);
+    err |= m > mdc ? 1u : 0u;
+    int64_t dcv = unmap_s(m);
+    err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+    int32_t left = (int32_t)dcv;
+    blk[0] = left;
+    // DC of the block above the next block, loaded one block ahead of its use
+    int32_t top_next = (1u < nblk && 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
+    uint32_t prev_dcc = dcat;
+    uint32_t b = 0, bx = 0;  // current block within the slice, its column
+    uint32_t pos = 1u, pcat = 0u;
+    bool has = false;
+    while (err == 0u) {
+        const uint32_t r = dl_sym(L, lut_run, true, cum_run);
+        const bool eob = r == 63u;
+        const uint32_t idx = pos + r;
+        if (!eob && idx > 63u) { err = 1u; break; }
+        if (eob && b + 1u >= nblk) { break; }  // last block done
+        // second symbol: the level (context by position or previous level) or the next block's DC
+        const uint32_t lc = lm == 1u ? pos_ctx(idx & 63u) : (lm == 2u ? prev_ctx(pcat, has) : 0u);
+        const uint32_t dctx = dm ? dcp_ctx(prev_dcc, true) : 0u;
+        const uint32_t* lut = eob ? (dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run) : lut_lvl + lc * LUT_BUCKETS;
+        const uint16_t* cum = eob ? cum_dc + dctx * CUM_LEN : cum_lvl + lc * CUM_LEN;
+        const bool use_lut = !eob || dc_lut;
+        const uint32_t cat = dl_sym(L, lut, use_lut, cum);
+        m = dl_suffix(L, cat);
+        if (!eob) {
+            err |= m > mlv ? 1u : 0u;
+            blk[zz[idx]] = unmap_s(m);
+            pcat = cat;
+            has = true;
+            pos = idx + 1u;
+        } else {
+            ++b;
+            blk += 64;
+            bx = bx + 1u == cols ? 0u : bx + 1u;
+            const bool ht = b >= cols;
+            err |= m > mdc ? 1u : 0u;
+            dcv = (int64_t)dc_pred(bx != 0u, left, ht, top_next) + unmap_s(m);
+            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+            left = (int32_t)dcv;
+            blk[0] = left;
+            top_next = (b + 1u < nblk && b + 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
+            prev_dcc = cat;
+            pos = 1u;
+            pcat = 0u;
+            has = false;
+        }
     }
-    if (threadIdx.x == 0) { status[si] = rc; }
+    if (err == 0u && L.cb != nbytes) { err = 1u; }
+    status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
 // ------------------------------------------------------------------ reconstruction
@@ -427,7 +421,7 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
     if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
-    const uint32_t* Q = reinterpret_cast<const uint32_t*>(tabs + (size_t)slice_tab[si] * DTAB_BYTES + MAX_CTX * CTX_BYTES);
+    const uint32_t* Q = reinterpret_cast<const uint32_t*>(tabs + (size_t)slice_tab[si] * DTAB_BYTES + TAB_Q);
     const uint32_t lb = gb - S.blk0;
     const uint32_t bx = lb % S.cols, by = S.y0 + lb / S.cols;
     const int64_t fc = P.bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (P.bd - 1u)) - 1u)) / 2047;
@@ -705,7 +699,6 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     std::vector<uint64_t> pkt_off(count, 0);
     std::vector<uint32_t> frame_slice0(count, 0);
     uint64_t out_elems = 0, pkt_bytes = 0, nblk = 0, alpha_res = 0;
-    uint32_t max_cols = 1;
     for (uint32_t f = 0; f < count; ++f) {
         const tcg_dec_frame& F = frames[f];
         frame_slice0[f] = (uint32_t)slices.size();
@@ -728,7 +721,6 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             P.frame = f;
             memcpy(P.qm, F.qm[p], sizeof(P.qm));
             if (P.kind == TCG_PLANE_COLOR) { nblk += (uint64_t)P.cols * P.rows; }
-            max_cols = P.cols > max_cols ? P.cols : max_cols;
             planes.push_back(P);
             if (F.deblock && p < 3u) {
                 const uint32_t w = P.vis_w, h = P.vis_h;
@@ -774,7 +766,8 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const uint32_t ns = (uint32_t)slices.size(), nc = (uint32_t)cslices.size(), na = (uint32_t)aslices.size();
     const size_t desc = align_up(planes.size() * sizeof(DPlane), 256) + align_up(ns * sizeof(DSlice), 256) +
                         align_up((size_t)(nc + na) * 4u + 16, 256) + align_up((size_t)ns * 4u + 16, 256) +
-                        align_up((size_t)nblk * 4u + 16, 256) + align_up(dbp.size() * sizeof(DbPlane) + 16, 256);
+                        align_up((size_t)nblk * 4u + 16, 256) + align_up(dbp.size() * sizeof(DbPlane) + 16, 256) +
+                        align_up((size_t)nc * 4u + 16, 256);
     if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
         !dreserve(C, B_DEC_TAB, (size_t)nc * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
         !dreserve(C, B_DEC_RES, (size_t)ns * 4u + 256) || !dreserve(C, B_ALPHA, alpha_res * 4u + 256) ||
@@ -793,12 +786,16 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     };
     std::vector<uint32_t> cs_as(cslices);
     cs_as.insert(cs_as.end(), aslices.begin(), aslices.end());
+    // chain lanes: largest slices first so a block's lanes finish together
+    std::vector<uint32_t> ord(cslices);
+    std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return slices[a].nblk > slices[b].nblk; });
     const size_t o_pl = put(planes.data(), planes.size() * sizeof(DPlane));
     const size_t o_sl = put(slices.data(), ns * sizeof(DSlice));
     const size_t o_ca = put(cs_as.data(), cs_as.size() * 4u);
     const size_t o_st = put(slice_tab.data(), slice_tab.size() * 4u);
     const size_t o_bs = put(blk_slice.data(), blk_slice.size() * 4u);
     const size_t o_db = put(dbp.data(), dbp.size() * sizeof(DbPlane));
+    const size_t o_or = put(ord.data(), ord.size() * 4u);
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
     const DPlane* d_pl = (const DPlane*)(dd + o_pl);
     const DSlice* d_sl = (const DSlice*)(dd + o_sl);
@@ -807,6 +804,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const uint32_t* d_st = (const uint32_t*)(dd + o_st);
     const uint32_t* d_bs = (const uint32_t*)(dd + o_bs);
     const DbPlane* d_db = (const DbPlane*)(dd + o_db);
+    const uint32_t* d_ord = (const uint32_t*)(dd + o_or);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
     call_begin(C);
     for (uint32_t f = 0; f < count; ++f) {
@@ -825,13 +823,14 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     }
     if (nc > 0) {
         TCG_LAUNCH(C, K_DTABLES, k_dtables, nc, 32, 0, d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
-        const size_t smem = (size_t)max_cols * 8u;
-        static size_t attr = 0;
-        if (smem > attr) {
-            cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            attr = smem;
+        static bool attr = false;
+        if (!attr) {
+            TCG_CHECK(cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DCH_SMEM));
+            attr = true;
         }
-        TCG_LAUNCH(C, K_DCHAIN, k_dchain, nc, 32, smem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
+        TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+        TCG_LAUNCH(C, K_DCHAIN, k_dchain, (nc + DCH_LANES - 1u) / DCH_LANES, 32, DCH_SMEM, d_sl, d_ord, nc, d_st, d_pl,
+                   d_pkt, d_tab, d_coef, d_status);
         TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_bs, d_st, d_pl, d_tab, d_coef,
                    d_status, (uint32_t)nblk, d_out);
     }

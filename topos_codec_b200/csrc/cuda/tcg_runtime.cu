@@ -1,4 +1,5 @@
 // tcg_runtime.cu - device init, context leases, frozen tables.
+#include <stdlib.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -24,6 +25,15 @@ static const char* k_names[K_COUNT] = {
     "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk"};
 
 void note_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+bool sync_each()
+{
+    static const bool on = [] {
+        const char* v = getenv("TCG_SYNC_EACH");
+        return v != nullptr && v[0] == '1';
+    }();
+    return on;
+}
 
 void call_begin(Ctx* c)
 {

@@ -70,12 +70,20 @@ void call_end(Ctx* c);  // after the stream was synchronised
 void kern_begin(Ctx* c, int id);
 void kern_end(Ctx* c);
 
+// Launch on the context's stream. With TCG_SYNC_EACH=1 in the environment
+// every launch is followed by a stream synchronisation, so a failing kernel is
+// named in the error instead of surfacing at a later call (diagnostics only).
 #define TCG_LAUNCH(C, id, kern, grid, block, smem, ...)                 \
     do {                                                                 \
         tcg::kern_begin((C), (id));                                      \
         kern<<<(grid), (block), (smem), (C)->stream>>>(__VA_ARGS__);     \
         tcg::kern_end((C));                                              \
         tcg::note_launch(1);                                             \
+        if (tcg::sync_each()) {                                          \
+            cudaError_t le_ = cudaGetLastError();                        \
+            if (le_ == cudaSuccess) { le_ = cudaStreamSynchronize((C)->stream); } \
+            if (le_ != cudaSuccess) { return tcg::cuda_fail(le_, #kern); } \
+        }                                                                \
     } while (0)
 
 // Lease a context (creates one when none is free). Thread-safe.
@@ -101,6 +109,8 @@ const DevTables& tables();
 
 bool ensure_init();
 void note_launch(uint32_t n = 1);
+// true when TCG_SYNC_EACH=1 was set in the environment at first use
+bool sync_each();
 
 // CUDA error -> host status + thread-local detail.
 int32_t cuda_fail(cudaError_t e, const char* what);
