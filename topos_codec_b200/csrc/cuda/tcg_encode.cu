@@ -355,52 +355,79 @@ __device__ __forceinline__ void put_suffix_ops(uint32_t*& o, uint32_t cat, uint3
     *o++ = op_chunk(b, m);
 }
 
+// One warp per 8x8 block: lane j owns zigzag positions j and j+32. The block's
+// operations are, in coding order, the end-of-block run, then for every
+// non-zero AC position from the highest down its suffix chunk(s), level and
+// run, then the DC suffix and DC category; a warp suffix-sum over positions
+// gives each lane the offset of its positions' operations, so the block's
+// words are written by neighbouring lanes.
 __global__ void __launch_bounds__(256) k_opgen(const EWork* __restrict__ work, const ESlice* __restrict__ slices,
                                                const int32_t* __restrict__ coef, const uint64_t* __restrict__ mask,
                                                const uint32_t* __restrict__ dcm, const uint32_t* __restrict__ opoff,
-                                               const uint32_t* __restrict__ stab, const ESliceRes* __restrict__ sres,
-                                               uint32_t* __restrict__ ops)
+                                               const ESliceRes* __restrict__ sres, uint32_t* __restrict__ ops)
 {
+    __shared__ uint8_t cats[8][64];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const EWork w = work[blockIdx.x];
-    if (threadIdx.x >= w.n) { return; }
+    const uint32_t k = blockIdx.y * 8u + warp;
+    if (k >= w.n) { return; }  // whole warp
     const ESlice& S = slices[w.slice];
-    const uint32_t lb = w.lb0 + threadIdx.x;
+    const uint32_t lb = w.lb0 + k;
     const uint32_t gb = S.blk0 + lb;
     const uint32_t pl = sres[w.slice].plen;
     const uint32_t lmod = (pl >> 16) & 3u, dmod = (pl >> 20) & 1u;
     uint32_t* o = ops + S.op_base + opoff[gb];
     const int32_t* c = coef + (size_t)gb * 64u;
-    *o++ = op_sym(T_RUN + 63u);  // EOB
-    uint64_t m = mask[gb];
-    // walk non-zero positions from the highest down; the forward-order
-    // neighbour of position p is the next lower set bit (or the DC at 0)
-    while (m != 0u) {
-        const uint32_t p = 63u - (uint32_t)__clzll((long long)m);
-        m &= ~((uint64_t)1 << p);
-        const uint32_t below = m != 0u ? 63u - (uint32_t)__clzll((long long)m) : 0u;
-        const uint32_t lv = map_s(c[p]);
-        const uint32_t lmv = lv > 0x07FFFFFFu ? 0x07FFFFFFu : lv;
-        const uint32_t cat = bitlen32(lmv);
-        put_suffix_ops(o, cat, lmv);
+    const uint64_t m = mask[gb];  // AC positions only (bit 0 clear)
+    uint32_t lmv[2], cat[2], cnt[2];
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        const uint32_t p = lane + 32u * h;
+        const bool nz = ((m >> p) & 1u) != 0u;
+        const uint32_t lv = nz ? map_s(c[p]) : 0u;
+        lmv[h] = lv > 0x07FFFFFFu ? 0x07FFFFFFu : lv;
+        cat[h] = nz ? bitlen32(lmv[h]) : 0u;
+        cnt[h] = nz ? 2u + suffix_chunks(cat[h]) : 0u;
+        cats[warp][p] = (uint8_t)cat[h];
+    }
+    // operations of the positions above each of this lane's two positions
+    const uint32_t packed = cnt[0] | (cnt[1] << 16);
+    uint32_t incl = packed;
+#pragma unroll
+    for (uint32_t d = 1; d < 32u; d <<= 1) {
+        const uint32_t t = __shfl_down_sync(0xFFFFFFFFu, incl, d);
+        if (lane + d < 32u) { incl += t; }
+    }
+    const uint32_t above = incl - packed;
+    const uint32_t all = __shfl_sync(0xFFFFFFFFu, incl, 0);
+    const uint32_t hi_total = all >> 16, total = (all & 0xFFFFu) + hi_total;
+    __syncwarp();
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        if (cnt[h] == 0u) { continue; }
+        const uint32_t p = lane + 32u * h;
+        uint32_t* q = o + 1u + (h ? (above >> 16) : hi_total + (above & 0xFFFFu));
+        const uint64_t lower = m & ((1ull << p) - 1ull);
+        const uint32_t below = lower != 0u ? 63u - (uint32_t)__clzll((long long)lower) : 0u;
+        put_suffix_ops(q, cat[h], lmv[h]);
         uint32_t ctx = 0u;
         if (lmod == 1u) {
             ctx = pos_ctx(p);
         } else if (lmod == 2u) {
-            uint32_t pc = 0u;
-            if (m != 0u) {
-                const uint32_t pv = map_s(c[below]);
-                pc = bitlen32(pv > 0x07FFFFFFu ? 0x07FFFFFFu : pv);
-            }
-            ctx = prev_ctx(pc, m != 0u);
+            ctx = prev_ctx(lower != 0u ? cats[warp][below] : 0u, lower != 0u);
         }
-        *o++ = op_sym(T_LVL + ctx * LVL_SYMS + cat);
-        *o++ = op_sym(T_RUN + (p - below - 1u));
+        *q++ = op_sym(T_LVL + ctx * LVL_SYMS + cat[h]);
+        *q = op_sym(T_RUN + (p - below - 1u));
     }
-    const uint32_t dm = dcm[gb];
-    const uint32_t ds = bitlen32(dm);
-    put_suffix_ops(o, ds, dm);
-    const uint32_t dctx = dmod ? dcp_ctx(lb > 0u ? bitlen32(dcm[gb - 1u]) : 0u, lb > 0u) : 0u;
-    *o++ = op_sym(T_DC + dctx * DC_SYMS + ds);
+    if (lane == 0u) {
+        o[0] = op_sym(T_RUN + 63u);  // EOB
+        uint32_t* q = o + 1u + total;
+        const uint32_t dm = dcm[gb];
+        const uint32_t ds = bitlen32(dm);
+        put_suffix_ops(q, ds, dm);
+        const uint32_t dctx = dmod ? dcp_ctx(lb > 0u ? bitlen32(dcm[gb - 1u]) : 0u, lb > 0u) : 0u;
+        *q = op_sym(T_DC + dctx * DC_SYMS + ds);
+    }
 }
 
 // =============================== rANS chains ===============================
@@ -500,6 +527,10 @@ __global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict_
     uint4 a = op_group(op4, 0u, nops), b = op_group(op4, 1u, nops);
     uint4 c = op_group(op4, 2u, nops), d = op_group(op4, 3u, nops);
     for (uint32_t g = 0; 4u * g < nops; g += 4u) {
+        // bring the operation words 256 bytes ahead into L1 so the group loads below hit it
+        const uint32_t pf = (uint32_t)(4u * (g + 16u) < nops);
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
+                     :: "l"(op4 + g + 16u), "r"(pf));
         ENC_GROUP(a);
         a = op_group(op4, g + 4u, nops);
         ENC_GROUP(b);
@@ -1032,8 +1063,8 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
                    d_hist, d_sres);
         TCG_LAUNCH(C, K_SELECT, k_select, nc, 32, 0, d_sl, d_cs, d_hist, T.log2, d_stab, d_prefix, d_sres);
         TCG_LAUNCH(C, K_OPSCAN, k_opscan, nc, 1024, 0, d_sl, d_cs, d_nops, d_opoff, d_sres);
-        TCG_LAUNCH(C, K_OPGEN, k_opgen, (uint32_t)work.size(), 256, 0, d_wk, d_sl, d_coef, d_mask, d_dcm, d_opoff, d_stab,
-                   d_sres, d_ops);
+        TCG_LAUNCH(C, K_OPGEN, k_opgen, dim3((uint32_t)work.size(), 32), 256, 0, d_wk, d_sl, d_coef, d_mask, d_dcm,
+                   d_opoff, d_sres, d_ops);
         static bool chain_attr = false;
         if (!chain_attr) {
             cudaFuncSetAttribute(k_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CHAIN_SMEM);
