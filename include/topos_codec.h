@@ -290,6 +290,13 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
 int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                       topos_frame_output* infos);
 
+/* Decode-chain tiling chosen for batches of the given number of colour slices:
+ * 0 = one lane per slice (eight slices per warp), 1 = one warp per slice,
+ * -1 = not chosen yet. The first batch of each size class (log2 of the slice
+ * count) times both tilings and keeps the faster; the environment variable
+ * TCG_DCHAIN=lane|warp overrides the choice. Both produce identical output. */
+int32_t tcg_dchain_tiling(uint32_t colour_slices);
+
 /* Device selection and teardown for the calling process. tcg_device_init is
  * implicit on first use (device 0 or the current CUDA device). */
 int32_t tcg_device_init(int32_t device);

@@ -195,3 +195,36 @@ def test_strided_io_and_buffer_too_small(product):
     assert product.encode(cfg, padded) == tight
     rc, pkt, st = product.encode_status(cfg, planes, out_cap=len(tight) - 1)
     assert rc == B.TC_ERR_BUFFER_TOO_SMALL and st.packet_size == len(tight)
+
+
+@pytest.mark.parametrize("tiling", ["lane", "warp"])
+def test_decode_tilings_vs_oracle(product, oracle, monkeypatch, tiling):
+    """Both decode-chain tilings (lane per slice, warp per slice) decode random
+    configurations and damaged packets exactly like the oracle."""
+    monkeypatch.setenv("TCG_DCHAIN", tiling)
+    rng = random.Random(123)
+    pkts = []
+    for i in range(16):
+        w, h, kw, ck = _random_config(rng)
+        rc, pkt, _ = oracle.encode_status(B.make_config(w, h, **ck), synth.make_frame_np(w, h, seed=700 + i, **kw))
+        if rc == 0:
+            pkts.append(pkt)
+    for pkt in list(pkts[:8]):
+        spans = _spans(pkt)
+        for _ in range(4):
+            p = bytearray(pkt)
+            ho, po, size = spans[rng.randrange(len(spans))]
+            p[po + rng.randrange(size)] ^= 1 + rng.randrange(255)
+            p[ho + 13:ho + 17] = struct.pack(">I", zlib.crc32(bytes(p[po:po + size])) & 0xFFFFFFFF)
+            pkts.append(bytes(p))
+    for pkt in pkts:
+        da, db = oracle.decode_status(pkt), product.decode_status(pkt)
+        assert da.status == db.status
+        assert da.slice_status == db.slice_status
+        for x, y in zip(da.planes, db.planes):
+            assert np.array_equal(x, y)
+    rc, frames = product.decode_batch(pkts[:16])
+    for pkt, f in zip(pkts[:16], frames):
+        d = oracle.decode_status(pkt)
+        for x, y in zip(d.planes, f.planes):
+            assert np.array_equal(x, y)

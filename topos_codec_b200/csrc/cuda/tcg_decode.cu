@@ -18,6 +18,7 @@
 //   k_dconceal  damaged slices: neutral fill of the visible band rows
 //                                               (codec.c:7975-7985)
 //   k_deblock_v / k_deblock_h  frame-level output filter (deblock.c:71-341)
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -407,6 +408,282 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
+// ------------------------------------------------------------------ chain, warp tiling
+//
+// Second tiling of the same decode (the tuner below picks per batch size):
+// one warp decodes one slice. The coder state is warp-uniform; lane j holds the
+// frequency and cumulative start of symbol j (and j+32 for the 64-symbol run
+// alphabet) of every context the slice uses, so a symbol search is one compare
+// per lane and the matching lane's next state is broadcast with a warp OR
+// reduction (exactly one lane matches: the alphabet partitions 0..4095).
+// Stream bytes come through a 64-bit bit window refilled one word at a time
+// from 128-byte chunks that the lanes load one chunk ahead. Error conditions
+// accumulate in a flag and end the slice at the next block boundary: any
+// error conceals the slice, so only whether one occurred matters, and reading
+// past the payload is harmless because it can only add to a consumed-byte
+// count that must end equal to the payload size.
+
+#define FULL_MASK 0xFFFFFFFFu
+
+struct Win {
+    uint32_t x;            // coder state
+    uint32_t whi, wlo;     // upcoming stream bits, first bit in the MSB of whi
+    uint32_t wbits;        // valid bits in whi:wlo
+    uint32_t cb;           // stream bytes moved into the state
+    uint32_t cur, nxt;     // lane j: word j of the current / next 128-byte chunk (big-endian)
+    uint32_t k;            // next word of the current chunk
+    const uint32_t* cp;    // aligned start of the chunk after the next one
+    const uint32_t* lim;   // one past the last word that overlaps the payload
+};
+
+__device__ __forceinline__ uint32_t win_load(const uint32_t* p, const uint32_t* lim)
+{
+    return p < lim ? __byte_perm(__ldg(p), 0u, 0x0123u) : 0u;
+}
+
+__device__ __forceinline__ uint32_t win_take(Win& w, uint32_t lane)
+{
+    const uint32_t word = __shfl_sync(FULL_MASK, w.cur, w.k);
+    w.k += 1u;
+    if (w.k == 32u) {
+        w.k = 0u;
+        w.cur = w.nxt;
+        w.nxt = win_load(w.cp + lane, w.lim);
+        w.cp += 32;
+    }
+    return word;
+}
+
+// keep at least 32 bits in the window (called after every renormalisation,
+// which consumes at most 24)
+__device__ __forceinline__ void win_refill(Win& w, uint32_t lane)
+{
+    if (w.wbits < 32u) {
+        const uint32_t word = win_take(w, lane);
+        w.whi |= word >> w.wbits;
+        w.wlo |= word << (32u - w.wbits);
+        w.wbits += 32u;
+    }
+}
+
+// state <- xn followed by as many stream bytes as bring it to [2^23, ...)
+__device__ __forceinline__ void win_renorm(Win& w, uint32_t xn, uint32_t lane)
+{
+    const bool c1 = xn < RANS_L, c2 = xn < (RANS_L >> 8), c3 = xn < (RANS_L >> 16);
+    const uint32_t x8 = __funnelshift_l(w.whi, xn, 8);
+    const uint32_t x16 = __funnelshift_l(w.whi, xn, 16);
+    const uint32_t x24 = __funnelshift_l(w.whi, xn, 24);
+    w.x = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : xn);
+    const uint32_t n8 = c2 ? (c3 ? 24u : 16u) : (c1 ? 8u : 0u);
+    w.whi = __funnelshift_l(w.wlo, w.whi, n8);
+    w.wlo <<= n8;
+    w.wbits -= n8;
+    w.cb += n8 >> 3;
+    win_refill(w, lane);
+}
+
+__device__ __forceinline__ void win_init(Win& w, const uint8_t* b, uint32_t n, uint32_t lane)
+{
+    const uintptr_t a = (uintptr_t)b;
+    const uint32_t* base = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)127);
+    w.lim = reinterpret_cast<const uint32_t*>((a + n + 3u) & ~(uintptr_t)3);
+    w.cur = win_load(base + lane, w.lim);
+    w.nxt = win_load(base + 32 + lane, w.lim);
+    w.cp = base + 64;
+    const uint32_t off = (uint32_t)(a & 127u);
+    w.k = off >> 2;
+    const uint32_t a8 = (off & 3u) * 8u;
+    const uint32_t w0 = win_take(w, lane);
+    const uint32_t w1 = win_take(w, lane);
+    w.x = __funnelshift_l(w1, w0, a8);  // first four payload bytes, big-endian
+    w.whi = w1 << a8;
+    w.wlo = 0u;
+    w.wbits = 32u - a8;
+    w.cb = 4u;
+    win_refill(w, lane);
+}
+
+// one symbol of an alphabet of at most 32 (lane j holds symbol j)
+__device__ __forceinline__ uint32_t dec_sym32(Win& w, uint32_t f, uint32_t c, uint32_t lane)
+{
+    const uint32_t x = w.x;
+    const uint32_t d = (x & 4095u) - c;
+    const bool in = d < f;
+    const uint32_t xn = f * (x >> 12) + d;
+    const uint32_t xv = __reduce_or_sync(FULL_MASK, in ? xn : 0u);
+    const uint32_t s = __reduce_or_sync(FULL_MASK, in ? lane : 0u);
+    win_renorm(w, xv, lane);
+    return s;
+}
+
+// one symbol of a 64-symbol alphabet (lane j holds symbols j and j+32)
+__device__ __forceinline__ uint32_t dec_sym64(Win& w, uint32_t fa, uint32_t ca, uint32_t fb, uint32_t cb,
+                                              uint32_t lane)
+{
+    const uint32_t x = w.x;
+    const uint32_t slot = x & 4095u, xs = x >> 12;
+    const uint32_t da = slot - ca, db = slot - cb;
+    const bool ia = da < fa, ib = db < fb;
+    const uint32_t v = ia ? fa * xs + da : (ib ? fb * xs + db : 0u);
+    const uint32_t xv = __reduce_or_sync(FULL_MASK, v);
+    const uint32_t s = __reduce_or_sync(FULL_MASK, ia ? lane : (ib ? lane + 32u : 0u));
+    win_renorm(w, xv, lane);
+    return s;
+}
+
+// raw chunk of wd bits (wd <= 23)
+__device__ __forceinline__ uint32_t dec_chunk(Win& w, uint32_t wd, uint32_t lane)
+{
+    const uint32_t v = w.x & ~(0xFFFFFFFFu << wd);
+    win_renorm(w, w.x >> wd, lane);
+    return v;
+}
+
+// category suffix: m = 2^(cat-1) | (cat-1 raw bits), split 16 + rest above 23
+__device__ __forceinline__ uint32_t dec_suffix(Win& w, uint32_t cat, uint32_t lane)
+{
+    const uint32_t b = cat > 1u ? cat - 1u : 0u;
+    uint32_t v;
+    if (b <= 23u) {
+        v = dec_chunk(w, b, lane);
+    } else {
+        const uint32_t lo = dec_chunk(w, 16u, lane);
+        v = (dec_chunk(w, b - 16u, lane) << 16) | lo;
+    }
+    return cat == 0u ? 0u : (1u << (cat - 1u)) | v;
+}
+
+template <uint32_t LM, uint32_t DM>
+__device__ __forceinline__ int32_t dchain_slice(const DSlice& S, const DPlane& P, const uint8_t* __restrict__ tb,
+                                                const uint8_t* __restrict__ stream, uint32_t nbytes,
+                                                int32_t* __restrict__ coef, int32_t* __restrict__ rows)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    // per-lane model entries
+    constexpr uint32_t ND = DM ? 5u : 1u;
+    constexpr uint32_t NL = LM == 1u ? 4u : (LM == 2u ? 5u : 1u);
+    uint32_t dcf[ND], dcc[ND], lvf[NL], lvc[NL];
+    auto ent = [&](uint32_t ctx, uint32_t s, uint32_t& f, uint32_t& c) {
+        const uint16_t* cu = reinterpret_cast<const uint16_t*>(tb + TAB_CUM + (size_t)ctx * CUM_BYTES);
+        c = cu[s];
+        f = (uint32_t)cu[s + 1u] - cu[s];  // 0 past the alphabet and for unused symbols
+    };
+#pragma unroll
+    for (uint32_t i = 0; i < ND; ++i) { ent(i, lane, dcf[i], dcc[i]); }
+#pragma unroll
+    for (uint32_t i = 0; i < NL; ++i) { ent(6u + i, lane, lvf[i], lvc[i]); }
+    uint32_t rfa, rca, rfb, rcb;
+    ent(5u, lane, rfa, rca);
+    ent(5u, lane + 32u, rfb, rcb);
+
+    Win w;
+    win_init(w, stream, nbytes, lane);
+    uint32_t err = w.x < RANS_L ? 1u : 0u;
+    const bool wide = P.bd > 12u;
+    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
+    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
+    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
+    int32_t* prow = rows;
+    int32_t* crow = rows + S.cols;
+    uint32_t prev_dcc = 0;
+    bool first = true;
+    for (uint32_t by = 0; by < S.bh && err == 0u; ++by) {
+        int32_t left = 0;
+        for (uint32_t bx = 0; bx < S.cols; ++bx) {
+            // DC
+            uint32_t f0 = dcf[0], c0 = dcc[0];
+            if (DM) {
+                const uint32_t dctx = first ? 0u : dcp_ctx(prev_dcc, true);
+#pragma unroll
+                for (uint32_t i = 1; i < ND; ++i) {
+                    f0 = dctx == i ? dcf[i] : f0;
+                    c0 = dctx == i ? dcc[i] : c0;
+                }
+            }
+            const int32_t top = by != 0u ? prow[bx] : 0;
+            const uint32_t dcat = dec_sym32(w, f0, c0, lane);
+            const uint32_t dmv = dec_suffix(w, dcat, lane);
+            err |= dmv > mdc ? 1u : 0u;
+            const int32_t pred = dc_pred(bx != 0u, left, by != 0u, top);
+            const int64_t dcv = (int64_t)pred + unmap_s(dmv);
+            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+            left = (int32_t)dcv;
+            if (lane == 0u) { crow[bx] = left; }
+            prev_dcc = dcat;
+            first = false;
+            int32_t clo = lane == 0u ? left : 0, chi = 0;
+            // AC: (run, level, suffix) until the end-of-block run symbol
+            uint32_t pos = 1u, pcat = 0u;
+            bool has = false;
+            for (;;) {
+                const uint32_t r = dec_sym64(w, rfa, rca, rfb, rcb, lane);
+                const uint32_t idx = pos + r;
+                if (r == 63u || idx > 63u) {
+                    err |= r != 63u ? 1u : 0u;
+                    break;
+                }
+                uint32_t fl = lvf[0], cl = lvc[0];
+                if (LM != 0u) {
+                    const uint32_t lc = LM == 1u ? pos_ctx(idx) : prev_ctx(pcat, has);
+#pragma unroll
+                    for (uint32_t i = 1; i < NL; ++i) {
+                        fl = lc == i ? lvf[i] : fl;
+                        cl = lc == i ? lvc[i] : cl;
+                    }
+                }
+                const uint32_t cat = dec_sym32(w, fl, cl, lane);
+                const uint32_t m = dec_suffix(w, cat, lane);
+                err |= m > mlv ? 1u : 0u;
+                const uint32_t nat = c_zigzag[idx];
+                const int32_t v = unmap_s(m);
+                if ((nat & 31u) == lane) {
+                    if (nat & 32u) { chi = v; } else { clo = v; }
+                }
+                pcat = cat;
+                has = true;
+                pos = idx + 1u;
+            }
+            int32_t* blk = coef + (size_t)(S.blk0 + by * S.cols + bx) * 64u;
+            blk[lane] = clo;
+            blk[32u + lane] = chi;
+            if (err != 0u) { break; }
+        }
+        __syncwarp();
+        int32_t* sw = prow; prow = crow; crow = sw;
+    }
+    if (err == 0u && w.cb != nbytes) { err = 1u; }
+    return err != 0u ? TCG_ERR_MALFORMED : 0;
+}
+
+// One warp per colour slice (one warp per block, so every slice of a batch is
+// resident at once); dynamic shared memory holds two DC rows of the slice.
+__global__ void __launch_bounds__(32) k_dchain_w(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                               const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
+                                               const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
+                                               int32_t* __restrict__ status)
+{
+    extern __shared__ __align__(16) int32_t rows[];
+    const uint32_t si = cslices[blockIdx.x];
+    if (status[si] != 0) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
+    const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
+    const uint8_t* stream = pkt + S.pay + plen;
+    const uint32_t nb = S.size - plen;
+    int32_t rc;
+    switch (lm * 2u + dm) {
+    case 0: rc = dchain_slice<0, 0>(S, P, tb, stream, nb, coef, rows); break;
+    case 1: rc = dchain_slice<0, 1>(S, P, tb, stream, nb, coef, rows); break;
+    case 2: rc = dchain_slice<1, 0>(S, P, tb, stream, nb, coef, rows); break;
+    case 3: rc = dchain_slice<1, 1>(S, P, tb, stream, nb, coef, rows); break;
+    case 4: rc = dchain_slice<2, 0>(S, P, tb, stream, nb, coef, rows); break;
+    default: rc = dchain_slice<2, 1>(S, P, tb, stream, nb, coef, rows); break;
+    }
+    if (threadIdx.x == 0) { status[si] = rc; }
+}
+
 // ------------------------------------------------------------------ reconstruction
 
 __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ blk_slice,
@@ -690,6 +967,38 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
     return qp < 64u ? s[qp] : hi[refined ? 1 : 0][qp - 64u];
 }
 
+// --------------------------------------------------------- decode-chain tuner
+//
+// Two tilings of the slice decode: one lane per slice (eight slices per warp:
+// cheap in issue slots, best when many slices share the GPU) and one warp
+// per slice (shorter step latency, best for small batches). The first batch
+// of each size class (by log2 of the colour-slice count) runs both and keeps
+// the faster; TCG_DCHAIN=lane|warp forces one.
+enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1 };
+
+static std::mutex g_tune_mu;
+static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
+                            -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
+
+static int dchain_forced()
+{
+    const char* v = getenv("TCG_DCHAIN");
+    if (v == nullptr) { return -1; }
+    if (strcmp(v, "lane") == 0) { return DCH_TILE_LANE; }
+    if (strcmp(v, "warp") == 0) { return DCH_TILE_WARP; }
+    return -1;
+}
+
+static uint32_t size_class(uint32_t nc) { return nc == 0u ? 0u : 32u - (uint32_t)__builtin_clz(nc); }
+
+extern "C" __attribute__((visibility("default"))) int32_t tcg_dchain_tiling(uint32_t nc)
+{
+    const int f = dchain_forced();
+    if (f >= 0) { return f; }
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    return g_tune[size_class(nc)];
+}
+
 static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
 {
     std::vector<DPlane> planes;
@@ -699,6 +1008,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     std::vector<uint64_t> pkt_off(count, 0);
     std::vector<uint32_t> frame_slice0(count, 0);
     uint64_t out_elems = 0, pkt_bytes = 0, nblk = 0, alpha_res = 0;
+    uint32_t max_cols = 1;
     for (uint32_t f = 0; f < count; ++f) {
         const tcg_dec_frame& F = frames[f];
         frame_slice0[f] = (uint32_t)slices.size();
@@ -721,6 +1031,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             P.frame = f;
             memcpy(P.qm, F.qm[p], sizeof(P.qm));
             if (P.kind == TCG_PLANE_COLOR) { nblk += (uint64_t)P.cols * P.rows; }
+            max_cols = P.cols > max_cols ? P.cols : max_cols;
             planes.push_back(P);
             if (F.deblock && p < 3u) {
                 const uint32_t w = P.vis_w, h = P.vis_h;
@@ -828,9 +1139,40 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             TCG_CHECK(cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DCH_SMEM));
             attr = true;
         }
-        TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-        TCG_LAUNCH(C, K_DCHAIN, k_dchain, (nc + DCH_LANES - 1u) / DCH_LANES, 32, DCH_SMEM, d_sl, d_ord, nc, d_st, d_pl,
-                   d_pkt, d_tab, d_coef, d_status);
+        const size_t wsmem = (size_t)max_cols * 8u;  // two DC rows per slice (warp tiling)
+        int tiling = dchain_forced();
+        bool measure = false;
+        const uint32_t cls = size_class(nc);
+        if (tiling < 0) {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            tiling = g_tune[cls];
+            measure = tiling < 0;
+        }
+        cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+        if (measure) {
+            for (auto& x : e) { TCG_CHECK(cudaEventCreate(&x)); }
+            TCG_CHECK(cudaEventRecord(e[0], st));
+        }
+        if (measure || tiling == DCH_TILE_LANE) {
+            TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+            TCG_LAUNCH(C, K_DCHAIN, k_dchain, (nc + DCH_LANES - 1u) / DCH_LANES, 32, DCH_SMEM, d_sl, d_ord, nc, d_st,
+                       d_pl, d_pkt, d_tab, d_coef, d_status);
+        }
+        if (measure) { TCG_CHECK(cudaEventRecord(e[1], st)); }
+        if (measure || tiling == DCH_TILE_WARP) {
+            // the warp tiling writes every coefficient of the blocks it decodes
+            TCG_LAUNCH(C, K_DCHAIN_W, k_dchain_w, nc, 32, wsmem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
+        }
+        if (measure) {
+            TCG_CHECK(cudaEventRecord(e[2], st));
+            TCG_CHECK(cudaEventSynchronize(e[2]));
+            float ms_lane = 0.f, ms_warp = 0.f;
+            cudaEventElapsedTime(&ms_lane, e[0], e[1]);
+            cudaEventElapsedTime(&ms_warp, e[1], e[2]);
+            for (auto& x : e) { cudaEventDestroy(x); }
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            g_tune[cls] = (int8_t)(ms_warp < ms_lane ? DCH_TILE_WARP : DCH_TILE_LANE);
+        }
         TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_bs, d_st, d_pl, d_tab, d_coef,
                    d_status, (uint32_t)nblk, d_out);
     }

@@ -44,7 +44,7 @@ enum BufId {
 // Kernel identities for optional per-kernel event timing.
 enum KernelId {
     K_FDCT, K_TOKENS, K_SELECT, K_OPSCAN, K_OPGEN, K_CHAIN, K_ALPHA, K_PACK_SIZES, K_PACK_COPY, K_PACK_CRC,
-    K_PACK_HEADER, K_DCRC, K_DTABLES, K_DCHAIN, K_DIDCT, K_DALPHA, K_DALPHA_MED, K_DCONCEAL, K_DEBLOCK_V,
+    K_PACK_HEADER, K_DCRC, K_DTABLES, K_DCHAIN, K_DCHAIN_W, K_DIDCT, K_DALPHA, K_DALPHA_MED, K_DCONCEAL, K_DEBLOCK_V,
     K_DEBLOCK_H, K_WALK, K_COUNT
 };
 
