@@ -290,6 +290,30 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
 int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                       topos_frame_output* infos);
 
+/* Continuous-batching request server. Encode and decode requests of single
+ * frames (any mix of sizes and configurations; buffers owned by the caller,
+ * host or device memory, valid until the request completes) enter two
+ * queues; a worker per direction codes everything that has arrived in one
+ * batched call, while requests arriving meanwhile wait for its next batch.
+ * The two workers run concurrently on their own streams. A batch admits
+ * requests while their estimated device bytes fit max_bytes_in_flight (0 =
+ * no limit) and the device's free memory, up to max_batch_frames (1..64).
+ * Every result equals the single-frame call's. tcg_server_wait blocks until
+ * the ticket's request is done and returns its status (as tc_frame_encode /
+ * tc_frame_decode would), its stats or frame information, and its latency
+ * from submission to completion. Decode requests are validated on
+ * submission: an invalid packet returns its error there. */
+typedef struct tcg_server tcg_server;
+int32_t tcg_server_create(uint64_t max_bytes_in_flight, uint32_t max_batch_frames, tcg_server** out);
+void tcg_server_destroy(tcg_server* server);
+int32_t tcg_server_submit_encode(tcg_server* server, const topos_frame_config* cfg, const topos_frame_input* input,
+                                 uint8_t* out, size_t out_cap, uint64_t* ticket);
+int32_t tcg_server_submit_decode(tcg_server* server, const uint8_t* packet, size_t size,
+                                 uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
+                                 const size_t strides[TC_FRAME_MAX_PLANES], uint64_t* ticket);
+int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, topos_frame_stats* stats,
+                        topos_frame_output* info, double* latency_ms);
+
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * 0 = one lane per slice (eight slices per warp), 1 = one warp per slice,
  * -1 = not chosen yet. The first batch of each size class (log2 of the slice

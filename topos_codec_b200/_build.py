@@ -18,11 +18,13 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 CUDA_HOME = os.path.dirname(os.path.dirname(os.path.realpath(NVCC)))
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ["-std=c11", "-O2", "-fPIC", "-Wall", "-Wextra", "-fvisibility=hidden", "-ffp-contract=off"]
+CXXFLAGS = ["-std=c++17", "-O2", "-fPIC", "-Wall", "-Wextra", "-fvisibility=hidden", f"-I{os.path.join(CUDA_HOME, 'include')}"]
 NVFLAGS = GENCODE + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden"]
 
 
 def _sources():
-    host = sorted(os.path.join(CSRC, "host", f) for f in os.listdir(os.path.join(CSRC, "host")) if f.endswith(".c"))
+    host = sorted(os.path.join(CSRC, "host", f) for f in os.listdir(os.path.join(CSRC, "host"))
+                  if f.endswith((".c", ".cpp")))
     cuda = sorted(os.path.join(CSRC, "cuda", f) for f in os.listdir(os.path.join(CSRC, "cuda")) if f.endswith(".cu"))
     return host, cuda
 
@@ -60,7 +62,10 @@ def build_library(verbose: bool = False) -> str:
     for src in host:
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")
         if _stale(obj, [src] + hdrs):
-            _run(["gcc"] + CFLAGS + ["-c", src, "-o", obj])
+            if src.endswith(".cpp"):
+                _run(["g++"] + CXXFLAGS + ["-c", src, "-o", obj])
+            else:
+                _run(["gcc"] + CFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in cuda:
         obj = os.path.join(OBJ, os.path.basename(src) + ".o")

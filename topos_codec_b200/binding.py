@@ -315,3 +315,79 @@ class ToposCodec:
             ctypes.memmove(ctypes.byref(one), ctypes.byref(infos[i]), ctypes.sizeof(FrameOutput))
             frames.append(DecodedFrame(planes[i], one, TC_OK))
         return rc, frames
+
+
+class Server:
+    """Continuous-batching request server of the library (tcg_server_*).
+
+    submit_encode/submit_decode take numpy arrays (host memory) or device
+    pointers; the caller keeps the buffers alive until wait() returns.
+    """
+
+    def __init__(self, codec: "ToposCodec", max_bytes_in_flight: int = 0, max_batch_frames: int = 64):
+        L = codec._lib
+        self._codec, self._lib = codec, L
+        L.tcg_server_create.restype = ctypes.c_int32
+        L.tcg_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]
+        L.tcg_server_destroy.restype = None
+        L.tcg_server_destroy.argtypes = [ctypes.c_void_p]
+        L.tcg_server_submit_encode.restype = ctypes.c_int32
+        L.tcg_server_submit_encode.argtypes = [ctypes.c_void_p, ctypes.POINTER(FrameConfig), ctypes.POINTER(FrameInput),
+                                               ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)]
+        L.tcg_server_submit_decode.restype = ctypes.c_int32
+        L.tcg_server_submit_decode.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                               ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]
+        L.tcg_server_wait.restype = ctypes.c_int32
+        L.tcg_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.POINTER(FrameStats), ctypes.POINTER(FrameOutput),
+                                      ctypes.POINTER(ctypes.c_double)]
+        h = ctypes.c_void_p()
+        rc = int(L.tcg_server_create(max_bytes_in_flight, max_batch_frames, ctypes.byref(h)))
+        if rc != TC_OK:
+            raise ToposCodecError(f"tcg_server_create failed [{rc}]: {codec.last_error()}", rc)
+        self._h = h
+        self._keep = {}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.tcg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def submit_encode(self, cfg: FrameConfig, planes, out_ptr: int, out_cap: int) -> int:
+        """planes: numpy uint16 arrays, or (pointer, stride) pairs of device planes."""
+        fi = FrameInput()
+        fi.struct_size, fi.abi_version = ctypes.sizeof(FrameInput), TOPOS_CODEC_ABI_VERSION
+        for i, p in enumerate(planes):
+            if isinstance(p, np.ndarray):
+                fi.planes[i], fi.strides[i] = p.ctypes.data, p.strides[0] // 2
+            else:
+                fi.planes[i], fi.strides[i] = p
+        t = ctypes.c_uint64()
+        rc = int(self._lib.tcg_server_submit_encode(self._h, ctypes.byref(cfg), ctypes.byref(fi), out_ptr, out_cap,
+                                                    ctypes.byref(t)))
+        if rc != TC_OK:
+            raise ToposCodecError(f"submit_encode failed [{rc}]: {self._codec.last_error()}", rc)
+        self._keep[t.value] = (planes, fi)
+        return t.value
+
+    def submit_decode(self, packet_ptr: int, size: int, plane_ptrs: Sequence[int]) -> int:
+        ptrs = (ctypes.c_void_p * TC_FRAME_MAX_PLANES)(*list(plane_ptrs) + [None] * (TC_FRAME_MAX_PLANES - len(plane_ptrs)))
+        t = ctypes.c_uint64()
+        rc = int(self._lib.tcg_server_submit_decode(self._h, packet_ptr, size, ptrs, None, ctypes.byref(t)))
+        if rc != TC_OK:
+            raise ToposCodecError(f"submit_decode failed [{rc}]: {self._codec.last_error()}", rc)
+        self._keep[t.value] = ptrs
+        return t.value
+
+    def wait(self, ticket: int):
+        """(status, stats, info, latency_ms) of a finished request."""
+        st, stats, info, lat = ctypes.c_int32(), FrameStats(), FrameOutput(), ctypes.c_double()
+        rc = int(self._lib.tcg_server_wait(self._h, ticket, ctypes.byref(st), ctypes.byref(stats), ctypes.byref(info),
+                                           ctypes.byref(lat)))
+        self._keep.pop(ticket, None)
+        if rc != TC_OK:
+            raise ToposCodecError(f"wait failed [{rc}]: {self._codec.last_error()}", rc)
+        return st.value, stats, info, lat.value
