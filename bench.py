@@ -141,6 +141,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=FRAMES)
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -390,6 +392,19 @@ def main():
         cpu = {"value": r, "unit": "frames/s", "cores": cores, "kind": "reference",
                "sample": f"{n} frames encoded+decoded frame-parallel in {el:.1f} s"}
 
+    # ---------------- serving: open-loop request stream at half the saturation rate ----------------
+    served = None
+    if world == 1 and not args.no_serve:
+        from topos_codec_b200 import serving
+        sat = serving.saturation_rps(gpu)
+        # a short discarded trace first: the decode-tiling tuner times both tilings
+        # on the first batch of each batch-size class
+        serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=3.0, seed=7)
+        served = serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=args.serve_seconds)
+        served.update({"load": 0.5, "saturation_rps": sat,
+                       "mix": "50/50 encode/decode; 1080p 40 %, 2160p 40 %, 720p 20 %; 10-bit 4:2:2 tiers 422/HQ",
+                       "latency": "server-side, submission to completion"})
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -406,6 +421,7 @@ def main():
             "kernels_ms": {k: round(v["ms"] / args.steps, 3) for k, v in kern.items()},
             "roofline": roof,
             "cpu_baseline": cpu,
+            "served": served,
             "e2e": {"value": nf * world / e2e_s, "unit": "frames/s",
                     "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes)},
         }
