@@ -202,8 +202,9 @@ def main():
     dev = torch.device("cuda", local)
     # inputs resident in HBM: uint16 planes
     frames_d = []
-    for i in range(nf):
-        ps = synth.make_frame(W, H, seed=rank, frame=i, device=dev)
+    from topos_codec_b200 import sharding
+    for seed, i in sharding.rank_frames(rank, nf):
+        ps = synth.make_frame(W, H, seed=seed, frame=i, device=dev)
         frames_d.append([p.to(torch.uint16) for p in ps])
     torch.cuda.synchronize()
     in_bytes = plane_bytes() * nf
@@ -283,12 +284,8 @@ def main():
     L.tcg_profile_enable(0)
     launches = L.tcg_kernel_launches() - launches0
     step_ms = (sum(enc_ms) + sum(dec_ms)) / args.steps
-    if world > 1:
-        t = torch.tensor([step_ms, sum(enc_ms) / args.steps, sum(dec_ms) / args.steps], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms, enc_avg, dec_avg = t.tolist()
-    else:
-        enc_avg, dec_avg = sum(enc_ms) / args.steps, sum(dec_ms) / args.steps
+    step_ms, enc_avg, dec_avg = sharding.max_over_ranks([step_ms, sum(enc_ms) / args.steps, sum(dec_ms) / args.steps],
+                                                         device=dev)
     value = nf * world / (step_ms / 1000.0)
 
     # per-kernel timings over the timed region
@@ -347,10 +344,7 @@ def main():
         decode_batch(pkt_ptrs_h, dec_ptrs_h)
     barrier()
     e2e_s = (time.perf_counter() - t0) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = t.item()
+    e2e_s = sharding.max_over_ranks([e2e_s], device=dev)[0]
     e2e_exact = all(out_h[i][: stats[i].packet_size].numpy().tobytes() == batched_pkts[i] for i in range(nf))
     exact = exact and e2e_exact
 
