@@ -186,19 +186,31 @@ constexpr uint32_t DCH_LANE_BYTES = DCH_LUT_SLOTS * LUT_BYTES + DCH_CUM_BYTES;
 constexpr uint32_t DCH_SMEM = 64u + DCH_LANES * DCH_LANE_BYTES;
 
 struct DLane {
-    uint32_t x;           // coder state
-    uint32_t whi, wlo;    // upcoming stream bits, first bit in the MSB of whi
-    uint32_t wbits;       // valid bits in whi:wlo
-    uint32_t nxt;         // next stream word (memory byte order)
-    uint32_t cb;          // stream bytes moved into the state
-    const uint32_t* wp;   // address of nxt
-    const uint32_t* wlim; // one past the last word that overlaps the payload
+    uint32_t x;            // coder state
+    uint32_t whi, wlo;     // upcoming stream bits, first bit in the MSB of whi
+    uint32_t wbits;        // valid bits in whi:wlo
+    uint32_t nxt;          // stream word wi (memory byte order)
+    uint32_t wi, wn;       // word index of nxt; words overlapping the payload
+    uint32_t a8;           // bit offset of the payload in its first word
+    const uint32_t* wb;    // first word of the payload (aligned down)
 };
 
-// keep at least 32 bits in the window (branch-free: every lane runs the same
-// instructions; only the loads are predicated). Entering a new 128-byte line
-// of the stream prefetches the line 256 bytes ahead into L1, so word loads
-// hit L1 instead of stalling the warp on DRAM.
+// Predicated global load / store: a predicate, not a branch.
+__device__ __forceinline__ uint32_t ldg_nc_if(const uint32_t* p, uint32_t old, bool pred)
+{
+    uint32_t v = old;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.global.nc.u32 %0, [%1];\n\t}"
+        : "+r"(v) : "l"(p), "r"((uint32_t)pred));
+    return v;
+}
+
+__device__ __forceinline__ void stg_if(int32_t* p, int32_t v, bool pred)
+{
+    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.s32 [%0], %1;\n\t}"
+                 :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
+}
+
+// keep at least 32 bits in the window (branch-free; only the load is predicated)
 __device__ __forceinline__ void dl_refill(DLane& L)
 {
     const bool need = L.wbits < 32u;
@@ -207,14 +219,16 @@ __device__ __forceinline__ void dl_refill(DLane& L)
     L.whi |= need ? (w >> sh) : 0u;
     L.wlo |= need ? (w << ((32u - sh) & 31u)) : 0u;
     L.wbits += need ? 32u : 0u;
-    L.wp += need ? 1 : 0;
-    const bool ld = need && L.wp < L.wlim;
-    uint32_t v = L.nxt;
-    if (ld) { v = __ldg(L.wp); }
-    L.nxt = v;
-    const uint32_t pf = (uint32_t)(ld && (((uintptr_t)L.wp & 127u) == 0u) && (L.wp + 64 < L.wlim));
+    L.wi += need ? 1u : 0u;
+    L.nxt = ldg_nc_if(L.wb + L.wi, L.nxt, need && L.wi < L.wn);
+}
+
+// bring the stream 256 bytes ahead of the window into L1 (once per loop iteration)
+__device__ __forceinline__ void dl_prefetch(const DLane& L)
+{
+    const uint32_t pf = (uint32_t)(L.wi + 64u < L.wn);
     asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
-                 :: "l"(L.wp + 64), "r"(pf));
+                 :: "l"(L.wb + L.wi + 64u), "r"(pf));
 }
 
 __device__ __forceinline__ void dl_renorm(DLane& L, uint32_t xn)
@@ -228,25 +242,29 @@ __device__ __forceinline__ void dl_renorm(DLane& L, uint32_t xn)
     L.whi = __funnelshift_l(L.wlo, L.whi, n8);
     L.wlo <<= n8;
     L.wbits -= n8;
-    L.cb += n8 >> 3;
     dl_refill(L);
+}
+
+// bytes moved into the state: the first four, then the window's intake minus what it still holds
+__device__ __forceinline__ uint32_t dl_consumed(const DLane& L)
+{
+    return 4u + ((32u - L.a8) + 32u * (L.wi - 2u) - L.wbits) / 8u;
 }
 
 __device__ __forceinline__ void dl_init(DLane& L, const uint8_t* b, uint32_t n)
 {
     const uintptr_t a = (uintptr_t)b;
-    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)3);
-    L.wlim = reinterpret_cast<const uint32_t*>((a + n + 3u) & ~(uintptr_t)3);
-    const uint32_t a8 = (uint32_t)(a & 3u) * 8u;
-    const uint32_t w0 = __byte_perm(__ldg(w), 0u, 0x0123u);
-    const uint32_t w1 = w + 1 < L.wlim ? __byte_perm(__ldg(w + 1), 0u, 0x0123u) : 0u;
-    L.x = __funnelshift_l(w1, w0, a8);  // first four payload bytes, big-endian
-    L.whi = w1 << a8;
+    L.wb = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)3);
+    L.wn = (uint32_t)((((a + n + 3u) & ~(uintptr_t)3) - (uintptr_t)L.wb) >> 2);
+    L.a8 = (uint32_t)(a & 3u) * 8u;
+    const uint32_t w0 = __byte_perm(__ldg(L.wb), 0u, 0x0123u);
+    const uint32_t w1 = 1u < L.wn ? __byte_perm(__ldg(L.wb + 1), 0u, 0x0123u) : 0u;
+    L.x = __funnelshift_l(w1, w0, L.a8);  // first four payload bytes, big-endian
+    L.whi = w1 << L.a8;
     L.wlo = 0u;
-    L.wbits = 32u - a8;
-    L.cb = 4u;
-    L.wp = w + 2;
-    L.nxt = L.wp < L.wlim ? __ldg(L.wp) : 0u;
+    L.wbits = 32u - L.a8;
+    L.wi = 2u;
+    L.nxt = 2u < L.wn ? __ldg(L.wb + 2) : 0u;
     dl_refill(L);
 }
 
@@ -381,9 +399,10 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const bool use_lut = !eob || dc_lut;
         const uint32_t cat = dl_sym(L, lut, use_lut, cum);
         m = dl_suffix(L, cat);
+        dl_prefetch(L);
         if (!eob) {
             err |= m > mlv ? 1u : 0u;
-            blk[zz[idx]] = unmap_s(m);
+            stg_if(blk + zz[idx], unmap_s(m), true);
             pcat = cat;
             has = true;
             pos = idx + 1u;
@@ -404,7 +423,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             has = false;
         }
     }
-    if (err == 0u && L.cb != nbytes) { err = 1u; }
+    if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
