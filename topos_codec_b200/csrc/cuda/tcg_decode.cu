@@ -231,18 +231,22 @@ __device__ __forceinline__ void dl_prefetch(const DLane& L)
                  :: "l"(L.wb + L.wi + 64u), "r"(pf));
 }
 
+// state <- xn followed by the stream bytes that bring it to [2^23, ...): the
+// byte count is (leading zeros - 1) / 8, clamped at 0 for states of 2^31 and
+// up (xn is never 0 here: a symbol step leaves at least 2^11, a raw chunk at
+// least 1). With Refill the window is topped up to 32 bits afterwards; a
+// symbol step takes at most 16 bits, so the run symbol, which always follows
+// a refilled step, skips it.
+template <bool Refill>
 __device__ __forceinline__ void dl_renorm(DLane& L, uint32_t xn)
 {
-    const bool c1 = xn < RANS_L, c2 = xn < (RANS_L >> 8), c3 = xn < (RANS_L >> 16);
-    const uint32_t x8 = __funnelshift_l(L.whi, xn, 8);
-    const uint32_t x16 = __funnelshift_l(L.whi, xn, 16);
-    const uint32_t x24 = __funnelshift_l(L.whi, xn, 24);
-    L.x = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : xn);
-    const uint32_t n8 = c2 ? (c3 ? 24u : 16u) : (c1 ? 8u : 0u);
+    const int32_t lz = __clz((int32_t)xn);
+    const uint32_t n8 = (uint32_t)max(lz - 1, 0) & 0x18u;
+    L.x = __funnelshift_l(L.whi, xn, n8);
     L.whi = __funnelshift_l(L.wlo, L.whi, n8);
     L.wlo <<= n8;
     L.wbits -= n8;
-    dl_refill(L);
+    if (Refill) { dl_refill(L); }
 }
 
 // bytes moved into the state: the first four, then the window's intake minus what it still holds
@@ -270,6 +274,7 @@ __device__ __forceinline__ void dl_init(DLane& L, const uint8_t* b, uint32_t n)
 
 // One symbol: through the bucket table when use_lut, otherwise by walking the
 // cumulative table from symbol 0. Both pointers always address valid tables.
+template <bool Refill>
 __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool use_lut, const uint16_t* cum)
 {
     const uint32_t x = L.x, slot = x & 4095u;
@@ -280,7 +285,7 @@ __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool u
         c0 = c1;
         c1 = cum[s + 1u];
     }
-    dl_renorm(L, (c1 - c0) * (x >> 12) + slot - c0);
+    dl_renorm<Refill>(L, (c1 - c0) * (x >> 12) + slot - c0);
     return s;
 }
 
@@ -288,7 +293,7 @@ __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool u
 __device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
 {
     const uint32_t v = L.x & ~(0xFFFFFFFFu << w);
-    dl_renorm(L, L.x >> w);
+    dl_renorm<true>(L, L.x >> w);
     return v;
 }
 
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     int32_t* blk = coef + (size_t)S.blk0 * 64u;
 
     // first block's DC (no left, no top, context 0)
-    uint32_t dcat = dl_sym(L, lut_dc, dc_lut, cum_dc);
+    uint32_t dcat = dl_sym<true>(L, lut_dc, dc_lut, cum_dc);
     uint32_t m = dl_suffix(L, dcat);
     err |= m > mdc ? 1u : 0u;
     int64_t dcv = unmap_s(m);
@@ -386,7 +391,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     uint32_t pos = 1u, pcat = 0u;
     bool has = false;
     while (err == 0u) {
-        const uint32_t r = dl_sym(L, lut_run, true, cum_run);
+        const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
         const bool eob = r == 63u;
         const uint32_t idx = pos + r;
         if (!eob && idx > 63u) { err = 1u; break; }
@@ -397,7 +402,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const uint32_t* lut = eob ? (dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run) : lut_lvl + lc * LUT_BUCKETS;
         const uint16_t* cum = eob ? cum_dc + dctx * CUM_LEN : cum_lvl + lc * CUM_LEN;
         const bool use_lut = !eob || dc_lut;
-        const uint32_t cat = dl_sym(L, lut, use_lut, cum);
+        const uint32_t cat = dl_sym<true>(L, lut, use_lut, cum);
         m = dl_suffix(L, cat);
         dl_prefetch(L);
         if (!eob) {
