@@ -315,10 +315,11 @@ int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, to
                         topos_frame_output* info, double* latency_ms);
 
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
- * 0 = one lane per slice (eight slices per warp), 1 = one warp per slice,
- * -1 = not chosen yet. The first batch of each size class (log2 of the slice
- * count) times both tilings and keeps the faster; the environment variable
- * TCG_DCHAIN=lane|warp overrides the choice. Both produce identical output. */
+ * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, or
+ * one warp per slice (1); -1 = not chosen yet. The first batch of each size
+ * class (log2 of the slice count) times every tiling and keeps the fastest;
+ * the environment variable TCG_DCHAIN=lane|lane4|lane2|lane1|warp overrides
+ * the choice ("lane" is 8 per warp). All produce identical output. */
 int32_t tcg_dchain_tiling(uint32_t colour_slices);
 
 /* Device selection and teardown for the calling process. tcg_device_init is

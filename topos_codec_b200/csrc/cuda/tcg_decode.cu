@@ -5,10 +5,12 @@
 //                                               (reference codec.c:8204-8225)
 //   k_dtables   per colour slice: flags/rows prefix -> rANS models, symbol
 //               lookup tables, quantiser steps    (slice_codec.c:554-625)
-//   k_dchain    one warp per colour slice: serial forward rANS2 decode with
-//               the symbol search spread over the lanes -> natural-order
-//               coefficients, DC reconstruction, domain checks
-//                                               (slice_codec.c:626-736)
+//   k_dchain    one lane per colour slice, 1-8 slices per warp: serial
+//               forward rANS2 decode through bucket tables in shared memory
+//               -> natural-order coefficients, DC reconstruction, domain
+//               checks                          (slice_codec.c:626-736)
+//   k_dchain_w  the same decode with one warp per colour slice, the symbol
+//               search spread over the lanes (a second tiling; a tuner picks)
 //   k_didct     per block: dequantise, exact inverse transform, clamp, crop
 //                                               (color_store.h:529-711)
 //   k_dalpha    per alpha slice: Rice run/level decode -> residuals
@@ -166,8 +168,8 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
 
 // ------------------------------------------------------------------ chain
 //
-// One lane per colour slice; a block holds DCH_LANES slices and copies their
-// lookup tables into shared memory. A lane's loop iteration decodes one run
+// One lane per colour slice; a block holds LANES slices (1, 2, 4 or 8; the
+// tuner below picks) and copies their lookup tables into shared memory. A lane's loop iteration decodes one run
 // symbol, then either a level (run < 63) or, after an end-of-block run, the
 // next block's DC category, and that category's raw suffix: every lane runs
 // the same instruction sequence whatever its slice is doing. Symbol lookup is
@@ -179,11 +181,10 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
 // the payload only grows a consumed-byte count that must end equal to the
 // payload size.
 
-constexpr uint32_t DCH_LANES = 8u;      // slices per block
 constexpr uint32_t DCH_LUT_SLOTS = 7u;  // shared-memory bucket tables per slice
 constexpr uint32_t DCH_CUM_BYTES = (MAX_CTX * CUM_BYTES + 15u) & ~15u;
 constexpr uint32_t DCH_LANE_BYTES = DCH_LUT_SLOTS * LUT_BYTES + DCH_CUM_BYTES;
-constexpr uint32_t DCH_SMEM = 64u + DCH_LANES * DCH_LANE_BYTES;
+__host__ __device__ constexpr uint32_t dch_smem(uint32_t lanes) { return 64u + lanes * DCH_LANE_BYTES; }
 
 struct DLane {
     uint32_t x;            // coder state
@@ -297,6 +298,57 @@ __device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
     return v;
 }
 
+// One symbol whose bucket entry e was read already, for a state below 2^31.
+// Renormalises without refilling and returns the symbol; lz receives the
+// leading-zero count of the new state (1..8: the state lies in [2^23, 2^31)).
+__device__ __forceinline__ uint32_t dl_sym_entry(DLane& L, uint32_t e, const uint16_t* cum, uint32_t& lz)
+{
+    const uint32_t x = L.x, slot = x & 4095u;
+    uint32_t s = e & 63u, c0 = (e >> 6) & 0xFFFu, c1 = e >> 18;
+    while (slot >= c1 && s < CUM_LEN - 2u) {
+        ++s;
+        c0 = c1;
+        c1 = cum[s + 1u];
+    }
+    // x < 2^31 and a symbol of frequency >= 1: xn in [2^11, 2^31), so 1..20 leading zeros
+    const uint32_t xn = (c1 - c0) * (x >> 12) + slot - c0;
+    const uint32_t lzn = (uint32_t)__clz((int32_t)xn);
+    const uint32_t n8 = (lzn - 1u) & 0x18u;
+    L.x = __funnelshift_l(L.whi, xn, n8);
+    L.whi = __funnelshift_l(L.wlo, L.whi, n8);
+    L.wlo <<= n8;
+    L.wbits -= n8;
+    lz = lzn - n8;
+    return s;
+}
+
+// Category suffix after a symbol step that left lz leading zeros in the state:
+// a chunk of b <= 23 bits leaves x >> b with lz + b leading zeros, so its
+// renormalisation needs no second count. Refills before (a chunk takes up to
+// 24 bits) and after.
+__device__ __forceinline__ uint32_t dl_suffix_lz(DLane& L, uint32_t cat, uint32_t lz)
+{
+    dl_refill(L);
+    const uint32_t b = cat > 1u ? cat - 1u : 0u;
+    uint32_t v;
+    if (b <= 23u) {
+        v = L.x & ~(0xFFFFFFFFu << b);
+        const uint32_t xn = L.x >> b;
+        const uint32_t n8 = (lz + b - 1u) & 0x18u;
+        L.x = __funnelshift_l(L.whi, xn, n8);
+        L.whi = __funnelshift_l(L.wlo, L.whi, n8);
+        L.wlo <<= n8;
+        L.wbits -= n8;
+        dl_refill(L);
+    } else {
+        const uint32_t lo = dl_chunk(L, 16u);
+        const uint32_t w2 = b - 16u;
+        v = (dl_chunk(L, w2 <= 23u ? w2 : 23u) << 16) | lo;
+    }
+    return cat == 0u ? 0u : (1u << ((cat - 1u) & 31u)) | v;
+}
+
+
 // category suffix: m = 2^(cat-1) | (cat-1 raw bits), split 16 + rest above 23
 __device__ __forceinline__ uint32_t dl_suffix(DLane& L, uint32_t cat)
 {
@@ -312,6 +364,7 @@ __device__ __forceinline__ uint32_t dl_suffix(DLane& L, uint32_t cat)
     return cat == 0u ? 0u : (1u << ((cat - 1u) & 31u)) | v;
 }
 
+template <uint32_t LANES>
 __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices, const uint32_t* __restrict__ order,
                                                uint32_t nc, const uint32_t* __restrict__ slice_tab,
                                                const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
@@ -324,8 +377,8 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     zz[t] = c_zigzag[t];
     zz[t + 32u] = c_zigzag[t + 32u];
     // stage every lane's tables: run and level contexts always, DC contexts when they fit
-    const uint32_t i0 = blockIdx.x * DCH_LANES;
-    for (uint32_t l = 0; l < DCH_LANES && i0 + l < nc; ++l) {
+    const uint32_t i0 = blockIdx.x * LANES;
+    for (uint32_t l = 0; l < LANES && i0 + l < nc; ++l) {
         const uint32_t sl = order[i0 + l];
         if (status[sl] != 0) { continue; }
         const uint8_t* tb = tabs + (size_t)slice_tab[sl] * DTAB_BYTES;
@@ -346,7 +399,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         }
     }
     __syncthreads();
-    if (t >= DCH_LANES || i0 + t >= nc) { return; }
+    if (t >= LANES || i0 + t >= nc) { return; }
     const uint32_t si = order[i0 + t];
     if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
@@ -390,7 +443,33 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     uint32_t b = 0, bx = 0;  // current block within the slice, its column
     uint32_t pos = 1u, pcat = 0u;
     bool has = false;
+    // run symbol 0 covers slots [0, f0) (f0 = 0 when it does not occur)
+    const uint32_t f0 = cum_run[1];
+    // level context of the coefficient at pos if the next run is 0
+    uint32_t lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? 4u : 0u);
     while (err == 0u) {
+        // Fast iteration: run 0 with a state that needs no renormalisation (in
+        // [2^23, 2^31)), i.e. one multiply-add, then the level at pos through a
+        // bucket entry read before that condition is known.
+        const uint32_t x = L.x, slot = x & 4095u;
+        const uint32_t x1 = f0 * (x >> 12) + slot;
+        const uint32_t* lutc = lut_lvl + lc0 * LUT_BUCKETS;
+        const uint32_t e1 = lutc[(x1 & 4095u) >> 4];
+        if (slot < f0 && x1 - RANS_L < 0x7F800000u && pos < 64u) {
+            L.x = x1;
+            uint32_t lz;
+            const uint32_t cat = dl_sym_entry(L, e1, cum_lvl + lc0 * CUM_LEN, lz);
+            m = dl_suffix_lz(L, cat, lz);
+            dl_prefetch(L);
+            err |= m > mlv ? 1u : 0u;
+            stg_if(blk + zz[pos], unmap_s(m), true);
+            pcat = cat;
+            has = true;
+            ++pos;
+            lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? cat_bucket(cat) : 0u);
+            continue;
+        }
+        // general iteration: any run symbol, end of block and the next block's DC
         const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
         const bool eob = r == 63u;
         const uint32_t idx = pos + r;
@@ -411,6 +490,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             pcat = cat;
             has = true;
             pos = idx + 1u;
+            lc0 = lm == 1u ? pos_ctx(pos & 63u) : (lm == 2u ? cat_bucket(cat) : 0u);
         } else {
             ++b;
             blk += 64;
@@ -426,6 +506,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             pos = 1u;
             pcat = 0u;
             has = false;
+            lc0 = lm == 1u ? pos_ctx(1u) : (lm == 2u ? 4u : 0u);
         }
     }
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
@@ -993,12 +1074,14 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 
 // --------------------------------------------------------- decode-chain tuner
 //
-// Two tilings of the slice decode: one lane per slice (eight slices per warp:
-// cheap in issue slots, best when many slices share the GPU) and one warp
-// per slice (shorter step latency, best for small batches). The first batch
-// of each size class (by log2 of the colour-slice count) runs both and keeps
-// the faster; TCG_DCHAIN=lane|warp forces one.
-enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1 };
+// Tilings of the slice decode: one lane per slice with 8, 4, 2 or 1 slices
+// per warp (more slices per warp cost fewer issue slots, fewer cost less
+// divergence on each lane's chain), and one warp per slice (lanes hold the
+// alphabet; shortest step, most issue slots). The first batch of each size
+// class (by log2 of the colour-slice count) runs every tiling and keeps the
+// fastest; TCG_DCHAIN=lane|lane4|lane2|lane1|warp forces one ("lane" is 8).
+enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4,
+                    DCH_TILINGS = 5 };
 
 static std::mutex g_tune_mu;
 static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
@@ -1009,6 +1092,9 @@ static int dchain_forced()
     const char* v = getenv("TCG_DCHAIN");
     if (v == nullptr) { return -1; }
     if (strcmp(v, "lane") == 0) { return DCH_TILE_LANE; }
+    if (strcmp(v, "lane4") == 0) { return DCH_TILE_LANE4; }
+    if (strcmp(v, "lane2") == 0) { return DCH_TILE_LANE2; }
+    if (strcmp(v, "lane1") == 0) { return DCH_TILE_LANE1; }
     if (strcmp(v, "warp") == 0) { return DCH_TILE_WARP; }
     return -1;
 }
@@ -1160,42 +1246,70 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         TCG_LAUNCH(C, K_DTABLES, k_dtables, nc, 32, 0, d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
         static bool attr = false;
         if (!attr) {
-            TCG_CHECK(cudaFuncSetAttribute(k_dchain, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)DCH_SMEM));
+            TCG_CHECK(cudaFuncSetAttribute(k_dchain<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dch_smem(8)));
+            TCG_CHECK(cudaFuncSetAttribute(k_dchain<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dch_smem(4)));
             attr = true;
         }
         const size_t wsmem = (size_t)max_cols * 8u;  // two DC rows per slice (warp tiling)
+        auto run = [&](int tiling) -> int32_t {
+            switch (tiling) {
+            case DCH_TILE_WARP:
+                // the warp tiling writes every coefficient of the blocks it decodes
+                TCG_LAUNCH(C, K_DCHAIN_W, k_dchain_w, nc, 32, wsmem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
+                return TCG_OK;
+            case DCH_TILE_LANE4:
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                TCG_LAUNCH(C, K_DCHAIN, k_dchain<4>, (nc + 3u) / 4u, 32, dch_smem(4), d_sl, d_ord, nc, d_st, d_pl,
+                           d_pkt, d_tab, d_coef, d_status);
+                return TCG_OK;
+            case DCH_TILE_LANE2:
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                TCG_LAUNCH(C, K_DCHAIN, k_dchain<2>, (nc + 1u) / 2u, 32, dch_smem(2), d_sl, d_ord, nc, d_st, d_pl,
+                           d_pkt, d_tab, d_coef, d_status);
+                return TCG_OK;
+            case DCH_TILE_LANE1:
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                TCG_LAUNCH(C, K_DCHAIN, k_dchain<1>, nc, 32, dch_smem(1), d_sl, d_ord, nc, d_st, d_pl, d_pkt, d_tab,
+                           d_coef, d_status);
+                return TCG_OK;
+            default:
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                TCG_LAUNCH(C, K_DCHAIN, k_dchain<8>, (nc + 7u) / 8u, 32, dch_smem(8), d_sl, d_ord, nc, d_st, d_pl,
+                           d_pkt, d_tab, d_coef, d_status);
+                return TCG_OK;
+            }
+        };
         int tiling = dchain_forced();
-        bool measure = false;
         const uint32_t cls = size_class(nc);
         if (tiling < 0) {
             std::lock_guard<std::mutex> g(g_tune_mu);
             tiling = g_tune[cls];
-            measure = tiling < 0;
         }
-        cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
-        if (measure) {
+        if (tiling >= 0) {
+            const int32_t rc = run(tiling);
+            if (rc != TCG_OK) { return rc; }
+        } else {
+            // every tiling decodes the whole batch once, each timed on the stream; the
+            // last run's output stands (all tilings write identical results)
+            cudaEvent_t e[DCH_TILINGS + 1];
             for (auto& x : e) { TCG_CHECK(cudaEventCreate(&x)); }
             TCG_CHECK(cudaEventRecord(e[0], st));
-        }
-        if (measure || tiling == DCH_TILE_LANE) {
-            TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-            TCG_LAUNCH(C, K_DCHAIN, k_dchain, (nc + DCH_LANES - 1u) / DCH_LANES, 32, DCH_SMEM, d_sl, d_ord, nc, d_st,
-                       d_pl, d_pkt, d_tab, d_coef, d_status);
-        }
-        if (measure) { TCG_CHECK(cudaEventRecord(e[1], st)); }
-        if (measure || tiling == DCH_TILE_WARP) {
-            // the warp tiling writes every coefficient of the blocks it decodes
-            TCG_LAUNCH(C, K_DCHAIN_W, k_dchain_w, nc, 32, wsmem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
-        }
-        if (measure) {
-            TCG_CHECK(cudaEventRecord(e[2], st));
-            TCG_CHECK(cudaEventSynchronize(e[2]));
-            float ms_lane = 0.f, ms_warp = 0.f;
-            cudaEventElapsedTime(&ms_lane, e[0], e[1]);
-            cudaEventElapsedTime(&ms_warp, e[1], e[2]);
+            for (int k = 0; k < DCH_TILINGS; ++k) {
+                const int32_t rc = run(k);
+                if (rc != TCG_OK) { return rc; }
+                TCG_CHECK(cudaEventRecord(e[k + 1], st));
+            }
+            TCG_CHECK(cudaEventSynchronize(e[DCH_TILINGS]));
+            int best = 0;
+            float best_ms = 0.f;
+            for (int k = 0; k < DCH_TILINGS; ++k) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e[k], e[k + 1]);
+                if (k == 0 || ms < best_ms) { best = k; best_ms = ms; }
+            }
             for (auto& x : e) { cudaEventDestroy(x); }
             std::lock_guard<std::mutex> g(g_tune_mu);
-            g_tune[cls] = (int8_t)(ms_warp < ms_lane ? DCH_TILE_WARP : DCH_TILE_LANE);
+            g_tune[cls] = (int8_t)best;
         }
         TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_bs, d_st, d_pl, d_tab, d_coef,
                    d_status, (uint32_t)nblk, d_out);
