@@ -211,14 +211,14 @@ __device__ __forceinline__ void stg_if(int32_t* p, int32_t v, bool pred)
                  :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
 }
 
-// keep at least 32 bits in the window (branch-free; only the load is predicated)
+// keep at least 32 bits in the window: a window of 32 bits or fewer takes the
+// next stream word below its valid bits (branch-free; only the load is predicated)
 __device__ __forceinline__ void dl_refill(DLane& L)
 {
-    const bool need = L.wbits < 32u;
-    const uint32_t w = __byte_perm(L.nxt, 0u, 0x0123u);
-    const uint32_t sh = L.wbits & 31u;
-    L.whi |= need ? (w >> sh) : 0u;
-    L.wlo |= need ? (w << ((32u - sh) & 31u)) : 0u;
+    const bool need = L.wbits <= 32u;
+    const uint32_t w = need ? __byte_perm(L.nxt, 0u, 0x0123u) : 0u;
+    L.whi |= __funnelshift_rc(w, 0u, L.wbits);  // w >> wbits
+    L.wlo |= __funnelshift_rc(0u, w, L.wbits);  // w << (32 - wbits)
     L.wbits += need ? 32u : 0u;
     L.wi += need ? 1u : 0u;
     L.nxt = ldg_nc_if(L.wb + L.wi, L.nxt, need && L.wi < L.wn);
@@ -443,32 +443,66 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     uint32_t b = 0, bx = 0;  // current block within the slice, its column
     uint32_t pos = 1u, pcat = 0u;
     bool has = false;
-    // run symbol 0 covers slots [0, f0) (f0 = 0 when it does not occur)
-    const uint32_t f0 = cum_run[1];
+    // Run symbol 0 covers slots [0, f0) (f0 = 0 when it does not occur). The
+    // fast iteration below needs a state below 2^31; a state in [2^23, 2^31)
+    // stays there, so only a damaged stream's first state can break that, and
+    // such a slice runs the general iteration throughout.
+    const uint32_t f0 = L.x < 0x80000000u ? cum_run[1] : 0u;
     // level context of the coefficient at pos if the next run is 0
     uint32_t lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? 4u : 0u);
-    while (err == 0u) {
-        // Fast iteration: run 0 with a state that needs no renormalisation (in
-        // [2^23, 2^31)), i.e. one multiply-add, then the level at pos through a
-        // bucket entry read before that condition is known.
+    for (;;) {
+        // at least 32 bits in the window; the fast iteration needs 40 (a level
+        // symbol takes up to 16, its suffix up to 24)
+        dl_refill(L);
+        // Fast iteration: run 0 with a state that needs no renormalisation,
+        // i.e. one multiply-add, then the level at pos through a bucket entry
+        // read before that condition is known.
         const uint32_t x = L.x, slot = x & 4095u;
         const uint32_t x1 = f0 * (x >> 12) + slot;
         const uint32_t* lutc = lut_lvl + lc0 * LUT_BUCKETS;
         const uint32_t e1 = lutc[(x1 & 4095u) >> 4];
-        if (slot < f0 && x1 - RANS_L < 0x7F800000u && pos < 64u) {
+        if (slot < f0 && x1 >= RANS_L && pos < 64u && L.wbits >= 40u) {
             L.x = x1;
-            uint32_t lz;
-            const uint32_t cat = dl_sym_entry(L, e1, cum_lvl + lc0 * CUM_LEN, lz);
-            m = dl_suffix_lz(L, cat, lz);
+            const uint32_t slot1 = x1 & 4095u;
+            uint32_t cat = e1 & 63u;
+            const uint32_t c0 = (e1 >> 6) & 0xFFFu, c1 = e1 >> 18;
+            int32_t level;
+            if (slot1 < c1 && cat - 1u < 24u) {
+                // the bucket's first symbol, a category of 1..24: one chunk of
+                // cat-1 <= 23 bits, renormalised by the count the level's
+                // leading zeros give (the state after a step lies in
+                // [2^23, 2^31), 1..8 leading zeros; the chunk adds b)
+                const uint32_t xn = (c1 - c0) * (x1 >> 12) + slot1 - c0;
+                const uint32_t lz = (uint32_t)__clz((int32_t)xn);
+                const uint32_t n8 = (lz - 1u) & 0x18u;
+                const uint32_t x2 = __funnelshift_l(L.whi, xn, n8);
+                uint32_t whi = __funnelshift_l(L.wlo, L.whi, n8);
+                uint32_t wlo = L.wlo << n8;
+                const uint32_t bw = cat - 1u, hb = 1u << bw;
+                const uint32_t mm = (x2 & (hb - 1u)) | hb;
+                const uint32_t n8s = (lz - n8 + bw - 1u) & 0x18u;
+                L.x = __funnelshift_l(whi, x2 >> bw, n8s);
+                L.whi = __funnelshift_l(wlo, whi, n8s);
+                L.wlo = wlo << n8s;
+                L.wbits -= n8 + n8s;
+                level = unmap_s(mm);
+            } else {
+                // bucket walk, a category of 0 or above 24: the general steps
+                uint32_t lz;
+                cat = dl_sym_entry(L, e1, cum_lvl + lc0 * CUM_LEN, lz);
+                m = dl_suffix(L, cat);
+                err |= m > mlv ? 1u : 0u;
+                level = unmap_s(m);
+            }
             dl_prefetch(L);
-            err |= m > mlv ? 1u : 0u;
-            stg_if(blk + zz[pos], unmap_s(m), true);
+            stg_if(blk + zz[pos], level, true);
             pcat = cat;
             has = true;
             ++pos;
             lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? cat_bucket(cat) : 0u);
             continue;
         }
+        if (err != 0u) { break; }
         // general iteration: any run symbol, end of block and the next block's DC
         const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
         const bool eob = r == 63u;
