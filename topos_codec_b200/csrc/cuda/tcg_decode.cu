@@ -139,12 +139,13 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
         if (ok) {
             uint16_t* cd = reinterpret_cast<uint16_t*>(tb + TAB_CUM + (size_t)ctx * CUM_BYTES);
             for (uint32_t k = 0; k < CUM_LEN; ++k) { cd[k] = k < n ? cu[k] : (uint16_t)4096u; }
-            // bucket b (slots 16b..16b+15) records the symbol holding slot 16b
+            // bucket b (slots 16b..16b+15) records the symbol holding slot 16b:
+            // its cumulative start (bits 0-11), index (12-17) and frequency (18-30)
             uint32_t* lut = reinterpret_cast<uint32_t*>(tb + TAB_LUT + (size_t)ctx * LUT_BYTES);
             for (uint32_t sy = 0; sy < n; ++sy) {
                 const uint32_t c0 = cu[sy], c1 = c0 + fr[sy];
                 for (uint32_t bk = (c0 + 15u) >> 4; bk < LUT_BUCKETS && (bk << 4) < c1; ++bk) {
-                    lut[bk] = sy | (c0 << 6) | (c1 << 18);
+                    lut[bk] = c0 | (sy << 12) | ((uint32_t)fr[sy] << 18);
                 }
             }
         }
@@ -184,7 +185,12 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
 constexpr uint32_t DCH_LUT_SLOTS = 7u;  // shared-memory bucket tables per slice
 constexpr uint32_t DCH_CUM_BYTES = (MAX_CTX * CUM_BYTES + 15u) & ~15u;
 constexpr uint32_t DCH_LANE_BYTES = DCH_LUT_SLOTS * LUT_BYTES + DCH_CUM_BYTES;
-__host__ __device__ constexpr uint32_t dch_smem(uint32_t lanes) { return 64u + lanes * DCH_LANE_BYTES; }
+// block head: zigzag order (64 bytes), then the level-context table: three
+// rows of 80 u16 (level models by position / by previous category / single),
+// each the offset of a context's bucket table in u32 words
+constexpr uint32_t DCH_CTX_ROW = 80u;
+constexpr uint32_t DCH_HEAD = 64u + ((3u * DCH_CTX_ROW * 2u + 15u) & ~15u);
+__host__ __device__ constexpr uint32_t dch_smem(uint32_t lanes) { return DCH_HEAD + lanes * DCH_LANE_BYTES; }
 
 struct DLane {
     uint32_t x;            // coder state
@@ -192,23 +198,19 @@ struct DLane {
     uint32_t wbits;        // valid bits in whi:wlo
     uint32_t nxt;          // stream word wi (memory byte order)
     uint32_t wi, wn;       // word index of nxt; words overlapping the payload
+    uint32_t wlast;        // last word a load may touch (max(wn, 1) - 1)
     uint32_t a8;           // bit offset of the payload in its first word
     const uint32_t* wb;    // first word of the payload (aligned down)
 };
 
-// Predicated global load / store: a predicate, not a branch.
+// Predicated global load (a predicate, not a branch) that also asks L2 for
+// the 256-byte segment around the word: the stream is read forwards.
 __device__ __forceinline__ uint32_t ldg_nc_if(const uint32_t* p, uint32_t old, bool pred)
 {
     uint32_t v = old;
-    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.global.nc.u32 %0, [%1];\n\t}"
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q ld.global.nc.L2::256B.u32 %0, [%1];\n\t}"
         : "+r"(v) : "l"(p), "r"((uint32_t)pred));
     return v;
-}
-
-__device__ __forceinline__ void stg_if(int32_t* p, int32_t v, bool pred)
-{
-    asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\t@q st.global.s32 [%0], %1;\n\t}"
-                 :: "l"(p), "r"(v), "r"((uint32_t)pred) : "memory");
 }
 
 // keep at least 32 bits in the window: a window of 32 bits or fewer takes the
@@ -221,15 +223,9 @@ __device__ __forceinline__ void dl_refill(DLane& L)
     L.wlo |= __funnelshift_rc(0u, w, L.wbits);  // w << (32 - wbits)
     L.wbits += need ? 32u : 0u;
     L.wi += need ? 1u : 0u;
-    L.nxt = ldg_nc_if(L.wb + L.wi, L.nxt, need && L.wi < L.wn);
-}
-
-// bring the stream 256 bytes ahead of the window into L1 (once per loop iteration)
-__device__ __forceinline__ void dl_prefetch(const DLane& L)
-{
-    const uint32_t pf = (uint32_t)(L.wi + 64u < L.wn);
-    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
-                 :: "l"(L.wb + L.wi + 64u), "r"(pf));
+    // past the payload the load repeats its last word: those bits are only
+    // consumed by a damaged stream, which the consumed-byte count rejects
+    L.nxt = ldg_nc_if(L.wb + min(L.wi, L.wlast), L.nxt, need);
 }
 
 // state <- xn followed by the stream bytes that bring it to [2^23, ...): the
@@ -261,6 +257,7 @@ __device__ __forceinline__ void dl_init(DLane& L, const uint8_t* b, uint32_t n)
     const uintptr_t a = (uintptr_t)b;
     L.wb = reinterpret_cast<const uint32_t*>(a & ~(uintptr_t)3);
     L.wn = (uint32_t)((((a + n + 3u) & ~(uintptr_t)3) - (uintptr_t)L.wb) >> 2);
+    L.wlast = L.wn > 0u ? L.wn - 1u : 0u;
     L.a8 = (uint32_t)(a & 3u) * 8u;
     const uint32_t w0 = __byte_perm(__ldg(L.wb), 0u, 0x0123u);
     const uint32_t w1 = 1u < L.wn ? __byte_perm(__ldg(L.wb + 1), 0u, 0x0123u) : 0u;
@@ -280,7 +277,7 @@ __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool u
 {
     const uint32_t x = L.x, slot = x & 4095u;
     const uint32_t e = use_lut ? lut[slot >> 4] : ((uint32_t)cum[1] << 18);
-    uint32_t s = e & 63u, c0 = (e >> 6) & 0xFFFu, c1 = e >> 18;
+    uint32_t s = (e >> 12) & 63u, c0 = e & 0xFFFu, c1 = c0 + (e >> 18);
     while (slot >= c1 && s < CUM_LEN - 2u) {
         ++s;
         c0 = c1;
@@ -297,57 +294,6 @@ __device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
     dl_renorm<true>(L, L.x >> w);
     return v;
 }
-
-// One symbol whose bucket entry e was read already, for a state below 2^31.
-// Renormalises without refilling and returns the symbol; lz receives the
-// leading-zero count of the new state (1..8: the state lies in [2^23, 2^31)).
-__device__ __forceinline__ uint32_t dl_sym_entry(DLane& L, uint32_t e, const uint16_t* cum, uint32_t& lz)
-{
-    const uint32_t x = L.x, slot = x & 4095u;
-    uint32_t s = e & 63u, c0 = (e >> 6) & 0xFFFu, c1 = e >> 18;
-    while (slot >= c1 && s < CUM_LEN - 2u) {
-        ++s;
-        c0 = c1;
-        c1 = cum[s + 1u];
-    }
-    // x < 2^31 and a symbol of frequency >= 1: xn in [2^11, 2^31), so 1..20 leading zeros
-    const uint32_t xn = (c1 - c0) * (x >> 12) + slot - c0;
-    const uint32_t lzn = (uint32_t)__clz((int32_t)xn);
-    const uint32_t n8 = (lzn - 1u) & 0x18u;
-    L.x = __funnelshift_l(L.whi, xn, n8);
-    L.whi = __funnelshift_l(L.wlo, L.whi, n8);
-    L.wlo <<= n8;
-    L.wbits -= n8;
-    lz = lzn - n8;
-    return s;
-}
-
-// Category suffix after a symbol step that left lz leading zeros in the state:
-// a chunk of b <= 23 bits leaves x >> b with lz + b leading zeros, so its
-// renormalisation needs no second count. Refills before (a chunk takes up to
-// 24 bits) and after.
-__device__ __forceinline__ uint32_t dl_suffix_lz(DLane& L, uint32_t cat, uint32_t lz)
-{
-    dl_refill(L);
-    const uint32_t b = cat > 1u ? cat - 1u : 0u;
-    uint32_t v;
-    if (b <= 23u) {
-        v = L.x & ~(0xFFFFFFFFu << b);
-        const uint32_t xn = L.x >> b;
-        const uint32_t n8 = (lz + b - 1u) & 0x18u;
-        L.x = __funnelshift_l(L.whi, xn, n8);
-        L.whi = __funnelshift_l(L.wlo, L.whi, n8);
-        L.wlo <<= n8;
-        L.wbits -= n8;
-        dl_refill(L);
-    } else {
-        const uint32_t lo = dl_chunk(L, 16u);
-        const uint32_t w2 = b - 16u;
-        v = (dl_chunk(L, w2 <= 23u ? w2 : 23u) << 16) | lo;
-    }
-    return cat == 0u ? 0u : (1u << ((cat - 1u) & 31u)) | v;
-}
-
 
 // category suffix: m = 2^(cat-1) | (cat-1 raw bits), split 16 + rest above 23
 __device__ __forceinline__ uint32_t dl_suffix(DLane& L, uint32_t cat)
@@ -373,9 +319,17 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
 {
     extern __shared__ __align__(16) uint8_t dsm[];
     uint8_t* zz = dsm;  // zigzag order, shared by the lanes
+    uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm + 64u);
     const uint32_t t = threadIdx.x;
     zz[t] = c_zigzag[t];
     zz[t + 32u] = c_zigzag[t + 32u];
+    // row 1 indexed by the next position (1..64), row 2 by the previous level's
+    // category (0..63; index 79 = no previous level in the block), row 0 zero
+    for (uint32_t i = t; i < 3u * DCH_CTX_ROW; i += 32u) {
+        const uint32_t row = i / DCH_CTX_ROW, k = i % DCH_CTX_ROW;
+        const uint32_t ctx = row == 1u ? pos_ctx(k) : (row == 2u ? (k < 64u ? cat_bucket(k) : 4u) : 0u);
+        ctab[i] = (uint16_t)(ctx * LUT_BUCKETS);
+    }
     // stage every lane's tables: run and level contexts always, DC contexts when they fit
     const uint32_t i0 = blockIdx.x * LANES;
     for (uint32_t l = 0; l < LANES && i0 + l < nc; ++l) {
@@ -386,7 +340,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const uint32_t lm = hdr[0], dm = hdr[1];
         const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u, nd = dm ? DCP_CTX : 1u;
         const uint32_t ndl = 1u + nl + nd <= DCH_LUT_SLOTS ? nd : 0u;
-        uint8_t* ls = dsm + 64u + (size_t)l * DCH_LANE_BYTES;
+        uint8_t* ls = dsm + DCH_HEAD + (size_t)l * DCH_LANE_BYTES;
         const uint32_t nlut = 1u + nl + ndl;
         for (uint32_t k = t; k < nlut * (LUT_BYTES / 16u); k += 32u) {
             const uint32_t slot = k / (LUT_BYTES / 16u), part = k % (LUT_BYTES / 16u);
@@ -409,7 +363,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
     const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u, nd = dm ? DCP_CTX : 1u;
     const bool dc_lut = 1u + nl + nd <= DCH_LUT_SLOTS;
-    const uint8_t* ls = dsm + 64u + (size_t)t * DCH_LANE_BYTES;
+    const uint8_t* ls = dsm + DCH_HEAD + (size_t)t * DCH_LANE_BYTES;
     const uint32_t* lut_run = reinterpret_cast<const uint32_t*>(ls);
     const uint32_t* lut_lvl = lut_run + LUT_BUCKETS;                               // + ctx * LUT_BUCKETS
     const uint32_t* lut_dc = dc_lut ? lut_lvl + nl * LUT_BUCKETS : lut_run;      // + ctx * LUT_BUCKETS when dc_lut
@@ -448,58 +402,48 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     // stays there, so only a damaged stream's first state can break that, and
     // such a slice runs the general iteration throughout.
     const uint32_t f0 = L.x < 0x80000000u ? cum_run[1] : 0u;
-    // level context of the coefficient at pos if the next run is 0
-    uint32_t lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? 4u : 0u);
+    // level context (bucket-table offset) of the coefficient at pos if the next
+    // run is 0: by position (lm 1), by the previous level's category (lm 2)
+    const bool by_pos = lm == 1u;
+    const uint16_t* ctl = ctab + (lm == 1u ? 1u : (lm == 2u ? 2u : 0u)) * DCH_CTX_ROW;
+    uint32_t lc0 = ctl[by_pos ? 1u : 79u];
     for (;;) {
         // at least 32 bits in the window; the fast iteration needs 40 (a level
         // symbol takes up to 16, its suffix up to 24)
         dl_refill(L);
-        // Fast iteration: run 0 with a state that needs no renormalisation,
-        // i.e. one multiply-add, then the level at pos through a bucket entry
-        // read before that condition is known.
+        // Fast iteration, computed in one straight line and kept only when it
+        // applies: run symbol 0 with a state that needs no renormalisation
+        // (one multiply-add), then the level at pos from its bucket entry when
+        // the slot lies in the bucket's first symbol and the category is 1..24,
+        // whose suffix is one chunk of cat-1 <= 23 bits. That chunk's
+        // renormalisation count follows from the level step's leading zeros:
+        // the state after a step lies in [2^23, 2^31) (1..8 leading zeros) and
+        // the chunk adds cat-1.
         const uint32_t x = L.x, slot = x & 4095u;
         const uint32_t x1 = f0 * (x >> 12) + slot;
-        const uint32_t* lutc = lut_lvl + lc0 * LUT_BUCKETS;
-        const uint32_t e1 = lutc[(x1 & 4095u) >> 4];
-        if (slot < f0 && x1 >= RANS_L && pos < 64u && L.wbits >= 40u) {
-            L.x = x1;
-            const uint32_t slot1 = x1 & 4095u;
-            uint32_t cat = e1 & 63u;
-            const uint32_t c0 = (e1 >> 6) & 0xFFFu, c1 = e1 >> 18;
-            int32_t level;
-            if (slot1 < c1 && cat - 1u < 24u) {
-                // the bucket's first symbol, a category of 1..24: one chunk of
-                // cat-1 <= 23 bits, renormalised by the count the level's
-                // leading zeros give (the state after a step lies in
-                // [2^23, 2^31), 1..8 leading zeros; the chunk adds b)
-                const uint32_t xn = (c1 - c0) * (x1 >> 12) + slot1 - c0;
-                const uint32_t lz = (uint32_t)__clz((int32_t)xn);
-                const uint32_t n8 = (lz - 1u) & 0x18u;
-                const uint32_t x2 = __funnelshift_l(L.whi, xn, n8);
-                uint32_t whi = __funnelshift_l(L.wlo, L.whi, n8);
-                uint32_t wlo = L.wlo << n8;
-                const uint32_t bw = cat - 1u, hb = 1u << bw;
-                const uint32_t mm = (x2 & (hb - 1u)) | hb;
-                const uint32_t n8s = (lz - n8 + bw - 1u) & 0x18u;
-                L.x = __funnelshift_l(whi, x2 >> bw, n8s);
-                L.whi = __funnelshift_l(wlo, whi, n8s);
-                L.wlo = wlo << n8s;
-                L.wbits -= n8 + n8s;
-                level = unmap_s(mm);
-            } else {
-                // bucket walk, a category of 0 or above 24: the general steps
-                uint32_t lz;
-                cat = dl_sym_entry(L, e1, cum_lvl + lc0 * CUM_LEN, lz);
-                m = dl_suffix(L, cat);
-                err |= m > mlv ? 1u : 0u;
-                level = unmap_s(m);
-            }
-            dl_prefetch(L);
-            stg_if(blk + zz[pos], level, true);
+        const uint32_t slot1 = x1 & 4095u;
+        const uint32_t e1 = lut_lvl[lc0 + (slot1 >> 4)];
+        const uint32_t c0 = e1 & 0xFFFu, cat = (e1 >> 12) & 63u, fq = e1 >> 18;
+        const uint32_t d = slot1 - c0;
+        const uint32_t xn = fq * (x1 >> 12) + d;
+        const uint32_t lz = (uint32_t)__clz((int32_t)xn);
+        const uint32_t n8 = (lz - 1u) & 0x18u;
+        const uint32_t x2 = __funnelshift_l(L.whi, xn, n8);
+        const uint32_t whi2 = __funnelshift_l(L.wlo, L.whi, n8);
+        const uint32_t wlo2 = L.wlo << n8;
+        const uint32_t bw = (cat - 1u) & 31u, hb = 1u << bw;
+        const uint32_t mm = (x2 & (hb - 1u)) | hb;
+        const uint32_t n8s = (lz - n8 + bw - 1u) & 0x18u;
+        if (slot < f0 && x1 >= RANS_L && pos < 64u && L.wbits >= 40u && d < fq && cat - 1u < 24u) {
+            L.x = __funnelshift_l(whi2, x2 >> bw, n8s);
+            L.whi = __funnelshift_l(wlo2, whi2, n8s);
+            L.wlo = wlo2 << n8s;
+            L.wbits -= n8 + n8s;
+            blk[zz[pos]] = unmap_s(mm);
+            ++pos;
             pcat = cat;
             has = true;
-            ++pos;
-            lc0 = lm == 1u ? pos_ctx(pos) : (lm == 2u ? cat_bucket(cat) : 0u);
+            lc0 = ctl[by_pos ? pos : cat];
             continue;
         }
         if (err != 0u) { break; }
@@ -515,16 +459,15 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const uint32_t* lut = eob ? (dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run) : lut_lvl + lc * LUT_BUCKETS;
         const uint16_t* cum = eob ? cum_dc + dctx * CUM_LEN : cum_lvl + lc * CUM_LEN;
         const bool use_lut = !eob || dc_lut;
-        const uint32_t cat = dl_sym<true>(L, lut, use_lut, cum);
-        m = dl_suffix(L, cat);
-        dl_prefetch(L);
+        const uint32_t sc = dl_sym<true>(L, lut, use_lut, cum);
+        m = dl_suffix(L, sc);
         if (!eob) {
             err |= m > mlv ? 1u : 0u;
-            stg_if(blk + zz[idx], unmap_s(m), true);
-            pcat = cat;
+            blk[zz[idx]] = unmap_s(m);
+            pcat = sc;
             has = true;
             pos = idx + 1u;
-            lc0 = lm == 1u ? pos_ctx(pos & 63u) : (lm == 2u ? cat_bucket(cat) : 0u);
+            lc0 = ctl[by_pos ? pos : sc];
         } else {
             ++b;
             blk += 64;
@@ -536,11 +479,11 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             left = (int32_t)dcv;
             blk[0] = left;
             top_next = (b + 1u < nblk && b + 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
-            prev_dcc = cat;
+            prev_dcc = sc;
             pos = 1u;
             pcat = 0u;
             has = false;
-            lc0 = lm == 1u ? pos_ctx(1u) : (lm == 2u ? 4u : 0u);
+            lc0 = ctl[by_pos ? 1u : 79u];
         }
     }
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
