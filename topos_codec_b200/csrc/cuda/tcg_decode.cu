@@ -213,6 +213,17 @@ __device__ __forceinline__ uint32_t ldg_nc_if(const uint32_t* p, uint32_t old, b
     return v;
 }
 
+// next stream word (a window of 32 bits or fewer takes it below its valid bits)
+__device__ __forceinline__ void dl_take_word(DLane& L)
+{
+    const uint32_t w = __byte_perm(L.nxt, 0u, 0x0123u);
+    L.whi |= __funnelshift_rc(w, 0u, L.wbits);  // w >> wbits
+    L.wlo |= __funnelshift_rc(0u, w, L.wbits);  // w << (32 - wbits)
+    L.wbits += 32u;
+    L.wi += 1u;
+    L.nxt = ldg_nc_if(L.wb + min(L.wi, L.wlast), L.nxt, true);
+}
+
 // keep at least 32 bits in the window: a window of 32 bits or fewer takes the
 // next stream word below its valid bits (branch-free; only the load is predicated)
 __device__ __forceinline__ void dl_refill(DLane& L)
@@ -408,9 +419,6 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     const uint16_t* ctl = ctab + (lm == 1u ? 1u : (lm == 2u ? 2u : 0u)) * DCH_CTX_ROW;
     uint32_t lc0 = ctl[by_pos ? 1u : 79u];
     for (;;) {
-        // at least 32 bits in the window; the fast iteration needs 40 (a level
-        // symbol takes up to 16, its suffix up to 24)
-        dl_refill(L);
         // Fast iteration, computed in one straight line and kept only when it
         // applies: run symbol 0 with a state that needs no renormalisation
         // (one multiply-add), then the level at pos from its bucket entry when
@@ -423,6 +431,10 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const uint32_t x1 = f0 * (x >> 12) + slot;
         const uint32_t slot1 = x1 & 4095u;
         const uint32_t e1 = lut_lvl[lc0 + (slot1 >> 4)];
+        // at least 32 bits in the window (a branch: about every other
+        // iteration); the fast iteration needs 40 (a level symbol takes up to
+        // 16, its suffix up to 24)
+        if (L.wbits <= 32u) { dl_take_word(L); }
         const uint32_t c0 = e1 & 0xFFFu, cat = (e1 >> 12) & 63u, fq = e1 >> 18;
         const uint32_t d = slot1 - c0;
         const uint32_t xn = fq * (x1 >> 12) + d;
@@ -439,7 +451,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             L.whi = __funnelshift_l(wlo2, whi2, n8s);
             L.wlo = wlo2 << n8s;
             L.wbits -= n8 + n8s;
-            blk[zz[pos]] = unmap_s(mm);
+            blk[zz[pos]] = (int32_t)mm;
             ++pos;
             pcat = cat;
             has = true;
@@ -463,7 +475,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         m = dl_suffix(L, sc);
         if (!eob) {
             err |= m > mlv ? 1u : 0u;
-            blk[zz[idx]] = unmap_s(m);
+            blk[zz[idx]] = (int32_t)m;
             pcat = sc;
             has = true;
             pos = idx + 1u;
@@ -717,7 +729,7 @@ __device__ __forceinline__ int32_t dchain_slice(const DSlice& S, const DPlane& P
                 const uint32_t m = dec_suffix(w, cat, lane);
                 err |= m > mlv ? 1u : 0u;
                 const uint32_t nat = c_zigzag[idx];
-                const int32_t v = unmap_s(m);
+                const int32_t v = (int32_t)m;  // zigzag-mapped; reconstruction unmaps
                 if ((nat & 31u) == lane) {
                     if (nat & 32u) { chi = v; } else { clo = v; }
                 }
@@ -767,6 +779,10 @@ __global__ void __launch_bounds__(32) k_dchain_w(const DSlice* __restrict__ slic
 }
 
 // ------------------------------------------------------------------ reconstruction
+//
+// Coefficient blocks hold the DC value at index 0 (signed) and the AC levels
+// in their zigzag-mapped form (m = 2v or -2v-1), which the chains store as
+// decoded; 0 maps to 0, so untouched positions read as zero levels.
 
 __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ blk_slice,
                                                const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
@@ -792,7 +808,8 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
         const int32_t vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            int64_t f = (int64_t)vv[j] * __ldg(Q + i * 4 + j);
+            const int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
+            int64_t f = (int64_t)lv * __ldg(Q + i * 4 + j);
             f = f > fc ? fc : (f < -fc ? -fc : f);
             c[i * 4 + j] = (int32_t)f;
         }
