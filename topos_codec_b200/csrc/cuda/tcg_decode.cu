@@ -140,12 +140,16 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
             uint16_t* cd = reinterpret_cast<uint16_t*>(tb + TAB_CUM + (size_t)ctx * CUM_BYTES);
             for (uint32_t k = 0; k < CUM_LEN; ++k) { cd[k] = k < n ? cu[k] : (uint16_t)4096u; }
             // bucket b (slots 16b..16b+15) records the symbol holding slot 16b:
-            // its cumulative start (bits 0-11), index (12-17) and frequency (18-30)
+            // its cumulative start (bits 0-11), index (12-17) and, for symbols
+            // 0..24 (the categories whose suffix is at most one 23-bit chunk;
+            // 1..24 for levels), frequency (18-30); 0 there sends the chain to
+            // its general step
             uint32_t* lut = reinterpret_cast<uint32_t*>(tb + TAB_LUT + (size_t)ctx * LUT_BYTES);
             for (uint32_t sy = 0; sy < n; ++sy) {
                 const uint32_t c0 = cu[sy], c1 = c0 + fr[sy];
+                const uint32_t ff = (sy <= 24u && (ctx < 6u || sy != 0u)) ? (uint32_t)fr[sy] : 0u;
                 for (uint32_t bk = (c0 + 15u) >> 4; bk < LUT_BUCKETS && (bk << 4) < c1; ++bk) {
-                    lut[bk] = c0 | (sy << 12) | ((uint32_t)fr[sy] << 18);
+                    lut[bk] = c0 | (sy << 12) | (ff << 18);
                 }
             }
         }
@@ -277,7 +281,7 @@ __device__ __forceinline__ void dl_init(DLane& L, const uint8_t* b, uint32_t n)
     L.wlo = 0u;
     L.wbits = 32u - L.a8;
     L.wi = 2u;
-    L.nxt = 2u < L.wn ? __ldg(L.wb + 2) : 0u;
+    L.nxt = __ldg(L.wb + min(2u, L.wlast));
     dl_refill(L);
 }
 
@@ -287,8 +291,8 @@ template <bool Refill>
 __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool use_lut, const uint16_t* cum)
 {
     const uint32_t x = L.x, slot = x & 4095u;
-    const uint32_t e = use_lut ? lut[slot >> 4] : ((uint32_t)cum[1] << 18);
-    uint32_t s = (e >> 12) & 63u, c0 = e & 0xFFFu, c1 = c0 + (e >> 18);
+    const uint32_t e = use_lut ? lut[slot >> 4] : 0u;
+    uint32_t s = (e >> 12) & 63u, c0 = e & 0xFFFu, c1 = cum[s + 1u];
     while (slot >= c1 && s < CUM_LEN - 2u) {
         ++s;
         c0 = c1;
@@ -364,9 +368,11 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         }
     }
     __syncthreads();
-    if (t >= LANES || i0 + t >= nc) { return; }
+    // the lanes with a slice to decode; they stay together until all are done
+    const bool live = t < LANES && i0 + t < nc && status[order[i0 + t]] == 0;
+    const uint32_t wmask = __ballot_sync(0xFFFFFFFFu, live);
+    if (!live) { return; }
     const uint32_t si = order[i0 + t];
-    if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
     const uint8_t* tb = tabs + (size_t)slice_tab[si] * DTAB_BYTES;
@@ -412,21 +418,38 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     // fast iteration below needs a state below 2^31; a state in [2^23, 2^31)
     // stays there, so only a damaged stream's first state can break that, and
     // such a slice runs the general iteration throughout.
-    const uint32_t f0 = L.x < 0x80000000u ? cum_run[1] : 0u;
+    const bool x_ok = L.x < 0x80000000u;
+    const uint32_t f0 = x_ok ? cum_run[1] : 0u;
     // level context (bucket-table offset) of the coefficient at pos if the next
     // run is 0: by position (lm 1), by the previous level's category (lm 2)
     const bool by_pos = lm == 1u;
     const uint16_t* ctl = ctab + (lm == 1u ? 1u : (lm == 2u ? 2u : 0u)) * DCH_CTX_ROW;
     uint32_t lc0 = ctl[by_pos ? 1u : 79u];
-    for (;;) {
+    // Lanes of a warp take the same path most of the time; the warp regathers
+    // at the top of every iteration (a lane that left for the general step
+    // would otherwise run apart from the others until the loop ends), and a
+    // finished lane idles until a vote every 8 iterations finds all done. A
+    // single lane leaves the loop at once.
+#define DCH_FINISH()                                         \
+    {                                                        \
+        if constexpr (LANES > 1u) { done = true; continue; } \
+        else { break; }                                      \
+    }
+    bool done = false;
+    for (uint32_t it = 1u;; ++it) {
+        if constexpr (LANES > 1u) {
+            __syncwarp(wmask);
+            if ((it & 7u) == 0u && __all_sync(wmask, done)) { break; }
+            if (done) { continue; }
+        }
         // Fast iteration, computed in one straight line and kept only when it
         // applies: run symbol 0 with a state that needs no renormalisation
         // (one multiply-add), then the level at pos from its bucket entry when
-        // the slot lies in the bucket's first symbol and the category is 1..24,
-        // whose suffix is one chunk of cat-1 <= 23 bits. That chunk's
-        // renormalisation count follows from the level step's leading zeros:
-        // the state after a step lies in [2^23, 2^31) (1..8 leading zeros) and
-        // the chunk adds cat-1.
+        // the slot lies in the bucket's first symbol and the category is 1..24
+        // (entries carry frequency 0 otherwise), whose suffix is one chunk of
+        // cat-1 <= 23 bits. That chunk's renormalisation count follows from
+        // the level step's leading zeros: the state after a step lies in
+        // [2^23, 2^31) (1..8 leading zeros) and the chunk adds cat-1.
         const uint32_t x = L.x, slot = x & 4095u;
         const uint32_t x1 = f0 * (x >> 12) + slot;
         const uint32_t slot1 = x1 & 4095u;
@@ -446,7 +469,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         const uint32_t bw = (cat - 1u) & 31u, hb = 1u << bw;
         const uint32_t mm = (x2 & (hb - 1u)) | hb;
         const uint32_t n8s = (lz - n8 + bw - 1u) & 0x18u;
-        if (slot < f0 && x1 >= RANS_L && pos < 64u && L.wbits >= 40u && d < fq && cat - 1u < 24u) {
+        if (slot < f0 && x1 >= RANS_L && pos < 64u && L.wbits >= 40u && d < fq) {
             L.x = __funnelshift_l(whi2, x2 >> bw, n8s);
             L.whi = __funnelshift_l(wlo2, whi2, n8s);
             L.wlo = wlo2 << n8s;
@@ -458,22 +481,25 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             lc0 = ctl[by_pos ? pos : cat];
             continue;
         }
-        if (err != 0u) { break; }
+        if (err != 0u) { DCH_FINISH(); }
         // general iteration: any run symbol, end of block and the next block's DC
         const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
-        const bool eob = r == 63u;
+        const bool geob = r == 63u;
         const uint32_t idx = pos + r;
-        if (!eob && idx > 63u) { err = 1u; break; }
-        if (eob && b + 1u >= nblk) { break; }  // last block done
+        if (!geob && idx > 63u) {
+            err = 1u;
+            DCH_FINISH();
+        }
+        if (geob && b + 1u >= nblk) { DCH_FINISH(); }  // last block done
         // second symbol: the level (context by position or previous level) or the next block's DC
         const uint32_t lc = lm == 1u ? pos_ctx(idx & 63u) : (lm == 2u ? prev_ctx(pcat, has) : 0u);
         const uint32_t dctx = dm ? dcp_ctx(prev_dcc, true) : 0u;
-        const uint32_t* lut = eob ? (dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run) : lut_lvl + lc * LUT_BUCKETS;
-        const uint16_t* cum = eob ? cum_dc + dctx * CUM_LEN : cum_lvl + lc * CUM_LEN;
-        const bool use_lut = !eob || dc_lut;
+        const uint32_t* lut = geob ? (dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run) : lut_lvl + lc * LUT_BUCKETS;
+        const uint16_t* cum = geob ? cum_dc + dctx * CUM_LEN : cum_lvl + lc * CUM_LEN;
+        const bool use_lut = !geob || dc_lut;
         const uint32_t sc = dl_sym<true>(L, lut, use_lut, cum);
         m = dl_suffix(L, sc);
-        if (!eob) {
+        if (!geob) {
             err |= m > mlv ? 1u : 0u;
             blk[zz[idx]] = (int32_t)m;
             pcat = sc;
@@ -498,6 +524,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             lc0 = ctl[by_pos ? 1u : 79u];
         }
     }
+#undef DCH_FINISH
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
@@ -1068,6 +1095,12 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 
 // --------------------------------------------------------- decode-chain tuner
 //
+// lane-tiling instantiations (named so the launch macro sees one argument)
+#define K_DCHAIN_L8 k_dchain<8>
+#define K_DCHAIN_L4 k_dchain<4>
+#define K_DCHAIN_L2 k_dchain<2>
+#define K_DCHAIN_L1 k_dchain<1>
+
 // Tilings of the slice decode: one lane per slice with 8, 4, 2 or 1 slices
 // per warp (more slices per warp cost fewer issue slots, fewer cost less
 // divergence on each lane's chain), and one warp per slice (lanes hold the
@@ -1253,22 +1286,22 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
                 return TCG_OK;
             case DCH_TILE_LANE4:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-                TCG_LAUNCH(C, K_DCHAIN, k_dchain<4>, (nc + 3u) / 4u, 32, dch_smem(4), d_sl, d_ord, nc, d_st, d_pl,
+                TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L4, (nc + 3u) / 4u, 32, dch_smem(4), d_sl, d_ord, nc, d_st, d_pl,
                            d_pkt, d_tab, d_coef, d_status);
                 return TCG_OK;
             case DCH_TILE_LANE2:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-                TCG_LAUNCH(C, K_DCHAIN, k_dchain<2>, (nc + 1u) / 2u, 32, dch_smem(2), d_sl, d_ord, nc, d_st, d_pl,
+                TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L2, (nc + 1u) / 2u, 32, dch_smem(2), d_sl, d_ord, nc, d_st, d_pl,
                            d_pkt, d_tab, d_coef, d_status);
                 return TCG_OK;
             case DCH_TILE_LANE1:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-                TCG_LAUNCH(C, K_DCHAIN, k_dchain<1>, nc, 32, dch_smem(1), d_sl, d_ord, nc, d_st, d_pl, d_pkt, d_tab,
+                TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L1, nc, 32, dch_smem(1), d_sl, d_ord, nc, d_st, d_pl, d_pkt, d_tab,
                            d_coef, d_status);
                 return TCG_OK;
             default:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-                TCG_LAUNCH(C, K_DCHAIN, k_dchain<8>, (nc + 7u) / 8u, 32, dch_smem(8), d_sl, d_ord, nc, d_st, d_pl,
+                TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L8, (nc + 7u) / 8u, 32, dch_smem(8), d_sl, d_ord, nc, d_st, d_pl,
                            d_pkt, d_tab, d_coef, d_status);
                 return TCG_OK;
             }
