@@ -317,7 +317,8 @@ int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, to
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, or
  * one warp per slice (1); -1 = not chosen yet. The first batch of each size
- * class (log2 of the slice count) times every tiling and keeps the fastest;
+ * class (log2 of the slice count) times 4, 2 and 1 slices per warp and keeps
+ * the fastest;
  * the environment variable TCG_DCHAIN=lane|lane4|lane2|lane1|warp overrides
  * the choice ("lane" is 8 per warp). All produce identical output. */
 int32_t tcg_dchain_tiling(uint32_t colour_slices);

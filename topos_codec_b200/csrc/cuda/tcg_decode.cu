@@ -1104,11 +1104,12 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 // Tilings of the slice decode: one lane per slice with 8, 4, 2 or 1 slices
 // per warp (more slices per warp cost fewer issue slots, fewer cost less
 // divergence on each lane's chain), and one warp per slice (lanes hold the
-// alphabet; shortest step, most issue slots). The first batch of each size
-// class (by log2 of the colour-slice count) runs every tiling and keeps the
-// fastest; TCG_DCHAIN=lane|lane4|lane2|lane1|warp forces one ("lane" is 8).
-enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4,
-                    DCH_TILINGS = 5 };
+// alphabet; most issue slots). The first batch of each size class (by log2 of
+// the colour-slice count) runs the tilings that can win (1, 2 and 4 slices
+// per warp: one per warp when the GPU has room for every chain, more when the
+// chains compete for issue slots) and keeps the fastest;
+// TCG_DCHAIN=lane|lane4|lane2|lane1|warp forces any one ("lane" is 8).
+enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4 };
 
 static std::mutex g_tune_mu;
 static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
@@ -1316,23 +1317,24 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             const int32_t rc = run(tiling);
             if (rc != TCG_OK) { return rc; }
         } else {
-            // every tiling decodes the whole batch once, each timed on the stream; the
+            // each candidate decodes the whole batch once, timed on the stream; the
             // last run's output stands (all tilings write identical results)
-            cudaEvent_t e[DCH_TILINGS + 1];
+            constexpr int cand[3] = {DCH_TILE_LANE4, DCH_TILE_LANE2, DCH_TILE_LANE1};
+            cudaEvent_t e[4];
             for (auto& x : e) { TCG_CHECK(cudaEventCreate(&x)); }
             TCG_CHECK(cudaEventRecord(e[0], st));
-            for (int k = 0; k < DCH_TILINGS; ++k) {
-                const int32_t rc = run(k);
+            for (int k = 0; k < 3; ++k) {
+                const int32_t rc = run(cand[k]);
                 if (rc != TCG_OK) { return rc; }
                 TCG_CHECK(cudaEventRecord(e[k + 1], st));
             }
-            TCG_CHECK(cudaEventSynchronize(e[DCH_TILINGS]));
-            int best = 0;
+            TCG_CHECK(cudaEventSynchronize(e[3]));
+            int best = cand[0];
             float best_ms = 0.f;
-            for (int k = 0; k < DCH_TILINGS; ++k) {
+            for (int k = 0; k < 3; ++k) {
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, e[k], e[k + 1]);
-                if (k == 0 || ms < best_ms) { best = k; best_ms = ms; }
+                if (k == 0 || ms < best_ms) { best = cand[k]; best_ms = ms; }
             }
             for (auto& x : e) { cudaEventDestroy(x); }
             std::lock_guard<std::mutex> g(g_tune_mu);
