@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(32) k_select(const ESlice* __restrict__ slices
 
 __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
                                                  const uint32_t* __restrict__ nops, uint32_t* __restrict__ opoff,
-                                                 ESliceRes* __restrict__ sres)
+                                                 uint32_t* __restrict__ ops, ESliceRes* __restrict__ sres)
 {
     __shared__ uint32_t wsum[32];
     __shared__ uint32_t carry;
@@ -333,6 +333,12 @@ __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slic
         __syncthreads();
     }
     if (threadIdx.x == 0) { sres[si].nops = carry; }
+    // identity operations (word 0) from the count up to the next multiple of
+    // 16, so the chain reads whole 16-operation iterations without masking
+    // (a slice window holds 256 words past its largest count)
+    if (threadIdx.x < 16u && carry + threadIdx.x < ((carry + 15u) & ~15u)) {
+        ops[S.op_base + carry + threadIdx.x] = 0u;
+    }
 }
 
 // ============================== op generation ==============================
@@ -470,19 +476,12 @@ __device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, c
     x = xn;
 }
 
-// Four consecutive operations of a slice (group g); positions at or past the
-// slice's operation count read as identities, and groups wholly past it are
-// not loaded.
-__device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t nops)
+// Four consecutive operations of a slice (group g). The slice's window holds
+// identity operations from its count to the next multiple of 16, and every
+// group the chain loads lies within the window or the next 256 words.
+__device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t)
 {
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (4u * g < nops) { v = __ldg(op4 + g); }
-    const uint32_t k = 4u * g;
-    v.x = k < nops ? v.x : 0u;
-    v.y = k + 1u < nops ? v.y : 0u;
-    v.z = k + 2u < nops ? v.z : 0u;
-    v.w = k + 3u < nops ? v.w : 0u;
-    return v;
+    return __ldg(op4 + g);
 }
 
 #define ENC_GROUP(v)                  \
@@ -944,7 +943,9 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
                     S.blk0 = P.blk0 + y0 * I.cols;
                     S.nblk = S.bh * I.cols;
                     S.op_base = ops_words;
-                    ops_words += (uint64_t)S.nblk * 256u;
+                    // at most 256 operations per block, then 256 words for the
+                    // identity padding and look-ahead reads of the chain
+                    ops_words += (uint64_t)S.nblk * 256u + 256u;
                     S.stage_cap = (uint64_t)S.nblk * 512u + 64u;
                     pay = PREFIX_MAX + 4u + S.stage_cap;
                     const uint32_t si = (uint32_t)slices.size();
@@ -1062,7 +1063,7 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
         TCG_LAUNCH(C, K_TOKENS, k_tokens, (uint32_t)work.size(), 256, tok_smem, d_wk, d_sl, d_coef, d_mask, d_dcm, d_nops,
                    d_hist, d_sres);
         TCG_LAUNCH(C, K_SELECT, k_select, nc, 32, 0, d_sl, d_cs, d_hist, T.log2, d_stab, d_prefix, d_sres);
-        TCG_LAUNCH(C, K_OPSCAN, k_opscan, nc, 1024, 0, d_sl, d_cs, d_nops, d_opoff, d_sres);
+        TCG_LAUNCH(C, K_OPSCAN, k_opscan, nc, 1024, 0, d_sl, d_cs, d_nops, d_opoff, d_ops, d_sres);
         TCG_LAUNCH(C, K_OPGEN, k_opgen, dim3((uint32_t)work.size(), 32), 256, 0, d_wk, d_sl, d_coef, d_mask, d_dcm,
                    d_opoff, d_sres, d_ops);
         static bool chain_attr = false;
