@@ -30,6 +30,12 @@ __device__ __constant__ uint8_t c_zigzag[64] = {
     12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13, 6, 7, 14, 21, 28,
     35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
     58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
+// the same order for compile-time indexing (unrolled loops over registers)
+__device__ constexpr uint8_t k_zigzag[64] = {
+    0, 1, 8, 16, 9, 2, 3, 10, 17, 24, 32, 25, 18, 11, 4, 5,
+    12, 19, 26, 33, 40, 48, 41, 34, 27, 20, 13, 6, 7, 14, 21, 28,
+    35, 42, 49, 56, 57, 50, 43, 36, 29, 22, 15, 23, 30, 37, 44, 51,
+    58, 59, 52, 45, 38, 31, 39, 46, 53, 60, 61, 54, 47, 55, 62, 63};
 
 // ------------------------------- small maps -------------------------------
 
@@ -214,7 +220,7 @@ __device__ __forceinline__ int32_t round_shift32(int64_t v)
 __device__ inline void idct8x8(const int32_t c[64], int32_t xh[64])
 {
     int64_t B[64];
-#pragma unroll 1
+#pragma unroll
     for (int u = 0; u < 8; ++u) {
         int64_t g[8];
 #pragma unroll
@@ -232,7 +238,7 @@ __device__ inline void idct8x8(const int32_t c[64], int32_t xh[64])
             B[u * 8 + 7 - x] = pe - po;
         }
     }
-#pragma unroll 1
+#pragma unroll
     for (int x = 0; x < 8; ++x) {
 #pragma unroll
         for (int y = 0; y < 4; ++y) {

@@ -846,11 +846,27 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
     const uint32_t px = bx * 8u, py = by * 8u;
     const uint32_t cw = min(8u, P.vis_w - px), ch = min(8u, P.vis_h - py);
     uint16_t* dst = out + P.out_off + (size_t)py * P.vis_w + px;
-    for (uint32_t y = 0; y < ch; ++y) {
-        for (uint32_t x = 0; x < cw; ++x) {
-            int32_t v = xh[y * 8 + x] + mid;
-            v = v < 0 ? 0 : (v > maxv ? maxv : v);
-            dst[(size_t)y * P.vis_w + x] = (uint16_t)v;
+    uint32_t pv[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i) {
+        const int32_t v = xh[i] + mid;
+        pv[i] = (uint32_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
+    }
+    if (cw == 8u && ch == 8u && (P.vis_w & 7u) == 0u) {
+        // whole block, 16-byte aligned rows (planes start on 64-sample boundaries)
+#pragma unroll
+        for (int y = 0; y < 8; ++y) {
+            const uint4 r = make_uint4(pv[y * 8] | (pv[y * 8 + 1] << 16), pv[y * 8 + 2] | (pv[y * 8 + 3] << 16),
+                                       pv[y * 8 + 4] | (pv[y * 8 + 5] << 16), pv[y * 8 + 6] | (pv[y * 8 + 7] << 16));
+            *reinterpret_cast<uint4*>(dst + (size_t)y * P.vis_w) = r;
+        }
+    } else {
+#pragma unroll
+        for (int y = 0; y < 8; ++y) {
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+                if ((uint32_t)y < ch && (uint32_t)x < cw) { dst[(size_t)y * P.vis_w + x] = (uint16_t)pv[y * 8 + x]; }
+            }
         }
     }
 }

@@ -88,14 +88,26 @@ __global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes,
     const int32_t mid = 1 << (P.bd - 1u);
     const bool wide = P.bd > 12u;
     int32_t x[64], F[64];
+    // a block inside the visible plane with 16-byte aligned rows (planes start
+    // on 64-sample boundaries) reads each row with one load; edge blocks
+    // replicate the last column and row
+    const bool inner = (P.vis_w & 7u) == 0u && bx * 8u + 8u <= P.vis_w && by * 8u + 8u <= P.vis_h;
 #pragma unroll
     for (int y = 0; y < 8; ++y) {
         const uint32_t sy = min(by * 8u + (uint32_t)y, P.vis_h - 1u);
         const uint16_t* row = src + (size_t)sy * P.vis_w;
+        uint32_t u[8];
+        if (inner) {
+            const uint4 r = __ldg(reinterpret_cast<const uint4*>(row + bx * 8u));
+            u[0] = r.x & 0xFFFFu; u[1] = r.x >> 16; u[2] = r.y & 0xFFFFu; u[3] = r.y >> 16;
+            u[4] = r.z & 0xFFFFu; u[5] = r.z >> 16; u[6] = r.w & 0xFFFFu; u[7] = r.w >> 16;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { u[k] = __ldg(row + min(bx * 8u + (uint32_t)k, P.vis_w - 1u)); }
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
-            const uint32_t sx = min(bx * 8u + (uint32_t)k, P.vis_w - 1u);
-            const int32_t d = (int32_t)__ldg(row + sx) - mid;
+            const int32_t d = (int32_t)u[k] - mid;
             x[y * 8 + k] = wide ? d : (int32_t)(int16_t)d;
         }
     }
@@ -124,7 +136,7 @@ __global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes,
 #pragma unroll
     for (int p = 0; p < 64; p += 4) {
         int4 v;
-        v.x = q[c_zigzag[p]]; v.y = q[c_zigzag[p + 1]]; v.z = q[c_zigzag[p + 2]]; v.w = q[c_zigzag[p + 3]];
+        v.x = q[k_zigzag[p]]; v.y = q[k_zigzag[p + 1]]; v.z = q[k_zigzag[p + 2]]; v.w = q[k_zigzag[p + 3]];
         m |= (uint64_t)(v.x != 0) << p | (uint64_t)(v.y != 0) << (p + 1) | (uint64_t)(v.z != 0) << (p + 2) |
              (uint64_t)(v.w != 0) << (p + 3);
         out[p >> 2] = v;
