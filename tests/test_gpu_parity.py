@@ -197,11 +197,11 @@ def test_strided_io_and_buffer_too_small(product):
     assert rc == B.TC_ERR_BUFFER_TOO_SMALL and st.packet_size == len(tight)
 
 
-@pytest.mark.parametrize("tiling", ["lane", "lane4", "lane2", "lane1", "warp"])
+@pytest.mark.parametrize("tiling", ["lane", "lane4", "lane2", "lane1", "warp", "split"])
 def test_decode_tilings_vs_oracle(product, oracle, monkeypatch, tiling):
     """Every decode-chain tiling (lane per slice with 8/4/2/1 slices per warp,
-    warp per slice) decodes random configurations and damaged packets exactly
-    like the oracle."""
+    warp per slice, the two-stream split) decodes random configurations and
+    damaged packets exactly like the oracle."""
     monkeypatch.setenv("TCG_DCHAIN", tiling)
     rng = random.Random(123)
     pkts = []

@@ -1121,11 +1121,15 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 // per warp (more slices per warp cost fewer issue slots, fewer cost less
 // divergence on each lane's chain), and one warp per slice (lanes hold the
 // alphabet; most issue slots). The first batch of each size class (by log2 of
-// the colour-slice count) runs the tilings that can win (1, 2 and 4 slices
-// per warp: one per warp when the GPU has room for every chain, more when the
-// chains compete for issue slots) and keeps the fastest;
-// TCG_DCHAIN=lane|lane4|lane2|lane1|warp forces any one ("lane" is 8).
-enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4 };
+// the colour-slice count) runs the tilings that can win and keeps the fastest:
+// 1, 2 and 4 slices per warp (one per warp when the GPU has room for every
+// chain, more when the chains compete for issue slots), and a split where the
+// largest slices (half of the batch's blocks) run one per warp while the rest
+// run four per warp on a second stream, so the short chains take fewer issue
+// slots from the long ones that set the batch time.
+// TCG_DCHAIN=lane|lane4|lane2|lane1|warp|split forces any one ("lane" is 8).
+enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4,
+                    DCH_TILE_SPLIT = 5 };
 
 static std::mutex g_tune_mu;
 static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
@@ -1140,6 +1144,7 @@ static int dchain_forced()
     if (strcmp(v, "lane2") == 0) { return DCH_TILE_LANE2; }
     if (strcmp(v, "lane1") == 0) { return DCH_TILE_LANE1; }
     if (strcmp(v, "warp") == 0) { return DCH_TILE_WARP; }
+    if (strcmp(v, "split") == 0) { return DCH_TILE_SPLIT; }
     return -1;
 }
 
@@ -1295,8 +1300,34 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             attr = true;
         }
         const size_t wsmem = (size_t)max_cols * 8u;  // two DC rows per slice (warp tiling)
+        // split point: the largest slices (in chain order) up to half of the blocks
+        uint32_t nsplit = 0;
+        {
+            uint64_t tot = 0, acc = 0;
+            for (uint32_t si : ord) { tot += slices[si].nblk; }
+            while (nsplit < nc && 2u * acc < tot) { acc += slices[ord[nsplit++]].nblk; }
+        }
         auto run = [&](int tiling) -> int32_t {
             switch (tiling) {
+            case DCH_TILE_SPLIT: {
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                tcg::kern_begin(C, K_DCHAIN);
+                TCG_CHECK(cudaEventRecord(C->fork, st));
+                TCG_CHECK(cudaStreamWaitEvent(C->side, C->fork, 0));
+                k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
+                                                               d_status);
+                if (nc > nsplit) {
+                    k_dchain<4><<<(nc - nsplit + 3u) / 4u, 32, dch_smem(4), C->side>>>(
+                        d_sl, d_ord + nsplit, nc - nsplit, d_st, d_pl, d_pkt, d_tab, d_coef, d_status);
+                }
+                tcg::note_launch(nc > nsplit ? 2u : 1u);
+                TCG_CHECK(cudaGetLastError());
+                TCG_CHECK(cudaEventRecord(C->join, C->side));
+                TCG_CHECK(cudaStreamWaitEvent(st, C->join, 0));
+                tcg::kern_end(C);
+                if (tcg::sync_each()) { TCG_CHECK(cudaStreamSynchronize(st)); }
+                return TCG_OK;
+            }
             case DCH_TILE_WARP:
                 // the warp tiling writes every coefficient of the blocks it decodes
                 TCG_LAUNCH(C, K_DCHAIN_W, k_dchain_w, nc, 32, wsmem, d_sl, d_cs, d_pl, d_pkt, d_tab, d_coef, d_status);
@@ -1335,19 +1366,19 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         } else {
             // each candidate decodes the whole batch once, timed on the stream; the
             // last run's output stands (all tilings write identical results)
-            constexpr int cand[3] = {DCH_TILE_LANE4, DCH_TILE_LANE2, DCH_TILE_LANE1};
-            cudaEvent_t e[4];
+            constexpr int cand[4] = {DCH_TILE_SPLIT, DCH_TILE_LANE4, DCH_TILE_LANE2, DCH_TILE_LANE1};
+            cudaEvent_t e[5];
             for (auto& x : e) { TCG_CHECK(cudaEventCreate(&x)); }
             TCG_CHECK(cudaEventRecord(e[0], st));
-            for (int k = 0; k < 3; ++k) {
+            for (int k = 0; k < 4; ++k) {
                 const int32_t rc = run(cand[k]);
                 if (rc != TCG_OK) { return rc; }
                 TCG_CHECK(cudaEventRecord(e[k + 1], st));
             }
-            TCG_CHECK(cudaEventSynchronize(e[3]));
+            TCG_CHECK(cudaEventSynchronize(e[4]));
             int best = cand[0];
             float best_ms = 0.f;
-            for (int k = 0; k < 3; ++k) {
+            for (int k = 0; k < 4; ++k) {
                 float ms = 0.f;
                 cudaEventElapsedTime(&ms, e[k], e[k + 1]);
                 if (k == 0 || ms < best_ms) { best = cand[k]; best_ms = ms; }

@@ -208,6 +208,9 @@ Ctx* ctx_acquire()
     }
     Ctx* c = new Ctx();
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
     for (int i = 0; ok && i < 2 * MAX_PROF; ++i) { ok = cudaEventCreate(&c->kev[i]) == cudaSuccess; }
@@ -288,7 +291,11 @@ extern "C" void tcg_shutdown(void)
         cudaStreamSynchronize(c->stream);
         for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
+        cudaStreamSynchronize(c->side);
         cudaEventDestroy(c->ev);
+        cudaEventDestroy(c->fork);
+        cudaEventDestroy(c->join);
+        cudaStreamDestroy(c->side);
         cudaStreamDestroy(c->stream);
         delete c;
         c = n;

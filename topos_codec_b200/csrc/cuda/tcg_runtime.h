@@ -52,6 +52,8 @@ constexpr int MAX_PROF = 64;
 
 struct Ctx {
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;                  // second stream for work split across two launches
+    cudaEvent_t fork = nullptr, join = nullptr;   // ordering between stream and side
     cudaEvent_t ev = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;    // whole-call device time
     cudaEvent_t kev[2 * MAX_PROF] = {};        // per-kernel timing (profiling on)
