@@ -452,14 +452,15 @@ __global__ void __launch_bounds__(256) k_opgen(const EWork* __restrict__ work, c
 
 // Coding-table entry of one operation: renormalisation threshold, division
 // magic m and shift l (q = umulhi(2x, m) >> l = x / f for x < 2^31), additive
-// term, and multiplier B | l << 24. Every operation is then
+// term, and B << 5 | l (a shift takes its amount from the low 5 bits, so l
+// needs no extraction). Every operation is then
 //   x <- q * B + x + add  after renormalisation against lim:
 // a symbol of frequency f has B = 4096 - f, add = cum (x/f*4096 + x%f + cum);
 // a raw chunk of w bits has f = 1 (q = x), B = 2^w - 1, add = the value
 // (x * 2^w + value); the 0-bit chunk is the identity.
 __device__ __forceinline__ uint4 chunk_entry(uint32_t w)
 {
-    return make_uint4(1u << (31u - w), 0x80000000u, 0u, (1u << w) - 1u);
+    return make_uint4(1u << (31u - w), 0x80000000u, 0u, ((1u << w) - 1u) << 5);
 }
 
 __device__ __forceinline__ uint4 symbol_entry(uint32_t word, const uint32_t* __restrict__ div_m,
@@ -467,7 +468,7 @@ __device__ __forceinline__ uint4 symbol_entry(uint32_t word, const uint32_t* __r
 {
     const uint32_t f = word >> 12;
     if (f == 0u) { return chunk_entry(0u); }  // symbol absent from the model: never coded
-    return make_uint4(f << 19, __ldg(div_m + f), word & 0xFFFu, (4096u - f) | ((uint32_t)__ldg(div_l + f) << 24));
+    return make_uint4(f << 19, __ldg(div_m + f), word & 0xFFFu, ((4096u - f) << 5) | (uint32_t)__ldg(div_l + f));
 }
 
 // One coding operation, branch-free; emitted bytes (0..3, least significant
@@ -479,8 +480,8 @@ __device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, c
     const uint32_t x8 = x >> 8, x16 = x >> 16, x24 = x >> 24;
     const bool c1 = x >= e.x, c2 = x8 >= e.x, c3 = x16 >= e.x;
     const uint32_t xr = c2 ? (c3 ? x24 : x16) : (c1 ? x8 : x);
-    const uint32_t q = __umulhi(xr << 1, e.y) >> (e.w >> 24);
-    const uint32_t xn = q * (e.w & 0xFFFFFFu) + (xr + e.z + v);
+    const uint32_t q = __funnelshift_r(__umulhi(xr << 1, e.y), 0u, e.w);  // >> l (e.w & 31)
+    const uint32_t xn = q * (e.w >> 5) + (xr + e.z + v);
     if (c1) { p[-1] = (uint8_t)x; }
     if (c2) { p[-2] = (uint8_t)x8; }
     if (c3) { p[-3] = (uint8_t)x16; }
