@@ -182,14 +182,22 @@ __global__ void __launch_bounds__(256) k_tokens(const EWork* __restrict__ work, 
         atomicAdd(&sh[(H_DC + dcc) * 32u + lane], 1u);
         atomicAdd(&sh[(H_JDC + ctx * DC_SYMS + dcc) * 32u + lane], 1u);
         uint32_t nops = 2u + suffix_chunks(dcc);  // EOB + DC symbol + DC suffix
-        uint64_t m = mask[gb];
+        const uint64_t m = mask[gb];
         uint32_t prev = 0u, pcat = 0u;
         bool has = false;
-        const int32_t* c = coef + (size_t)gb * 64u;
-        while (m != 0u) {
-            const uint32_t p = (uint32_t)__ffsll((long long)m) - 1u;
-            m &= m - 1u;
-            uint32_t lm = map_s(c[p]);
+        // the whole block (zigzag order) in 16 independent loads, then the
+        // positions in order over registers
+        int32_t cv[64];
+        const int4* c4 = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int4 v = c4[i];
+            cv[4 * i] = v.x; cv[4 * i + 1] = v.y; cv[4 * i + 2] = v.z; cv[4 * i + 3] = v.w;
+        }
+#pragma unroll
+        for (uint32_t p = 1; p < 64u; ++p) {
+            if (((m >> p) & 1u) == 0u) { continue; }
+            uint32_t lm = map_s(cv[p]);
             if (lm > 0x07FFFFFFu) { lm = 0x07FFFFFFu; viol = true; }
             const uint32_t cat = bitlen32(lm);
             const uint32_t run = p - prev - 1u;
@@ -832,6 +840,10 @@ __global__ void k_pack_sizes(const EFrame* __restrict__ frames, uint32_t nf, con
 }
 
 // grid (slice, part): copy prefix | state | stream (or the alpha bytes) into the packet
+// Slice payloads into the packets: the prefix, the final coder state (4 bytes,
+// big-endian) and the stream bytes. Each thread writes 4-byte aligned words of
+// the destination; a word lying in the stream part takes its 4 bytes from the
+// two aligned stream words that cover them, the rest go byte by byte.
 __global__ void __launch_bounds__(256) k_pack_copy(const EFrame* __restrict__ frames, const ESlice* __restrict__ slices,
                                                    const ESliceRes* __restrict__ sres, const uint8_t* __restrict__ prefix,
                                                    const uint8_t* __restrict__ stage, uint8_t* __restrict__ pkt,
@@ -847,13 +859,34 @@ __global__ void __launch_bounds__(256) k_pack_copy(const EFrame* __restrict__ fr
     const uint8_t* stream = S.kind == TCG_PLANE_COLOR ? stage + S.stage_base + S.stage_cap - R.nbytes
                                                       : stage + S.stage_base;
     const uint32_t total = R.payload;
-    const uint32_t stride = gridDim.y * blockDim.x;
-    for (uint32_t i = blockIdx.y * blockDim.x + threadIdx.x; i < total; i += stride) {
-        uint8_t v;
-        if (i < plen) { v = prefix[(size_t)si * PREFIX_MAX + i]; }
-        else if (i < head) { v = (uint8_t)(R.xfin >> (8u * (3u - (i - plen)))); }
-        else { v = stream[i - head]; }
-        dst[i] = v;
+    const uint8_t* pre = prefix + (size_t)si * PREFIX_MAX;
+    const uint32_t xfin = R.xfin;
+    auto byte_at = [&](uint32_t i) -> uint8_t {
+        if (i < plen) { return pre[i]; }
+        if (i < head) { return (uint8_t)(xfin >> (8u * (3u - (i - plen)))); }
+        return stream[i - head];
+    };
+    const uint32_t tid = blockIdx.y * blockDim.x + threadIdx.x, stride = gridDim.y * blockDim.x;
+    const uint32_t lead = (uint32_t)((4u - ((uintptr_t)dst & 3u)) & 3u);  // bytes before the first aligned word
+    const uint32_t nw = total > lead ? (total - lead) / 4u : 0u;
+    const uint32_t tail0 = lead + 4u * nw;
+    if (tid < lead && tid < total) { dst[tid] = byte_at(tid); }
+    if (tail0 + tid < total) { dst[tail0 + tid] = byte_at(tail0 + tid); }  // at most 3 tail bytes
+    uint32_t* dw = reinterpret_cast<uint32_t*>(dst + lead);
+    for (uint32_t w = tid; w < nw; w += stride) {
+        const uint32_t i = lead + 4u * w;
+        uint32_t word;
+        if (i >= head) {
+            const uintptr_t sa = (uintptr_t)(stream + (i - head));
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(sa & ~(uintptr_t)3);
+            const uint32_t sh = (uint32_t)(sa & 3u);
+            // the second word is read only when the 4 bytes straddle it (all are stream bytes)
+            word = __byte_perm(sw[0], sh != 0u ? sw[1] : 0u, 0x3210u + sh * 0x1111u);
+        } else {
+            word = (uint32_t)byte_at(i) | ((uint32_t)byte_at(i + 1u) << 8) | ((uint32_t)byte_at(i + 2u) << 16) |
+                   ((uint32_t)byte_at(i + 3u) << 24);
+        }
+        dw[w] = word;
     }
     (void)cap_frames;
 }
