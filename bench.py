@@ -9,6 +9,14 @@ is round-trip frames/s; encode and decode rates are reported beside it, with
 the plain per-frame GPU path on the same frames for comparison.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--serve-seconds S] [--no-serve] [--no-extra]
+
+Beside the headline the line reports (key `workloads`) a 64-frame mixed batch
+(720p..8K, four tiers, qp 2..16) and a 32-frame 4096x2160 12-bit GBR 4:4:4 +
+16-bit alpha batch, each batched against the plain per-frame path, the latter
+also against the reference library on 8 frames and on damaged copies of its
+packets; and (key `served`) open-loop request streams at 25/50/75/100 % of the
+server's saturation beside the plain per-request path.
 
 Under torchrun every rank codes its own 60-frame batch (weak scaling, no
 collective on the data path); time is the max over ranks.
@@ -143,6 +151,7 @@ def main():
     ap.add_argument("--frames", type=int, default=FRAMES)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the mixed-batch and GBR 4:4:4 + alpha workloads")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -386,18 +395,65 @@ def main():
         cpu = {"value": r, "unit": "frames/s", "cores": cores, "kind": "reference",
                "sample": f"{n} frames encoded+decoded frame-parallel in {el:.1f} s"}
 
-    # ---------------- serving: open-loop request stream at half the saturation rate ----------------
+    # ---------------- further workloads: mixed batch, GBR 4:4:4 + alpha ----------------
+    extra = {}
+    if world == 1 and not args.no_extra:
+        from concurrent.futures import ThreadPoolExecutor
+        from topos_codec_b200 import workloads as WL
+        specs = WL.mixed_specs(64, seed=0)
+        mcfgs = [WL.mixed_config(w, h, t, q) for (w, h, t, q) in specs]
+        mframes = [[p.to(torch.uint16).contiguous() for p in synth.make_frame(w, h, seed=11, frame=i, device=dev)]
+                   for i, (w, h, _, _) in enumerate(specs)]
+        r = WL.batched_vs_plain(gpu, mcfgs, mframes)
+        r.pop("packets")
+        r["workload"] = ("64 frames, resolution uniform over 1280x720/1920x1080/3840x2160/7680x4320, tier uniform "
+                         "over proxy/lt/422/hq, qp uniform 2..16 (seed 0), 10-bit 4:2:2")
+        r["resolutions"] = {f"{w}x{h}": sum(1 for s in specs if s[:2] == (w, h)) for (w, h) in WL.MIXED_RES}
+        extra["mixed_batch"] = r
+        del mframes
+        gcfg = WL.gbr_config()
+        gframes = [[p.to(torch.uint16).contiguous() for p in
+                    synth.make_frame(4096, 2160, seed=21, frame=i, bit_depth=12, pixel_format=2, limited=False,
+                                     alpha=True, sigma=12, device=dev)] for i in range(32)]
+        r = WL.batched_vs_plain(gpu, [gcfg] * 32, gframes)
+        gpk = r.pop("packets")
+        r["workload"] = "32 frames 4096x2160 12-bit GBR 4:4:4 full range + 16-bit alpha, qp 2"
+        if rank == 0 and os.path.exists(REF_LIB):
+            ref = B.ToposCodec(REF_LIB)
+            sub = [[p.cpu().numpy() for p in gframes[i]] for i in range(8)]
+            with ThreadPoolExecutor(8) as ex:
+                rpk = list(ex.map(lambda f: ref.encode(gcfg, f), sub))
+            r["reference_packets_equal_8_frames"] = all(a == b for a, b in zip(rpk, gpk[:8]))
+            r["damaged_decode_vs_reference"] = WL.concealment_parity(gpu, ref, WL.corrupt_slices(rpk, 0.01, seed=5))
+            r["damaged_decode_vs_reference"]["corruption"] = "1 % of the slices of 8 reference packets, one payload byte each"
+        extra["gbr4444_alpha"] = r
+        del gframes
+        torch.cuda.empty_cache()
+
+    # ---------------- serving: open-loop request streams at 25/50/75/100 % of saturation ----------------
     served = None
     if world == 1 and not args.no_serve:
         from topos_codec_b200 import serving
         sat = serving.saturation_rps(gpu)
-        # a short discarded trace first: the decode-tiling tuner times both tilings
+        # a short discarded trace first: the decode-tiling tuner times the tilings
         # on the first batch of each batch-size class
         serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=3.0, seed=7)
-        served = serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=args.serve_seconds)
+        loads = {}
+        for ld in (0.25, 0.5, 0.75, 1.0):
+            loads[ld] = serving.run_trace(gpu, rate_rps=ld * sat, duration_s=args.serve_seconds, seed=int(ld * 100))
+        served = dict(loads[0.5])
+        psat = serving.plain_saturation_rps(gpu)
+        plain = {"saturation_rps": psat,
+                 "at_half_batched_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * sat,
+                                                                       duration_s=args.serve_seconds),
+                 "at_half_plain_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * psat,
+                                                                     duration_s=args.serve_seconds)}
         served.update({"load": 0.5, "saturation_rps": sat,
                        "mix": "50/50 encode/decode; 1080p 40 %, 2160p 40 %, 720p 20 %; 10-bit 4:2:2 tiers 422/HQ",
-                       "latency": "server-side, submission to completion"})
+                       "latency": "server-side, submission to completion",
+                       "loads": {str(k): {x: v[x] for x in ("offered_rps", "throughput_rps", "p50_ms", "p99_ms",
+                                                            "p999_ms", "errors")} for k, v in loads.items()},
+                       "plain_per_request": plain})
 
     if rank == 0:
         line = {
@@ -416,6 +472,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "served": served,
+            "workloads": extra,
             "e2e": {"value": nf * world / e2e_s, "unit": "frames/s",
                     "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes)},
         }

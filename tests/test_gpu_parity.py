@@ -229,3 +229,42 @@ def test_decode_tilings_vs_oracle(product, oracle, monkeypatch, tiling):
         d = oracle.decode_status(pkt)
         for x, y in zip(d.planes, f.planes):
             assert np.array_equal(x, y)
+
+
+def test_mixed_tier_batch_vs_oracle(product, oracle):
+    """A batch mixing resolutions, tiers (the product's tier mapping) and QPs
+    encodes and decodes exactly like the oracle, frame by frame."""
+    from topos_codec_b200 import workloads as WL
+    specs = [(1280, 720, "proxy", 16), (1920, 1080, "hq", 2), (3840, 2160, "422", 9), (1280, 720, "lt", 5),
+             (3840, 2160, "hq", 4)]
+    cfgs = [WL.mixed_config(*s) for s in specs]
+    frames = [synth.make_frame_np(w, h, seed=90 + i) for i, (w, h, _, _) in enumerate(specs)]
+    rc, pkts, rcs, _ = product.encode_batch(cfgs, frames)
+    assert rc == 0 and rcs == [0] * len(specs)
+    for c, f, p in zip(cfgs, frames, pkts):
+        assert p == oracle.encode(c, f)
+    rc, dec = product.decode_batch(pkts)
+    assert rc == 0
+    for p, d in zip(pkts, dec):
+        o = oracle.decode(p)
+        for x, y in zip(o.planes, d.planes):
+            assert np.array_equal(x, y)
+
+
+def test_gbr4444_alpha_full_size_damaged_vs_oracle(product, oracle):
+    """4096x2160 12-bit GBR 4:4:4 with a 16-bit alpha plane at qp 2: identical
+    packet, then damaged copies (1 % of the slices, one payload byte each)
+    decode with the oracle's per-slice concealment status and pixels."""
+    from topos_codec_b200 import workloads as WL
+    cfg = WL.gbr_config()
+    planes = synth.make_frame_np(4096, 2160, seed=21, bit_depth=12, pixel_format=2, limited=False, alpha=True,
+                                 sigma=12)
+    pkt = product.encode(cfg, planes)
+    assert pkt == oracle.encode(cfg, planes)
+    for seed in range(3):
+        bad = WL.corrupt_slices([pkt], 0.01, seed=seed)[0]
+        d, o = product.decode_status(bad), oracle.decode_status(bad)
+        assert d.status == o.status and d.slice_status == o.slice_status
+        assert any(s != 0 for s in o.slice_status)
+        for x, y in zip(o.planes, d.planes):
+            assert np.array_equal(x, y)

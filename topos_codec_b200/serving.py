@@ -163,3 +163,82 @@ def _saturation_pass(codec, n: int, seed: int, max_batch_frames: int) -> float:
         return n / (time.perf_counter() - t0)
     finally:
         srv.close()
+
+
+def run_trace_plain(codec, rate_rps: float, duration_s: float, seed: int = 0) -> Dict:
+    """The same Poisson request stream served by the plain per-frame calls, one
+    request at a time in arrival order (the drop-in path without batching);
+    latency runs from each request's arrival to its completion."""
+    import ctypes
+    import queue
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = random.Random(seed)
+    kinds = [(wh, t) for wh, _ in RESOLUTIONS for t in TIERS]
+    slots = {k: _Slot(codec, torch, dev, k[0][0], k[0][1], k[1], seed) for k in kinds}
+    L = codec._lib
+    torch.cuda.synchronize()
+    q: "queue.Queue" = queue.Queue()
+    lat: List[float] = []
+    errors = [0]
+
+    def worker():
+        st = B.FrameStats()
+        while True:
+            item = q.get()
+            if item is None:
+                return
+            key, enc, t_arr = item
+            s = slots[key]
+            if enc:
+                fi = B.FrameInput()
+                fi.struct_size, fi.abi_version = ctypes.sizeof(B.FrameInput), B.TOPOS_CODEC_ABI_VERSION
+                for p, t in enumerate(s.planes):
+                    fi.planes[p], fi.strides[p] = t.data_ptr(), t.shape[1]
+                rc = int(L.tc_frame_encode(ctypes.byref(s.cfg), ctypes.byref(fi), ctypes.c_void_p(s.out.data_ptr()),
+                                           s.cap, ctypes.byref(st)))
+            else:
+                ptrs = (ctypes.c_void_p * B.TC_FRAME_MAX_PLANES)(*[t.data_ptr() for t in s.dec])
+                info = B.FrameOutput()
+                rc = int(L.tc_frame_decode(ctypes.c_void_p(s.pkt.data_ptr()), s.pkt.numel(), ptrs, None,
+                                           ctypes.byref(info)))
+            if rc not in (0, 1):
+                errors[0] += 1
+            lat.append((time.perf_counter() - t_arr) * 1e3)
+
+    th = threading.Thread(target=worker)
+    th.start()
+    weights = [w for _, w in RESOLUTIONS]
+    t0 = time.perf_counter()
+    t_next = t0
+    n = 0
+    while True:
+        t_next += rng.expovariate(rate_rps)
+        if t_next - t0 > duration_s:
+            break
+        wh = rng.choices([r for r, _ in RESOLUTIONS], weights)[0]
+        key = (wh, rng.choice(TIERS))
+        enc = rng.random() < 0.5
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        q.put((key, enc, t_next))
+        n += 1
+    q.put(None)
+    th.join()
+    wall = time.perf_counter() - t0
+    lat.sort()
+
+    def pct(p):
+        return lat[min(len(lat) - 1, int(p * len(lat)))] if lat else None
+
+    return {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
+            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "p999_ms": pct(0.999), "max_ms": lat[-1] if lat else None,
+            "errors": errors[0]}
+
+
+def plain_saturation_rps(codec, n: int = 48, seed: int = 1) -> float:
+    """Requests per second of the plain per-frame calls on n requests of the mix back to back."""
+    r = run_trace_plain(codec, rate_rps=1e6, duration_s=n / 1e6, seed=seed)
+    return r["requests"] / max(r["duration_s"], 1e-9)
+

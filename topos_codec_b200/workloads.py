@@ -1,0 +1,167 @@
+"""Benchmark workloads beside the 4K HQ batch, measured through the C ABI.
+
+* Mixed batch: 64 frames whose resolution (1280x720, 1920x1080, 3840x2160,
+  7680x4320), tier (proxy, lt, 422, hq) and fixed QP (2..16) are drawn from a
+  seeded generator; 10-bit 4:2:2 limited range. Tier mapping of the product
+  layer: quantisation matrix 4 and DEBLOCK for every tier; at 3840 wide and
+  up the 422 and HQ tiers take the flat matrix and the refined qp table.
+* GBR 4:4:4 + alpha: 4096x2160 12-bit GBR full range, 16-bit alpha (hard
+  ellipses with 4-pixel ramps), fixed QP 2, 32 frames; copies of packets with
+  1 % of their slices byte-corrupted check the per-slice concealment status
+  and pixels against the reference library.
+
+Each is coded as one batched call and as one plain call per frame on the same
+device-resident inputs; device time comes from the library's own stream
+events (tcg_last_device_ms) and both forms must give identical bytes.
+"""
+from __future__ import annotations
+
+import ctypes
+import random
+import struct
+from concurrent.futures import ThreadPoolExecutor
+from typing import Dict, List, Sequence
+
+import numpy as np
+
+from . import binding as B, synth
+
+MIXED_RES = [(1280, 720), (1920, 1080), (3840, 2160), (7680, 4320)]
+MIXED_TIERS = ["proxy", "lt", "422", "hq"]
+
+
+def mixed_config(w: int, h: int, tier: str, qp: int) -> B.FrameConfig:
+    big = w >= 3840 and tier in ("422", "hq")
+    return B.make_config(w, h, qp=qp, qmatrix_id=0 if big else 4, features=3 if big else 1)
+
+
+def mixed_specs(n: int = 64, seed: int = 0):
+    rng = random.Random(seed)
+    return [(*rng.choice(MIXED_RES), rng.choice(MIXED_TIERS), rng.randint(2, 16)) for _ in range(n)]
+
+
+def gbr_config(w: int = 4096, h: int = 2160) -> B.FrameConfig:
+    return B.make_config(w, h, qp=2, bit_depth=12, pixel_format=2, profile=5, alpha_mode=1, alpha_bit_depth=16,
+                         color_range=1)
+
+
+def _lib(codec):
+    L = codec._lib
+    L.tcg_last_device_ms.restype = ctypes.c_double
+    return L
+
+
+def _inputs(frames) -> ctypes.Array:
+    arr = (B.FrameInput * len(frames))()
+    for i, planes in enumerate(frames):
+        arr[i].struct_size = ctypes.sizeof(B.FrameInput)
+        arr[i].abi_version = B.TOPOS_CODEC_ABI_VERSION
+        for p, t in enumerate(planes):
+            arr[i].planes[p] = t.data_ptr()
+            arr[i].strides[p] = t.shape[1]
+    return arr
+
+
+def batched_vs_plain(codec, cfgs: Sequence[B.FrameConfig], frames, repeats: int = 2) -> Dict:
+    """Encode and decode the frames (device-resident uint16 planes) batched and
+    per frame. Returns device times, bit-exactness of the two forms and the
+    batched packets (host bytes)."""
+    import torch
+    L = _lib(codec)
+    n = len(cfgs)
+    dev = frames[0][0].device
+    carr = (B.FrameConfig * n)(*cfgs)
+    ins = _inputs(frames)
+    caps = [codec.packet_bound(c) for c in cfgs]
+    outs = [torch.empty(c, dtype=torch.uint8, device=dev) for c in caps]
+    optr = (ctypes.c_void_p * n)(*[t.data_ptr() for t in outs])
+    ocap = (ctypes.c_size_t * n)(*caps)
+    st = (B.FrameStats * n)()
+    rcs = (ctypes.c_int32 * n)()
+    dec = [[torch.empty(s, dtype=torch.uint16, device=dev) for s in B.plane_shapes(c)] for c in cfgs]
+    dptr = (ctypes.c_void_p * (B.TC_FRAME_MAX_PLANES * n))()
+    for i in range(n):
+        for p, t in enumerate(dec[i]):
+            dptr[B.TC_FRAME_MAX_PLANES * i + p] = t.data_ptr()
+    infos = (B.FrameOutput * n)()
+
+    def enc_batch() -> float:
+        rc = int(L.tcg_frame_encode_batch(carr, ins, n, optr, ocap, st, rcs))
+        if rc != 0:
+            raise RuntimeError(f"batched encode failed [{rc}]: {codec.last_error()}")
+        return L.tcg_last_device_ms()
+
+    def dec_batch() -> float:
+        arr = (B.BatchPacket * n)()
+        for i in range(n):
+            arr[i].data, arr[i].size = outs[i].data_ptr(), st[i].packet_size
+        rc = int(L.tc_frame_decode_batch(arr, n, dptr, None, infos))
+        if rc not in (B.TC_OK, B.TC_WARN_CONCEALED):
+            raise RuntimeError(f"batched decode failed [{rc}]: {codec.last_error()}")
+        return L.tcg_last_device_ms()
+
+    enc_batch()  # first batch of each size class also tunes the decode tiling
+    dec_batch()
+    enc_ms = min(enc_batch() for _ in range(repeats))
+    dec_ms = min(dec_batch() for _ in range(repeats))
+    pkts = [outs[i][: st[i].packet_size].cpu().numpy().tobytes() for i in range(n)]
+    # plain per-frame path on the same inputs
+    exact = True
+    p_enc = p_dec = 0.0
+    one = torch.empty(max(caps), dtype=torch.uint8, device=dev)
+    s1 = B.FrameStats()
+    for i in range(n):
+        rc = int(L.tc_frame_encode(ctypes.byref(carr[i]), ctypes.byref(ins[i]), ctypes.c_void_p(one.data_ptr()),
+                                   caps[i], ctypes.byref(s1)))
+        p_enc += L.tcg_last_device_ms()
+        exact = exact and rc == 0 and one[: s1.packet_size].cpu().numpy().tobytes() == pkts[i]
+        got = [torch.empty_like(t) for t in dec[i]]
+        ptrs = (ctypes.c_void_p * B.TC_FRAME_MAX_PLANES)(*[t.data_ptr() for t in got])
+        info = B.FrameOutput()
+        rc = int(L.tc_frame_decode(ctypes.c_void_p(outs[i].data_ptr()), st[i].packet_size, ptrs, None,
+                                   ctypes.byref(info)))
+        p_dec += L.tcg_last_device_ms()
+        exact = exact and rc in (B.TC_OK, B.TC_WARN_CONCEALED) and all(
+            torch.equal(a.view(torch.int16), b.view(torch.int16)) for a, b in zip(got, dec[i]))
+    return {"frames": n, "batched_encode_ms": enc_ms, "batched_decode_ms": dec_ms, "plain_encode_ms": p_enc,
+            "plain_decode_ms": p_dec, "batched_vs_plain": (p_enc + p_dec) / (enc_ms + dec_ms),
+            "encode_fps": n / (enc_ms / 1e3), "decode_fps": n / (dec_ms / 1e3), "bit_exact": bool(exact),
+            "packets": pkts}
+
+
+def slice_spans(pkt: bytes):
+    """(header offset, payload offset, payload size) of every slice of a packet."""
+    off, out = 53, []
+    while off + 17 <= len(pkt):
+        size = struct.unpack(">I", pkt[off:off + 4])[0]
+        out.append((off, off + 17, size))
+        off += 17 + size
+    return out
+
+
+def corrupt_slices(pkts: List[bytes], fraction: float = 0.01, seed: int = 5) -> List[bytes]:
+    """Copies of the packets with the given fraction of all slices (at least one)
+    byte-corrupted at seeded payload positions; slice headers stay intact."""
+    rng = random.Random(seed)
+    spans = [(f, s) for f, p in enumerate(pkts) for s in slice_spans(p) if s[2] > 0]
+    k = max(1, int(round(fraction * len(spans))))
+    out = [bytearray(p) for p in pkts]
+    for f, (_, po, size) in rng.sample(spans, k):
+        i = po + rng.randrange(size)
+        out[f][i] ^= 1 + rng.randrange(255)
+    return [bytes(p) for p in out]
+
+
+def concealment_parity(product, reference, pkts: List[bytes], threads: int = 8) -> Dict:
+    """Decode damaged packets with both libraries: per-slice status, return code
+    and pixels must agree."""
+    with ThreadPoolExecutor(threads) as ex:
+        ref = list(ex.map(reference.decode_status, pkts))
+    ok = True
+    concealed = 0
+    for p, r in zip(pkts, ref):
+        d = product.decode_status(p)
+        concealed += sum(1 for s in r.slice_status if s != 0)
+        ok = ok and d.status == r.status and d.slice_status == r.slice_status and all(
+            np.array_equal(a, b) for a, b in zip(d.planes, r.planes))
+    return {"frames": len(pkts), "concealed_slices": concealed, "parity": bool(ok)}
