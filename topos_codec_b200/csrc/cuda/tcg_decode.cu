@@ -1291,6 +1291,28 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         TCG_CHECK(cudaMemsetAsync(d_status, 0, (size_t)ns * 4u, st));
         TCG_LAUNCH(C, K_DCRC, k_dcrc, ns, 256, 0, d_sl, d_pkt, T.crc, d_status);
     }
+    if (na > 0) {
+        // Alpha slices (Rice run/level decode, then MED reconstruction) share no
+        // slice, status entry or output plane with the colour slices, so they
+        // run on a third stream beside the colour chain; the stream rejoins
+        // before concealment.
+        cudaStream_t as = C->aux;
+        TCG_CHECK(cudaEventRecord(C->afork, st));
+        TCG_CHECK(cudaStreamWaitEvent(as, C->afork, 0));
+        TCG_CHECK(cudaMemsetAsync(d_ares, 0, alpha_res * 4u, as));
+        TCG_LAUNCH_ON(C, as, K_DALPHA, k_dalpha, (na + 63u) / 64u, 64, 0, d_sl, d_as, na, d_pl, d_pkt, d_ares,
+                      d_status);
+        uint32_t max_w = 8;
+        for (uint32_t a : aslices) { max_w = std::max(max_w, planes[slices[a].plane].coded_w); }
+        const size_t esmem = (size_t)max_w * 4u;
+        static size_t eattr = 0;
+        if (esmem > eattr) {
+            cudaFuncSetAttribute(k_dalpha_med, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
+            eattr = esmem;
+        }
+        TCG_LAUNCH_ON(C, as, K_DALPHA_MED, k_dalpha_med, na, 128, esmem, d_sl, d_as, d_pl, d_ares, d_status, d_out);
+        TCG_CHECK(cudaEventRecord(C->ajoin, as));
+    }
     if (nc > 0) {
         TCG_LAUNCH(C, K_DTABLES, k_dtables, nc, 32, 0, d_sl, d_cs, d_pl, d_pkt, T.qscale, d_tab, d_status);
         static bool attr = false;
@@ -1391,17 +1413,8 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
                    d_status, (uint32_t)nblk, d_out);
     }
     if (na > 0) {
-        TCG_CHECK(cudaMemsetAsync(d_ares, 0, alpha_res * 4u, st));
-        TCG_LAUNCH(C, K_DALPHA, k_dalpha, (na + 63u) / 64u, 64, 0, d_sl, d_as, na, d_pl, d_pkt, d_ares, d_status);
-        uint32_t max_w = 8;
-        for (uint32_t a : aslices) { max_w = std::max(max_w, planes[slices[a].plane].coded_w); }
-        const size_t esmem = (size_t)max_w * 4u;
-        static size_t eattr = 0;
-        if (esmem > eattr) {
-            cudaFuncSetAttribute(k_dalpha_med, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)esmem);
-            eattr = esmem;
-        }
-        TCG_LAUNCH(C, K_DALPHA_MED, k_dalpha_med, na, 128, esmem, d_sl, d_as, d_pl, d_ares, d_status, d_out);
+        // the alpha planes have been on their own stream since the CRC check
+        TCG_CHECK(cudaStreamWaitEvent(st, C->ajoin, 0));
     }
     if (ns > 0) {
         TCG_LAUNCH(C, K_DCONCEAL, k_dconceal, ns, 256, 0, d_sl, d_pl, d_status, d_out);

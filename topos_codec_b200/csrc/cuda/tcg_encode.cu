@@ -1097,6 +1097,20 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
     uint8_t* d_stage = dptr<uint8_t>(C, B_STAGE);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
 
+    if (!aslices.empty()) {
+        // Alpha slices (MED residuals, Rice pairs) read only the samples and write
+        // only their own staging windows and results, so they run on a third
+        // stream beside the colour path; the stream rejoins before packing.
+        cudaStream_t as = C->aux;
+        TCG_CHECK(cudaEventRecord(C->afork, st));
+        TCG_CHECK(cudaStreamWaitEvent(as, C->afork, 0));
+        for (uint32_t a : aslices) {
+            TCG_CHECK(cudaMemsetAsync(d_stage + slices[a].stage_base, 0, slices[a].stage_cap, as));
+        }
+        TCG_LAUNCH_ON(C, as, K_ALPHA, k_alpha, (uint32_t)aslices.size(), 256, 0, d_sl, d_as, d_pl, d_pix, d_stage,
+                      d_sres, d_aerr);
+        TCG_CHECK(cudaEventRecord(C->ajoin, as));
+    }
     if (nblk > 0) {
         TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)cplanes.size(),
                    (uint32_t)nblk, d_pix, d_coef, d_mask);
@@ -1121,10 +1135,8 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
                    d_ops, d_stab, T.div_m, T.div_l, d_stage, d_sres);
     }
     if (!aslices.empty()) {
-        for (uint32_t a : aslices) {
-            TCG_CHECK(cudaMemsetAsync(d_stage + slices[a].stage_base, 0, slices[a].stage_cap, st));
-        }
-        TCG_LAUNCH(C, K_ALPHA, k_alpha, (uint32_t)aslices.size(), 256, 0, d_sl, d_as, d_pl, d_pix, d_stage, d_sres, d_aerr);
+        // the alpha slices have been on their own stream since the samples arrived
+        TCG_CHECK(cudaStreamWaitEvent(st, C->ajoin, 0));
     }
     TCG_LAUNCH(C, K_PACK_SIZES, k_pack_sizes, (count + 127u) / 128u, 128, 0, d_fr, count, d_sl, d_sres, d_fres);
     TCG_LAUNCH(C, K_PACK_COPY, k_pack_copy, dim3(ns, 8), 256, 0, d_fr, d_sl, d_sres, d_prefix, d_stage, d_pkt, count);

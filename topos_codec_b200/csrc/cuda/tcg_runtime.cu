@@ -39,6 +39,12 @@ void call_begin(Ctx* c)
 {
     c->prof = g_prof_on.load(std::memory_order_relaxed) != 0;
     c->kn = 0;
+    // work a failed earlier call may have left on the context's other streams
+    // comes before this call's work
+    cudaEventRecord(c->join, c->side);
+    cudaStreamWaitEvent(c->stream, c->join, 0);
+    cudaEventRecord(c->ajoin, c->aux);
+    cudaStreamWaitEvent(c->stream, c->ajoin, 0);
     cudaEventRecord(c->t0, c->stream);
 }
 
@@ -53,6 +59,20 @@ void kern_end(Ctx* c)
 {
     if (!c->prof || c->kn >= MAX_PROF) { return; }
     cudaEventRecord(c->kev[2 * c->kn + 1], c->stream);
+    c->kn++;
+}
+
+void kern_begin_on(Ctx* c, int id, cudaStream_t s)
+{
+    if (!c->prof || c->kn >= MAX_PROF) { return; }
+    c->kid[c->kn] = id;
+    cudaEventRecord(c->kev[2 * c->kn], s);
+}
+
+void kern_end_on(Ctx* c, cudaStream_t s)
+{
+    if (!c->prof || c->kn >= MAX_PROF) { return; }
+    cudaEventRecord(c->kev[2 * c->kn + 1], s);
     c->kn++;
 }
 
@@ -209,6 +229,9 @@ Ctx* ctx_acquire()
     Ctx* c = new Ctx();
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->afork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->ajoin, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) == cudaSuccess &&
@@ -292,6 +315,10 @@ extern "C" void tcg_shutdown(void)
         for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
         cudaStreamSynchronize(c->side);
+        cudaStreamSynchronize(c->aux);
+        cudaEventDestroy(c->afork);
+        cudaEventDestroy(c->ajoin);
+        cudaStreamDestroy(c->aux);
         cudaEventDestroy(c->ev);
         cudaEventDestroy(c->fork);
         cudaEventDestroy(c->join);

@@ -54,6 +54,8 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;                  // second stream for work split across two launches
     cudaEvent_t fork = nullptr, join = nullptr;   // ordering between stream and side
+    cudaStream_t aux = nullptr;                   // third stream for independent work (alpha planes)
+    cudaEvent_t afork = nullptr, ajoin = nullptr; // ordering between stream and aux
     cudaEvent_t ev = nullptr;
     cudaEvent_t t0 = nullptr, t1 = nullptr;    // whole-call device time
     cudaEvent_t kev[2 * MAX_PROF] = {};        // per-kernel timing (profiling on)
@@ -71,6 +73,8 @@ void call_begin(Ctx* c);
 void call_end(Ctx* c);  // after the stream was synchronised
 void kern_begin(Ctx* c, int id);
 void kern_end(Ctx* c);
+void kern_begin_on(Ctx* c, int id, cudaStream_t s);  // timing events on another of the context's streams
+void kern_end_on(Ctx* c, cudaStream_t s);
 
 // Launch on the context's stream. With TCG_SYNC_EACH=1 in the environment
 // every launch is followed by a stream synchronisation, so a failing kernel is
@@ -84,6 +88,20 @@ void kern_end(Ctx* c);
         if (tcg::sync_each()) {                                          \
             cudaError_t le_ = cudaGetLastError();                        \
             if (le_ == cudaSuccess) { le_ = cudaStreamSynchronize((C)->stream); } \
+            if (le_ != cudaSuccess) { return tcg::cuda_fail(le_, #kern); } \
+        }                                                                \
+    } while (0)
+
+// The same on a given stream of the context.
+#define TCG_LAUNCH_ON(C, strm, id, kern, grid, block, smem, ...)         \
+    do {                                                                 \
+        tcg::kern_begin_on((C), (id), (strm));                           \
+        kern<<<(grid), (block), (smem), (strm)>>>(__VA_ARGS__);          \
+        tcg::kern_end_on((C), (strm));                                   \
+        tcg::note_launch(1);                                             \
+        if (tcg::sync_each()) {                                          \
+            cudaError_t le_ = cudaGetLastError();                        \
+            if (le_ == cudaSuccess) { le_ = cudaStreamSynchronize(strm); } \
             if (le_ != cudaSuccess) { return tcg::cuda_fail(le_, #kern); } \
         }                                                                \
     } while (0)

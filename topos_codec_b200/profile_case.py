@@ -1,10 +1,11 @@
 """One batched encode + decode of a small synthetic case, for kernel profiling.
 
-    python -m topos_codec_b200.profile_case [--size 1920x1080] [--frames 1] [--qp 4] [--repeat 1]
+    python -m topos_codec_b200.profile_case [--size 1920x1080] [--frames 1] [--qp 4] [--repeat 1] [--gbr]
 
 Runs the same library path as bench.py (device-resident samples, packets and
 planes) on a case small enough for a full-metric profiler capture, and prints
-the per-kernel device times of the last repetition.
+the per-kernel device times of the last repetition. --gbr codes 12-bit GBR
+4:4:4 with a 16-bit alpha plane at qp 2 instead of 10-bit 4:2:2.
 """
 from __future__ import annotations
 
@@ -23,6 +24,7 @@ def main() -> None:
     ap.add_argument("--frames", type=int, default=1)
     ap.add_argument("--qp", type=int, default=4)
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--gbr", action="store_true")
     a = ap.parse_args()
     w, h = (int(v) for v in a.size.split("x"))
     n = a.frames
@@ -30,12 +32,18 @@ def main() -> None:
     L = gpu._lib
     L.tcg_profile_read.argtypes = [ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_uint64)]
-    cfg = B.make_config(w, h, qp=a.qp, qmatrix_id=0 if w >= 3840 else 4, features=3 if w >= 3840 else 1)
-    frames = [[p.to(torch.uint16) for p in synth.make_frame(w, h, seed=0, frame=i, device="cuda")] for i in range(n)]
-    cw = (w + 1) // 2
-    cap = (w * h + 2 * cw * h) * 4 + (1 << 20)
+    if a.gbr:
+        from .workloads import gbr_config
+        cfg = gbr_config(w, h)
+        kw = dict(bit_depth=12, pixel_format=2, limited=False, alpha=True, sigma=12)
+    else:
+        cfg = B.make_config(w, h, qp=a.qp, qmatrix_id=0 if w >= 3840 else 4, features=3 if w >= 3840 else 1)
+        kw = {}
+    frames = [[p.to(torch.uint16) for p in synth.make_frame(w, h, seed=0, frame=i, device="cuda", **kw)]
+              for i in range(n)]
+    cap = gpu.packet_bound(cfg)
     outs = [torch.empty(cap, dtype=torch.uint8, device="cuda") for _ in range(n)]
-    dec = [[torch.empty((h, x), dtype=torch.uint16, device="cuda") for x in (w, cw, cw)] for _ in range(n)]
+    dec = [[torch.empty(s, dtype=torch.uint16, device="cuda") for s in B.plane_shapes(cfg)] for _ in range(n)]
     cfgs = (B.FrameConfig * n)(*[cfg] * n)
     ins = (B.FrameInput * n)()
     for i, fr in enumerate(frames):
@@ -48,8 +56,8 @@ def main() -> None:
     rcs = (ctypes.c_int32 * n)()
     dptr = (ctypes.c_void_p * (4 * n))()
     for i in range(n):
-        for p in range(3):
-            dptr[4 * i + p] = dec[i][p].data_ptr()
+        for p, t in enumerate(dec[i]):
+            dptr[4 * i + p] = t.data_ptr()
     infos = (B.FrameOutput * n)()
     for r in range(a.repeat):
         if r == a.repeat - 1:
