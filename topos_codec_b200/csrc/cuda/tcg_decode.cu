@@ -7,7 +7,7 @@
 //               lookup tables, quantiser steps    (slice_codec.c:554-625)
 //   k_dchain    one lane per colour slice, 1-8 slices per warp: serial
 //               forward rANS2 decode through bucket tables in shared memory
-//               -> natural-order coefficients, DC reconstruction, domain
+//               -> zigzag-order coefficients, DC reconstruction, domain
 //               checks                          (slice_codec.c:626-736)
 //   k_dchain_w  the same decode with one warp per colour slice, the symbol
 //               search spread over the lanes (a second tiling; a tuner picks)
@@ -189,11 +189,11 @@ __global__ void __launch_bounds__(32) k_dtables(const DSlice* __restrict__ slice
 constexpr uint32_t DCH_LUT_SLOTS = 7u;  // shared-memory bucket tables per slice
 constexpr uint32_t DCH_CUM_BYTES = (MAX_CTX * CUM_BYTES + 15u) & ~15u;
 constexpr uint32_t DCH_LANE_BYTES = DCH_LUT_SLOTS * LUT_BYTES + DCH_CUM_BYTES;
-// block head: zigzag order (64 bytes), then the level-context table: three
-// rows of 80 u16 (level models by position / by previous category / single),
-// each the offset of a context's bucket table in u32 words
+// block head: the level-context table, three rows of 80 u16 (level models by
+// position / by previous category / single), each the offset of a context's
+// bucket table in u32 words
 constexpr uint32_t DCH_CTX_ROW = 80u;
-constexpr uint32_t DCH_HEAD = 64u + ((3u * DCH_CTX_ROW * 2u + 15u) & ~15u);
+constexpr uint32_t DCH_HEAD = (3u * DCH_CTX_ROW * 2u + 15u) & ~15u;
 __host__ __device__ constexpr uint32_t dch_smem(uint32_t lanes) { return DCH_HEAD + lanes * DCH_LANE_BYTES; }
 
 struct DLane {
@@ -333,11 +333,8 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
                                                int32_t* __restrict__ status)
 {
     extern __shared__ __align__(16) uint8_t dsm[];
-    uint8_t* zz = dsm;  // zigzag order, shared by the lanes
-    uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm + 64u);
+    uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm);
     const uint32_t t = threadIdx.x;
-    zz[t] = c_zigzag[t];
-    zz[t + 32u] = c_zigzag[t + 32u];
     // row 1 indexed by the next position (1..64), row 2 by the previous level's
     // category (0..63; index 79 = no previous level in the block), row 0 zero
     for (uint32_t i = t; i < 3u * DCH_CTX_ROW; i += 32u) {
@@ -474,7 +471,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
             L.whi = __funnelshift_l(wlo2, whi2, n8s);
             L.wlo = wlo2 << n8s;
             L.wbits -= n8 + n8s;
-            blk[zz[pos]] = (int32_t)mm;
+            blk[pos] = (int32_t)mm;
             ++pos;
             pcat = cat;
             has = true;
@@ -501,7 +498,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
         m = dl_suffix(L, sc);
         if (!geob) {
             err |= m > mlv ? 1u : 0u;
-            blk[zz[idx]] = (int32_t)m;
+            blk[idx] = (int32_t)m;
             pcat = sc;
             has = true;
             pos = idx + 1u;
@@ -755,10 +752,9 @@ __device__ __forceinline__ int32_t dchain_slice(const DSlice& S, const DPlane& P
                 const uint32_t cat = dec_sym32(w, fl, cl, lane);
                 const uint32_t m = dec_suffix(w, cat, lane);
                 err |= m > mlv ? 1u : 0u;
-                const uint32_t nat = c_zigzag[idx];
-                const int32_t v = (int32_t)m;  // zigzag-mapped; reconstruction unmaps
-                if ((nat & 31u) == lane) {
-                    if (nat & 32u) { chi = v; } else { clo = v; }
+                const int32_t v = (int32_t)m;  // zigzag-mapped level at zigzag position idx
+                if ((idx & 31u) == lane) {
+                    if (idx & 32u) { chi = v; } else { clo = v; }
                 }
                 pcat = cat;
                 has = true;
@@ -807,9 +803,10 @@ __global__ void __launch_bounds__(32) k_dchain_w(const DSlice* __restrict__ slic
 
 // ------------------------------------------------------------------ reconstruction
 //
-// Coefficient blocks hold the DC value at index 0 (signed) and the AC levels
-// in their zigzag-mapped form (m = 2v or -2v-1), which the chains store as
-// decoded; 0 maps to 0, so untouched positions read as zero levels.
+// Coefficient blocks are in zigzag order, as the chains decode them: the DC
+// value at index 0 (signed) and the AC levels in their zigzag-mapped form
+// (m = 2v or -2v-1); 0 maps to 0, so untouched positions read as zero levels.
+// Reconstruction places them in natural order while loading.
 
 __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ blk_slice,
                                                const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
@@ -836,9 +833,10 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
-            int64_t f = (int64_t)lv * __ldg(Q + i * 4 + j);
+            const int nat = k_zigzag[i * 4 + j];
+            int64_t f = (int64_t)lv * __ldg(Q + nat);
             f = f > fc ? fc : (f < -fc ? -fc : f);
-            c[i * 4 + j] = (int32_t)f;
+            c[nat] = (int32_t)f;
         }
     }
     idct8x8(c, xh);
