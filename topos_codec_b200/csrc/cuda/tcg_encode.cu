@@ -354,9 +354,9 @@ __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slic
     }
     if (threadIdx.x == 0) { sres[si].nops = carry; }
     // identity operations (word 0) from the count up to the next multiple of
-    // 16, so the chain reads whole 16-operation iterations without masking
+    // 32, so the chain reads whole 32-operation iterations without masking
     // (a slice window holds 256 words past its largest count)
-    if (threadIdx.x < 16u && carry + threadIdx.x < ((carry + 15u) & ~15u)) {
+    if (threadIdx.x < 32u && carry + threadIdx.x < ((carry + 31u) & ~31u)) {
         ops[S.op_base + carry + threadIdx.x] = 0u;
     }
 }
@@ -498,8 +498,8 @@ __device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, c
 }
 
 // Four consecutive operations of a slice (group g). The slice's window holds
-// identity operations from its count to the next multiple of 16, and every
-// group the chain loads lies within the window or the next 256 words.
+// identity operations from its count to the next multiple of 32, and every
+// group the chain loads lies within the window (at most 63 words past the count).
 __device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t)
 {
     return __ldg(op4 + g);
@@ -518,8 +518,8 @@ constexpr size_t CHAIN_SMEM = (size_t)CHAIN_LANES * OP_ENTRIES * sizeof(uint4);
 
 // One lane per colour slice. The lane expands its slice's symbol table into
 // per-operation coding entries in shared memory, then walks the operations in
-// coding order, sixteen per iteration with the operation words loaded sixteen
-// ahead of their use. Bytes go downwards from the end of the lane's staging
+// coding order, 32 per iteration with the operation words loaded 32 ahead of
+// their use. Bytes go downwards from the end of the lane's staging
 // window, so the stream reads forwards.
 __global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict__ slices,
                                                        const uint32_t* __restrict__ order, uint32_t n,
@@ -544,21 +544,24 @@ __global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict_
     uint8_t* const end = stage + S.stage_base + S.stage_cap;  // emitted byte k lives at end[-1-k]
     uint8_t* p = end;
     uint32_t x = RANS_L;
-    uint4 a = op_group(op4, 0u, nops), b = op_group(op4, 1u, nops);
-    uint4 c = op_group(op4, 2u, nops), d = op_group(op4, 3u, nops);
-    for (uint32_t g = 0; 4u * g < nops; g += 4u) {
-        // bring the operation words 256 bytes ahead into L1 so the group loads below hit it
-        const uint32_t pf = (uint32_t)(4u * (g + 16u) < nops);
+    // eight groups (32 operations) in registers, each reloaded eight groups ahead
+    // of its use, and an L1 prefetch 512 bytes ahead
+    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops);
+    uint4 q2 = op_group(op4, 2u, nops), q3 = op_group(op4, 3u, nops);
+    uint4 q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
+    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops);
+    for (uint32_t g = 0; 4u * g < nops; g += 8u) {
+        const uint32_t pf = (uint32_t)(4u * (g + 32u) < nops);
         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
-                     :: "l"(op4 + g + 16u), "r"(pf));
-        ENC_GROUP(a);
-        a = op_group(op4, g + 4u, nops);
-        ENC_GROUP(b);
-        b = op_group(op4, g + 5u, nops);
-        ENC_GROUP(c);
-        c = op_group(op4, g + 6u, nops);
-        ENC_GROUP(d);
-        d = op_group(op4, g + 7u, nops);
+                     :: "l"(op4 + g + 32u), "r"(pf));
+        ENC_GROUP(q0); q0 = op_group(op4, g + 8u, nops);
+        ENC_GROUP(q1); q1 = op_group(op4, g + 9u, nops);
+        ENC_GROUP(q2); q2 = op_group(op4, g + 10u, nops);
+        ENC_GROUP(q3); q3 = op_group(op4, g + 11u, nops);
+        ENC_GROUP(q4); q4 = op_group(op4, g + 12u, nops);
+        ENC_GROUP(q5); q5 = op_group(op4, g + 13u, nops);
+        ENC_GROUP(q6); q6 = op_group(op4, g + 14u, nops);
+        ENC_GROUP(q7); q7 = op_group(op4, g + 15u, nops);
     }
     sres[si].nbytes = (uint32_t)(end - p);
     sres[si].xfin = x;
