@@ -808,7 +808,10 @@ __global__ void __launch_bounds__(32) k_dchain_w(const DSlice* __restrict__ slic
 // (m = 2v or -2v-1); 0 maps to 0, so untouched positions read as zero levels.
 // Reconstruction places them in natural order while loading.
 
-__global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ blk_slice,
+// The block's colour slice is found by a binary search over the colour slices,
+// which are in increasing order of their first block.
+__global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+                                               uint32_t ncs,
                                                const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
                                                const uint8_t* __restrict__ tabs, const int32_t* __restrict__ coef,
                                                const int32_t* __restrict__ status, uint32_t total,
@@ -816,7 +819,12 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
 {
     const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
     if (gb >= total) { return; }
-    const uint32_t si = blk_slice[gb];
+    uint32_t lo = 0, hi = ncs - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (slices[cslices[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1u; }
+    }
+    const uint32_t si = cslices[lo];
     if (status[si] != 0) { return; }
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
@@ -1160,7 +1168,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
 {
     std::vector<DPlane> planes;
     std::vector<DSlice> slices;
-    std::vector<uint32_t> cslices, aslices, slice_tab, blk_slice;
+    std::vector<uint32_t> cslices, aslices, slice_tab;
     std::vector<DbPlane> dbp;
     std::vector<uint64_t> pkt_off(count, 0);
     std::vector<uint32_t> frame_slice0(count, 0);
@@ -1227,14 +1235,10 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             slices.push_back(S);
         }
     }
-    blk_slice.resize(nblk);
-    for (uint32_t si : cslices) {
-        for (uint32_t k = 0; k < slices[si].nblk; ++k) { blk_slice[slices[si].blk0 + k] = si; }
-    }
     const uint32_t ns = (uint32_t)slices.size(), nc = (uint32_t)cslices.size(), na = (uint32_t)aslices.size();
     const size_t desc = align_up(planes.size() * sizeof(DPlane), 256) + align_up(ns * sizeof(DSlice), 256) +
                         align_up((size_t)(nc + na) * 4u + 16, 256) + align_up((size_t)ns * 4u + 16, 256) +
-                        align_up((size_t)nblk * 4u + 16, 256) + align_up(dbp.size() * sizeof(DbPlane) + 16, 256) +
+                        align_up(dbp.size() * sizeof(DbPlane) + 16, 256) +
                         align_up((size_t)nc * 4u + 16, 256);
     if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
         !dreserve(C, B_DEC_TAB, (size_t)nc * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
@@ -1261,7 +1265,6 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const size_t o_sl = put(slices.data(), ns * sizeof(DSlice));
     const size_t o_ca = put(cs_as.data(), cs_as.size() * 4u);
     const size_t o_st = put(slice_tab.data(), slice_tab.size() * 4u);
-    const size_t o_bs = put(blk_slice.data(), blk_slice.size() * 4u);
     const size_t o_db = put(dbp.data(), dbp.size() * sizeof(DbPlane));
     const size_t o_or = put(ord.data(), ord.size() * 4u);
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
@@ -1270,7 +1273,6 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const uint32_t* d_cs = (const uint32_t*)(dd + o_ca);
     const uint32_t* d_as = d_cs + nc;
     const uint32_t* d_st = (const uint32_t*)(dd + o_st);
-    const uint32_t* d_bs = (const uint32_t*)(dd + o_bs);
     const DbPlane* d_db = (const DbPlane*)(dd + o_db);
     const uint32_t* d_ord = (const uint32_t*)(dd + o_or);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
@@ -1407,7 +1409,7 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
             std::lock_guard<std::mutex> g(g_tune_mu);
             g_tune[cls] = (int8_t)best;
         }
-        TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_bs, d_st, d_pl, d_tab, d_coef,
+        TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_cs, nc, d_st, d_pl, d_tab, d_coef,
                    d_status, (uint32_t)nblk, d_out);
     }
     if (na > 0) {
@@ -1437,8 +1439,12 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         for (uint32_t p = 0; p < F.planes; ++p, ++pg) {
             const DPlane& P = planes[pg];
             const size_t pitch = (F.dst_stride[p] ? F.dst_stride[p] : P.vis_w) * 2u;
-            TCG_CHECK(cudaMemcpy2DAsync(F.dst[p], pitch, d_out + P.out_off, (size_t)P.vis_w * 2u, (size_t)P.vis_w * 2u,
-                                        P.vis_h, cudaMemcpyDefault, st));
+            if (pitch == (size_t)P.vis_w * 2u) {  // tight rows: one flat copy
+                TCG_CHECK(cudaMemcpyAsync(F.dst[p], d_out + P.out_off, pitch * P.vis_h, cudaMemcpyDefault, st));
+            } else {
+                TCG_CHECK(cudaMemcpy2DAsync(F.dst[p], pitch, d_out + P.out_off, (size_t)P.vis_w * 2u,
+                                            (size_t)P.vis_w * 2u, P.vis_h, cudaMemcpyDefault, st));
+            }
         }
     }
     int32_t* hs = (int32_t*)C->h[1].p;

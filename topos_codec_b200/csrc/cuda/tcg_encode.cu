@@ -1076,8 +1076,13 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
         for (uint32_t f = 0; f < count; ++f) {
             for (uint32_t p = 0; p < frames[f].planes; ++p, ++pg) {
                 const tcg_enc_plane& I = frames[f].plane[p];
-                TCG_CHECK(cudaMemcpy2DAsync(d_pix + planes[pg].pix_off, (size_t)I.vis_w * 2u, I.src, I.stride * 2u,
-                                            (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, st));
+                if (I.stride == I.vis_w) {  // tight rows: one flat copy
+                    TCG_CHECK(cudaMemcpyAsync(d_pix + planes[pg].pix_off, I.src, (size_t)I.vis_w * I.vis_h * 2u,
+                                              cudaMemcpyDefault, st));
+                } else {
+                    TCG_CHECK(cudaMemcpy2DAsync(d_pix + planes[pg].pix_off, (size_t)I.vis_w * 2u, I.src,
+                                                I.stride * 2u, (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, st));
+                }
             }
         }
     }
