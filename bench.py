@@ -355,7 +355,16 @@ def main():
     e2e_s = (time.perf_counter() - t0) / args.steps
     e2e_s = sharding.max_over_ranks([e2e_s], device=dev)[0]
     e2e_exact = all(out_h[i][: stats[i].packet_size].numpy().tobytes() == batched_pkts[i] for i in range(nf))
+    e2e_exact = e2e_exact and all(torch.equal(dec_h[i][p].view(torch.int16), dec_d[i][p].cpu().view(torch.int16))
+                                  for i in range(nf) for p in range(3))
     exact = exact and e2e_exact
+    # host-memory batches are coded in pipelined chunks (copies of one chunk
+    # overlap the kernels of another); report the split the library used
+    L.tcg_pipeline_plan.restype = ctypes.c_uint32
+    fb = (ctypes.c_uint64 * nf)(*[in_bytes // nf] * nf)
+    e2e_chunks = int(L.tcg_pipeline_plan(0, fb, nf, (ctypes.c_uint32 * 5)()))
+    fb = (ctypes.c_uint64 * nf)(*[(in_bytes + pkt_bytes) // nf] * nf)
+    e2e_dchunks = int(L.tcg_pipeline_plan(1, fb, nf, (ctypes.c_uint32 * 5)()))
 
     # ---------------- roofline of the dominant kernel ----------------
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -474,7 +483,8 @@ def main():
             "served": served,
             "workloads": extra,
             "e2e": {"value": nf * world / e2e_s, "unit": "frames/s",
-                    "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes)},
+                    "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes),
+                    "encode_chunks": e2e_chunks, "decode_chunks": e2e_dchunks},
         }
         print(json.dumps(line))
     if world > 1:

@@ -317,12 +317,28 @@ int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, to
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, one
  * warp per slice (1), or a split (5: the largest slices, half of the blocks,
- * one per warp and the rest four per warp on a second stream); -1 = not
+ * one per warp and the rest four per warp in a second launch that starts
+ * beside the first as its programmatic dependent on the same stream); -1 = not
  * chosen yet. The first batch of each size class (log2 of the slice count)
  * times the split and 4, 2 and 1 slices per warp and keeps the fastest;
  * the environment variable TCG_DCHAIN=lane|lane4|lane2|lane1|warp|split overrides
  * the choice ("lane" is 8 per warp). All produce identical output. */
 int32_t tcg_dchain_tiling(uint32_t colour_slices);
+
+/* Batches whose inputs or outputs are in host memory are coded as chunks on
+ * separate streams (encode up to four, decode up to three): chunk i's
+ * host-to-device copies queue behind chunk i-1's, so the copies of later
+ * chunks overlap the kernels of earlier ones and each chunk's results return
+ * while later chunks still compute. A batch is chunked when its host copy
+ * bytes (encode: samples; decode: packets plus planes) reach 256 MB, one chunk
+ * per 64 MB. The output is identical to the unchunked call's.
+ * tcg_pipeline_plan reports the split the library would use for an encode
+ * (decode = 0) or decode (decode != 0) batch with the given per-frame copy
+ * bytes: it returns the chunk count k (1 = no chunking) and fills starts[0..k]
+ * (frames [starts[i], starts[i+1]) form chunk i; starts must hold 5 entries).
+ * The environment variable TCG_PIPELINE=<n> forces n chunks (0 or 1: never
+ * chunk; at most four). Host work only; needs no device. */
+uint32_t tcg_pipeline_plan(int32_t decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts);
 
 /* Device selection and teardown for the calling process. tcg_device_init is
  * implicit on first use (device 0 or the current CUDA device). */
@@ -335,7 +351,8 @@ uint64_t tcg_kernel_launches(void);
 
 /* Device time in milliseconds of the calling thread's last frame call,
  * measured with CUDA events on the stream the call's kernels ran on (from the
- * first upload to the last download). */
+ * first upload to the last download; for a chunked host-memory batch, from
+ * the first chunk's start to the last chunk's end). */
 double tcg_last_device_ms(void);
 
 /* Optional per-kernel timing: when enabled, every kernel launch is bracketed

@@ -176,3 +176,49 @@ def test_reference_python_binding_loads_this_library(built):
     assert lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == B.TC_ERR_NOT_IMPLEMENTED
     lib.tc_scalable_status_name.restype = ctypes.c_char_p
     assert lib.tc_scalable_status_name(1) == b"reference" and lib.tc_scalable_status_name(9) == b"unknown"
+
+
+def _plan(L, sizes, decode=0):
+    n = len(sizes)
+    arr = (ctypes.c_uint64 * max(n, 1))(*sizes)
+    starts = (ctypes.c_uint32 * 5)()
+    k = int(L.tcg_pipeline_plan(ctypes.c_int32(decode), arr, ctypes.c_uint32(n), starts))
+    return k, list(starts[: k + 1])
+
+
+def test_pipeline_plan_splits_host_batches(product, monkeypatch):
+    """Chunking of host-memory batches: no split below 256 MB of copies, one
+    chunk per 64 MB up to four (encode) or three (decode), every chunk
+    non-empty and contiguous, chunk bytes within one frame of an even share;
+    TCG_PIPELINE forces the count (up to four)."""
+    L = product._lib
+    L.tcg_pipeline_plan.restype = ctypes.c_uint32
+    monkeypatch.delenv("TCG_PIPELINE", raising=False)
+    MB = 1 << 20
+    assert _plan(L, [33 * MB] * 7) == (1, [0, 7])           # 231 MB: one piece
+    assert _plan(L, [33 * MB] * 60)[0] == 4                  # 3840x2160 4:2:2 batch
+    assert _plan(L, [63 * MB] * 60, decode=1)[0] == 3        # its packets and planes
+    assert _plan(L, [300 * MB]) == (1, [0, 1])               # one frame never splits
+    assert _plan(L, [160 * MB, 160 * MB]) == (2, [0, 1, 2])
+    assert _plan(L, []) == (1, [0, 0])
+    rng = random.Random(3)
+    for trial in range(300):
+        n = rng.randint(1, 70)
+        sizes = [rng.choice([0, rng.randint(1, 80 * MB)]) for _ in range(n)]
+        total = sum(sizes)
+        decode = trial % 2
+        k, st = _plan(L, sizes, decode)
+        want = 1 if total < 256 * MB else min(3 if decode else 4, total // (64 * MB), n)
+        assert k == max(1, want)
+        assert st[0] == 0 and st[-1] == n and all(a < b for a, b in zip(st, st[1:]))
+        if k > 1:
+            big = max(sizes)
+            for i in range(k - 1):  # every chunk but the last stops at its share
+                assert sum(sizes[: st[i + 1]]) < total // k * (i + 1) + big or st[i + 1] - st[i] == 1
+    monkeypatch.setenv("TCG_PIPELINE", "3")
+    assert _plan(L, [1, 1, 1, 1, 1]) == (3, [0, 1, 2, 5])
+    assert _plan(L, [1, 1]) == (2, [0, 1, 2])
+    monkeypatch.setenv("TCG_PIPELINE", "9")
+    assert _plan(L, [1] * 8, decode=1) == (4, [0, 2, 4, 6, 8])
+    monkeypatch.setenv("TCG_PIPELINE", "0")
+    assert _plan(L, [33 * MB] * 60) == (1, [0, 60])

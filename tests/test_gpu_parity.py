@@ -146,6 +146,39 @@ def test_batch_decode_equals_single(product):
             assert np.array_equal(x, y)
 
 
+@pytest.mark.parametrize("chunks", ["2", "3", "4"])
+def test_pipelined_host_batches_vs_oracle(product, oracle, monkeypatch, chunks):
+    """Host-memory batches split into chunks on separate contexts and streams
+    (TCG_PIPELINE forces the split that large batches get by size): packets
+    byte-identical to the oracle, pixels and per-slice concealment of a batch
+    holding damaged packets identical to the oracle's."""
+    sizes = [(1280, 720), (64, 48), (1920, 1080), (333, 77), (640, 360), (256, 128)]
+    cfgs, frames = [], []
+    for i, (w, h) in enumerate(sizes):
+        frames.append(synth.make_frame_np(w, h, seed=80 + i))
+        cfgs.append(B.make_config(w, h, qp=2 + 3 * i, qmatrix_id=4 if i % 2 else 0, features=1 + (i % 2), slice_rows=2))
+    monkeypatch.setenv("TCG_PIPELINE", chunks)
+    rc, pkts, rcs, _ = product.encode_batch(cfgs, frames)
+    assert rc == 0 and rcs == [0] * len(sizes)
+    for c, f, p in zip(cfgs, frames, pkts):
+        assert p == oracle.encode(c, f)
+    rng = random.Random(int(chunks))
+    batch = list(pkts)
+    for k in (1, 4):  # one damaged payload byte in two of the packets
+        p = bytearray(batch[k])
+        _, po, size = _spans(batch[k])[rng.randrange(len(_spans(batch[k])))]
+        p[po + rng.randrange(size)] ^= 0x5A
+        batch[k] = bytes(p)
+    rc, got = product.decode_batch(batch)
+    assert rc in (B.TC_OK, B.TC_WARN_CONCEALED)
+    for p, f in zip(batch, got):
+        want = oracle.decode_status(p)
+        assert want.status in (B.TC_OK, B.TC_WARN_CONCEALED)
+        assert f.info.concealed_slices == sum(1 for s in want.slice_status if s != 0)
+        for x, y in zip(want.planes, f.planes):
+            assert np.array_equal(x, y)
+
+
 def test_device_resident_encode_decode(product):
     """Device pointers for samples, packets and output planes (no host staging):
     same packet and pixels as the host-memory path, including a damaged packet

@@ -333,6 +333,9 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
                                                int32_t* __restrict__ status)
 {
     extern __shared__ __align__(16) uint8_t dsm[];
+    // A chain launch that follows this one on the stream as a programmatic
+    // dependent (the split tiling) may start at once: it decodes other slices.
+    cudaTriggerProgrammaticLaunchCompletion();
     uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm);
     const uint32_t t = threadIdx.x;
     // row 1 indexed by the next position (1..64), row 2 by the previous level's
@@ -368,7 +371,14 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     // the lanes with a slice to decode; they stay together until all are done
     const bool live = t < LANES && i0 + t < nc && status[order[i0 + t]] == 0;
     const uint32_t wmask = __ballot_sync(0xFFFFFFFFu, live);
-    if (!live) { return; }
+    if (!live) {
+        // A programmatic dependent completes only after the launch before it
+        // (cudaGridDependencySynchronize; no effect in an ordinary launch), so
+        // the kernels after it see both: the live lanes wait at their end, lane 0
+        // here when the warp has none.
+        if (wmask == 0u && t == 0u) { cudaGridDependencySynchronize(); }
+        return;
+    }
     const uint32_t si = order[i0 + t];
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
@@ -524,6 +534,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
 #undef DCH_FINISH
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
+    cudaGridDependencySynchronize();
 }
 
 // ------------------------------------------------------------------ chain, warp tiling
@@ -1164,14 +1175,27 @@ extern "C" __attribute__((visibility("default"))) int32_t tcg_dchain_tiling(uint
     return g_tune[size_class(nc)];
 }
 
-static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
+// What decode_outputs and decode_finish need of a launched batch.
+struct DecPending {
+    std::vector<uint32_t> frame_slice0;  // first slice index of each frame
+    std::vector<DPlane> planes;          // output offsets and sizes, frames in order
+    uint32_t ns = 0;                     // slices
+};
+
+// Enqueue one batch on the context's streams: descriptors, packet copies and
+// kernels. The packet copies start after `after` (when given) and C->gate is
+// recorded behind them.
+static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count, cudaEvent_t after,
+                             DecPending& pend)
 {
-    std::vector<DPlane> planes;
+    std::vector<uint32_t>& frame_slice0 = pend.frame_slice0;
+    std::vector<DPlane>& planes = pend.planes;
+    planes.clear();
     std::vector<DSlice> slices;
     std::vector<uint32_t> cslices, aslices, slice_tab;
     std::vector<DbPlane> dbp;
     std::vector<uint64_t> pkt_off(count, 0);
-    std::vector<uint32_t> frame_slice0(count, 0);
+    frame_slice0.assign(count, 0u);
     uint64_t out_elems = 0, pkt_bytes = 0, nblk = 0, alpha_res = 0;
     uint32_t max_cols = 1;
     for (uint32_t f = 0; f < count; ++f) {
@@ -1277,10 +1301,12 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     const uint32_t* d_ord = (const uint32_t*)(dd + o_or);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
     call_begin(C);
+    if (after != nullptr) { TCG_CHECK(cudaStreamWaitEvent(st, after, 0)); }
     for (uint32_t f = 0; f < count; ++f) {
         if (frames[f].skip) { continue; }
         TCG_CHECK(cudaMemcpyAsync(d_pkt + pkt_off[f], frames[f].packet, frames[f].size, cudaMemcpyDefault, st));
     }
+    TCG_CHECK(cudaEventRecord(C->gate, st));
     int32_t* d_status = dptr<int32_t>(C, B_DEC_RES);
     int32_t* d_coef = dptr<int32_t>(C, B_DEC_COEF);
     uint8_t* d_tab = dptr<uint8_t>(C, B_DEC_TAB);
@@ -1294,9 +1320,10 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
     if (na > 0) {
         // Alpha slices (Rice run/level decode, then MED reconstruction) share no
         // slice, status entry or output plane with the colour slices, so they
-        // run on a third stream beside the colour chain; the stream rejoins
+        // run on a second stream beside the colour chain; the stream rejoins
         // before concealment.
-        cudaStream_t as = C->aux;
+        cudaStream_t as = aux_stream(C);
+        if (as == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
         TCG_CHECK(cudaEventRecord(C->afork, st));
         TCG_CHECK(cudaStreamWaitEvent(as, C->afork, 0));
         TCG_CHECK(cudaMemsetAsync(d_ares, 0, alpha_res * 4u, as));
@@ -1332,20 +1359,31 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         auto run = [&](int tiling) -> int32_t {
             switch (tiling) {
             case DCH_TILE_SPLIT: {
+                // Both launches on the one stream: the second is a programmatic
+                // dependent of the first, so it starts as soon as every block of
+                // the first has (at its start), and it completes only after the
+                // first has, so the reconstruction after it sees all slices.
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
                 tcg::kern_begin(C, K_DCHAIN);
-                TCG_CHECK(cudaEventRecord(C->fork, st));
-                TCG_CHECK(cudaStreamWaitEvent(C->side, C->fork, 0));
                 k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
                                                                d_status);
+                TCG_CHECK(cudaGetLastError());
                 if (nc > nsplit) {
-                    k_dchain<4><<<(nc - nsplit + 3u) / 4u, 32, dch_smem(4), C->side>>>(
-                        d_sl, d_ord + nsplit, nc - nsplit, d_st, d_pl, d_pkt, d_tab, d_coef, d_status);
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    at[0].val.programmaticStreamSerializationAllowed = 1;
+                    cudaLaunchConfig_t lc = {};
+                    lc.gridDim = dim3((nc - nsplit + 3u) / 4u);
+                    lc.blockDim = dim3(32);
+                    lc.dynamicSmemBytes = dch_smem(4);
+                    lc.stream = st;
+                    lc.attrs = at;
+                    lc.numAttrs = 1;
+                    TCG_CHECK(cudaLaunchKernelEx(&lc, k_dchain<4>, (const DSlice*)d_sl, (const uint32_t*)(d_ord + nsplit),
+                                                 (uint32_t)(nc - nsplit), (const uint32_t*)d_st, (const DPlane*)d_pl,
+                                                 (const uint8_t*)d_pkt, (const uint8_t*)d_tab, d_coef, d_status));
                 }
                 tcg::note_launch(nc > nsplit ? 2u : 1u);
-                TCG_CHECK(cudaGetLastError());
-                TCG_CHECK(cudaEventRecord(C->join, C->side));
-                TCG_CHECK(cudaStreamWaitEvent(st, C->join, 0));
                 tcg::kern_end(C);
                 if (tcg::sync_each()) { TCG_CHECK(cudaStreamSynchronize(st)); }
                 return TCG_OK;
@@ -1431,7 +1469,18 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
                    d_db, (uint32_t)dbp.size(), d_out);
     }
     TCG_CHECK(cudaGetLastError());
-    // outputs to the caller's planes
+    pend.ns = ns;
+    return 0;
+}
+
+// Enqueue the copies of a launched batch's planes to the callers' buffers and
+// of its slice statuses to pinned host memory.
+static int32_t decode_outputs(Ctx* C, const tcg_dec_frame* frames, const DecPending& pend)
+{
+    cudaStream_t st = C->stream;
+    const std::vector<DPlane>& planes = pend.planes;
+    const uint16_t* d_out = dptr<uint16_t>(C, B_DEC_OUT);
+    const uint32_t count = (uint32_t)pend.frame_slice0.size();
     uint32_t pg = 0;
     for (uint32_t f = 0; f < count; ++f) {
         const tcg_dec_frame& F = frames[f];
@@ -1448,15 +1497,70 @@ static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
         }
     }
     int32_t* hs = (int32_t*)C->h[1].p;
-    if (ns > 0) { TCG_CHECK(cudaMemcpyAsync(hs, d_status, (size_t)ns * 4u, cudaMemcpyDeviceToHost, st)); }
-    TCG_CHECK(cudaStreamSynchronize(st));
+    if (pend.ns > 0) {
+        TCG_CHECK(cudaMemcpyAsync(hs, dptr<int32_t>(C, B_DEC_RES), (size_t)pend.ns * 4u, cudaMemcpyDeviceToHost, st));
+    }
+    return 0;
+}
+
+// Wait for a batch whose outputs were enqueued and report each slice's status.
+static int32_t decode_finish(Ctx* C, const tcg_dec_frame* frames, const DecPending& pend)
+{
+    const std::vector<uint32_t>& frame_slice0 = pend.frame_slice0;
+    TCG_CHECK(cudaStreamSynchronize(C->stream));
     call_end(C);
-    for (uint32_t f = 0; f < count; ++f) {
+    const int32_t* hs = (const int32_t*)C->h[1].p;
+    for (uint32_t f = 0; f < (uint32_t)frame_slice0.size(); ++f) {
         const tcg_dec_frame& F = frames[f];
         if (F.skip) { continue; }
         for (uint32_t i = 0; i < F.slices; ++i) { F.slice_status[i] = hs[frame_slice0[f] + i] != 0 ? 1u : 0u; }
     }
     return 0;
+}
+
+static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
+{
+    DecPending pend;
+    int32_t rc = decode_launch(C, frames, count, nullptr, pend);
+    if (rc == 0) { rc = decode_outputs(C, frames, pend); }
+    return rc != 0 ? rc : decode_finish(C, frames, pend);
+}
+
+// Host-memory batch in chunks on as many contexts (pipeline_plan): chunk i's
+// packet copies queue behind chunk i-1's, so later chunks' packets arrive while
+// earlier chunks decode, and earlier chunks' planes go back while later ones
+// still decode. Every chunk's packet copies and kernels are enqueued before any
+// chunk's output copies, so no upload is queued behind a download that waits
+// for kernels. The reported device time spans the first chunk's start to the
+// last chunk's end.
+static int32_t decode_pipelined(const tcg_dec_frame* frames, const uint32_t* starts, uint32_t k)
+{
+    Ctx* cs[PIPE_MAX_CHUNKS] = {};
+    DecPending fs0[PIPE_MAX_CHUNKS];
+    int32_t rc = 0;
+    uint32_t launched = 0;
+    for (uint32_t i = 0; i < k && rc == 0; ++i) {
+        cs[i] = ctx_acquire();
+        if (cs[i] == nullptr) {
+            rc = TCG_ERR_NOT_IMPLEMENTED;
+            break;
+        }
+        launched = i + 1u;
+        rc = decode_launch(cs[i], frames + starts[i], starts[i + 1] - starts[i], i ? cs[i - 1]->gate : nullptr, fs0[i]);
+    }
+    for (uint32_t i = 0; i < launched && rc == 0; ++i) { rc = decode_outputs(cs[i], frames + starts[i], fs0[i]); }
+    double span = 0.0;
+    for (uint32_t i = 0; i < launched; ++i) {
+        if (rc == 0) {
+            rc = decode_finish(cs[i], frames + starts[i], fs0[i]);
+            if (rc == 0) { span = std::max(span, event_span_ms(cs[0]->t0, cs[i]->t1)); }
+        } else {
+            cudaStreamSynchronize(cs[i]->stream);
+        }
+    }
+    for (uint32_t i = 0; i < launched; ++i) { ctx_release(cs[i]); }
+    if (rc == 0) { set_last_ms(span); }
+    return rc;
 }
 
 // ------------------------------------------------------------------ packet walk
@@ -1558,6 +1662,21 @@ static int32_t noalloc_base(uint8_t** base)
 
 extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
 {
+    uint32_t first = 0;
+    while (first < count && frames[first].skip) { ++first; }
+    if (count >= 2u && first < count &&
+        (tcg::host_memory(frames[first].packet) || tcg::host_memory(frames[first].dst[0]))) {
+        // copy bytes per frame: the packet in, the planes out
+        std::vector<uint64_t> bytes(count, 0);
+        for (uint32_t f = 0; f < count; ++f) {
+            if (frames[f].skip) { continue; }
+            bytes[f] = frames[f].size;
+            for (uint32_t p = 0; p < frames[f].planes; ++p) { bytes[f] += (uint64_t)frames[f].vis_w[p] * frames[f].vis_h[p] * 2u; }
+        }
+        uint32_t starts[tcg::PIPE_MAX_CHUNKS + 1];
+        const uint32_t k = tcg::pipeline_plan(true, bytes.data(), count, starts);
+        if (k > 1u) { return tcg::decode_pipelined(frames, starts, k); }
+    }
     tcg::Ctx* c = tcg::ctx_acquire();
     if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
     const int32_t rc = tcg::decode_impl(c, frames, count);

@@ -945,13 +945,17 @@ __global__ void k_pack_header(const EFrame* __restrict__ frames, uint32_t nf, co
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1u) / a * a; }
 
-static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs,
-                           const size_t* caps, tcg_enc_result* res)
+// Enqueue one batch on the context's streams: descriptors, sample copies,
+// kernels and the copy of the per-frame results to pinned host memory. The
+// sample copies start after `after` (when given) and C->gate is recorded
+// behind them. ef receives the frame table encode_results needs.
+static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count, cudaEvent_t after,
+                             std::vector<EFrame>& ef)
 {
     // ---------------- host planning ----------------
     std::vector<EPlane> planes;
     std::vector<ESlice> slices;
-    std::vector<EFrame> ef(count);
+    ef.assign(count, EFrame());
     std::vector<uint32_t> cplanes, cslices, aslices;
     std::vector<EWork> work;
     uint64_t pix_elems = 0, nblk = 0, ops_words = 0, stage_bytes = 0, pkt_bytes = 0;
@@ -1071,6 +1075,7 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
 
     // samples: one 2-D copy per plane (host or device source, caller stride)
     uint16_t* d_pix = dptr<uint16_t>(C, B_PIX);
+    if (after != nullptr) { TCG_CHECK(cudaStreamWaitEvent(st, after, 0)); }
     {
         uint32_t pg = 0;
         for (uint32_t f = 0; f < count; ++f) {
@@ -1086,6 +1091,7 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
             }
         }
     }
+    TCG_CHECK(cudaEventRecord(C->gate, st));
     ESliceRes* d_sres = dptr<ESliceRes>(C, B_SRES);
     EFrameRes* d_fres = dptr<EFrameRes>(C, B_FRES);
     uint32_t* d_aerr = reinterpret_cast<uint32_t*>(dptr<uint8_t>(C, B_FRES) + align_up(count * sizeof(EFrameRes), 16));
@@ -1107,9 +1113,10 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
 
     if (!aslices.empty()) {
         // Alpha slices (MED residuals, Rice pairs) read only the samples and write
-        // only their own staging windows and results, so they run on a third
+        // only their own staging windows and results, so they run on a second
         // stream beside the colour path; the stream rejoins before packing.
-        cudaStream_t as = C->aux;
+        cudaStream_t as = aux_stream(C);
+        if (as == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
         TCG_CHECK(cudaEventRecord(C->afork, st));
         TCG_CHECK(cudaStreamWaitEvent(as, C->afork, 0));
         for (uint32_t a : aslices) {
@@ -1157,6 +1164,19 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
     uint32_t* ha = (uint32_t*)((uint8_t*)C->h[1].p + align_up(count * sizeof(EFrameRes), 16));
     TCG_CHECK(cudaMemcpyAsync(hf, d_fres, count * sizeof(EFrameRes), cudaMemcpyDeviceToHost, st));
     TCG_CHECK(cudaMemcpyAsync(ha, d_aerr, count * 4u, cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
+// Wait for a launched batch's per-frame results, fill res and enqueue the copy
+// of every packet that fits its buffer (the caller synchronises the stream).
+static int32_t encode_results(Ctx* C, const std::vector<EFrame>& ef, uint8_t* const* outs, const size_t* caps,
+                              tcg_enc_result* res)
+{
+    const uint32_t count = (uint32_t)ef.size();
+    cudaStream_t st = C->stream;
+    const uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
+    const EFrameRes* hf = (const EFrameRes*)C->h[1].p;
+    const uint32_t* ha = (const uint32_t*)((const uint8_t*)C->h[1].p + align_up(count * sizeof(EFrameRes), 16));
     TCG_CHECK(cudaStreamSynchronize(st));
     for (uint32_t f = 0; f < count; ++f) {
         tcg_enc_result& r = res[f];
@@ -1184,9 +1204,57 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
         }
         r.rc = 0;
     }
-    TCG_CHECK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs,
+                           const size_t* caps, tcg_enc_result* res)
+{
+    std::vector<EFrame> ef;
+    int32_t rc = encode_launch(C, frames, count, nullptr, ef);
+    if (rc == 0) { rc = encode_results(C, ef, outs, caps, res); }
+    if (rc != 0) { return rc; }
+    TCG_CHECK(cudaStreamSynchronize(C->stream));
     call_end(C);
     return 0;
+}
+
+// Host-memory batch in chunks on as many contexts (pipeline_plan): all chunks
+// are launched first, chunk i's sample copies queued behind chunk i-1's, then
+// each chunk's results are read and its packets copied back in order while
+// later chunks still compute. The reported device time spans the first
+// chunk's start to the last chunk's end.
+static int32_t encode_pipelined(const tcg_enc_frame* frames, const uint32_t* starts, uint32_t k, uint8_t* const* outs,
+                                const size_t* caps, tcg_enc_result* res)
+{
+    Ctx* cs[PIPE_MAX_CHUNKS] = {};
+    std::vector<EFrame> ef[PIPE_MAX_CHUNKS];
+    int32_t rc = 0;
+    uint32_t launched = 0;
+    for (uint32_t i = 0; i < k && rc == 0; ++i) {
+        cs[i] = ctx_acquire();
+        if (cs[i] == nullptr) {
+            rc = TCG_ERR_NOT_IMPLEMENTED;
+            break;
+        }
+        launched = i + 1u;
+        rc = encode_launch(cs[i], frames + starts[i], starts[i + 1] - starts[i], i ? cs[i - 1]->gate : nullptr, ef[i]);
+    }
+    for (uint32_t i = 0; i < launched && rc == 0; ++i) {
+        rc = encode_results(cs[i], ef[i], outs + starts[i], caps + starts[i], res + starts[i]);
+    }
+    double span = 0.0;
+    for (uint32_t i = 0; i < launched; ++i) {
+        const cudaError_t e = cudaStreamSynchronize(cs[i]->stream);
+        if (rc == 0 && e != cudaSuccess) { rc = cuda_fail(e, "pipelined encode"); }
+        if (rc == 0) {
+            call_end(cs[i]);
+            span = std::max(span, event_span_ms(cs[0]->t0, cs[i]->t1));
+        }
+    }
+    for (uint32_t i = 0; i < launched; ++i) { ctx_release(cs[i]); }
+    if (rc == 0) { set_last_ms(span); }
+    return rc;
 }
 
 }  // namespace tcg
@@ -1194,6 +1262,17 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
 extern "C" int32_t tcg_encode(const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs, const size_t* caps,
                               tcg_enc_result* res)
 {
+    if (count >= 2u && tcg::host_memory(frames[0].plane[0].src)) {
+        std::vector<uint64_t> bytes(count, 0);
+        for (uint32_t f = 0; f < count; ++f) {
+            for (uint32_t p = 0; p < frames[f].planes; ++p) {
+                bytes[f] += (uint64_t)frames[f].plane[p].vis_w * frames[f].plane[p].vis_h * 2u;
+            }
+        }
+        uint32_t starts[tcg::PIPE_MAX_CHUNKS + 1];
+        const uint32_t k = tcg::pipeline_plan(false, bytes.data(), count, starts);
+        if (k > 1u) { return tcg::encode_pipelined(frames, starts, k, outs, caps, res); }
+    }
     tcg::Ctx* c = tcg::ctx_acquire();
     if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
     const int32_t rc = tcg::encode_impl(c, frames, count, outs, caps, res);

@@ -3,6 +3,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "tcg_runtime.h"
@@ -41,11 +42,28 @@ void call_begin(Ctx* c)
     c->kn = 0;
     // work a failed earlier call may have left on the context's other streams
     // comes before this call's work
-    cudaEventRecord(c->join, c->side);
-    cudaStreamWaitEvent(c->stream, c->join, 0);
-    cudaEventRecord(c->ajoin, c->aux);
-    cudaStreamWaitEvent(c->stream, c->ajoin, 0);
+    if (c->aux_open) {
+        cudaEventRecord(c->ajoin, c->aux);
+        cudaStreamWaitEvent(c->stream, c->ajoin, 0);
+    }
     cudaEventRecord(c->t0, c->stream);
+}
+
+cudaStream_t aux_stream(Ctx* c)
+{
+    // events first: the stream exists only with both of them
+    if ((c->afork == nullptr && cudaEventCreateWithFlags(&c->afork, cudaEventDisableTiming) != cudaSuccess) ||
+        (c->ajoin == nullptr && cudaEventCreateWithFlags(&c->ajoin, cudaEventDisableTiming) != cudaSuccess)) {
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "event creation failed");
+        return nullptr;
+    }
+    if (c->aux == nullptr && cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
+        c->aux = nullptr;
+        tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "stream creation failed");
+        return nullptr;
+    }
+    c->aux_open = true;
+    return c->aux;
 }
 
 void kern_begin(Ctx* c, int id)
@@ -76,6 +94,58 @@ void kern_end_on(Ctx* c, cudaStream_t s)
     c->kn++;
 }
 
+// A batch is pipelined when its host copies total at least 256 MB (about 5 ms
+// of PCIe time), with one chunk per 64 MB up to PIPE_MAX_CHUNKS.
+constexpr uint64_t PIPE_MIN_BYTES = 256ull << 20;
+constexpr uint64_t PIPE_CHUNK_BYTES = 64ull << 20;
+
+uint32_t pipeline_plan(bool decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts)
+{
+    const char* env = getenv("TCG_PIPELINE");
+    const int forced = env != nullptr && env[0] != '\0' ? atoi(env) : -1;
+    uint64_t total = 0;
+    for (uint32_t f = 0; f < count; ++f) { total += frame_bytes[f]; }
+    uint64_t k = 1;
+    if (forced >= 0) {
+        k = forced < 1 ? 1u : (uint64_t)forced;
+    } else if (total >= PIPE_MIN_BYTES) {
+        k = std::min<uint64_t>(total / PIPE_CHUNK_BYTES, decode ? PIPE_DECODE_CHUNKS : PIPE_ENCODE_CHUNKS);
+    }
+    k = std::min<uint64_t>(std::min<uint64_t>(k, PIPE_MAX_CHUNKS), count);
+    k = k < 1u ? 1u : k;
+    // chunk j-1 = [starts[j-1], starts[j]) takes frames until its share of the
+    // bytes is reached, keeping at least one frame for each later chunk
+    uint32_t f = 0;
+    uint64_t acc = 0;
+    starts[0] = 0;
+    for (uint32_t j = 1; j < (uint32_t)k; ++j) {
+        const uint64_t target = total / k * j;
+        do { acc += frame_bytes[f++]; } while (f < count - ((uint32_t)k - j) && acc < target);
+        starts[j] = f;
+    }
+    starts[k] = count;
+    return (uint32_t)k;
+}
+
+bool host_memory(const void* p)
+{
+    if (p == nullptr) { return false; }
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeUnregistered;
+}
+
+double event_span_ms(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    return cudaEventElapsedTime(&ms, a, b) == cudaSuccess ? (double)ms : 0.0;
+}
+
+void set_last_ms(double ms) { t_last_ms = ms; }
+
 void call_end(Ctx* c)
 {
     cudaEventRecord(c->t1, c->stream);
@@ -83,6 +153,8 @@ void call_end(Ctx* c)
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
     t_last_ms = ms;
+    // a completed call rejoined its other streams before its last work
+    c->aux_open = false;
     if (c->prof && c->kn > 0) {
         std::lock_guard<std::mutex> lk(g_mu);
         for (int i = 0; i < c->kn; ++i) {
@@ -228,13 +300,7 @@ Ctx* ctx_acquire()
     }
     Ctx* c = new Ctx();
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->afork, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->ajoin, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&c->gate, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
     for (int i = 0; ok && i < 2 * MAX_PROF; ++i) { ok = cudaEventCreate(&c->kev[i]) == cudaSuccess; }
     if (!ok) {
@@ -311,19 +377,19 @@ extern "C" void tcg_shutdown(void)
     tcg::Ctx* c = tcg::g_free;
     while (c != nullptr) {
         tcg::Ctx* n = c->next;
-        cudaStreamSynchronize(c->stream);
+        // all of the context's streams are idle before its buffers go
+        for (cudaStream_t s : {c->stream, c->aux}) {
+            if (s != nullptr) { cudaStreamSynchronize(s); }
+        }
         for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
-        cudaStreamSynchronize(c->side);
-        cudaStreamSynchronize(c->aux);
-        cudaEventDestroy(c->afork);
-        cudaEventDestroy(c->ajoin);
-        cudaStreamDestroy(c->aux);
-        cudaEventDestroy(c->ev);
-        cudaEventDestroy(c->fork);
-        cudaEventDestroy(c->join);
-        cudaStreamDestroy(c->side);
-        cudaStreamDestroy(c->stream);
+        for (cudaEvent_t e : {c->afork, c->ajoin, c->gate, c->t0, c->t1}) {
+            if (e != nullptr) { cudaEventDestroy(e); }
+        }
+        for (auto& e : c->kev) { if (e) { cudaEventDestroy(e); } }
+        for (cudaStream_t s : {c->stream, c->aux}) {
+            if (s != nullptr) { cudaStreamDestroy(s); }
+        }
         delete c;
         c = n;
     }
@@ -336,6 +402,11 @@ extern "C" uint64_t tcg_launch_count(void)
 }
 
 extern "C" double tcg_last_ms(void) { return tcg::t_last_ms; }
+
+extern "C" uint32_t tcg_pipeline_chunks(int32_t decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts)
+{
+    return tcg::pipeline_plan(decode != 0, frame_bytes, count, starts);
+}
 
 extern "C" void tcg_prof_enable(int32_t on) { tcg::g_prof_on.store(on != 0 ? 1 : 0); }
 

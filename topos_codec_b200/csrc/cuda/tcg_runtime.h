@@ -52,11 +52,14 @@ constexpr int MAX_PROF = 64;
 
 struct Ctx {
     cudaStream_t stream = nullptr;
-    cudaStream_t side = nullptr;                  // second stream for work split across two launches
-    cudaEvent_t fork = nullptr, join = nullptr;   // ordering between stream and side
-    cudaStream_t aux = nullptr;                   // third stream for independent work (alpha planes)
+    // The second stream is created on first use (aux_stream): the streams of a
+    // process share a small set of hardware work queues (8 unless
+    // CUDA_DEVICE_MAX_CONNECTIONS says otherwise), and two streams on one queue
+    // wait for each other's work, so a context holds no stream it does not use.
+    cudaStream_t aux = nullptr;                   // second stream for independent work (alpha planes)
     cudaEvent_t afork = nullptr, ajoin = nullptr; // ordering between stream and aux
-    cudaEvent_t ev = nullptr;
+    bool aux_open = false;                        // work queued there since the last completed call
+    cudaEvent_t gate = nullptr;                // recorded after a call's input copies (pipelined chunks)
     cudaEvent_t t0 = nullptr, t1 = nullptr;    // whole-call device time
     cudaEvent_t kev[2 * MAX_PROF] = {};        // per-kernel timing (profiling on)
     int kid[MAX_PROF] = {};
@@ -73,7 +76,7 @@ void call_begin(Ctx* c);
 void call_end(Ctx* c);  // after the stream was synchronised
 void kern_begin(Ctx* c, int id);
 void kern_end(Ctx* c);
-void kern_begin_on(Ctx* c, int id, cudaStream_t s);  // timing events on another of the context's streams
+void kern_begin_on(Ctx* c, int id, cudaStream_t s);  // timing events on the context's other stream
 void kern_end_on(Ctx* c, cudaStream_t s);
 
 // Launch on the context's stream. With TCG_SYNC_EACH=1 in the environment
@@ -105,6 +108,36 @@ void kern_end_on(Ctx* c, cudaStream_t s);
             if (le_ != cudaSuccess) { return tcg::cuda_fail(le_, #kern); } \
         }                                                                \
     } while (0)
+
+// Host-memory batches are coded as up to PIPE_MAX_CHUNKS chunks, each on its
+// own context: chunk i's input copies wait for chunk i-1's (an event), so the
+// copies of later chunks overlap the kernels of earlier ones and each chunk's
+// results go back while later chunks still compute. The frame ranges split the
+// batch's copy bytes evenly. pipeline_plan returns the chunk count (1 = code
+// the batch in one piece, at most PIPE_ENCODE_CHUNKS or PIPE_DECODE_CHUNKS)
+// and fills starts[0..k]. TCG_PIPELINE=<n> in the environment forces n chunks
+// (0 or 1: never pipeline; at most PIPE_MAX_CHUNKS).
+//
+// Decode stops at three chunks: the chunks' entropy chains run side by side,
+// and with four chunks of a 60-frame 3840x2160 batch their single-warp blocks
+// land unevenly on the SM sub-partitions, so every chain slows (per 60 frames:
+// 3 chunks 134-138 ms, 4 chunks 167-180 ms, one piece 161 ms). The encode
+// chain packs 32 slices per warp and keeps gaining up to four (114 ms; one
+// piece 150 ms).
+constexpr uint32_t PIPE_MAX_CHUNKS = 4;
+constexpr uint32_t PIPE_ENCODE_CHUNKS = 4;
+constexpr uint32_t PIPE_DECODE_CHUNKS = 3;
+uint32_t pipeline_plan(bool decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts);
+bool host_memory(const void* p);  // pinned or pageable host memory (not device or managed)
+void set_last_ms(double ms);      // device time reported by tcg_last_ms for this thread's last call
+// Device time between two completed events of this device (0 on error).
+double event_span_ms(cudaEvent_t a, cudaEvent_t b);
+
+// The context's second stream, created on first use, with the call's
+// pending-work flag set (call_begin of the next call orders that work before
+// its own when this call fails before rejoining it). nullptr (error set) when
+// the stream cannot be created.
+cudaStream_t aux_stream(Ctx* c);
 
 // Lease a context (creates one when none is free). Thread-safe.
 Ctx* ctx_acquire();

@@ -642,6 +642,10 @@ TC_EXPORT int32_t tcg_device_init(int32_t device) { return tcg_init(device); }
 TC_EXPORT void tcg_device_release(void) { tcg_shutdown(); }
 TC_EXPORT uint64_t tcg_kernel_launches(void) { return tcg_launch_count(); }
 TC_EXPORT double tcg_last_device_ms(void) { return tcg_last_ms(); }
+TC_EXPORT uint32_t tcg_pipeline_plan(int32_t decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts)
+{
+    return tcg_pipeline_chunks(decode, frame_bytes, count, starts);
+}
 TC_EXPORT void tcg_profile_enable(int32_t on) { tcg_prof_enable(on); }
 TC_EXPORT void tcg_profile_reset(void) { tcg_prof_reset(); }
 TC_EXPORT int32_t tcg_profile_read(uint32_t id, const char** name, double* ms, uint64_t* launches)

@@ -97,6 +97,8 @@ void tcg_shutdown(void);
 uint64_t tcg_launch_count(void);
 /* device time (ms, CUDA events on the library stream) of this thread's last call */
 double tcg_last_ms(void);
+/* split of a host-memory batch into pipelined chunks (see tcg_pipeline_plan) */
+uint32_t tcg_pipeline_chunks(int32_t decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts);
 /* optional per-kernel event timing (process totals) */
 void tcg_prof_enable(int32_t on);
 void tcg_prof_reset(void);
