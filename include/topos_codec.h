@@ -317,8 +317,7 @@ int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, to
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, one
  * warp per slice (1), or a split (5: the largest slices, half of the blocks,
- * one per warp and the rest four per warp in a second launch that starts
- * beside the first as its programmatic dependent on the same stream); -1 = not
+ * one per warp and the rest four per warp on a second stream); -1 = not
  * chosen yet. The first batch of each size class (log2 of the slice count)
  * times the split and 4, 2 and 1 slices per warp and keeps the fastest;
  * the environment variable TCG_DCHAIN=lane|lane4|lane2|lane1|warp|split overrides

@@ -333,9 +333,6 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
                                                int32_t* __restrict__ status)
 {
     extern __shared__ __align__(16) uint8_t dsm[];
-    // A chain launch that follows this one on the stream as a programmatic
-    // dependent (the split tiling) may start at once: it decodes other slices.
-    cudaTriggerProgrammaticLaunchCompletion();
     uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm);
     const uint32_t t = threadIdx.x;
     // row 1 indexed by the next position (1..64), row 2 by the previous level's
@@ -371,14 +368,7 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     // the lanes with a slice to decode; they stay together until all are done
     const bool live = t < LANES && i0 + t < nc && status[order[i0 + t]] == 0;
     const uint32_t wmask = __ballot_sync(0xFFFFFFFFu, live);
-    if (!live) {
-        // A programmatic dependent completes only after the launch before it
-        // (cudaGridDependencySynchronize; no effect in an ordinary launch), so
-        // the kernels after it see both: the live lanes wait at their end, lane 0
-        // here when the warp has none.
-        if (wmask == 0u && t == 0u) { cudaGridDependencySynchronize(); }
-        return;
-    }
+    if (!live) { return; }
     const uint32_t si = order[i0 + t];
     const DSlice& S = slices[si];
     const DPlane& P = planes[S.plane];
@@ -534,7 +524,6 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
 #undef DCH_FINISH
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
-    cudaGridDependencySynchronize();
 }
 
 // ------------------------------------------------------------------ chain, warp tiling
@@ -1184,9 +1173,10 @@ struct DecPending {
 
 // Enqueue one batch on the context's streams: descriptors, packet copies and
 // kernels. The packet copies start after `after` (when given) and C->gate is
-// recorded behind them.
+// recorded behind them. load_nc: colour slices of the whole pipelined batch
+// this one is a chunk of (0: the batch is decoded alone).
 static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count, cudaEvent_t after,
-                             DecPending& pend)
+                             uint32_t load_nc, DecPending& pend)
 {
     std::vector<uint32_t>& frame_slice0 = pend.frame_slice0;
     std::vector<DPlane>& planes = pend.planes;
@@ -1320,7 +1310,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     if (na > 0) {
         // Alpha slices (Rice run/level decode, then MED reconstruction) share no
         // slice, status entry or output plane with the colour slices, so they
-        // run on a second stream beside the colour chain; the stream rejoins
+        // run on a third stream beside the colour chain; the stream rejoins
         // before concealment.
         cudaStream_t as = aux_stream(C);
         if (as == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
@@ -1359,31 +1349,22 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
         auto run = [&](int tiling) -> int32_t {
             switch (tiling) {
             case DCH_TILE_SPLIT: {
-                // Both launches on the one stream: the second is a programmatic
-                // dependent of the first, so it starts as soon as every block of
-                // the first has (at its start), and it completes only after the
-                // first has, so the reconstruction after it sees all slices.
+                cudaStream_t sd = side_stream(C);
+                if (sd == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
                 tcg::kern_begin(C, K_DCHAIN);
+                TCG_CHECK(cudaEventRecord(C->fork, st));
+                TCG_CHECK(cudaStreamWaitEvent(sd, C->fork, 0));
                 k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
                                                                d_status);
-                TCG_CHECK(cudaGetLastError());
                 if (nc > nsplit) {
-                    cudaLaunchAttribute at[1];
-                    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-                    at[0].val.programmaticStreamSerializationAllowed = 1;
-                    cudaLaunchConfig_t lc = {};
-                    lc.gridDim = dim3((nc - nsplit + 3u) / 4u);
-                    lc.blockDim = dim3(32);
-                    lc.dynamicSmemBytes = dch_smem(4);
-                    lc.stream = st;
-                    lc.attrs = at;
-                    lc.numAttrs = 1;
-                    TCG_CHECK(cudaLaunchKernelEx(&lc, k_dchain<4>, (const DSlice*)d_sl, (const uint32_t*)(d_ord + nsplit),
-                                                 (uint32_t)(nc - nsplit), (const uint32_t*)d_st, (const DPlane*)d_pl,
-                                                 (const uint8_t*)d_pkt, (const uint8_t*)d_tab, d_coef, d_status));
+                    k_dchain<4><<<(nc - nsplit + 3u) / 4u, 32, dch_smem(4), sd>>>(
+                        d_sl, d_ord + nsplit, nc - nsplit, d_st, d_pl, d_pkt, d_tab, d_coef, d_status);
                 }
                 tcg::note_launch(nc > nsplit ? 2u : 1u);
+                TCG_CHECK(cudaGetLastError());
+                TCG_CHECK(cudaEventRecord(C->join, sd));
+                TCG_CHECK(cudaStreamWaitEvent(st, C->join, 0));
                 tcg::kern_end(C);
                 if (tcg::sync_each()) { TCG_CHECK(cudaStreamSynchronize(st)); }
                 return TCG_OK;
@@ -1414,12 +1395,16 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 return TCG_OK;
             }
         };
+        // A chunk of a pipelined batch decodes beside the other chunks: it takes
+        // the tiling chosen for the whole batch's slice count (the split when
+        // none is chosen yet) and is never timed alone.
         int tiling = dchain_forced();
-        const uint32_t cls = size_class(nc);
+        const uint32_t cls = size_class(load_nc != 0u ? load_nc : nc);
         if (tiling < 0) {
             std::lock_guard<std::mutex> g(g_tune_mu);
             tiling = g_tune[cls];
         }
+        if (tiling < 0 && load_nc != 0u) { tiling = DCH_TILE_SPLIT; }
         if (tiling >= 0) {
             const int32_t rc = run(tiling);
             if (rc != TCG_OK) { return rc; }
@@ -1429,13 +1414,18 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
             constexpr int cand[4] = {DCH_TILE_SPLIT, DCH_TILE_LANE4, DCH_TILE_LANE2, DCH_TILE_LANE1};
             cudaEvent_t e[5];
             for (auto& x : e) { TCG_CHECK(cudaEventCreate(&x)); }
-            TCG_CHECK(cudaEventRecord(e[0], st));
-            for (int k = 0; k < 4; ++k) {
-                const int32_t rc = run(cand[k]);
-                if (rc != TCG_OK) { return rc; }
-                TCG_CHECK(cudaEventRecord(e[k + 1], st));
+            int32_t rc = cudaEventRecord(e[0], st) == cudaSuccess ? TCG_OK : cuda_fail(cudaGetLastError(), "tuner");
+            for (int k = 0; k < 4 && rc == TCG_OK; ++k) {
+                rc = run(cand[k]);
+                if (rc == TCG_OK && cudaEventRecord(e[k + 1], st) != cudaSuccess) {
+                    rc = cuda_fail(cudaGetLastError(), "tuner");
+                }
             }
-            TCG_CHECK(cudaEventSynchronize(e[4]));
+            if (rc == TCG_OK && cudaEventSynchronize(e[4]) != cudaSuccess) { rc = cuda_fail(cudaGetLastError(), "tuner"); }
+            if (rc != TCG_OK) {
+                for (auto& x : e) { cudaEventDestroy(x); }
+                return rc;
+            }
             int best = cand[0];
             float best_ms = 0.f;
             for (int k = 0; k < 4; ++k) {
@@ -1521,7 +1511,7 @@ static int32_t decode_finish(Ctx* C, const tcg_dec_frame* frames, const DecPendi
 static int32_t decode_impl(Ctx* C, const tcg_dec_frame* frames, uint32_t count)
 {
     DecPending pend;
-    int32_t rc = decode_launch(C, frames, count, nullptr, pend);
+    int32_t rc = decode_launch(C, frames, count, nullptr, 0u, pend);
     if (rc == 0) { rc = decode_outputs(C, frames, pend); }
     return rc != 0 ? rc : decode_finish(C, frames, pend);
 }
@@ -1539,6 +1529,13 @@ static int32_t decode_pipelined(const tcg_dec_frame* frames, const uint32_t* sta
     DecPending fs0[PIPE_MAX_CHUNKS];
     int32_t rc = 0;
     uint32_t launched = 0;
+    uint32_t load_nc = 0;  // colour slices of the whole batch
+    for (uint32_t f = 0; f < starts[k]; ++f) {
+        if (frames[f].skip) { continue; }
+        for (uint32_t i = 0; i < frames[f].slices; ++i) {
+            load_nc += (frames[f].slice[i].plane == 3u && frames[f].alpha_mode != 0u) ? 0u : 1u;
+        }
+    }
     for (uint32_t i = 0; i < k && rc == 0; ++i) {
         cs[i] = ctx_acquire();
         if (cs[i] == nullptr) {
@@ -1546,7 +1543,8 @@ static int32_t decode_pipelined(const tcg_dec_frame* frames, const uint32_t* sta
             break;
         }
         launched = i + 1u;
-        rc = decode_launch(cs[i], frames + starts[i], starts[i + 1] - starts[i], i ? cs[i - 1]->gate : nullptr, fs0[i]);
+        rc = decode_launch(cs[i], frames + starts[i], starts[i + 1] - starts[i], i ? cs[i - 1]->gate : nullptr,
+                           std::max(load_nc, 1u), fs0[i]);
     }
     for (uint32_t i = 0; i < launched && rc == 0; ++i) { rc = decode_outputs(cs[i], frames + starts[i], fs0[i]); }
     double span = 0.0;

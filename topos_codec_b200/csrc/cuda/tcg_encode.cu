@@ -1113,7 +1113,7 @@ static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count
 
     if (!aslices.empty()) {
         // Alpha slices (MED residuals, Rice pairs) read only the samples and write
-        // only their own staging windows and results, so they run on a second
+        // only their own staging windows and results, so they run on a third
         // stream beside the colour path; the stream rejoins before packing.
         cudaStream_t as = aux_stream(C);
         if (as == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }

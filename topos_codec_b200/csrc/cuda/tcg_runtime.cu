@@ -42,6 +42,10 @@ void call_begin(Ctx* c)
     c->kn = 0;
     // work a failed earlier call may have left on the context's other streams
     // comes before this call's work
+    if (c->side_open) {
+        cudaEventRecord(c->join, c->side);
+        cudaStreamWaitEvent(c->stream, c->join, 0);
+    }
     if (c->aux_open) {
         cudaEventRecord(c->ajoin, c->aux);
         cudaStreamWaitEvent(c->stream, c->ajoin, 0);
@@ -49,22 +53,25 @@ void call_begin(Ctx* c)
     cudaEventRecord(c->t0, c->stream);
 }
 
-cudaStream_t aux_stream(Ctx* c)
+static cudaStream_t open_stream(cudaStream_t* s, cudaEvent_t* fork, cudaEvent_t* join, bool* open)
 {
     // events first: the stream exists only with both of them
-    if ((c->afork == nullptr && cudaEventCreateWithFlags(&c->afork, cudaEventDisableTiming) != cudaSuccess) ||
-        (c->ajoin == nullptr && cudaEventCreateWithFlags(&c->ajoin, cudaEventDisableTiming) != cudaSuccess)) {
+    if ((*fork == nullptr && cudaEventCreateWithFlags(fork, cudaEventDisableTiming) != cudaSuccess) ||
+        (*join == nullptr && cudaEventCreateWithFlags(join, cudaEventDisableTiming) != cudaSuccess)) {
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "event creation failed");
         return nullptr;
     }
-    if (c->aux == nullptr && cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess) {
-        c->aux = nullptr;
+    if (*s == nullptr && cudaStreamCreateWithFlags(s, cudaStreamNonBlocking) != cudaSuccess) {
+        *s = nullptr;
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "stream creation failed");
         return nullptr;
     }
-    c->aux_open = true;
-    return c->aux;
+    *open = true;
+    return *s;
 }
+
+cudaStream_t side_stream(Ctx* c) { return open_stream(&c->side, &c->fork, &c->join, &c->side_open); }
+cudaStream_t aux_stream(Ctx* c) { return open_stream(&c->aux, &c->afork, &c->ajoin, &c->aux_open); }
 
 void kern_begin(Ctx* c, int id)
 {
@@ -154,6 +161,7 @@ void call_end(Ctx* c)
     cudaEventElapsedTime(&ms, c->t0, c->t1);
     t_last_ms = ms;
     // a completed call rejoined its other streams before its last work
+    c->side_open = false;
     c->aux_open = false;
     if (c->prof && c->kn > 0) {
         std::lock_guard<std::mutex> lk(g_mu);
@@ -378,16 +386,16 @@ extern "C" void tcg_shutdown(void)
     while (c != nullptr) {
         tcg::Ctx* n = c->next;
         // all of the context's streams are idle before its buffers go
-        for (cudaStream_t s : {c->stream, c->aux}) {
+        for (cudaStream_t s : {c->stream, c->side, c->aux}) {
             if (s != nullptr) { cudaStreamSynchronize(s); }
         }
         for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
-        for (cudaEvent_t e : {c->afork, c->ajoin, c->gate, c->t0, c->t1}) {
+        for (cudaEvent_t e : {c->fork, c->join, c->afork, c->ajoin, c->gate, c->t0, c->t1}) {
             if (e != nullptr) { cudaEventDestroy(e); }
         }
         for (auto& e : c->kev) { if (e) { cudaEventDestroy(e); } }
-        for (cudaStream_t s : {c->stream, c->aux}) {
+        for (cudaStream_t s : {c->stream, c->side, c->aux}) {
             if (s != nullptr) { cudaStreamDestroy(s); }
         }
         delete c;

@@ -52,13 +52,16 @@ constexpr int MAX_PROF = 64;
 
 struct Ctx {
     cudaStream_t stream = nullptr;
-    // The second stream is created on first use (aux_stream): the streams of a
-    // process share a small set of hardware work queues (8 unless
-    // CUDA_DEVICE_MAX_CONNECTIONS says otherwise), and two streams on one queue
-    // wait for each other's work, so a context holds no stream it does not use.
-    cudaStream_t aux = nullptr;                   // second stream for independent work (alpha planes)
+    // The second and third streams are created on first use (side_stream,
+    // aux_stream): the streams of a process share a small set of hardware work
+    // queues (8 unless CUDA_DEVICE_MAX_CONNECTIONS says otherwise), and two
+    // streams on one queue can wait for each other's work, so a context holds
+    // no stream it does not use and orders nothing on one it did not use.
+    cudaStream_t side = nullptr;                  // second stream for work split across two launches
+    cudaEvent_t fork = nullptr, join = nullptr;   // ordering between stream and side
+    cudaStream_t aux = nullptr;                   // third stream for independent work (alpha planes)
     cudaEvent_t afork = nullptr, ajoin = nullptr; // ordering between stream and aux
-    bool aux_open = false;                        // work queued there since the last completed call
+    bool side_open = false, aux_open = false;     // work queued there since the last completed call
     cudaEvent_t gate = nullptr;                // recorded after a call's input copies (pipelined chunks)
     cudaEvent_t t0 = nullptr, t1 = nullptr;    // whole-call device time
     cudaEvent_t kev[2 * MAX_PROF] = {};        // per-kernel timing (profiling on)
@@ -76,7 +79,7 @@ void call_begin(Ctx* c);
 void call_end(Ctx* c);  // after the stream was synchronised
 void kern_begin(Ctx* c, int id);
 void kern_end(Ctx* c);
-void kern_begin_on(Ctx* c, int id, cudaStream_t s);  // timing events on the context's other stream
+void kern_begin_on(Ctx* c, int id, cudaStream_t s);  // timing events on another of the context's streams
 void kern_end_on(Ctx* c, cudaStream_t s);
 
 // Launch on the context's stream. With TCG_SYNC_EACH=1 in the environment
@@ -133,10 +136,11 @@ void set_last_ms(double ms);      // device time reported by tcg_last_ms for thi
 // Device time between two completed events of this device (0 on error).
 double event_span_ms(cudaEvent_t a, cudaEvent_t b);
 
-// The context's second stream, created on first use, with the call's
+// The context's second / third stream, created on first use, with the call's
 // pending-work flag set (call_begin of the next call orders that work before
 // its own when this call fails before rejoining it). nullptr (error set) when
 // the stream cannot be created.
+cudaStream_t side_stream(Ctx* c);
 cudaStream_t aux_stream(Ctx* c);
 
 // Lease a context (creates one when none is free). Thread-safe.
