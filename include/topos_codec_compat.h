@@ -50,10 +50,35 @@ void tc_dev_symbol_hist_reset(void);
 void tc_dev_symbol_hist_get(uint64_t* dc, uint64_t* run, uint64_t* lvl);
 void tc_dev_symbol_pair_hist_get(uint32_t plane, uint64_t* pair_hist);
 
-/* reference: native/include/topos_codec.h:325 (rate-controlled encode) */
+/* reference: native/include/topos_codec.h:316-328, native/src/codec/codec.c:7789
+ * (size-targeted encode). Implemented: the reference's deterministic qp
+ * searches (strict by default: the smallest qp in [qp_min, qp_max] whose
+ * packet fits target_bytes; the legacy linear and "r6" searches by
+ * TOPOS_SIZED_SEARCH or tc_dev_set_sized_mode) over exact packet sizes that
+ * the GPU encodes a window of qps at a time; the packet, stats, qp_used and
+ * every status equal the reference's for the same call sequence. qp_min >
+ * qp_max or either above 95 is TC_ERR_INVALID_ARGUMENT; a target no qp meets
+ * returns the qp_max packet (best effort); out is written only on TC_OK and
+ * a final packet larger than out_cap is TC_ERR_BUFFER_TOO_SMALL with its size
+ * in stats. */
 int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const topos_frame_input* input, uint32_t target_bytes,
                               uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used, uint8_t* out, size_t out_cap,
                               topos_frame_stats* stats);
+
+/* reference: native/src/codec/codec.c:7110-7178 (developer switches of the
+ * size-targeted encode). Implemented: the search mode (0 strict, 1 linear,
+ * 2 r6; other values select strict; overrides TOPOS_SIZED_SEARCH), the legacy
+ * two-valued form, turning off the cross-call qp hint or its two-point model,
+ * turning off the exact-count probe (the strict search then falls back to the
+ * linear one), and the counters of calls and probe encodes. */
+void tc_dev_set_sized_mode(int32_t mode);
+void tc_dev_set_sized_search(int legacy);
+void tc_dev_set_qp_hint(int disable);
+void tc_dev_set_qp_hint_model(int disable);
+void tc_dev_set_sized_m7(int disable);
+void tc_dev_sized_reset(void);
+uint64_t tc_dev_sized_iters(void);
+uint64_t tc_dev_sized_calls(void);
 /* reference: native/include/topos_codec.h:364 (scaled decode) */
 int32_t tc_decode_scale_dimensions(uint32_t source_width, uint32_t source_height, int32_t scale,
                                    uint32_t* target_width, uint32_t* target_height);

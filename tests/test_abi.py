@@ -173,7 +173,9 @@ def test_reference_python_binding_loads_this_library(built):
         assert codec.packet_bound(theirs) == ours.packet_bound(mine)
     lib = codec._lib
     lib.tc_frame_encode_sized.restype = ctypes.c_int32
-    assert lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == B.TC_ERR_NOT_IMPLEMENTED
+    assert lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == B.TC_ERR_INVALID_ARGUMENT
+    lib.tc_decode_scale_dimensions.restype = ctypes.c_int32
+    assert lib.tc_decode_scale_dimensions(64, 64, 1, None, None) == B.TC_ERR_NOT_IMPLEMENTED
     lib.tc_scalable_status_name.restype = ctypes.c_char_p
     assert lib.tc_scalable_status_name(1) == b"reference" and lib.tc_scalable_status_name(9) == b"unknown"
 
@@ -222,3 +224,33 @@ def test_pipeline_plan_splits_host_batches(product, monkeypatch):
     assert _plan(L, [1] * 8, decode=1) == (4, [0, 2, 4, 6, 8])
     monkeypatch.setenv("TCG_PIPELINE", "0")
     assert _plan(L, [33 * MB] * 60) == (1, [0, 60])
+
+
+def test_sized_encode_argument_checks_match_reference(product, reference):
+    """tc_frame_encode_sized's checks before any encode, status for status with
+    the reference library: NULL config, qp ranges (reversed, above 95),
+    pixel format 3 and the temporal generations."""
+    planes = [np.zeros((16, 16), np.uint16) for _ in range(3)]
+    ins = [x._input(planes) for x in (product, reference)]
+    cases = []
+    base = B.make_config(16, 16, qp=8, qmatrix_id=4, features=1)
+    for lo, hi in [(30, 20), (0, 96), (96, 96)]:
+        cases.append((base, lo, hi))
+    for gen in (9, 10, 11):
+        c = B.make_config(16, 16, qp=8)
+        c.reserved[0] = gen
+        cases.append((c, 0, 63))
+    for lib_pair in [(product._lib, ins[0]), (reference._lib, ins[1])]:
+        lib_pair[0].tc_frame_encode_sized.restype = ctypes.c_int32
+    for cfg, lo, hi in cases:
+        got = []
+        for lib, fi in [(product._lib, ins[0]), (reference._lib, ins[1])]:
+            out = (ctypes.c_uint8 * 4096)()
+            qp_used = ctypes.c_uint8(77)
+            rc = int(lib.tc_frame_encode_sized(ctypes.byref(cfg), ctypes.byref(fi), ctypes.c_uint32(1000),
+                                               ctypes.c_uint8(lo), ctypes.c_uint8(hi), ctypes.byref(qp_used), out,
+                                               ctypes.c_size_t(4096), None))
+            got.append(rc)
+        assert got[0] == got[1] and got[0] < 0, (cfg.reserved[0], lo, hi, got)
+    assert product._lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == \
+        reference._lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None)

@@ -1259,6 +1259,108 @@ static int32_t encode_pipelined(const tcg_enc_frame* frames, const uint32_t* sta
 
 }  // namespace tcg
 
+// ------------------------------------------------------------ sized sessions
+
+struct tcg_sized {
+    tcg::Ctx* C = nullptr;
+    void* planes = nullptr;                       // device copy of host-memory sample planes
+    const void* src[4] = {};                      // plane sources the variants read
+    size_t stride[4] = {};
+    std::vector<void*> regions;                   // one device packet region per encode call
+    std::vector<std::pair<uint8_t*, size_t>> slot; // kept packets: address, capacity
+};
+
+extern "C" int32_t tcg_sized_open(const tcg_enc_frame* base, tcg_sized** out)
+{
+    *out = nullptr;
+    tcg::Ctx* C = tcg::ctx_acquire();
+    if (C == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
+    tcg_sized* s = new tcg_sized();
+    s->C = C;
+    size_t host_bytes = 0;
+    for (uint32_t p = 0; p < base->planes; ++p) {
+        const tcg_enc_plane& I = base->plane[p];
+        s->src[p] = I.src;
+        s->stride[p] = I.stride;
+        if (tcg::host_memory(I.src)) { host_bytes += tcg::align_up((size_t)I.vis_w * I.vis_h * 2u, 256); }
+    }
+    if (host_bytes > 0) {
+        // every probe reads the samples from HBM: one upload, tight rows
+        if (cudaMallocAsync(&s->planes, host_bytes, C->stream) != cudaSuccess) {
+            tcg_sized_close(s);
+            return tcg::cuda_fail(cudaErrorMemoryAllocation, "sized planes");
+        }
+        size_t off = 0;
+        for (uint32_t p = 0; p < base->planes; ++p) {
+            const tcg_enc_plane& I = base->plane[p];
+            if (!tcg::host_memory(I.src)) { continue; }
+            uint8_t* dst = (uint8_t*)s->planes + off;
+            const cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)I.vis_w * 2u, I.src, I.stride * 2u,
+                                                    (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, C->stream);
+            if (e != cudaSuccess) {
+                tcg_sized_close(s);
+                return tcg::cuda_fail(e, "sized upload");
+            }
+            s->src[p] = dst;
+            s->stride[p] = I.vis_w;
+            off += tcg::align_up((size_t)I.vis_w * I.vis_h * 2u, 256);
+        }
+    }
+    *out = s;
+    return 0;
+}
+
+extern "C" int32_t tcg_sized_encode(tcg_sized* s, const tcg_enc_frame* frames, uint32_t count, const size_t* caps,
+                                    tcg_enc_result* res, uint32_t* slots)
+{
+    if (count == 0u) { return 0; }
+    std::vector<tcg_enc_frame> fr(frames, frames + count);
+    std::vector<uint8_t*> outs(count);
+    size_t total = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        for (uint32_t p = 0; p < fr[i].planes; ++p) {
+            fr[i].plane[p].src = (const uint16_t*)s->src[p];
+            fr[i].plane[p].stride = s->stride[p];
+        }
+        total += tcg::align_up(caps[i], 256);
+    }
+    void* region = nullptr;
+    if (cudaMallocAsync(&region, total, s->C->stream) != cudaSuccess) {
+        return tcg::cuda_fail(cudaErrorMemoryAllocation, "sized packets");
+    }
+    s->regions.push_back(region);
+    size_t off = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        outs[i] = (uint8_t*)region + off;
+        slots[i] = (uint32_t)s->slot.size();
+        s->slot.emplace_back(outs[i], caps[i]);
+        off += tcg::align_up(caps[i], 256);
+    }
+    return tcg::encode_impl(s->C, fr.data(), count, outs.data(), caps, res);
+}
+
+extern "C" int32_t tcg_sized_fetch(tcg_sized* s, uint32_t slot, uint8_t* out, size_t size)
+{
+    if (slot >= s->slot.size() || size > s->slot[slot].second) {
+        tcg_host_set_error(TCG_ERR_INVALID_ARGUMENT, "sized fetch: no such packet");
+        return TCG_ERR_INVALID_ARGUMENT;
+    }
+    if (size == 0u) { return 0; }
+    TCG_CHECK(cudaMemcpyAsync(out, s->slot[slot].first, size, cudaMemcpyDefault, s->C->stream));
+    TCG_CHECK(cudaStreamSynchronize(s->C->stream));
+    return 0;
+}
+
+extern "C" void tcg_sized_close(tcg_sized* s)
+{
+    if (s == nullptr) { return; }
+    for (void* r : s->regions) { cudaFreeAsync(r, s->C->stream); }
+    if (s->planes != nullptr) { cudaFreeAsync(s->planes, s->C->stream); }
+    cudaStreamSynchronize(s->C->stream);
+    tcg::ctx_release(s->C);
+    delete s;
+}
+
 extern "C" int32_t tcg_encode(const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs, const size_t* caps,
                               tcg_enc_result* res)
 {

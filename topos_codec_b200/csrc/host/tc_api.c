@@ -194,8 +194,8 @@ TC_EXPORT int32_t tc_frame_plane_geometry(const topos_frame_output* info, uint32
 
 /* Validation and job building for one frame (reference codec.c:5730-5806 for
  * setup, :5413-5460 for per-plane qp/quantiser derivation). */
-static int32_t prepare_encode(const topos_frame_config* cfg, const topos_frame_input* in, tcg_enc_frame* jf,
-                              uint32_t* slice_count, uint8_t* qp_base)
+int32_t tc_prepare_encode(const topos_frame_config* cfg, const topos_frame_input* in, tcg_enc_frame* jf,
+                          uint32_t* slice_count, uint8_t* qp_base)
 {
     int32_t rc = tc_frame_config_validate(cfg);
     if (rc != TC_OK) { return rc; }
@@ -267,7 +267,7 @@ static int32_t prepare_encode(const topos_frame_config* cfg, const topos_frame_i
     return TC_OK;
 }
 
-static void fill_stats(topos_frame_stats* st, const tcg_enc_result* r, uint32_t slices, uint8_t qp)
+void tc_fill_enc_stats(topos_frame_stats* st, const tcg_enc_result* r, uint32_t slices, uint8_t qp)
 {
     st->packet_size = r->packet_size;
     st->color_payload_bytes = r->color_payload;
@@ -279,7 +279,7 @@ static void fill_stats(topos_frame_stats* st, const tcg_enc_result* r, uint32_t 
     st->alpha_max_abs_error = (uint16_t)r->alpha_max_err;
 }
 
-static int32_t result_status(int32_t rc, size_t need, size_t cap)
+int32_t tc_enc_result_status(int32_t rc, size_t need, size_t cap)
 {
     switch (rc) {
     case TC_OK: return TC_OK;
@@ -304,15 +304,15 @@ TC_EXPORT int32_t tc_frame_encode(const topos_frame_config* cfg, const topos_fra
     tcg_enc_frame jf;
     uint32_t slices = 0;
     uint8_t qp = 0;
-    int32_t rc = prepare_encode(cfg, input, &jf, &slices, &qp);
+    int32_t rc = tc_prepare_encode(cfg, input, &jf, &slices, &qp);
     if (rc != TC_OK) { return rc; }
     tcg_enc_result r;
     uint8_t* const outs[1] = {out};
     const size_t caps[1] = {out == NULL ? 0u : out_cap};
     rc = tcg_encode(&jf, 1u, outs, caps, &r);
     if (rc != TC_OK) { return rc; }
-    if (r.rc == TC_OK || r.rc == TC_ERR_BUFFER_TOO_SMALL) { fill_stats(stats, &r, slices, qp); }
-    return result_status(r.rc, r.packet_size, out_cap);
+    if (r.rc == TC_OK || r.rc == TC_ERR_BUFFER_TOO_SMALL) { tc_fill_enc_stats(stats, &r, slices, qp); }
+    return tc_enc_result_status(r.rc, r.packet_size, out_cap);
 }
 
 /* extension: many frames in one device launch sequence */
@@ -343,7 +343,7 @@ TC_EXPORT int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs, const t
             stats[i].struct_size = (uint32_t)sizeof(topos_frame_stats);
             stats[i].abi_version = TOPOS_CODEC_ABI_VERSION;
         }
-        rcs[i] = prepare_encode(&cfgs[i], &inputs[i], &jobs[n], &nsl[i], &qps[i]);
+        rcs[i] = tc_prepare_encode(&cfgs[i], &inputs[i], &jobs[n], &nsl[i], &qps[i]);
         if (rcs[i] == TC_OK) {
             idx[n] = i;
             o2[n] = outs[i];
@@ -357,9 +357,9 @@ TC_EXPORT int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs, const t
     for (uint32_t k = 0; k < n && call == TC_OK; ++k) {
         const uint32_t i = idx[k];
         if (stats != NULL && (res[k].rc == TC_OK || res[k].rc == TC_ERR_BUFFER_TOO_SMALL)) {
-            fill_stats(&stats[i], &res[k], nsl[i], qps[i]);
+            tc_fill_enc_stats(&stats[i], &res[k], nsl[i], qps[i]);
         }
-        rcs[i] = result_status(res[k].rc, res[k].packet_size, c2[k]);
+        rcs[i] = tc_enc_result_status(res[k].rc, res[k].packet_size, c2[k]);
     }
     for (uint32_t i = 0; i < count; ++i) {
         if (call != TC_OK && rcs[i] == TC_OK) { rcs[i] = call; }

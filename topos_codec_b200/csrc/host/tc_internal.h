@@ -89,4 +89,13 @@ int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v);
 int32_t tc_parse_compact(const uint8_t* rec, size_t n, tc_view* v);
 void tc_fill_info(const tc_hdr* h, topos_frame_output* o);
 
+/* encode job of one frame (validation as tc_frame_encode), its stats and the
+ * public status of a per-frame result (tc_api.c) */
+struct tcg_enc_frame;
+struct tcg_enc_result;
+int32_t tc_prepare_encode(const topos_frame_config* cfg, const topos_frame_input* in, struct tcg_enc_frame* jf,
+                          uint32_t* slice_count, uint8_t* qp_base);
+void tc_fill_enc_stats(topos_frame_stats* st, const struct tcg_enc_result* r, uint32_t slices, uint8_t qp);
+int32_t tc_enc_result_status(int32_t rc, size_t need, size_t cap);
+
 #endif /* TC_INTERNAL_H */

@@ -1,0 +1,709 @@
+/* tc_sized.c - size-targeted encode (tc_frame_encode_sized).
+ *
+ * The reference searches qp one probe at a time: each probe is an exact
+ * packet-size count at one qp, and the next qp depends on the sizes seen so
+ * far (reference: native/src/codec/codec.c:7789-7880 entry, :7199-7262 legacy
+ * linear search, :7271-7402 probe bookkeeping, :7404-7552 "r6" fast search,
+ * :7554-7787 strict search). Its answer and every error it returns depend
+ * only on those sizes, so this file runs the same three searches, step for
+ * step, over a table of exact packet sizes that the GPU fills a window of qps
+ * at a time: a probe of a qp the table lacks encodes it together with the
+ * nearest unprobed qps (one batched launch sequence, the samples uploaded
+ * once per call), and every probe's packet stays on the device so the chosen
+ * one is copied out without a final encode.
+ *
+ * Process state as in the reference: the search mode (TOPOS_SIZED_SEARCH =
+ * strict | linear | r6, or tc_dev_set_sized_mode), and the strict search's
+ * cross-call qp hint (the last two distinct chosen qps with their sizes),
+ * held by one process-wide record that a call borrows when it is free and
+ * replaces by an empty one when another call holds it (reference:
+ * codec.c:1002-1046, enc_loan_acquire). The hint only moves the first probe;
+ * with sizes that fall as qp rises the chosen qp does not depend on it.
+ */
+#include <math.h>
+#include <stdatomic.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../../../include/topos_codec_compat.h"
+#include "../tcg_device.h"
+#include "tc_internal.h"
+
+#define SIZED_MAX_PTS 24
+#define SIZED_PROBE_BUDGET 24u
+/* the reference's exact-count probe needs a cache of every colour
+ * coefficient; past 512 MiB of it (codec.c:6034) the strict search falls back
+ * to the linear one */
+#define SIZED_FCACHE_MAX_BYTES (512ull * 1024ull * 1024ull)
+/* probe window: qps encoded per launch, and the device bytes one window may take */
+#define SIZED_WINDOW 17u
+#define SIZED_WINDOW_BYTES (24ull << 30)
+
+/* ------------------------------------------------------------ process state */
+
+typedef struct sized_hint {
+    int valid;
+    uint32_t q, bytes;         /* last chosen qp and its size */
+    uint32_t prev, prev_bytes; /* the distinct one before it (bytes 0 = none) */
+} sized_hint;
+
+static sized_hint g_hint;
+static atomic_int g_hint_busy;
+static atomic_int g_mode;          /* 0 strict, 1 linear, 2 r6 */
+static atomic_int g_mode_env_read;
+static atomic_int g_hint_disable;
+static atomic_int g_hint_model_disable;
+static atomic_int g_m7_disable;
+static _Atomic uint64_t g_iters;
+static _Atomic uint64_t g_calls;
+
+static void mode_env_init(void)
+{
+    if (atomic_exchange(&g_mode_env_read, 1) != 0) { return; }
+    const char* env = getenv("TOPOS_SIZED_SEARCH");
+    if (env == NULL) { return; }
+    if (strcmp(env, "linear") == 0) {
+        atomic_store(&g_mode, 1);
+    } else if (strcmp(env, "r6") == 0) {
+        atomic_store(&g_mode, 2);
+    } else if (strcmp(env, "strict") == 0) {
+        atomic_store(&g_mode, 0);
+    }
+}
+
+/* reference: codec.c:7136-7143 */
+TC_EXPORT void tc_dev_set_sized_mode(int32_t mode)
+{
+    atomic_store(&g_mode_env_read, 1);
+    atomic_store(&g_mode, (mode < 0 || mode > 2) ? 0 : mode);
+}
+
+/* reference: codec.c:7147-7150 */
+TC_EXPORT void tc_dev_set_sized_search(int legacy) { tc_dev_set_sized_mode(legacy ? 1 : 0); }
+/* reference: codec.c:7155-7159 */
+TC_EXPORT void tc_dev_set_qp_hint(int disable) { atomic_store(&g_hint_disable, disable ? 1 : 0); }
+/* reference: codec.c:7165-7169 */
+TC_EXPORT void tc_dev_set_qp_hint_model(int disable) { atomic_store(&g_hint_model_disable, disable ? 1 : 0); }
+/* reference: codec.c:7174-7178 */
+TC_EXPORT void tc_dev_set_sized_m7(int disable) { atomic_store(&g_m7_disable, disable ? 1 : 0); }
+
+/* reference: codec.c:7110-7123 */
+TC_EXPORT void tc_dev_sized_reset(void)
+{
+    atomic_store(&g_iters, 0u);
+    atomic_store(&g_calls, 0u);
+}
+TC_EXPORT uint64_t tc_dev_sized_iters(void) { return atomic_load(&g_iters); }
+TC_EXPORT uint64_t tc_dev_sized_calls(void) { return atomic_load(&g_calls); }
+
+static void count_encode(void) { atomic_fetch_add(&g_iters, 1u); }
+
+/* --------------------------------------------------------------- size table */
+
+typedef struct size_table {
+    tcg_sized* sess;
+    const topos_frame_config* cfg;
+    const topos_frame_input* in;
+    uint32_t qp_min, qp_max, window;
+    uint8_t known[TC_QP_MAX + 1u];
+    int32_t rc[TC_QP_MAX + 1u];       /* per-frame status of the probe */
+    uint32_t bytes[TC_QP_MAX + 1u];   /* exact packet size (reference probe count) */
+    uint32_t slot[TC_QP_MAX + 1u];
+    tcg_enc_result res[TC_QP_MAX + 1u];
+    uint32_t slices;
+    size_t cap;
+} size_table;
+
+/* Encodes qp q and up to window-1 of the nearest unprobed qps of
+ * [qp_min, qp_max] in one launch sequence. A call-level failure is returned;
+ * per-qp statuses land in the table. */
+static int32_t table_fill(size_table* t, uint32_t q)
+{
+    uint32_t qs[SIZED_WINDOW];
+    uint32_t n = 0;
+    qs[n++] = q;
+    for (uint32_t d = 1; n < t->window && (q + d <= t->qp_max || q >= t->qp_min + d); ++d) {
+        if (q + d <= t->qp_max && !t->known[q + d] && n < t->window) { qs[n++] = q + d; }
+        if (q >= t->qp_min + d && !t->known[q - d] && n < t->window) { qs[n++] = q - d; }
+    }
+    tcg_enc_frame jobs[SIZED_WINDOW];
+    size_t caps[SIZED_WINDOW];
+    tcg_enc_result res[SIZED_WINDOW];
+    uint32_t slots[SIZED_WINDOW];
+    for (uint32_t i = 0; i < n; ++i) {
+        topos_frame_config c = *t->cfg;
+        c.qp_base = (uint8_t)qs[i];
+        uint32_t nsl = 0;
+        uint8_t qpb = 0;
+        const int32_t rc = tc_prepare_encode(&c, t->in, &jobs[i], &nsl, &qpb);
+        if (rc != TC_OK) { return rc; }
+        t->slices = nsl;
+        caps[i] = t->cap;
+    }
+    const int32_t rc = tcg_sized_encode(t->sess, jobs, n, caps, res, slots);
+    if (rc != TC_OK) { return rc; }
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t qi = qs[i];
+        const tcg_enc_result* r = &res[i];
+        /* the reference's probe counts the bytes whatever their total */
+        const uint64_t b = 53u + 17u * (uint64_t)(r->color_slices + r->alpha_slices) + r->color_payload +
+                           r->alpha_payload;
+        t->known[qi] = 1u;
+        t->rc[qi] = r->rc;
+        t->bytes[qi] = (uint32_t)b;
+        t->slot[qi] = slots[i];
+        t->res[qi] = *r;
+    }
+    return TC_OK;
+}
+
+/* Probe of qp q: TC_OK with its exact size, or its error. A counting probe
+ * (the reference's exact-count probe from its coefficient cache) reports the
+ * size of a packet past the 256 MiB packet limit; a whole-frame probe fails
+ * there as the encode does. */
+static int32_t table_probe(size_table* t, uint32_t q, int counting, uint32_t* bytes)
+{
+    if (!t->known[q]) {
+        const int32_t rc = table_fill(t, q);
+        if (rc != TC_OK) { return rc; }
+    }
+    const int32_t r = t->rc[q];
+    if (r != TC_OK && !(counting && r == TC_ERR_LIMIT_EXCEEDED)) {
+        return tc_enc_result_status(r, t->res[q].packet_size, 0u);
+    }
+    *bytes = t->bytes[q];
+    return TC_OK;
+}
+
+/* The packet of probed qp q to out (the commit of the reference's final or
+ * last probe): stats always, the bytes only when they fit. */
+static int32_t table_commit(size_table* t, uint32_t q, uint8_t* out, size_t out_cap, topos_frame_stats* stats)
+{
+    uint32_t b = 0;
+    int32_t rc = table_probe(t, q, 0, &b);
+    if (rc != TC_OK) { return rc; }
+    const tcg_enc_result* r = &t->res[q];
+    memset(stats, 0, sizeof(*stats));
+    stats->struct_size = (uint32_t)sizeof(topos_frame_stats);
+    stats->abi_version = TOPOS_CODEC_ABI_VERSION;
+    tc_fill_enc_stats(stats, r, t->slices, (uint8_t)q);
+    if ((size_t)r->packet_size > out_cap) {
+        return tc_fail(TC_ERR_BUFFER_TOO_SMALL, "out_cap %zu < %zu bytes needed", out_cap, (size_t)r->packet_size);
+    }
+    if (out != NULL && r->packet_size > 0u) {
+        rc = tcg_sized_fetch(t->sess, t->slot[q], out, r->packet_size);
+        if (rc != TC_OK) { return rc; }
+    }
+    return TC_OK;
+}
+
+/* --------------------------------------------------------------- probe log */
+
+/* reference: codec.c:7271-7289 (sized_probe_ctx) */
+typedef struct probe_log {
+    size_table* t;
+    uint32_t target, qp_min, qp_max;
+    uint32_t pts_qp[SIZED_MAX_PTS], pts_bytes[SIZED_MAX_PTS], npts;
+    uint32_t budget;
+    int violated;
+    uint32_t last_qp;
+    int has_last;
+    int m7;
+} probe_log;
+
+/* reference: codec.c:7303-7351 (sized_encode_at): one probe, its point
+ * recorded and checked against the earlier ones for monotonicity */
+static int32_t encode_at(probe_log* c, uint32_t qp)
+{
+    if (c->budget == 0u) {
+        c->violated = 1;
+        return TC_ERR_LIMIT_EXCEEDED;
+    }
+    uint32_t b = 0;
+    const int32_t rc = table_probe(c->t, qp, c->m7, &b);
+    count_encode();
+    c->budget--;
+    c->last_qp = qp;
+    c->has_last = 1;
+    if (rc < 0) { return rc; }
+    for (uint32_t i = 0; i < c->npts; ++i) {
+        if (c->pts_qp[i] < qp && c->pts_bytes[i] < b) { c->violated = 1; }
+        if (c->pts_qp[i] > qp && c->pts_bytes[i] > b) { c->violated = 1; }
+    }
+    c->pts_qp[c->npts] = qp;
+    c->pts_bytes[c->npts] = b;
+    c->npts++;
+    return TC_OK;
+}
+
+static int bytes_at(const probe_log* c, uint32_t qp, uint32_t* out)
+{
+    for (uint32_t i = 0; i < c->npts; ++i) {
+        if (c->pts_qp[i] == qp) {
+            *out = c->pts_bytes[i];
+            return 1;
+        }
+    }
+    return 0;
+}
+
+/* reference: codec.c:7375-7398 (sized_fit_slope, r6 search) */
+static double fit_slope(const probe_log* c)
+{
+    for (uint32_t i = c->npts; i-- > 1u;) {
+        const uint32_t q1 = c->pts_qp[i], b1 = c->pts_bytes[i];
+        for (uint32_t j = i; j-- > 0u;) {
+            const uint32_t q0 = c->pts_qp[j], b0 = c->pts_bytes[j];
+            if (q1 > q0 && b0 > b1 && b0 > 0u) {
+                const double dr = log2((double)b0 / (double)b1);
+                if (dr > 0.05) {
+                    double s = (double)(q1 - q0) / dr;
+                    s = s < 1.0 ? 1.0 : (s > 16.0 ? 16.0 : s);
+                    return s;
+                }
+            }
+        }
+    }
+    return 4.0;
+}
+
+/* reference: codec.c:7554-7572 (strict_slope_from_pts) */
+static double strict_slope(const probe_log* c, double def)
+{
+    for (uint32_t i = c->npts; i-- > 1u;) {
+        const uint32_t q1 = c->pts_qp[i], b1 = c->pts_bytes[i];
+        for (uint32_t j = i; j-- > 0u;) {
+            const uint32_t q0 = c->pts_qp[j], b0 = c->pts_bytes[j];
+            if (q1 > q0 && b0 > b1 && b1 > 0u) {
+                const double dr = log2((double)b0 / (double)b1);
+                if (dr > 0.05) {
+                    double s = (double)(q1 - q0) / dr;
+                    s = s < 1.0 ? 1.0 : (s > 16.0 ? 16.0 : s);
+                    return s;
+                }
+            }
+        }
+    }
+    return def;
+}
+
+static uint32_t clamp_u32(uint32_t v, uint32_t lo, uint32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/* ------------------------------------------------------------------ searches */
+
+/* reference: codec.c:7199-7262. Coarse +8 steps then +1 steps up while over
+ * the target; then, while under 3/4 of it, one qp down at a time, undoing a
+ * step that overshoots. The last probe's packet is the answer. */
+static int32_t search_linear(size_table* t, uint32_t qp_base, uint32_t target, uint32_t qp_min, uint32_t qp_max,
+                             uint8_t* qp_used, uint8_t* out, size_t out_cap, topos_frame_stats* sp)
+{
+    uint32_t qp = clamp_u32(qp_base, qp_min, qp_max);
+    uint32_t iters = 0u;
+    const uint32_t max_iters = 24u;
+    uint32_t size = 0u;
+    int32_t rc = table_probe(t, qp, 0, &size);
+    count_encode();
+    iters++;
+    while (rc >= 0 && size > target && qp + 8u <= qp_max && iters < max_iters) {
+        qp += 8u;
+        rc = table_probe(t, qp, 0, &size);
+        count_encode();
+        iters++;
+    }
+    while (rc >= 0 && size > target && qp < qp_max && iters < max_iters) {
+        qp += 1u;
+        rc = table_probe(t, qp, 0, &size);
+        count_encode();
+        iters++;
+    }
+    while (rc >= 0 && size <= target && (uint64_t)size * 4u < (uint64_t)target * 3u && qp > qp_min &&
+           iters < max_iters) {
+        const uint32_t cand = qp - 1u;
+        uint32_t s2 = 0u;
+        const int32_t rc2 = table_probe(t, cand, 0, &s2);
+        count_encode();
+        iters++;
+        if (rc2 >= 0 && s2 <= target) {
+            qp = cand;
+            size = s2;
+            rc = rc2;
+            continue;
+        }
+        rc = table_probe(t, qp, 0, &size); /* back to the last packet that fitted */
+        count_encode();
+        iters++;
+        break;
+    }
+    if (rc >= 0) { rc = table_commit(t, qp, out, out_cap, sp); }
+    if (qp_used != NULL) { *qp_used = (uint8_t)qp; }
+    return rc;
+}
+
+/* reference: codec.c:7404-7552. The linear search's upward steps probe for
+ * probe; its downward reclaim is found by interpolation and bisection; a
+ * search the linear one would have cut off at 24 encodes falls back to it. */
+static int32_t search_fast(probe_log* c, uint32_t qp_base, uint8_t* qp_used, uint8_t* out, size_t out_cap,
+                           topos_frame_stats* sp, int* fallback)
+{
+    const uint32_t target = c->target, qp_min = c->qp_min, qp_max = c->qp_max;
+    const uint32_t q0 = clamp_u32(qp_base, qp_min, qp_max);
+    uint32_t q_final = q0;
+    uint32_t size = 0u;
+    int32_t rc = encode_at(c, q0);
+    if (rc < 0 || c->violated) { goto done; }
+    (void)bytes_at(c, q0, &size);
+    uint32_t qp = q0, iters = 1u;
+    while (rc >= 0 && size > target && qp + 8u <= qp_max && iters < 24u) {
+        qp += 8u;
+        rc = encode_at(c, qp);
+        if (rc < 0 || c->violated) { goto done; }
+        (void)bytes_at(c, qp, &size);
+        iters++;
+    }
+    while (rc >= 0 && size > target && qp < qp_max && iters < 24u) {
+        qp += 1u;
+        rc = encode_at(c, qp);
+        if (rc < 0 || c->violated) { goto done; }
+        (void)bytes_at(c, qp, &size);
+        iters++;
+    }
+    const uint32_t q_a = qp;
+    q_final = q_a;
+    int restore_extra = 0;
+    {
+        uint32_t ba = 0;
+        (void)bytes_at(c, q_a, &ba);
+        const int fits_a = ba <= target;
+        const int p_a = (uint64_t)ba * 4u < (uint64_t)target * 3u;
+        if (fits_a && p_a && q_a > qp_min && iters < 24u) {
+            uint32_t lo = q_a, hi = 0;
+            int have_notp = 0;
+            for (;;) {
+                uint32_t next;
+                if (!have_notp) {
+                    double dist = fit_slope(c) * log2((0.75 * (double)target) / (double)ba);
+                    if (dist < 0.0) { dist = 0.0; }
+                    const uint32_t d = (uint32_t)(dist + 0.999);
+                    next = clamp_u32(lo - d - 1u, qp_min, lo - 1u);
+                } else {
+                    next = (hi + lo) / 2u;
+                    if (next == hi) { next = hi + 1u; }
+                    if (next >= lo) { next = lo - 1u; }
+                }
+                rc = encode_at(c, next);
+                if (rc < 0 || c->violated) { goto done; }
+                uint32_t bn = 0;
+                (void)bytes_at(c, next, &bn);
+                const int p_n = (uint64_t)bn * 4u < (uint64_t)target * 3u;
+                if (p_n) {
+                    lo = next;
+                    ba = bn;
+                    if (lo == qp_min) { break; }
+                } else {
+                    have_notp = 1;
+                    hi = next;
+                    if (hi + 1u == lo) { break; }
+                }
+                if (have_notp && hi + 1u >= lo) { break; }
+                if (!have_notp && lo == qp_min) { break; }
+            }
+            if (have_notp) {
+                uint32_t bc = 0;
+                (void)bytes_at(c, hi, &bc);
+                if (bc <= target) {
+                    q_final = hi;
+                } else {
+                    q_final = hi + 1u;
+                    restore_extra = 2;
+                }
+            } else {
+                q_final = qp_min;
+            }
+        }
+    }
+    {
+        uint32_t iters_check = iters;
+        if (q_final < q_a) { iters_check += q_a - q_final; }
+        iters_check += (uint32_t)restore_extra;
+        if (iters_check > 24u) {
+            c->violated = 1;
+            goto done;
+        }
+    }
+    if (c->m7 != 0) {
+        count_encode(); /* the reference's final encode from its coefficient cache */
+    } else if (!c->has_last || c->last_qp != q_final) {
+        rc = encode_at(c, q_final);
+        if (rc < 0 || c->violated) { goto done; }
+    }
+    rc = table_commit(c->t, q_final, out, out_cap, sp);
+done:
+    if (c->violated != 0) {
+        *fallback = 1;
+        return TC_OK;
+    }
+    if (qp_used != NULL) { *qp_used = (uint8_t)q_final; }
+    return rc;
+}
+
+/* reference: codec.c:7578-7787. The smallest qp of [qp_min, qp_max] whose
+ * packet fits: slope jumps from a seed (the cross-call hint, else qp_base)
+ * until the answer is bracketed, then log interpolation inside the bracket.
+ * A probe budget of 24, monotonic sizes and the coefficient cache are its
+ * preconditions; without one it falls back to the linear search. */
+static int32_t search_strict(probe_log* c, sized_hint* e, uint32_t qp_base, uint8_t* qp_used, uint8_t* out,
+                             size_t out_cap, topos_frame_stats* sp, int* fallback)
+{
+    const uint32_t target = c->target, qp_min = c->qp_min, qp_max = c->qp_max;
+    if (c->m7 == 0) {
+        *fallback = 1;
+        return TC_OK;
+    }
+    uint32_t q0 = qp_base;
+    const int hint_on = atomic_load(&g_hint_disable) == 0;
+    const int model_on = atomic_load(&g_hint_model_disable) == 0;
+    if (hint_on && e->valid != 0) {
+        q0 = e->q;
+        if (model_on && e->bytes > 0u && target > 0u) {
+            const double dr = log2((double)e->bytes / (double)target);
+            double slope = 0.0;
+            if (e->prev_bytes > 0u && e->prev != e->q) {
+                const uint32_t q_hi = e->q > e->prev ? e->q : e->prev;
+                const uint32_t q_lo = q_hi == e->q ? e->prev : e->q;
+                const uint32_t b_hi = q_hi == e->q ? e->bytes : e->prev_bytes;
+                const uint32_t b_lo = q_hi == e->q ? e->prev_bytes : e->bytes;
+                if (q_hi > q_lo && b_lo > b_hi && b_hi > 0u) {
+                    slope = (double)(q_hi - q_lo) / log2((double)b_lo / (double)b_hi);
+                }
+            }
+            if (slope > 0.0) {
+                slope = slope < 0.25 ? 0.25 : (slope > 32.0 ? 32.0 : slope);
+            } else {
+                slope = 8.0;
+            }
+            double dq = slope * dr;
+            dq = dq > 32.0 ? 32.0 : (dq < -32.0 ? -32.0 : dq);
+            const double q_seed = (double)q0 + dq;
+            q0 = q_seed > 0.0 ? (uint32_t)(q_seed + 0.5) : 0u;
+        }
+    }
+    q0 = clamp_u32(q0, qp_min, qp_max);
+    int have_lo = 0, have_hi = 0;
+    uint32_t lo = 0u, hi = 0u, q_final = qp_max;
+    double prior_slope = 4.0;
+    if (model_on && e->bytes > 0u && e->prev_bytes > 0u && e->prev != e->q) {
+        const uint32_t q_hi = e->q > e->prev ? e->q : e->prev;
+        const uint32_t q_lo = q_hi == e->q ? e->prev : e->q;
+        const uint32_t b_hi = q_hi == e->q ? e->bytes : e->prev_bytes;
+        const uint32_t b_lo = q_hi == e->q ? e->prev_bytes : e->bytes;
+        if (q_hi > q_lo && b_lo > b_hi && b_hi > 0u) {
+            double s = (double)(q_hi - q_lo) / log2((double)b_lo / (double)b_hi);
+            prior_slope = s < 1.0 ? 1.0 : (s > 16.0 ? 16.0 : s);
+        }
+    }
+    int32_t rc = encode_at(c, q0);
+    if (rc < 0 || c->violated) { goto done; }
+    {
+        uint32_t b0 = 0u;
+        (void)bytes_at(c, q0, &b0);
+        if (b0 <= target) {
+            lo = q0;
+            have_lo = 1;
+        } else {
+            hi = q0;
+            have_hi = 1;
+        }
+    }
+    for (;;) {
+        if (have_lo && (!have_hi ? (lo == qp_min) : (lo == hi + 1u))) {
+            q_final = lo;
+            break;
+        }
+        if (have_hi && !have_lo && hi == qp_max) {
+            q_final = qp_max; /* nothing fits: the largest qp, best effort */
+            break;
+        }
+        if (c->budget == 0u) {
+            c->violated = 1;
+            break;
+        }
+        uint32_t q;
+        if (!have_lo) {
+            uint32_t bh = 0u;
+            (void)bytes_at(c, hi, &bh);
+            const double dr = target > 0u && bh > target ? log2((double)bh / (double)target) : 16.0;
+            const double slope = strict_slope(c, prior_slope);
+            uint32_t dq = (uint32_t)(slope * dr + 0.999);
+            dq = dq < 1u ? 1u : (dq > 32u ? 32u : dq);
+            q = hi + dq;
+            if (q >= qp_max) { q = qp_max; }
+        } else if (!have_hi) {
+            uint32_t bl = 0u;
+            (void)bytes_at(c, lo, &bl);
+            const double dr = bl > 0u && (double)target > (double)bl ? log2((double)target / (double)bl) : 16.0;
+            const double slope = strict_slope(c, prior_slope);
+            uint32_t dq = (uint32_t)(slope * dr + 0.999);
+            dq = dq < 1u ? 1u : (dq > 32u ? 32u : dq);
+            q = (dq < lo) ? lo - dq : qp_min;
+            if (q < qp_min) { q = qp_min; }
+            if (q >= lo) { q = lo - 1u; }
+        } else {
+            uint32_t bh = 0u, bl = 0u;
+            (void)bytes_at(c, hi, &bh);
+            (void)bytes_at(c, lo, &bl);
+            double q_pred;
+            if (bh > 0u && bl > 0u && bh > bl) {
+                q_pred = (double)hi + ((double)lo - (double)hi) *
+                                          (log2((double)bh) - log2((double)(target > 0u ? target : 1u))) /
+                                          (log2((double)bh) - log2((double)bl));
+            } else {
+                q_pred = (double)((hi + lo) / 2u);
+            }
+            q = (uint32_t)(q_pred + 0.5);
+            if (q <= hi) { q = hi + 1u; }
+            if (q >= lo) { q = lo - 1u; }
+            uint32_t dummy = 0u;
+            if (bytes_at(c, q, &dummy)) {
+                uint32_t mid = (hi + lo) / 2u;
+                if (mid <= hi || mid >= lo) { mid = hi + 1u; }
+                q = mid;
+                for (; q < lo; ++q) {
+                    if (!bytes_at(c, q, &dummy)) { break; }
+                }
+                if (q >= lo) {
+                    q_final = lo;
+                    break;
+                }
+            }
+        }
+        rc = encode_at(c, q);
+        if (rc < 0 || c->violated) { break; }
+        uint32_t b = 0u;
+        (void)bytes_at(c, q, &b);
+        if (b <= target) {
+            if (!have_lo || q < lo) { lo = q; }
+            have_lo = 1;
+        } else {
+            if (!have_hi || q > hi) { hi = q; }
+            have_hi = 1;
+        }
+    }
+done:
+    if (c->violated != 0) {
+        *fallback = 1;
+        return TC_OK;
+    }
+    if (rc < 0) { return rc; }
+    rc = table_commit(c->t, q_final, out, out_cap, sp);
+    count_encode();
+    if (rc < 0) { return rc; }
+    if (qp_used != NULL) { *qp_used = (uint8_t)q_final; }
+    {
+        uint32_t bf = 0u;
+        if (bytes_at(c, q_final, &bf) != 0) {
+            if (e->valid != 0 && e->q != q_final) {
+                e->prev = e->q;
+                e->prev_bytes = e->bytes;
+            }
+            e->q = q_final;
+            e->valid = 1;
+            e->bytes = bf;
+        }
+    }
+    return rc;
+}
+
+/* ----------------------------------------------------------------- entry */
+
+/* reference: native/src/codec/codec.c:7789-7880 */
+TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const topos_frame_input* input,
+                                        uint32_t target_bytes, uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used,
+                                        uint8_t* out, size_t out_cap, topos_frame_stats* stats)
+{
+    int32_t rc = tc_frame_config_validate(cfg);
+    if (rc != TC_OK) { return rc; }
+    if ((cfg->reserved[0] & 0xFFu) == 9u) {
+        return tc_fail(TC_ERR_NOT_IMPLEMENTED, "v8 sized encode lands in format-plan batch 2");
+    }
+    if ((cfg->reserved[0] & 0xFFu) == 10u || (cfg->reserved[0] & 0xFFu) == 11u) {
+        return tc_fail(TC_ERR_NOT_IMPLEMENTED,
+                       "temporal sized encode is not a write path (fixed anchor-qp P0; use tc_gop_context_encode_frame)");
+    }
+    if (cfg->pixel_format == 3u) {
+        return tc_fail(TC_ERR_NOT_IMPLEMENTED, "TRAW sized rate control is a post-v1 option; use fixed anchor-qp tiers");
+    }
+    if (qp_min > TC_QP_MAX || qp_max > TC_QP_MAX || qp_min > qp_max) {
+        return tc_fail(TC_ERR_INVALID_ARGUMENT, "qp range %u..%u invalid", (unsigned)qp_min, (unsigned)qp_max);
+    }
+    topos_frame_stats local;
+    memset(&local, 0, sizeof(local));
+    topos_frame_stats* sp = stats != NULL ? stats : &local;
+    mode_env_init();
+    atomic_fetch_add(&g_calls, 1u);
+
+    /* the frame at its own qp: validation of the input exactly as a plain
+     * encode, and the geometry that sizes the probe window */
+    tcg_enc_frame base;
+    uint32_t nsl = 0;
+    uint8_t qpb = 0;
+    rc = tc_prepare_encode(cfg, input, &base, &nsl, &qpb);
+    if (rc != TC_OK) { return rc; }
+    uint64_t cblocks = 0, samples = 0;
+    for (uint32_t p = 0; p < base.planes; ++p) {
+        samples += (uint64_t)base.plane[p].vis_w * base.plane[p].vis_h;
+        if (base.plane[p].kind == TCG_PLANE_COLOR) { cblocks += (uint64_t)base.plane[p].cols * base.plane[p].rows; }
+    }
+    size_table* t = (size_table*)calloc(1, sizeof(size_table));
+    if (t == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "sized encode table"); }
+    t->cfg = cfg;
+    t->in = input;
+    t->qp_min = qp_min;
+    t->qp_max = qp_max;
+    t->cap = tc_frame_packet_bound(cfg);
+    {
+        /* device bytes of one probe: packet, samples and the coder's per-block buffers */
+        const uint64_t per = (uint64_t)t->cap + samples * 2u + cblocks * 2048u;
+        uint64_t w = SIZED_WINDOW_BYTES / (per > 0u ? per : 1u);
+        w = w < 1u ? 1u : (w > SIZED_WINDOW ? SIZED_WINDOW : w);
+        t->window = (uint32_t)w;
+    }
+    rc = tcg_sized_open(&base, &t->sess);
+    if (rc != TC_OK) {
+        free(t);
+        return rc;
+    }
+
+    /* the cross-call hint record: borrowed when free, an empty one otherwise */
+    sized_hint fresh;
+    memset(&fresh, 0, sizeof(fresh));
+    int expected = 0;
+    const int borrowed = atomic_compare_exchange_strong(&g_hint_busy, &expected, 1);
+    sized_hint* e = borrowed ? &g_hint : &fresh;
+
+    probe_log c;
+    memset(&c, 0, sizeof(c));
+    c.t = t;
+    c.target = target_bytes;
+    c.qp_min = qp_min;
+    c.qp_max = qp_max;
+    c.budget = SIZED_PROBE_BUDGET;
+    c.m7 = atomic_load(&g_m7_disable) == 0 && cblocks * 256u <= SIZED_FCACHE_MAX_BYTES;
+
+    uint8_t qu = 0;
+    int fallback = 0;
+    const int mode = atomic_load(&g_mode);
+    if (mode == 1) {
+        rc = search_linear(t, cfg->qp_base, target_bytes, qp_min, qp_max, &qu, out, out_cap, sp);
+    } else {
+        rc = mode == 2 ? search_fast(&c, cfg->qp_base, &qu, out, out_cap, sp, &fallback)
+                       : search_strict(&c, e, cfg->qp_base, &qu, out, out_cap, sp, &fallback);
+        if (fallback != 0) {
+            rc = search_linear(t, cfg->qp_base, target_bytes, qp_min, qp_max, &qu, out, out_cap, sp);
+        }
+    }
+    if (borrowed) { atomic_store(&g_hint_busy, 0); }
+    tcg_sized_close(t->sess);
+    free(t);
+    if (qp_used != NULL) { *qp_used = qu; }
+    return rc;
+}

@@ -39,15 +39,6 @@ TC_EXPORT void tc_dev_symbol_pair_hist_get(uint32_t plane, uint64_t* pair_hist)
     if (pair_hist != NULL) { memset(pair_hist, 0, 64u * 28u * sizeof(uint64_t)); }
 }
 
-TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const topos_frame_input* input,
-                                        uint32_t target_bytes, uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used,
-                                        uint8_t* out, size_t out_cap, topos_frame_stats* stats)
-{
-    (void)cfg; (void)input; (void)target_bytes; (void)qp_min; (void)qp_max; (void)qp_used; (void)out; (void)out_cap;
-    (void)stats;
-    return NOT_PATH("tc_frame_encode_sized");
-}
-
 TC_EXPORT int32_t tc_decode_scale_dimensions(uint32_t source_width, uint32_t source_height, int32_t scale,
                                              uint32_t* target_width, uint32_t* target_height)
 {

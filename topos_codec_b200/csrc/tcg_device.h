@@ -84,6 +84,21 @@ typedef struct tcg_dec_frame {
     int32_t skip;           /* in: nonzero = frame already rejected by the host */
 } tcg_dec_frame;
 
+/* Size-targeted encode sessions. A session leases one context for its whole
+ * life, holds a device copy of the frame's sample planes (uploaded once when
+ * they are in host memory) and keeps the packet of every probe on the device.
+ * tcg_sized_encode codes count variants of the session's frame (the planes of
+ * `base` are used, whatever frames[i] holds; headers and quantisers differ) in
+ * one launch sequence, with res[i] as from tcg_encode and slots[i] naming the
+ * kept packet; caps[i] bounds packet i. tcg_sized_fetch copies the first size
+ * bytes of a kept packet to out (host or device memory). */
+typedef struct tcg_sized tcg_sized;
+int32_t tcg_sized_open(const tcg_enc_frame* base, tcg_sized** out);
+int32_t tcg_sized_encode(tcg_sized* s, const tcg_enc_frame* frames, uint32_t count, const size_t* caps,
+                         tcg_enc_result* res, uint32_t* slots);
+int32_t tcg_sized_fetch(tcg_sized* s, uint32_t slot, uint8_t* out, size_t size);
+void tcg_sized_close(tcg_sized* s);
+
 /* Decodes count frames in one device launch sequence; per-slice status is
  * written to each frame's slice_status. Returns TC_OK when the device work ran,
  * or a call-level error. */
