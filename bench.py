@@ -440,6 +440,17 @@ def main():
             r["damaged_decode_vs_reference"]["corruption"] = "1 % of the slices of 8 reference packets, one payload byte each"
         extra["gbr4444_alpha"] = r
         del gframes
+        # size-targeted encode: 8 frames of the bench workload from host memory, target = the
+        # first frame's packet at qp 24, qp searched over 0..63 (strict search, hints on)
+        sframes = [[p.cpu().numpy() for p in frames_d[i]] for i in range(min(nf, 8))]
+        c24 = B.make_config(W, H, **{**CFG, "qp": 24})
+        target = len(gpu.encode(c24, sframes[0]))
+        ref = B.ToposCodec(REF_LIB) if (rank == 0 and os.path.exists(REF_LIB)) else None
+        r = WL.sized_vs_reference(gpu, ref, cfg, sframes, target, 0, 63, ref_threads=min(16, os.cpu_count() or 1))
+        r["workload"] = ("3840x2160 10-bit 4:2:2 HQ from host memory, tc_frame_encode_sized per frame in order, "
+                         "target = frame 0 at qp 24, qp 0..63")
+        extra["sized_encode"] = r
+        del sframes
         torch.cuda.empty_cache()
 
     # ---------------- serving: open-loop request streams at 25/50/75/100 % of saturation ----------------

@@ -4,8 +4,6 @@ sequence the status, chosen qp, packet bytes, stats and probe-encode count
 agree, in the strict (default), linear and r6 search modes, including the
 cross-call qp hint, qp ranges above 63, unreachable and trivially met
 targets, a too-small output buffer and a 4:4:4 + alpha frame."""
-import ctypes
-
 import numpy as np
 import pytest
 
@@ -14,28 +12,13 @@ from topos_codec_b200 import binding as B, synth
 pytestmark = pytest.mark.gpu
 
 
-def _setup(lib):
-    lib.tc_frame_encode_sized.restype = ctypes.c_int32
-    lib.tc_dev_sized_iters.restype = ctypes.c_uint64
-    lib.tc_dev_set_sized_mode.restype = None
-    lib.tc_dev_set_qp_hint.restype = None
-
-
 def _sized(codec, cfg, planes, target, qp_min, qp_max, cap=None):
     lib = codec._lib
-    fi = codec._input(planes)
-    cap = codec.packet_bound(cfg) if cap is None else cap
-    out = np.full(max(cap, 1), 0xA5, dtype=np.uint8)
-    st = B.FrameStats()
-    qp_used = ctypes.c_uint8(0xEE)
     it0 = lib.tc_dev_sized_iters()
-    rc = int(lib.tc_frame_encode_sized(ctypes.byref(cfg), ctypes.byref(fi), ctypes.c_uint32(target),
-                                       ctypes.c_uint8(qp_min), ctypes.c_uint8(qp_max), ctypes.byref(qp_used),
-                                       out.ctypes.data, ctypes.c_size_t(cap), ctypes.byref(st)))
+    rc, pkt, st, qp, out = codec.encode_sized_status(cfg, planes, target, qp_min, qp_max, cap)
     iters = lib.tc_dev_sized_iters() - it0
-    pkt = out[: st.packet_size].tobytes() if rc == 0 else b""
     untouched = bool(np.all(out == 0xA5)) if rc != 0 else None
-    return {"rc": rc, "qp": qp_used.value, "pkt": pkt, "size": st.packet_size, "qp_base": st.qp_base,
+    return {"rc": rc, "qp": qp, "pkt": pkt, "size": st.packet_size, "qp_base": st.qp_base,
             "color": st.color_payload_bytes, "alpha": st.alpha_payload_bytes, "slices": st.slice_count,
             "iters": iters, "untouched": untouched}
 
@@ -49,8 +32,6 @@ def _both(product, reference, cfg, planes, target, qp_min, qp_max, cap=None):
 
 @pytest.fixture(scope="module")
 def libs(product, reference):
-    for c in (product, reference):
-        _setup(c._lib)
     yield product, reference
     for c in (product, reference):
         c._lib.tc_dev_set_sized_mode(0)

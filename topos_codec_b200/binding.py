@@ -188,6 +188,20 @@ class ToposCodec:
         L.tc_frame_config_validate.argtypes = [ctypes.POINTER(FrameConfig)]
         L.tc_last_error.restype = ctypes.c_char_p
         L.tc_last_error.argtypes = []
+        if hasattr(L, "tc_frame_encode_sized"):
+            L.tc_frame_encode_sized.restype = ctypes.c_int32
+            L.tc_frame_encode_sized.argtypes = [ctypes.POINTER(FrameConfig), ctypes.POINTER(FrameInput),
+                                                ctypes.c_uint32, ctypes.c_uint8, ctypes.c_uint8,
+                                                ctypes.POINTER(ctypes.c_uint8), ctypes.c_void_p, ctypes.c_size_t,
+                                                ctypes.POINTER(FrameStats)]
+        for name, res in (("tc_dev_sized_iters", ctypes.c_uint64), ("tc_dev_sized_calls", ctypes.c_uint64)):
+            if hasattr(L, name):
+                getattr(L, name).restype = res
+                getattr(L, name).argtypes = []
+        for name in ("tc_dev_set_sized_mode", "tc_dev_set_qp_hint", "tc_dev_set_qp_hint_model", "tc_dev_set_sized_m7"):
+            if hasattr(L, name):
+                getattr(L, name).restype = None
+                getattr(L, name).argtypes = [ctypes.c_int32]
         self.has_encode_batch = hasattr(L, "tcg_frame_encode_batch")
         if self.has_encode_batch:
             L.tcg_frame_encode_batch.restype = ctypes.c_int32
@@ -235,6 +249,30 @@ class ToposCodec:
         if rc != TC_OK:
             raise ToposCodecError(f"tc_frame_encode failed [{rc}]: {self.last_error()}", rc)
         return pkt
+
+    def encode_sized_status(self, cfg: FrameConfig, planes: Sequence[np.ndarray], target_bytes: int,
+                            qp_min: int = 0, qp_max: int = 95, out_cap: Optional[int] = None,
+                            out: Optional[np.ndarray] = None):
+        """tc_frame_encode_sized: (status, packet, stats, qp_used, output buffer). Without `out` the
+        output buffer is a new one filled with 0xA5 (to see what a failing call leaves)."""
+        fi = self._input(planes)
+        cap = self.packet_bound(cfg) if out_cap is None else out_cap
+        if out is None:
+            out = np.full(max(cap, 1), 0xA5, dtype=np.uint8)
+        cap = min(cap, out.size)
+        st = FrameStats()
+        qp_used = ctypes.c_uint8(0xEE)
+        rc = int(self._lib.tc_frame_encode_sized(ctypes.byref(cfg), ctypes.byref(fi), target_bytes, qp_min, qp_max,
+                                                 ctypes.byref(qp_used), out.ctypes.data, cap, ctypes.byref(st)))
+        pkt = out[: st.packet_size].tobytes() if rc == TC_OK else b""
+        return rc, pkt, st, qp_used.value, out
+
+    def encode_sized(self, cfg: FrameConfig, planes: Sequence[np.ndarray], target_bytes: int, qp_min: int = 0,
+                     qp_max: int = 95) -> Tuple[bytes, int]:
+        rc, pkt, _, qp, _ = self.encode_sized_status(cfg, planes, target_bytes, qp_min, qp_max)
+        if rc != TC_OK:
+            raise ToposCodecError(f"tc_frame_encode_sized failed [{rc}]: {self.last_error()}", rc)
+        return pkt, qp
 
     def encode_frame(self, cfg: FrameConfig, planes: Sequence[np.ndarray]) -> Tuple[bytes, dict]:
         rc, pkt, st = self.encode_status(cfg, planes)

@@ -1260,14 +1260,21 @@ static int32_t encode_pipelined(const tcg_enc_frame* frames, const uint32_t* sta
 }  // namespace tcg
 
 // ------------------------------------------------------------ sized sessions
+//
+// A session leases one context for the call. Host-memory sample planes are
+// uploaded once into the context's grow-only B_SIZED_PIX buffer. Probe packets
+// go to B_SIZED_PKT, split in two halves used in turn by successive launches,
+// so the packets of the last two launches stay available; an older one is
+// reported as no longer kept and the caller encodes that qp again.
 
 struct tcg_sized {
     tcg::Ctx* C = nullptr;
-    void* planes = nullptr;                       // device copy of host-memory sample planes
-    const void* src[4] = {};                      // plane sources the variants read
+    const void* src[4] = {};                     // plane sources the variants read
     size_t stride[4] = {};
-    std::vector<void*> regions;                   // one device packet region per encode call
-    std::vector<std::pair<uint8_t*, size_t>> slot; // kept packets: address, capacity
+    uint32_t launches = 0;                       // encode calls so far
+    size_t half = 0;                             // bytes of one half of B_SIZED_PKT
+    struct Slot { uint32_t launch; size_t off, cap; };
+    std::vector<Slot> slot;
 };
 
 extern "C" int32_t tcg_sized_open(const tcg_enc_frame* base, tcg_sized** out)
@@ -1286,15 +1293,15 @@ extern "C" int32_t tcg_sized_open(const tcg_enc_frame* base, tcg_sized** out)
     }
     if (host_bytes > 0) {
         // every probe reads the samples from HBM: one upload, tight rows
-        if (cudaMallocAsync(&s->planes, host_bytes, C->stream) != cudaSuccess) {
+        if (!tcg::dreserve(C, tcg::B_SIZED_PIX, host_bytes)) {
             tcg_sized_close(s);
-            return tcg::cuda_fail(cudaErrorMemoryAllocation, "sized planes");
+            return TCG_ERR_OUT_OF_MEMORY;
         }
         size_t off = 0;
         for (uint32_t p = 0; p < base->planes; ++p) {
             const tcg_enc_plane& I = base->plane[p];
             if (!tcg::host_memory(I.src)) { continue; }
-            uint8_t* dst = (uint8_t*)s->planes + off;
+            uint8_t* dst = tcg::dptr<uint8_t>(C, tcg::B_SIZED_PIX) + off;
             const cudaError_t e = cudaMemcpy2DAsync(dst, (size_t)I.vis_w * 2u, I.src, I.stride * 2u,
                                                     (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, C->stream);
             if (e != cudaSuccess) {
@@ -1316,24 +1323,27 @@ extern "C" int32_t tcg_sized_encode(tcg_sized* s, const tcg_enc_frame* frames, u
     if (count == 0u) { return 0; }
     std::vector<tcg_enc_frame> fr(frames, frames + count);
     std::vector<uint8_t*> outs(count);
-    size_t total = 0;
+    size_t need = 0;
     for (uint32_t i = 0; i < count; ++i) {
         for (uint32_t p = 0; p < fr[i].planes; ++p) {
             fr[i].plane[p].src = (const uint16_t*)s->src[p];
             fr[i].plane[p].stride = s->stride[p];
         }
-        total += tcg::align_up(caps[i], 256);
+        need += tcg::align_up(caps[i], 256);
     }
-    void* region = nullptr;
-    if (cudaMallocAsync(&region, total, s->C->stream) != cudaSuccess) {
-        return tcg::cuda_fail(cudaErrorMemoryAllocation, "sized packets");
+    if (need > s->half) {
+        // growing the store drops what it kept
+        s->half = need;
+        for (auto& k : s->slot) { k.launch = UINT32_MAX; }
     }
-    s->regions.push_back(region);
-    size_t off = 0;
+    if (!tcg::dreserve(s->C, tcg::B_SIZED_PKT, 2u * s->half)) { return TCG_ERR_OUT_OF_MEMORY; }
+    const uint32_t launch = s->launches++;
+    size_t off = (launch & 1u) * s->half;
+    uint8_t* base = tcg::dptr<uint8_t>(s->C, tcg::B_SIZED_PKT);
     for (uint32_t i = 0; i < count; ++i) {
-        outs[i] = (uint8_t*)region + off;
+        outs[i] = base + off;
         slots[i] = (uint32_t)s->slot.size();
-        s->slot.emplace_back(outs[i], caps[i]);
+        s->slot.push_back({launch, off, caps[i]});
         off += tcg::align_up(caps[i], 256);
     }
     return tcg::encode_impl(s->C, fr.data(), count, outs.data(), caps, res);
@@ -1341,12 +1351,15 @@ extern "C" int32_t tcg_sized_encode(tcg_sized* s, const tcg_enc_frame* frames, u
 
 extern "C" int32_t tcg_sized_fetch(tcg_sized* s, uint32_t slot, uint8_t* out, size_t size)
 {
-    if (slot >= s->slot.size() || size > s->slot[slot].second) {
+    if (slot >= s->slot.size() || size > s->slot[slot].cap) {
         tcg_host_set_error(TCG_ERR_INVALID_ARGUMENT, "sized fetch: no such packet");
         return TCG_ERR_INVALID_ARGUMENT;
     }
+    const tcg_sized::Slot& k = s->slot[slot];
+    if (k.launch == UINT32_MAX || k.launch + 2u < s->launches) { return 1; }  // no longer kept
     if (size == 0u) { return 0; }
-    TCG_CHECK(cudaMemcpyAsync(out, s->slot[slot].first, size, cudaMemcpyDefault, s->C->stream));
+    TCG_CHECK(cudaMemcpyAsync(out, tcg::dptr<uint8_t>(s->C, tcg::B_SIZED_PKT) + k.off, size, cudaMemcpyDefault,
+                              s->C->stream));
     TCG_CHECK(cudaStreamSynchronize(s->C->stream));
     return 0;
 }
@@ -1354,8 +1367,6 @@ extern "C" int32_t tcg_sized_fetch(tcg_sized* s, uint32_t slot, uint8_t* out, si
 extern "C" void tcg_sized_close(tcg_sized* s)
 {
     if (s == nullptr) { return; }
-    for (void* r : s->regions) { cudaFreeAsync(r, s->C->stream); }
-    if (s->planes != nullptr) { cudaFreeAsync(s->planes, s->C->stream); }
     cudaStreamSynchronize(s->C->stream);
     tcg::ctx_release(s->C);
     delete s;

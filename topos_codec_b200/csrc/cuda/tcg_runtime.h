@@ -38,7 +38,7 @@ struct HBuf {
 enum BufId {
     B_PIX, B_COEF, B_MASK, B_DCM, B_NOPS, B_OPOFF, B_HIST, B_STAB, B_OPS, B_STAGE,
     B_SRES, B_PKT, B_DESC, B_FRES, B_ALPHA, B_DEC_COEF, B_DEC_TAB, B_DEC_OUT, B_DEC_PKT,
-    B_DEC_RES, B_TMP0, B_TMP1, B_COUNT
+    B_DEC_RES, B_TMP0, B_TMP1, B_SIZED_PIX, B_SIZED_PKT, B_COUNT
 };
 
 // Kernel identities for optional per-kernel event timing.

@@ -9,8 +9,8 @@
  * step, over a table of exact packet sizes that the GPU fills a window of qps
  * at a time: a probe of a qp the table lacks encodes it together with the
  * nearest unprobed qps (one batched launch sequence, the samples uploaded
- * once per call), and every probe's packet stays on the device so the chosen
- * one is copied out without a final encode.
+ * once per call), and the packets of the last two launches stay on the
+ * device, so the chosen one is normally copied out without a final encode.
  *
  * Process state as in the reference: the search mode (TOPOS_SIZED_SEARCH =
  * strict | linear | r6, or tc_dev_set_sized_mode), and the strict search's
@@ -192,7 +192,16 @@ static int32_t table_commit(size_table* t, uint32_t q, uint8_t* out, size_t out_
     }
     if (out != NULL && r->packet_size > 0u) {
         rc = tcg_sized_fetch(t->sess, t->slot[q], out, r->packet_size);
-        if (rc != TC_OK) { return rc; }
+        if (rc == 1) {
+            /* the packet was dropped by later probe launches: encode it alone again */
+            t->known[q] = 0u;
+            const uint32_t w = t->window;
+            t->window = 1u;
+            rc = table_fill(t, q);
+            t->window = w;
+            if (rc == TC_OK) { rc = tcg_sized_fetch(t->sess, t->slot[q], out, r->packet_size); }
+        }
+        if (rc != TC_OK) { return rc < 0 ? rc : tc_fail(TC_ERR_INVALID_ARGUMENT, "sized packet lost"); }
     }
     return TC_OK;
 }

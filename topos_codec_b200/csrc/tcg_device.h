@@ -86,12 +86,14 @@ typedef struct tcg_dec_frame {
 
 /* Size-targeted encode sessions. A session leases one context for its whole
  * life, holds a device copy of the frame's sample planes (uploaded once when
- * they are in host memory) and keeps the packet of every probe on the device.
- * tcg_sized_encode codes count variants of the session's frame (the planes of
- * `base` are used, whatever frames[i] holds; headers and quantisers differ) in
- * one launch sequence, with res[i] as from tcg_encode and slots[i] naming the
- * kept packet; caps[i] bounds packet i. tcg_sized_fetch copies the first size
- * bytes of a kept packet to out (host or device memory). */
+ * they are in host memory) and keeps the packets of its last two probe
+ * launches on the device. tcg_sized_encode codes count variants of the
+ * session's frame (the planes of `base` are used, whatever frames[i] holds;
+ * headers and quantisers differ) in one launch sequence, with res[i] as from
+ * tcg_encode and slots[i] naming the packet; caps[i] bounds packet i.
+ * tcg_sized_fetch copies the first size bytes of a packet to out (host or
+ * device memory): 0 when done, 1 when the packet is no longer kept (encode
+ * that variant again), a negative status on error. */
 typedef struct tcg_sized tcg_sized;
 int32_t tcg_sized_open(const tcg_enc_frame* base, tcg_sized** out);
 int32_t tcg_sized_encode(tcg_sized* s, const tcg_enc_frame* frames, uint32_t count, const size_t* caps,

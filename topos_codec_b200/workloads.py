@@ -10,9 +10,13 @@
   1 % of their slices byte-corrupted check the per-slice concealment status
   and pixels against the reference library.
 
-Each is coded as one batched call and as one plain call per frame on the same
-device-resident inputs; device time comes from the library's own stream
-events (tcg_last_device_ms) and both forms must give identical bytes.
+* Size-targeted encode: 3840x2160 10-bit 4:2:2 HQ frames from host memory,
+  one tc_frame_encode_sized call per frame with a byte target, beside the
+  reference library on the host cores.
+
+The first two are coded as one batched call and as one plain call per frame
+on the same device-resident inputs; device time comes from the library's own
+stream events (tcg_last_device_ms) and both forms must give identical bytes.
 """
 from __future__ import annotations
 
@@ -127,6 +131,47 @@ def batched_vs_plain(codec, cfgs: Sequence[B.FrameConfig], frames, repeats: int 
             "plain_decode_ms": p_dec, "batched_vs_plain": (p_enc + p_dec) / (enc_ms + dec_ms),
             "encode_fps": n / (enc_ms / 1e3), "decode_fps": n / (dec_ms / 1e3), "bit_exact": bool(exact),
             "packets": pkts}
+
+
+def sized_vs_reference(product, reference, cfg: B.FrameConfig, frames, target: int, qp_min: int = 0,
+                       qp_max: int = 63, ref_threads: int = 16) -> Dict:
+    """tc_frame_encode_sized on host-memory frames, one call per frame in order
+    (as an encoder would run it), through this library and the reference
+    library (its slice pool at ref_threads): per-frame wall time, chosen qps,
+    probe encodes and whether packets, qps and probe counts agree. The two
+    libraries must start from the same cross-call hint history (for instance,
+    neither has made a size-targeted call before), as the probe sequence
+    depends on it."""
+    import time
+    out = np.empty(product.packet_bound(cfg), np.uint8)
+    res = {}
+    if reference is not None:
+        reference._lib.tc_dev_set_thread_count(ctypes.c_int32(ref_threads))
+    for name, codec in (("gpu", product), ("reference", reference)):
+        if codec is None:
+            continue
+        L = codec._lib
+        i0 = L.tc_dev_sized_iters()
+        t0 = time.perf_counter()
+        got = []
+        for f in frames:
+            rc, pkt, st, qp, _ = codec.encode_sized_status(cfg, f, target, qp_min, qp_max, out=out)
+            if rc != 0:
+                raise RuntimeError(f"{name} sized encode failed [{rc}]: {codec.last_error()}")
+            got.append((qp, pkt))
+        el = time.perf_counter() - t0
+        res[name] = {"ms_per_frame": 1e3 * el / len(frames), "qps": [q for q, _ in got],
+                     "probes_per_frame": (L.tc_dev_sized_iters() - i0) / len(frames), "packets": got}
+    r = {"frames": len(frames), "target_bytes": int(target), "qp_range": [qp_min, qp_max],
+         "gpu_ms_per_frame": res["gpu"]["ms_per_frame"], "gpu_probes_per_frame": res["gpu"]["probes_per_frame"],
+         "qps": res["gpu"]["qps"]}
+    if "reference" in res:
+        r["reference_ms_per_frame"] = res["reference"]["ms_per_frame"]
+        r["reference_threads"] = ref_threads
+        r["speedup_vs_reference"] = res["reference"]["ms_per_frame"] / res["gpu"]["ms_per_frame"]
+        r["parity"] = res["gpu"]["packets"] == res["reference"]["packets"] and \
+            res["gpu"]["probes_per_frame"] == res["reference"]["probes_per_frame"]
+    return r
 
 
 def slice_spans(pkt: bytes):
