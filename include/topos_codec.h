@@ -324,6 +324,22 @@ int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, to
  * the choice ("lane" is 8 per warp). All produce identical output. */
 int32_t tcg_dchain_tiling(uint32_t colour_slices);
 
+/* Size-targeted encode of many frames (extension beside tc_frame_encode_sized):
+ * frame i is searched for target_bytes[i] in [qp_min, qp_max] exactly as a
+ * tc_frame_encode_sized call made while another call holds the cross-call qp
+ * hint (an empty hint record), so the results do not depend on frame order.
+ * Up to six searches run side by side on their own contexts (fewer when
+ * their probe windows would take more than 96 GB of device memory), so their
+ * probe launches overlap on the GPU. Per frame: rcs[i] (as the single call
+ * returns), qp_used[i] (may be NULL), stats[i] (may be NULL) and the packet in
+ * outs[i] (NULL = size only, capacity out_caps[i]). Returns the first nonzero
+ * rcs[i], or TC_OK. tc_last_error describes only errors of argument checks
+ * made on the calling thread. */
+int32_t tcg_frame_encode_sized_batch(const topos_frame_config* cfgs, const topos_frame_input* inputs, uint32_t count,
+                                     const uint32_t* target_bytes, uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used,
+                                     uint8_t* const* outs, const size_t* out_caps, topos_frame_stats* stats,
+                                     int32_t* rcs);
+
 /* Batches whose inputs or outputs are in host memory are coded as chunks on
  * separate streams (encode up to four, decode up to three): chunk i's
  * host-to-device copies queue behind chunk i-1's, so the copies of later

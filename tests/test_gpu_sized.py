@@ -96,3 +96,51 @@ def test_sized_buffer_too_small_and_alpha_vs_reference(libs):
     for target in (full, full * 2 // 3, full // 3):
         r = _both(product, reference, cfg, planes, target, 0, 63)
         assert r["rc"] == 0 and r["alpha"] > 0
+
+
+def test_sized_batch_vs_reference_single_calls(libs):
+    """tcg_frame_encode_sized_batch: each frame as the reference's single call
+    with an empty hint record (hint and its model off), whatever the order;
+    searches run side by side on separate contexts."""
+    import ctypes
+    product, reference = libs
+    for c in libs:
+        c._lib.tc_dev_set_sized_mode(0)
+        c._lib.tc_dev_set_qp_hint(1)
+    reference._lib.tc_dev_set_qp_hint_model(1)
+    try:
+        specs = [(256, 128, 5), (640, 360, 6), (192, 96, 7), (256, 128, 8), (640, 360, 9), (96, 64, 10), (320, 192, 11)]
+        cfgs, frames, targets = [], [], []
+        for k, (w, h, seed) in enumerate(specs):
+            cfg, planes = _frame(w, h, seed=seed, qp=4 + 7 * k)
+            full = len(product.encode(cfg, planes))
+            cfgs.append(cfg)
+            frames.append(planes)
+            targets.append([full, full // 2, full * 3, 40][k % 4])
+        n = len(specs)
+        L = product._lib
+        L.tcg_frame_encode_sized_batch.restype = ctypes.c_int32
+        caps = [product.packet_bound(c) for c in cfgs]
+        bufs = [np.empty(c, np.uint8) for c in caps]
+        carr = (B.FrameConfig * n)(*cfgs)
+        iarr = (B.FrameInput * n)(*[product._input(f) for f in frames])
+        tarr = (ctypes.c_uint32 * n)(*targets)
+        qps = (ctypes.c_uint8 * n)()
+        optr = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bufs])
+        ocap = (ctypes.c_size_t * n)(*caps)
+        st = (B.FrameStats * n)()
+        rcs = (ctypes.c_int32 * n)()
+        it0 = L.tc_dev_sized_iters()
+        rc = int(L.tcg_frame_encode_sized_batch(carr, iarr, ctypes.c_uint32(n), tarr, ctypes.c_uint8(0),
+                                                ctypes.c_uint8(63), qps, optr, ocap, st, rcs))
+        iters = L.tc_dev_sized_iters() - it0
+        assert rc == 0 and list(rcs) == [0] * n
+        ri0 = reference._lib.tc_dev_sized_iters()
+        for i in range(n):
+            want = _sized(reference, cfgs[i], frames[i], targets[i], 0, 63)
+            assert want["rc"] == 0 and want["qp"] == qps[i], i
+            assert bufs[i][: st[i].packet_size].tobytes() == want["pkt"], i
+            assert st[i].packet_size == want["size"] and st[i].qp_base == want["qp_base"], i
+        assert iters == reference._lib.tc_dev_sized_iters() - ri0
+    finally:
+        reference._lib.tc_dev_set_qp_hint_model(0)

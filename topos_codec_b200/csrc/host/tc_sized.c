@@ -21,6 +21,7 @@
  * with sizes that fall as qp rises the chosen qp does not depend on it.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdatomic.h>
 #include <stdlib.h>
 #include <string.h>
@@ -38,6 +39,9 @@
 /* probe window: qps encoded per launch, and the device bytes one window may take */
 #define SIZED_WINDOW 17u
 #define SIZED_WINDOW_BYTES (24ull << 30)
+/* batch form: searches side by side, and the device bytes all their windows may take */
+#define SIZED_BATCH_WORKERS 6u
+#define SIZED_BATCH_BYTES (96ull << 30)
 
 /* ------------------------------------------------------------ process state */
 
@@ -97,6 +101,17 @@ TC_EXPORT uint64_t tc_dev_sized_iters(void) { return atomic_load(&g_iters); }
 TC_EXPORT uint64_t tc_dev_sized_calls(void) { return atomic_load(&g_calls); }
 
 static void count_encode(void) { atomic_fetch_add(&g_iters, 1u); }
+
+/* qps per probe launch for a frame with the given packet bound, samples and
+ * colour blocks: device bytes of one probe are the packet, the samples and the
+ * coder's per-block buffers */
+static uint32_t sized_window(size_t cap, uint64_t samples, uint64_t cblocks)
+{
+    const uint64_t per = (uint64_t)cap + samples * 2u + cblocks * 2048u;
+    uint64_t w = SIZED_WINDOW_BYTES / (per > 0u ? per : 1u);
+    w = w < 1u ? 1u : (w > SIZED_WINDOW ? SIZED_WINDOW : w);
+    return (uint32_t)w;
+}
 
 /* --------------------------------------------------------------- size table */
 
@@ -624,10 +639,11 @@ done:
 
 /* ----------------------------------------------------------------- entry */
 
-/* reference: native/src/codec/codec.c:7789-7880 */
-TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const topos_frame_input* input,
-                                        uint32_t target_bytes, uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used,
-                                        uint8_t* out, size_t out_cap, topos_frame_stats* stats)
+/* One size-targeted encode. process_hint: use the process-wide hint record
+ * when it is free (the single call), else an empty one (batch workers). */
+static int32_t sized_one(const topos_frame_config* cfg, const topos_frame_input* input, uint32_t target_bytes,
+                         uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used, uint8_t* out, size_t out_cap,
+                         topos_frame_stats* stats, int process_hint)
 {
     int32_t rc = tc_frame_config_validate(cfg);
     if (rc != TC_OK) { return rc; }
@@ -669,13 +685,7 @@ TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const top
     t->qp_min = qp_min;
     t->qp_max = qp_max;
     t->cap = tc_frame_packet_bound(cfg);
-    {
-        /* device bytes of one probe: packet, samples and the coder's per-block buffers */
-        const uint64_t per = (uint64_t)t->cap + samples * 2u + cblocks * 2048u;
-        uint64_t w = SIZED_WINDOW_BYTES / (per > 0u ? per : 1u);
-        w = w < 1u ? 1u : (w > SIZED_WINDOW ? SIZED_WINDOW : w);
-        t->window = (uint32_t)w;
-    }
+    t->window = sized_window(t->cap, samples, cblocks);
     rc = tcg_sized_open(&base, &t->sess);
     if (rc != TC_OK) {
         free(t);
@@ -686,7 +696,7 @@ TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const top
     sized_hint fresh;
     memset(&fresh, 0, sizeof(fresh));
     int expected = 0;
-    const int borrowed = atomic_compare_exchange_strong(&g_hint_busy, &expected, 1);
+    const int borrowed = process_hint && atomic_compare_exchange_strong(&g_hint_busy, &expected, 1);
     sized_hint* e = borrowed ? &g_hint : &fresh;
 
     probe_log c;
@@ -715,4 +725,96 @@ TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const top
     free(t);
     if (qp_used != NULL) { *qp_used = qu; }
     return rc;
+}
+
+/* reference: native/src/codec/codec.c:7789-7880 */
+TC_EXPORT int32_t tc_frame_encode_sized(const topos_frame_config* cfg, const topos_frame_input* input,
+                                        uint32_t target_bytes, uint8_t qp_min, uint8_t qp_max, uint8_t* qp_used,
+                                        uint8_t* out, size_t out_cap, topos_frame_stats* stats)
+{
+    return sized_one(cfg, input, target_bytes, qp_min, qp_max, qp_used, out, out_cap, stats, 1);
+}
+
+/* ------------------------------------------------------------------ batch */
+
+typedef struct sized_batch {
+    const topos_frame_config* cfgs;
+    const topos_frame_input* inputs;
+    const uint32_t* targets;
+    uint8_t qp_min, qp_max;
+    uint8_t* qp_used;
+    uint8_t* const* outs;
+    const size_t* caps;
+    topos_frame_stats* stats;
+    int32_t* rcs;
+    uint32_t count;
+    atomic_uint next;
+} sized_batch;
+
+static void* sized_worker(void* arg)
+{
+    sized_batch* b = (sized_batch*)arg;
+    for (;;) {
+        const uint32_t i = atomic_fetch_add(&b->next, 1u);
+        if (i >= b->count) { break; }
+        uint8_t q = 0;
+        b->rcs[i] = sized_one(&b->cfgs[i], &b->inputs[i], b->targets[i], b->qp_min, b->qp_max, &q,
+                              b->outs[i], b->outs[i] == NULL ? 0u : b->caps[i],
+                              b->stats != NULL ? &b->stats[i] : NULL, 0);
+        if (b->qp_used != NULL) { b->qp_used[i] = q; }
+    }
+    return NULL;
+}
+
+/* extension: many size-targeted encodes at once. Every frame is searched as a
+ * single call made with an empty cross-call hint record (the reference's
+ * behaviour when its record is held by another call), so results do not
+ * depend on the order of the frames; up to six searches run side by side,
+ * each on its own context, and their probe launches overlap on the GPU. */
+TC_EXPORT int32_t tcg_frame_encode_sized_batch(const topos_frame_config* cfgs, const topos_frame_input* inputs,
+                                               uint32_t count, const uint32_t* target_bytes, uint8_t qp_min,
+                                               uint8_t qp_max, uint8_t* qp_used, uint8_t* const* outs,
+                                               const size_t* out_caps, topos_frame_stats* stats, int32_t* rcs)
+{
+    if (count == 0u) { return TC_OK; }
+    if (cfgs == NULL || inputs == NULL || target_bytes == NULL || outs == NULL || out_caps == NULL || rcs == NULL) {
+        return tc_fail(TC_ERR_INVALID_ARGUMENT, "batch arguments NULL");
+    }
+    if (count > TC_BATCH_MAX_FRAMES) { return tc_fail(TC_ERR_LIMIT_EXCEEDED, "batch count %u", count); }
+    sized_batch b;
+    memset(&b, 0, sizeof(b));
+    b.cfgs = cfgs;
+    b.inputs = inputs;
+    b.targets = target_bytes;
+    b.qp_min = qp_min;
+    b.qp_max = qp_max;
+    b.qp_used = qp_used;
+    b.outs = outs;
+    b.caps = out_caps;
+    b.stats = stats;
+    b.rcs = rcs;
+    b.count = count;
+    atomic_init(&b.next, 0u);
+    /* searches side by side: bounded by the device bytes of their probe windows */
+    uint32_t workers = count < SIZED_BATCH_WORKERS ? count : SIZED_BATCH_WORKERS;
+    {
+        /* the first frame's geometry, counted as four full planes */
+        const size_t cap = tc_frame_packet_bound(&cfgs[0]);
+        const uint64_t px = (uint64_t)cfgs[0].visible_width * cfgs[0].visible_height;
+        const uint64_t samples = px * 4u, cblocks = px / 16u;
+        const uint64_t per = (uint64_t)sized_window(cap, samples, cblocks) * ((uint64_t)cap + samples * 2u + cblocks * 2048u);
+        const uint64_t fit = per > 0u ? SIZED_BATCH_BYTES / per : workers;
+        if (fit < workers) { workers = fit < 1u ? 1u : (uint32_t)fit; }
+    }
+    pthread_t th[SIZED_BATCH_WORKERS];
+    uint32_t started = 0;
+    for (uint32_t w = 1; w < workers; ++w) {
+        if (pthread_create(&th[started], NULL, sized_worker, &b) == 0) { started++; }
+    }
+    sized_worker(&b);
+    for (uint32_t w = 0; w < started; ++w) { pthread_join(th[w], NULL); }
+    for (uint32_t i = 0; i < count; ++i) {
+        if (rcs[i] != TC_OK) { return rcs[i]; }
+    }
+    return TC_OK;
 }
