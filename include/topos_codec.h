@@ -314,6 +314,125 @@ int32_t tcg_server_submit_decode(tcg_server* server, const uint8_t* packet, size
 int32_t tcg_server_wait(tcg_server* server, uint64_t ticket, int32_t* status, topos_frame_stats* stats,
                         topos_frame_output* info, double* latency_ms);
 
+/* ---------------- decode delivery modes and persistent decoder contexts ----------------
+ * Reference: native/include/topos_codec.h:340-380 (scaled and reduced decode),
+ * :425-572 (plane views, requests, surfaces, decoder contexts); behaviour
+ * native/src/codec/codec.c:9100-9376 and 9378-9805, decoder_ctx.c. Types and
+ * layouts are the reference's. A decode request selects the delivered grid:
+ * FULL (source size), SCALED (target_width x target_height, each target
+ * sample the reconstruction at (x * source / target) rounded down), REDUCED
+ * (fixed ratio 1/2, 1/3, 1/4, 1/8: the same sampling of a reconstruction
+ * that keeps the first 24, 16, 10 or 4 zigzag coefficients) or AUTO_2K (the
+ * source when it fits 2048x2048, else the first reduced ratio that does,
+ * or an explicit target). Deblocking runs on the delivered planes: on the
+ * 8-sample grid at full size, on the 4-sample grid for an exact half, not at
+ * all for other scaled grids. DROP_ALPHA skips the alpha slices (reported
+ * OK, unchecked) and delivers three planes. Every pointer may be host or
+ * device memory. Decoder contexts hold no state the result depends on: they
+ * are thin handles over the stateless calls. */
+typedef enum tc_decode_scale {
+    TC_DECODE_SCALE_FULL = 0,
+    TC_DECODE_SCALE_HALF = 1,
+    TC_DECODE_SCALE_THIRD = 2,
+    TC_DECODE_SCALE_QUARTER = 3,
+    TC_DECODE_SCALE_EIGHTH = 4
+} tc_decode_scale;
+
+typedef struct topos_plane_view {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint16_t* pixels;
+    size_t stride;          /* uint16 elements; 0 = tight */
+} topos_plane_view;
+
+enum {
+    TC_DECODE_MEMORY_CPU = 0u,
+    TC_DECODE_MEMORY_HOST_VISIBLE_GPU = 1u
+};
+
+typedef enum topos_decode_mode {
+    TC_DECODE_MODE_FULL = 0u,
+    TC_DECODE_MODE_SCALED = 1u,
+    TC_DECODE_MODE_REDUCED = 2u,
+    TC_DECODE_MODE_AUTO_2K = 3u
+} topos_decode_mode;
+
+typedef enum tc_decode_quality {
+    TC_DECODE_QUALITY_DEFAULT = 0u,
+    TC_DECODE_QUALITY_FAST = 1u,
+    TC_DECODE_QUALITY_BALANCED = 2u,
+    TC_DECODE_QUALITY_HIGH = 3u
+} tc_decode_quality;
+
+typedef struct topos_decode_request {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t mode;          /* topos_decode_mode */
+    uint32_t scale;         /* tc_decode_scale; REDUCED only */
+    uint32_t target_width;  /* SCALED / AUTO_2K; 0 together with height */
+    uint32_t target_height;
+    uint32_t quality;       /* tc_decode_quality; checked and kept */
+    uint32_t memory_type;   /* TC_DECODE_MEMORY_* */
+    uint32_t flags;         /* TC_DECODE_FLAG_* */
+    uint32_t reserved[4];   /* zero */
+} topos_decode_request;
+
+#define TC_DECODE_FLAG_DROP_ALPHA (1u << 0)
+
+typedef struct topos_decode_surface {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t memory_type;
+    uint32_t reserved;
+    topos_plane_view planes[TC_FRAME_MAX_PLANES];
+} topos_decode_surface;
+
+typedef struct topos_decoder_config {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint32_t max_slice_workers; /* kept; the GPU decode has no host worker pool */
+    uint32_t reserved[7];
+} topos_decoder_config;
+
+typedef struct tc_decoder tc_decoder;
+
+/* ceil(source / 1, 2, 3, 4, 8) */
+int32_t tc_decode_scale_dimensions(uint32_t source_width, uint32_t source_height, tc_decode_scale scale,
+                                   uint32_t* target_width, uint32_t* target_height);
+int32_t tc_frame_decode_scaled(const uint8_t* data, size_t size, uint32_t target_width, uint32_t target_height,
+                               uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
+                               const size_t strides[TC_FRAME_MAX_PLANES], topos_frame_output* out_info);
+int32_t tc_frame_decode_reduced(const uint8_t* data, size_t size, tc_decode_scale scale,
+                                uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
+                                const size_t strides[TC_FRAME_MAX_PLANES], topos_frame_output* out_info);
+int32_t tc_frame_decode_batch_reduced(const topos_batch_packet* packets, uint32_t count, tc_decode_scale scale,
+                                      uint16_t* const* planes_out, const size_t* strides, topos_frame_output* infos);
+int32_t tc_frame_decode_request(const uint8_t* data, size_t size, const topos_decode_request* request,
+                                uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
+                                const size_t strides[TC_FRAME_MAX_PLANES], topos_frame_output* out_info);
+
+int32_t tc_decoder_create(const topos_decoder_config* cfg, tc_decoder** out);
+void tc_decoder_destroy(tc_decoder* dec);
+int32_t tc_decoder_set_max_slice_workers(tc_decoder* dec, uint32_t workers);
+int32_t tc_decoder_prepare(tc_decoder* dec, const uint8_t* packet, size_t size, topos_frame_output* info);
+int32_t tc_decoder_prepare_request(tc_decoder* dec, const uint8_t* packet, size_t size,
+                                   const topos_decode_request* request, topos_frame_output* info);
+int32_t tc_decoder_decode(tc_decoder* dec, const uint8_t* packet, size_t size,
+                          const topos_plane_view out[TC_FRAME_MAX_PLANES], topos_frame_output* info);
+int32_t tc_decoder_decode_request(tc_decoder* dec, const uint8_t* packet, size_t size,
+                                  const topos_decode_request* request,
+                                  const topos_plane_view out[TC_FRAME_MAX_PLANES], topos_frame_output* info);
+int32_t tc_decoder_decode_batch(tc_decoder* dec, const topos_batch_packet* packets, uint32_t count,
+                                const topos_plane_view* out, topos_frame_output* infos);
+int32_t tc_decoder_decode_batch_request(tc_decoder* dec, const topos_batch_packet* packets, uint32_t count,
+                                        const topos_decode_request* request, const topos_plane_view* out,
+                                        topos_frame_output* infos);
+int32_t tc_decoder_decode_surface(tc_decoder* dec, const uint8_t* packet, size_t size,
+                                  const topos_decode_surface* surface, topos_frame_output* info);
+int32_t tc_decoder_decode_surface_request(tc_decoder* dec, const uint8_t* packet, size_t size,
+                                          const topos_decode_request* request, const topos_decode_surface* surface,
+                                          topos_frame_output* info);
+
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, one
  * warp per slice (1), or a split (5: the largest slices, half of the blocks,

@@ -16,13 +16,9 @@
 extern "C" {
 #endif
 
-typedef struct tc_decoder tc_decoder;
 typedef struct topos_gop_context topos_gop_context;
 typedef struct topos_mux topos_mux;
 typedef struct topos_movie topos_movie;
-typedef struct topos_plane_view topos_plane_view;
-typedef struct topos_decode_request topos_decode_request;
-typedef struct topos_decode_surface topos_decode_surface;
 typedef struct topos_gop_frame_info topos_gop_frame_info;
 typedef struct topos_movie_config topos_movie_config;
 typedef struct topos_io topos_io;
@@ -79,24 +75,6 @@ void tc_dev_set_sized_m7(int disable);
 void tc_dev_sized_reset(void);
 uint64_t tc_dev_sized_iters(void);
 uint64_t tc_dev_sized_calls(void);
-/* reference: native/include/topos_codec.h:364 (scaled decode) */
-int32_t tc_decode_scale_dimensions(uint32_t source_width, uint32_t source_height, int32_t scale,
-                                   uint32_t* target_width, uint32_t* target_height);
-
-/* reference: native/include/topos_codec.h:516-568 (persistent decoder) */
-void tc_decoder_destroy(tc_decoder* dec);
-int32_t tc_decoder_prepare(tc_decoder* dec, const uint8_t* packet, size_t size, topos_frame_output* info);
-int32_t tc_decoder_prepare_request(tc_decoder* dec, const uint8_t* packet, size_t size,
-                                   const topos_decode_request* request, topos_frame_output* info);
-int32_t tc_decoder_decode(tc_decoder* dec, const uint8_t* packet, size_t size, const topos_plane_view* out,
-                          topos_frame_output* info);
-int32_t tc_decoder_decode_batch_request(tc_decoder* dec, const topos_batch_packet* packets, uint32_t count,
-                                        const topos_decode_request* request, const topos_plane_view* out,
-                                        topos_frame_output* infos);
-int32_t tc_decoder_decode_surface_request(tc_decoder* dec, const uint8_t* packet, size_t size,
-                                          const topos_decode_request* request, const topos_decode_surface* surface,
-                                          topos_frame_output* info);
-
 /* reference: native/include/topos_codec.h:613-646 (GOP / P-frame context) */
 void tc_gop_context_close(topos_gop_context* ctx);
 int32_t tc_gop_context_observe(topos_gop_context* ctx, const uint8_t* data, size_t size, topos_gop_frame_info* info);

@@ -175,7 +175,11 @@ def test_reference_python_binding_loads_this_library(built):
     lib.tc_frame_encode_sized.restype = ctypes.c_int32
     assert lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == B.TC_ERR_INVALID_ARGUMENT
     lib.tc_decode_scale_dimensions.restype = ctypes.c_int32
-    assert lib.tc_decode_scale_dimensions(64, 64, 1, None, None) == B.TC_ERR_NOT_IMPLEMENTED
+    tw, th = ctypes.c_uint32(), ctypes.c_uint32()
+    assert lib.tc_decode_scale_dimensions(3841, 2161, 2, ctypes.byref(tw), ctypes.byref(th)) == 0
+    assert (tw.value, th.value) == (1281, 721)
+    lib.tc_gop_context_observe.restype = ctypes.c_int32
+    assert lib.tc_gop_context_observe(None, None, 0, None) == B.TC_ERR_NOT_IMPLEMENTED
     lib.tc_scalable_status_name.restype = ctypes.c_char_p
     assert lib.tc_scalable_status_name(1) == b"reference" and lib.tc_scalable_status_name(9) == b"unknown"
 
@@ -244,3 +248,58 @@ def test_sized_encode_argument_checks_match_reference(product, reference):
         assert got[0] == got[1] and got[0] < 0, (cfg.reserved[0], lo, hi, got)
     assert product._lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None) == \
         reference._lib.tc_frame_encode_sized(None, None, 0, 0, 0, None, None, 0, None)
+
+
+def _request_cases():
+    """(request, label) pairs: every mode, scale and flag, and the invalid forms."""
+    out = [(B.make_request(0), "full"), (B.make_request(0, flags=1), "full-drop-alpha")]
+    for t in [(1, 1), (17, 9), (64, 48), (10 ** 5, 8), (8, 0)]:
+        out.append((B.make_request(1, target=t), f"scaled {t}"))
+    for sc in range(6):
+        out.append((B.make_request(2, scale=sc), f"reduced {sc}"))
+    out += [(B.make_request(3), "auto2k"), (B.make_request(3, target=(20, 10)), "auto2k target"),
+            (B.make_request(2, scale=1, target=(4, 4)), "reduced with target"),
+            (B.make_request(0, scale=1), "full with scale"), (B.make_request(4), "bad mode"),
+            (B.make_request(0, quality=4), "bad quality"), (B.make_request(0, memory_type=2), "bad memory"),
+            (B.make_request(0, flags=2), "bad flag"), (B.make_request(1, target=(8, 8), quality=3, memory_type=1), "ok")]
+    bad = B.make_request(0)
+    bad.reserved[2] = 1
+    out.append((bad, "reserved"))
+    bad = B.make_request(0)
+    bad.struct_size = 8
+    out.append((bad, "struct size"))
+    return out
+
+
+def test_decode_request_query_matches_reference(product, reference):
+    """tc_frame_decode_request and tc_decoder_prepare_request in query mode
+    (no output planes): status and frame information equal the reference
+    library's for every mode, scale, flag and invalid request on the fixture
+    packets (4:2:2, 4:4:4 + alpha, 1x1)."""
+    names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    for lib in (product._lib, reference._lib):
+        lib.tc_frame_decode_request.restype = ctypes.c_int32
+        lib.tc_decoder_prepare_request.restype = ctypes.c_int32
+        lib.tc_decoder_create.restype = ctypes.c_int32
+    decs = []
+    for lib in (product._lib, reference._lib):
+        d = ctypes.c_void_p()
+        assert lib.tc_decoder_create(None, ctypes.byref(d)) == 0
+        decs.append(d)
+    try:
+        for name in names:
+            pkt = bytes(np.load(os.path.join(GOLDEN, name + ".npz"))["packet"])
+            buf = np.frombuffer(pkt, np.uint8)
+            for req, label in _request_cases():
+                got = []
+                for lib, d in zip((product._lib, reference._lib), decs):
+                    a, b = B.FrameOutput(), B.FrameOutput()
+                    ra = int(lib.tc_frame_decode_request(ctypes.c_void_p(buf.ctypes.data), ctypes.c_size_t(len(pkt)),
+                                                         ctypes.byref(req), None, None, ctypes.byref(a)))
+                    rb = int(lib.tc_decoder_prepare_request(d, ctypes.c_void_p(buf.ctypes.data), ctypes.c_size_t(len(pkt)),
+                                                            ctypes.byref(req), ctypes.byref(b)))
+                    got.append((ra, bytes(a) if ra == 0 else None, rb, bytes(b) if rb == 0 else None))
+                assert got[0] == got[1], (name, label, got[0][0], got[1][0], got[0][2], got[1][2])
+    finally:
+        product._lib.tc_decoder_destroy(decs[0])
+        reference._lib.tc_decoder_destroy(decs[1])

@@ -355,6 +355,41 @@ class ToposCodec:
         return rc, frames
 
 
+class DecodeRequest(ctypes.Structure):
+    """topos_decode_request (reference native/include/topos_codec.h:465-476)."""
+    _fields_ = [("struct_size", ctypes.c_uint32), ("abi_version", ctypes.c_uint32), ("mode", ctypes.c_uint32),
+                ("scale", ctypes.c_uint32), ("target_width", ctypes.c_uint32), ("target_height", ctypes.c_uint32),
+                ("quality", ctypes.c_uint32), ("memory_type", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 4)]
+
+
+def make_request(mode: int = 0, scale: int = 0, target=(0, 0), flags: int = 0, quality: int = 0,
+                 memory_type: int = 0) -> DecodeRequest:
+    r = DecodeRequest()
+    r.struct_size, r.abi_version = ctypes.sizeof(DecodeRequest), TOPOS_CODEC_ABI_VERSION
+    r.mode, r.scale, r.quality, r.memory_type, r.flags = mode, scale, quality, memory_type, flags
+    r.target_width, r.target_height = target
+    return r
+
+
+def decode_request(codec: "ToposCodec", packet: bytes, req: DecodeRequest, fill: int = 0) -> "DecodedFrame":
+    """tc_frame_decode_request into host planes sized from its own query."""
+    L = codec._lib
+    L.tc_frame_decode_request.restype = ctypes.c_int32
+    buf = np.frombuffer(packet, dtype=np.uint8)
+    info = FrameOutput()
+    rc = int(L.tc_frame_decode_request(ctypes.c_void_p(buf.ctypes.data if len(packet) else 0), ctypes.c_size_t(len(packet)),
+                                       ctypes.byref(req), None, None, ctypes.byref(info)))
+    if rc != TC_OK:
+        return DecodedFrame([], info, rc)
+    planes = [np.full(s, fill, dtype=np.uint16) for s in ToposCodec.geometry(info)]
+    ptrs = (ctypes.c_void_p * TC_FRAME_MAX_PLANES)(*[p.ctypes.data for p in planes])
+    info = FrameOutput()
+    rc = int(L.tc_frame_decode_request(ctypes.c_void_p(buf.ctypes.data), ctypes.c_size_t(len(packet)), ctypes.byref(req),
+                                       ptrs, None, ctypes.byref(info)))
+    return DecodedFrame(planes, info, rc)
+
+
 class Server:
     """Continuous-batching request server of the library (tcg_server_*).
 

@@ -56,6 +56,9 @@ struct DPlane {
     uint32_t bd, kind, alpha_shift, refined;
     uint32_t blk0;
     uint32_t frame;
+    uint32_t climit;    // highest zigzag position kept (63 = all)
+    uint64_t dst_off;   // delivered plane (the reconstruction itself unless scaled)
+    uint32_t dst_w, dst_h;
     uint16_t qm[64];
 };
 
@@ -834,13 +837,15 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
     const int64_t fc = P.bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (P.bd - 1u)) - 1u)) / 2047;
     int32_t c[64], xh[64];
     const int4* src = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
+    const uint32_t climit = P.climit;  // reduced delivery drops the high zigzag positions
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         const int4 v = src[i];
         const int32_t vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
+            int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
+            lv = (uint32_t)(i * 4 + j) <= climit ? lv : 0;
             const int nat = k_zigzag[i * 4 + j];
             int64_t f = (int64_t)lv * __ldg(Q + nat);
             f = f > fc ? fc : (f < -fc ? -fc : f);
@@ -875,6 +880,26 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
             }
         }
     }
+}
+
+// Scaled delivery (reference color_store.h:223-313 scaled samples,
+// codec.c:7955-7964 alpha, 7987-8000 concealment): target sample (x, y) of a
+// plane is the reconstruction at (x * vis_w / dst_w, y * vis_h / dst_h),
+// rounded down. One thread per target sample; grid.y = plane.
+struct DecimPlane {
+    uint64_t src_off, dst_off;
+    uint32_t vis_w, vis_h, dst_w, dst_h;
+};
+
+__global__ void __launch_bounds__(256) k_decimate(const DecimPlane* __restrict__ dp, uint16_t* __restrict__ out)
+{
+    const DecimPlane P = dp[blockIdx.y];
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)P.dst_w * P.dst_h) { return; }
+    const uint32_t ty = (uint32_t)(i / P.dst_w), tx = (uint32_t)(i % P.dst_w);
+    const uint32_t sx = (uint32_t)(((uint64_t)tx * P.vis_w) / P.dst_w);
+    const uint32_t sy = (uint32_t)(((uint64_t)ty * P.vis_h) / P.dst_h);
+    out[P.dst_off + i] = out[P.src_off + (uint64_t)sy * P.vis_w + sx];
 }
 
 // ------------------------------------------------------------------ alpha
@@ -1030,6 +1055,7 @@ __global__ void __launch_bounds__(256) k_dconceal(const DSlice* __restrict__ sli
 struct DbPlane {
     uint64_t off;
     uint32_t w, h, alpha, beta, clip, maxv;
+    uint32_t unit;      // edge grid: 8 at full size, 4 on an exact half
 };
 
 __device__ __forceinline__ bool db_gate(int32_t p1, int32_t p0, int32_t q0, int32_t q1, int32_t a, int32_t b)
@@ -1061,10 +1087,10 @@ __device__ __forceinline__ void db_apply(uint16_t* a, uint16_t* b, uint16_t* c, 
 __global__ void k_deblock_v(const DbPlane* __restrict__ dp, uint32_t np, uint16_t* __restrict__ out)
 {
     const DbPlane P = dp[blockIdx.y];
-    const uint32_t edges = P.w / 8u - 1u;
+    const uint32_t edges = P.w / P.unit - 1u;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (uint64_t)edges * P.h) { return; }
-    const uint32_t y = (uint32_t)(i / edges), x0 = 8u * (uint32_t)(i % edges + 1u);
+    const uint32_t y = (uint32_t)(i / edges), x0 = P.unit * (uint32_t)(i % edges + 1u);
     uint16_t* r = out + P.off + (size_t)y * P.w;
     const int32_t p1 = r[x0 - 2], p0 = r[x0 - 1], q0 = r[x0], q1 = r[x0 + 1];
     if (db_gate(p1, p0, q0, q1, (int32_t)P.alpha, (int32_t)P.beta)) {
@@ -1078,11 +1104,11 @@ __global__ void k_deblock_v(const DbPlane* __restrict__ dp, uint32_t np, uint16_
 __global__ void k_deblock_h(const DbPlane* __restrict__ dp, uint32_t np, uint16_t* __restrict__ out)
 {
     const DbPlane P = dp[blockIdx.y];
-    const uint32_t edges = P.h / 8u - 1u;
+    const uint32_t edges = P.h / P.unit - 1u;
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (uint64_t)edges * P.w) { return; }
     const uint32_t r = (uint32_t)(i / P.w) + 1u, x = (uint32_t)(i % P.w);
-    const uint32_t y0 = 8u * r;
+    const uint32_t y0 = P.unit * r;
     uint16_t* b = out + P.off + x;
     uint16_t* a2 = b + (size_t)(y0 - 2u) * P.w;
     uint16_t* a1 = b + (size_t)(y0 - 1u) * P.w;
@@ -1166,7 +1192,8 @@ extern "C" __attribute__((visibility("default"))) int32_t tcg_dchain_tiling(uint
 
 // What decode_outputs and decode_finish need of a launched batch.
 struct DecPending {
-    std::vector<uint32_t> frame_slice0;  // first slice index of each frame
+    std::vector<uint32_t> frame_slice0;  // each frame's first entry in slice_map
+    std::vector<int32_t> slice_map;      // device slice of every packet slice (-1: not decoded)
     std::vector<DPlane> planes;          // output offsets and sizes, frames in order
     uint32_t ns = 0;                     // slices
 };
@@ -1181,16 +1208,18 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     std::vector<uint32_t>& frame_slice0 = pend.frame_slice0;
     std::vector<DPlane>& planes = pend.planes;
     planes.clear();
+    pend.slice_map.clear();
     std::vector<DSlice> slices;
     std::vector<uint32_t> cslices, aslices, slice_tab;
     std::vector<DbPlane> dbp;
+    std::vector<DecimPlane> decim;
     std::vector<uint64_t> pkt_off(count, 0);
     frame_slice0.assign(count, 0u);
     uint64_t out_elems = 0, pkt_bytes = 0, nblk = 0, alpha_res = 0;
     uint32_t max_cols = 1;
     for (uint32_t f = 0; f < count; ++f) {
         const tcg_dec_frame& F = frames[f];
-        frame_slice0[f] = (uint32_t)slices.size();
+        frame_slice0[f] = (uint32_t)pend.slice_map.size();
         if (F.skip) { continue; }
         pkt_off[f] = pkt_bytes;
         pkt_bytes = align_up(pkt_bytes + F.size, 256);
@@ -1208,25 +1237,46 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
             P.refined = F.refined;
             P.blk0 = (uint32_t)nblk;
             P.frame = f;
+            P.climit = F.climit;
             memcpy(P.qm, F.qm[p], sizeof(P.qm));
+            if (F.scaled) {
+                // the delivered plane follows its reconstruction in the same buffer
+                P.dst_off = out_elems;
+                P.dst_w = F.dst_w[p];
+                P.dst_h = F.dst_h[p];
+                out_elems = align_up(out_elems + (uint64_t)P.dst_w * P.dst_h, 64);
+                DecimPlane dm = {P.out_off, P.dst_off, P.vis_w, P.vis_h, P.dst_w, P.dst_h};
+                if (P.dst_w > 0u && P.dst_h > 0u) { decim.push_back(dm); }
+            } else {
+                P.dst_off = P.out_off;
+                P.dst_w = P.vis_w;
+                P.dst_h = P.vis_h;
+            }
             if (P.kind == TCG_PLANE_COLOR) { nblk += (uint64_t)P.cols * P.rows; }
             max_cols = P.cols > max_cols ? P.cols : max_cols;
             planes.push_back(P);
-            if (F.deblock && p < 3u) {
-                const uint32_t w = P.vis_w, h = P.vis_h;
-                if (w >= 16u && h >= 16u && (w % 8u) == 0u && (h % 8u) == 0u && F.qp_base <= 95u) {
+            const uint32_t u = F.db_unit;
+            if (u != 0u && p < 3u) {
+                // deblocking of the delivered plane (reference deblock.c:305-329)
+                const uint32_t w = P.dst_w, h = P.dst_h;
+                if (w >= 2u * u && h >= 2u * u && (w % u) == 0u && (h % u) == 0u && F.qp_base <= 95u) {
                     const uint32_t sc = host_qp_scale(F.refined, F.qp_base);
                     uint32_t step = (sc * 3u + 173056u / 2u) / 173056u;
                     step = step < 1u ? 1u : step;
                     uint32_t a = step * 2u;
                     a = a < 3u ? 3u : (a > 48u ? 48u : a);
-                    DbPlane d = {P.out_off, w, h, a, a / 2u + 2u, a >> 1, (1u << F.bit_depth) - 1u};
+                    DbPlane d = {P.dst_off, w, h, a, a / 2u + 2u, a >> 1, (1u << F.bit_depth) - 1u, u};
                     dbp.push_back(d);
                 }
             }
         }
         for (uint32_t i = 0; i < F.slices; ++i) {
             const tcg_dec_slice& I = F.slice[i];
+            if (I.plane >= F.planes) {  // a plane not delivered (dropped alpha)
+                pend.slice_map.push_back(-1);
+                continue;
+            }
+            pend.slice_map.push_back((int32_t)slices.size());
             DSlice S;
             memset(&S, 0, sizeof(S));
             const DPlane& P = planes[pg0 + I.plane];
@@ -1253,7 +1303,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const size_t desc = align_up(planes.size() * sizeof(DPlane), 256) + align_up(ns * sizeof(DSlice), 256) +
                         align_up((size_t)(nc + na) * 4u + 16, 256) + align_up((size_t)ns * 4u + 16, 256) +
                         align_up(dbp.size() * sizeof(DbPlane) + 16, 256) +
-                        align_up((size_t)nc * 4u + 16, 256);
+                        align_up((size_t)nc * 4u + 16, 256) + align_up(decim.size() * sizeof(DecimPlane) + 16, 256);
     if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
         !dreserve(C, B_DEC_TAB, (size_t)nc * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
         !dreserve(C, B_DEC_RES, (size_t)ns * 4u + 256) || !dreserve(C, B_ALPHA, alpha_res * 4u + 256) ||
@@ -1281,6 +1331,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const size_t o_st = put(slice_tab.data(), slice_tab.size() * 4u);
     const size_t o_db = put(dbp.data(), dbp.size() * sizeof(DbPlane));
     const size_t o_or = put(ord.data(), ord.size() * 4u);
+    const size_t o_dm = put(decim.data(), decim.size() * sizeof(DecimPlane));
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
     const DPlane* d_pl = (const DPlane*)(dd + o_pl);
     const DSlice* d_sl = (const DSlice*)(dd + o_sl);
@@ -1289,6 +1340,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const uint32_t* d_st = (const uint32_t*)(dd + o_st);
     const DbPlane* d_db = (const DbPlane*)(dd + o_db);
     const uint32_t* d_ord = (const uint32_t*)(dd + o_or);
+    const DecimPlane* d_dm = (const DecimPlane*)(dd + o_dm);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
     call_begin(C);
     if (after != nullptr) { TCG_CHECK(cudaStreamWaitEvent(st, after, 0)); }
@@ -1447,11 +1499,17 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     if (ns > 0) {
         TCG_LAUNCH(C, K_DCONCEAL, k_dconceal, ns, 256, 0, d_sl, d_pl, d_status, d_out);
     }
+    if (!decim.empty()) {
+        uint64_t mt = 0;
+        for (const DecimPlane& d : decim) { mt = std::max<uint64_t>(mt, (uint64_t)d.dst_w * d.dst_h); }
+        TCG_LAUNCH(C, K_DECIMATE, k_decimate, dim3((uint32_t)((mt + 255u) / 256u), (uint32_t)decim.size()), 256, 0,
+                   d_dm, d_out);
+    }
     if (!dbp.empty()) {
         uint64_t mv = 0, mh = 0;
         for (const DbPlane& d : dbp) {
-            mv = std::max<uint64_t>(mv, (uint64_t)(d.w / 8u - 1u) * d.h);
-            mh = std::max<uint64_t>(mh, (uint64_t)(d.h / 8u - 1u) * d.w);
+            mv = std::max<uint64_t>(mv, (uint64_t)(d.w / d.unit - 1u) * d.h);
+            mh = std::max<uint64_t>(mh, (uint64_t)(d.h / d.unit - 1u) * d.w);
         }
         TCG_LAUNCH(C, K_DEBLOCK_V, k_deblock_v, dim3((uint32_t)((mv + 255u) / 256u), (uint32_t)dbp.size()), 256, 0,
                    d_db, (uint32_t)dbp.size(), d_out);
@@ -1477,12 +1535,13 @@ static int32_t decode_outputs(Ctx* C, const tcg_dec_frame* frames, const DecPend
         if (F.skip) { continue; }
         for (uint32_t p = 0; p < F.planes; ++p, ++pg) {
             const DPlane& P = planes[pg];
-            const size_t pitch = (F.dst_stride[p] ? F.dst_stride[p] : P.vis_w) * 2u;
-            if (pitch == (size_t)P.vis_w * 2u) {  // tight rows: one flat copy
-                TCG_CHECK(cudaMemcpyAsync(F.dst[p], d_out + P.out_off, pitch * P.vis_h, cudaMemcpyDefault, st));
+            if (P.dst_w == 0u || P.dst_h == 0u) { continue; }
+            const size_t pitch = (F.dst_stride[p] ? F.dst_stride[p] : P.dst_w) * 2u;
+            if (pitch == (size_t)P.dst_w * 2u) {  // tight rows: one flat copy
+                TCG_CHECK(cudaMemcpyAsync(F.dst[p], d_out + P.dst_off, pitch * P.dst_h, cudaMemcpyDefault, st));
             } else {
-                TCG_CHECK(cudaMemcpy2DAsync(F.dst[p], pitch, d_out + P.out_off, (size_t)P.vis_w * 2u,
-                                            (size_t)P.vis_w * 2u, P.vis_h, cudaMemcpyDefault, st));
+                TCG_CHECK(cudaMemcpy2DAsync(F.dst[p], pitch, d_out + P.dst_off, (size_t)P.dst_w * 2u,
+                                            (size_t)P.dst_w * 2u, P.dst_h, cudaMemcpyDefault, st));
             }
         }
     }
@@ -1503,7 +1562,10 @@ static int32_t decode_finish(Ctx* C, const tcg_dec_frame* frames, const DecPendi
     for (uint32_t f = 0; f < (uint32_t)frame_slice0.size(); ++f) {
         const tcg_dec_frame& F = frames[f];
         if (F.skip) { continue; }
-        for (uint32_t i = 0; i < F.slices; ++i) { F.slice_status[i] = hs[frame_slice0[f] + i] != 0 ? 1u : 0u; }
+        for (uint32_t i = 0; i < F.slices; ++i) {
+            const int32_t k = pend.slice_map[frame_slice0[f] + i];
+            F.slice_status[i] = (k >= 0 && hs[k] != 0) ? 1u : 0u;
+        }
     }
     return 0;
 }

@@ -23,7 +23,7 @@ static thread_local double t_last_ms = 0.0;
 static const char* k_names[K_COUNT] = {
     "k_fdct", "k_tokens", "k_select", "k_opscan", "k_opgen", "k_chain", "k_alpha", "k_pack_sizes", "k_pack_copy",
     "k_pack_crc", "k_pack_header", "k_dcrc", "k_dtables", "k_dchain", "k_dchain_w", "k_didct", "k_dalpha", "k_dalpha_med",
-    "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk"};
+    "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk", "k_decimate"};
 
 void note_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 

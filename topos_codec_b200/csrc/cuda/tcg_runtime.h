@@ -45,7 +45,7 @@ enum BufId {
 enum KernelId {
     K_FDCT, K_TOKENS, K_SELECT, K_OPSCAN, K_OPGEN, K_CHAIN, K_ALPHA, K_PACK_SIZES, K_PACK_COPY, K_PACK_CRC,
     K_PACK_HEADER, K_DCRC, K_DTABLES, K_DCHAIN, K_DCHAIN_W, K_DIDCT, K_DALPHA, K_DALPHA_MED, K_DCONCEAL, K_DEBLOCK_V,
-    K_DEBLOCK_H, K_WALK, K_COUNT
+    K_DEBLOCK_H, K_WALK, K_DECIMATE, K_COUNT
 };
 
 constexpr int MAX_PROF = 64;

@@ -418,19 +418,51 @@ static int32_t parse_packets(const topos_batch_packet* pk, uint32_t n, tc_view* 
     return rc;
 }
 
+void tc_plan_full(tc_dec_plan* p)
+{
+    memset(p, 0, sizeof(*p));
+    p->climit = 63u;
+}
+
+/* reference: codec.c:9366-9376 (tc_apply_decode_plan_info) */
+void tc_apply_plan_info(const tc_dec_plan* plan, const tc_hdr* h, topos_frame_output* o)
+{
+    if (plan->tw != 0u) {  /* a resolved target, the source size included: coded = delivered */
+        o->visible_width = (uint16_t)plan->tw;
+        o->visible_height = (uint16_t)plan->th;
+        o->coded_width = (uint16_t)plan->tw;
+        o->coded_height = (uint16_t)plan->th;
+    }
+    if (plan->drop_alpha && o->alpha_mode != 0u && o->plane_count >= 4u) {
+        o->plane_count = 3u;
+        o->alpha_mode = 0u;
+        o->alpha_bit_depth = 0u;
+    }
+    (void)h;
+}
+
 static int32_t build_decode(const tc_view* v, const uint8_t* data, uint16_t* const* planes_out, const size_t* strides,
-                            tcg_dec_frame* jf, tcg_dec_slice* sl, topos_frame_output* o)
+                            const tc_dec_plan* plan, tcg_dec_frame* jf, tcg_dec_slice* sl, topos_frame_output* o)
 {
     const tc_hdr* h = &v->h;
     memset(jf, 0, sizeof(*jf));
-    for (uint32_t p = 0; p < h->planes; ++p) {
+    const uint32_t np = (plan->drop_alpha && h->amode != 0u && h->planes >= 4u) ? 3u : h->planes;
+    for (uint32_t p = 0; p < np; ++p) {
         if (planes_out[p] == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "planes_out[%u] == NULL", p); }
+        uint32_t dw = h->pvw[p], dh = h->pvh[p];
+        if (plan->scaled) {
+            const int c422 = h->pf == 0u && (p == 1u || p == 2u);
+            dw = c422 ? (plan->tw + 1u) / 2u : plan->tw;
+            dh = plan->th;
+        }
         const size_t s = strides != NULL ? strides[p] : 0u;
-        if (s != 0u && s < (size_t)h->pvw[p]) {
-            return tc_fail(TC_ERR_INVALID_ARGUMENT, "plane %u stride %zu < visible width %u", p, s, h->pvw[p]);
+        if (s != 0u && s < (size_t)dw) {
+            return tc_fail(TC_ERR_INVALID_ARGUMENT, "plane %u stride %zu < visible width %u", p, s, dw);
         }
         jf->dst[p] = planes_out[p];
         jf->dst_stride[p] = s;
+        jf->dst_w[p] = dw;
+        jf->dst_h[p] = dh;
         jf->vis_w[p] = h->pvw[p]; jf->vis_h[p] = h->pvh[p]; jf->coded_w[p] = h->pcw[p];
         jf->cols[p] = h->bcols[p]; jf->rows[p] = h->brows[p];
         const int chroma = h->pf != 3u && (p == 1u || p == 2u);
@@ -438,7 +470,13 @@ static int32_t build_decode(const tc_view* v, const uint8_t* data, uint16_t* con
     }
     jf->packet = data;
     jf->size = h->size;
-    jf->planes = h->planes;
+    jf->planes = np;
+    jf->climit = plan->climit;
+    jf->scaled = plan->scaled;
+    /* deblocking grid of the delivered planes (reference codec.c:8649-8660) */
+    jf->db_unit = (h->flags & 0x4u) == 0u ? 0u
+                  : !plan->scaled ? 8u
+                  : (plan->tw * 2u == h->vw && plan->th * 2u == h->vh) ? 4u : 0u;
     jf->bit_depth = h->bd;
     jf->alpha_mode = h->amode;
     jf->alpha_shift = h->amode == 2u ? 16u - h->abd : 0u;
@@ -501,7 +539,9 @@ TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* co
     }
     tcg_dec_frame jf;
     tcg_dec_slice sl[TC_MAX_SLICE_COUNT];
-    rc = build_decode(v, data, planes_out, strides, &jf, sl, o);
+    tc_dec_plan full;
+    tc_plan_full(&full);
+    rc = build_decode(v, data, planes_out, strides, &full, &jf, sl, o);
     if (rc == TC_OK) { rc = tcg_decode(&jf, 1u); }
     if (rc == TC_OK) { rc = finish_frame(&v->h, o); }
     free(v);
@@ -568,9 +608,10 @@ TC_EXPORT int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packet
     return TC_OK;
 }
 
-/* reference: native/src/codec/codec.c:9639-9805 */
-TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
-                                        const size_t* strides, topos_frame_output* infos)
+/* reference: native/src/codec/codec.c:9639-9789 (tc_frame_decode_batch_mode),
+ * decoder_ctx.c:652-760 (its plan-resolving form) */
+int32_t tc_decode_batch_mode(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
+                             const size_t* strides, topos_frame_output* infos, tc_plan_fn fn, const void* ctx)
 {
     if (count == 0u) { return TC_OK; }
     if (count > TC_BATCH_MAX_FRAMES) { return tc_fail(TC_ERR_LIMIT_EXCEEDED, "batch count %u > %u", count, TC_BATCH_MAX_FRAMES); }
@@ -586,33 +627,46 @@ TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint3
         if (rc != TC_OK) { free(v); return rc; }
     }
     int32_t* frc = (int32_t*)calloc(count, sizeof(int32_t));
-    tcg_dec_frame* jf = (tcg_dec_frame*)calloc(count, sizeof(tcg_dec_frame));
-    tcg_dec_slice* sl = (tcg_dec_slice*)calloc((size_t)count * TC_MAX_SLICE_COUNT, sizeof(tcg_dec_slice));
-    if (frc == NULL || jf == NULL || sl == NULL) {
-        free(v); free(frc); free(jf); free(sl);
+    tc_dec_plan* plans = (tc_dec_plan*)calloc(count, sizeof(tc_dec_plan));
+    tcg_dec_frame* jf = planes_out != NULL ? (tcg_dec_frame*)calloc(count, sizeof(tcg_dec_frame)) : NULL;
+    tcg_dec_slice* sl = planes_out != NULL
+        ? (tcg_dec_slice*)calloc((size_t)count * TC_MAX_SLICE_COUNT, sizeof(tcg_dec_slice)) : NULL;
+    if (frc == NULL || plans == NULL || (planes_out != NULL && (jf == NULL || sl == NULL))) {
+        free(v); free(frc); free(plans); free(jf); free(sl);
         return tc_fail(TC_ERR_OUT_OF_MEMORY, "decode batch staging");
     }
-    for (uint32_t i = 0; i < count; ++i) {
+    int32_t call = TC_OK;
+    for (uint32_t i = 0; i < count && call == TC_OK; ++i) {
         topos_frame_output* o = &infos[i];
         memset(o, 0, sizeof(*o));
         o->struct_size = (uint32_t)sizeof(topos_frame_output);
         o->abi_version = TOPOS_CODEC_ABI_VERSION;
         tc_fill_info(&v[i].h, o);
-        if (planes_out == NULL) { continue; }
-        if (v[i].h.major == 7u && v[i].h.em == 8u && v[i].h.ftype != 0u) {
-            free(v); free(frc); free(jf); free(sl);
-            return tc_fail(TC_ERR_STATE, "v7r3 P-frame decode requires a GOP context (stateless entry is I-only)");
+        if (planes_out != NULL && v[i].h.major == 7u && v[i].h.em == 8u && v[i].h.ftype != 0u) {
+            call = tc_fail(TC_ERR_STATE, "v7r3 P-frame decode requires a GOP context (stateless entry is I-only)");
+            break;
         }
-        for (uint32_t p = 0; p < v[i].h.planes; ++p) {
+        tc_plan_full(&plans[i]);
+        if (fn != NULL) {
+            const int32_t prc = fn(ctx, &v[i].h, &plans[i]);
+            if (prc != TC_OK) {
+                if (planes_out == NULL) { call = prc; break; }
+                frc[i] = prc;
+                continue;
+            }
+        }
+        tc_apply_plan_info(&plans[i], &v[i].h, o);
+        if (planes_out == NULL) { continue; }
+        for (uint32_t p = 0; p < o->plane_count; ++p) {
             if (planes_out[(size_t)i * 4u + p] == NULL) {
                 frc[i] = tc_fail(TC_ERR_INVALID_ARGUMENT, "frame %u planes_out[%u] == NULL", i, p);
                 break;
             }
         }
     }
-    if (planes_out == NULL) {
-        free(v); free(frc); free(jf); free(sl);
-        return TC_OK;
+    if (call != TC_OK || planes_out == NULL) {
+        free(v); free(frc); free(plans); free(jf); free(sl);
+        return call;
     }
     for (uint32_t i = 0; i < count; ++i) {
         jf[i].skip = 1;
@@ -622,18 +676,25 @@ TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint3
             continue;
         }
         frc[i] = build_decode(&v[i], packets[i].data, planes_out + (size_t)i * 4u,
-                              strides != NULL ? strides + (size_t)i * 4u : NULL, &jf[i],
+                              strides != NULL ? strides + (size_t)i * 4u : NULL, &plans[i], &jf[i],
                               sl + (size_t)i * TC_MAX_SLICE_COUNT, &infos[i]);
         jf[i].skip = frc[i] != TC_OK;
     }
-    int32_t call = tcg_decode(jf, count);
+    call = tcg_decode(jf, count);
     int32_t first = TC_OK;
     for (uint32_t i = 0; i < count; ++i) {
         if (frc[i] == TC_OK) { frc[i] = call != TC_OK ? call : finish_frame(&v[i].h, &infos[i]); }
         if (first == TC_OK) { first = frc[i]; }
     }
-    free(v); free(frc); free(jf); free(sl);
+    free(v); free(frc); free(plans); free(jf); free(sl);
     return first;
+}
+
+/* reference: native/src/codec/codec.c:9791-9805 */
+TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
+                                        const size_t* strides, topos_frame_output* infos)
+{
+    return tc_decode_batch_mode(packets, count, planes_out, strides, infos, NULL, NULL);
 }
 
 /* ============================== device control ============================== */

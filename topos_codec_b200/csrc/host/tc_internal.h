@@ -89,6 +89,26 @@ int32_t tc_parse_structure(const uint8_t* d, size_t n, tc_view* v);
 int32_t tc_parse_compact(const uint8_t* rec, size_t n, tc_view* v);
 void tc_fill_info(const tc_hdr* h, topos_frame_output* o);
 
+/* Delivered grid of a decoded frame (reference codec.c:8560-8640, 8700-8745):
+ * full size, or scaled to tw x th (4:2:2 chroma ceil(tw/2)) from a
+ * reconstruction keeping zigzag positions <= climit; drop_alpha delivers
+ * three planes and leaves the alpha slices undecoded. A nonzero tw also
+ * reports tw x th as both the visible and the coded size of the frame, as a
+ * resolved request does even at full size. */
+typedef struct tc_dec_plan {
+    uint32_t scaled, tw, th, climit, drop_alpha;
+} tc_dec_plan;
+/* a frame's plan from its header: TC_OK or the frame's status */
+typedef int32_t (*tc_plan_fn)(const void* ctx, const tc_hdr* h, tc_dec_plan* plan);
+void tc_plan_full(tc_dec_plan* p);
+void tc_apply_plan_info(const tc_dec_plan* plan, const tc_hdr* h, topos_frame_output* o);
+/* The batch decode of tc_frame_decode_batch with a plan per frame (fn NULL =
+ * full size): a packet failing its structural parse fails the call; a plan
+ * that cannot be resolved fails the call in query mode (planes_out NULL) and
+ * only its frame otherwise; returns the first nonzero frame status. */
+int32_t tc_decode_batch_mode(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
+                             const size_t* strides, topos_frame_output* infos, tc_plan_fn fn, const void* ctx);
+
 /* encode job of one frame (validation as tc_frame_encode), its stats and the
  * public status of a per-frame result (tc_api.c) */
 struct tcg_enc_frame;

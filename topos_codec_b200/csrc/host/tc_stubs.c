@@ -39,51 +39,6 @@ TC_EXPORT void tc_dev_symbol_pair_hist_get(uint32_t plane, uint64_t* pair_hist)
     if (pair_hist != NULL) { memset(pair_hist, 0, 64u * 28u * sizeof(uint64_t)); }
 }
 
-TC_EXPORT int32_t tc_decode_scale_dimensions(uint32_t source_width, uint32_t source_height, int32_t scale,
-                                             uint32_t* target_width, uint32_t* target_height)
-{
-    (void)source_width; (void)source_height; (void)scale; (void)target_width; (void)target_height;
-    return NOT_PATH("tc_decode_scale_dimensions");
-}
-
-TC_EXPORT void tc_decoder_destroy(tc_decoder* dec) { (void)dec; }
-
-TC_EXPORT int32_t tc_decoder_prepare(tc_decoder* dec, const uint8_t* packet, size_t size, topos_frame_output* info)
-{
-    (void)dec; (void)packet; (void)size; (void)info;
-    return NOT_PATH("tc_decoder_prepare");
-}
-
-TC_EXPORT int32_t tc_decoder_prepare_request(tc_decoder* dec, const uint8_t* packet, size_t size,
-                                             const topos_decode_request* request, topos_frame_output* info)
-{
-    (void)dec; (void)packet; (void)size; (void)request; (void)info;
-    return NOT_PATH("tc_decoder_prepare_request");
-}
-
-TC_EXPORT int32_t tc_decoder_decode(tc_decoder* dec, const uint8_t* packet, size_t size, const topos_plane_view* out,
-                                    topos_frame_output* info)
-{
-    (void)dec; (void)packet; (void)size; (void)out; (void)info;
-    return NOT_PATH("tc_decoder_decode");
-}
-
-TC_EXPORT int32_t tc_decoder_decode_batch_request(tc_decoder* dec, const topos_batch_packet* packets, uint32_t count,
-                                                  const topos_decode_request* request, const topos_plane_view* out,
-                                                  topos_frame_output* infos)
-{
-    (void)dec; (void)packets; (void)count; (void)request; (void)out; (void)infos;
-    return NOT_PATH("tc_decoder_decode_batch_request");
-}
-
-TC_EXPORT int32_t tc_decoder_decode_surface_request(tc_decoder* dec, const uint8_t* packet, size_t size,
-                                                    const topos_decode_request* request,
-                                                    const topos_decode_surface* surface, topos_frame_output* info)
-{
-    (void)dec; (void)packet; (void)size; (void)request; (void)surface; (void)info;
-    return NOT_PATH("tc_decoder_decode_surface_request");
-}
-
 TC_EXPORT void tc_gop_context_close(topos_gop_context* ctx) { (void)ctx; }
 
 TC_EXPORT int32_t tc_gop_context_observe(topos_gop_context* ctx, const uint8_t* data, size_t size,

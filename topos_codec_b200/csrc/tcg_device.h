@@ -82,6 +82,18 @@ typedef struct tcg_dec_frame {
     size_t dst_stride[4];   /* uint16 elements */
     uint8_t* slice_status;  /* out: TC_FRAME_SLICE_* per slice (host memory) */
     int32_t skip;           /* in: nonzero = frame already rejected by the host */
+    /* delivery (reference codec.c:8560-8640 slice tasks, 8700-8745 deblock):
+     * planes >= `planes` are not decoded (their slices report OK, unchecked);
+     * coefficients past zigzag position climit are dropped before the inverse
+     * transform (63 keeps all); with `scaled`, plane p is delivered as
+     * dst_w[p] x dst_h[p] samples, target (x, y) taking the reconstruction at
+     * (x * vis_w / dst_w, y * vis_h / dst_h) rounded down; db_unit is the
+     * grid of the delivered colour planes' deblocking (8 full size, 4 for an
+     * exact half, 0 none) */
+    uint32_t climit;
+    uint32_t scaled;
+    uint32_t dst_w[4], dst_h[4];
+    uint32_t db_unit;
 } tcg_dec_frame;
 
 /* Size-targeted encode sessions. A session leases one context for its whole
