@@ -451,6 +451,11 @@ def main():
                          "target = frame 0 at qp 24, qp 0..63")
         extra["sized_encode"] = r
         del sframes
+        # preview decode: the batch's packets at half size (1920x1080, 24 zigzag coefficients kept)
+        r = WL.preview_vs_reference(gpu, ref, batched_pkts, scale=1)
+        r["workload"] = "the 60 3840x2160 HQ packets decoded at 1/2 size, device-resident"
+        extra["preview_decode"] = r
+        torch.cuda.empty_cache()
         torch.cuda.empty_cache()
 
     # ---------------- serving: open-loop request streams at 25/50/75/100 % of saturation ----------------

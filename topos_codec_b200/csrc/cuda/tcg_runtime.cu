@@ -327,6 +327,23 @@ void ctx_release(Ctx* c)
     g_free = c;
 }
 
+// Frees the device buffers of every context in the free pool (their streams
+// first run dry); the next call on such a context allocates again.
+void trim_idle()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (Ctx* c = g_free; c != nullptr; c = c->next) {
+        for (cudaStream_t s : {c->stream, c->side, c->aux}) {
+            if (s != nullptr) { cudaStreamSynchronize(s); }
+        }
+        for (auto& b : c->d) {
+            if (b.p != nullptr) { cudaFree(b.p); }
+            b.p = nullptr;
+            b.cap = 0;
+        }
+    }
+}
+
 bool dreserve(Ctx* c, BufId id, size_t bytes)
 {
     DBuf& b = c->d[id];
@@ -339,6 +356,15 @@ bool dreserve(Ctx* c, BufId id, size_t bytes)
     }
     size_t want = bytes + bytes / 8 + 4096;
     if (cudaMalloc(&b.p, want) != cudaSuccess) {
+        // idle contexts keep the buffers of their largest call: give those
+        // back and try once more
+        cudaGetLastError();
+        b.p = nullptr;
+        trim_idle();
+        if (cudaMalloc(&b.p, want) == cudaSuccess) {
+            b.cap = want;
+            return true;
+        }
         cudaGetLastError();
         b.p = nullptr;
         char msg[128];
@@ -432,6 +458,22 @@ extern "C" int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uin
     if (ms) { *ms = tcg::g_prof_ms[id]; }
     if (launches) { *launches = tcg::g_prof_n[id]; }
     return 0;
+}
+
+extern "C" void tcg_trim_idle(void)
+{
+    if (tcg::ensure_init()) { tcg::trim_idle(); }
+}
+
+extern "C" void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes)
+{
+    size_t f = 0, t = 0;
+    if (!tcg::ensure_init() || cudaMemGetInfo(&f, &t) != cudaSuccess) {
+        cudaGetLastError();
+        f = t = 0;
+    }
+    *free_bytes = f;
+    *total_bytes = t;
 }
 
 extern "C" int32_t tcg_is_device_ptr(const void* p)

@@ -149,6 +149,8 @@ void ctx_release(Ctx* c);
 
 // Ensure device buffer capacity; returns false (and sets the error) on failure.
 bool dreserve(Ctx* c, BufId id, size_t bytes);
+// Frees the device buffers of every idle (pooled) context.
+void trim_idle();
 bool hreserve(Ctx* c, int id, size_t bytes);
 
 template <typename T>

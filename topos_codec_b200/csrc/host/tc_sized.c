@@ -795,7 +795,8 @@ TC_EXPORT int32_t tcg_frame_encode_sized_batch(const topos_frame_config* cfgs, c
     b.rcs = rcs;
     b.count = count;
     atomic_init(&b.next, 0u);
-    /* searches side by side: bounded by the device bytes of their probe windows */
+    /* searches side by side: bounded by the device bytes of their probe
+     * windows, against the smaller of a fixed budget and 3/4 of free memory */
     uint32_t workers = count < SIZED_BATCH_WORKERS ? count : SIZED_BATCH_WORKERS;
     {
         /* the first frame's geometry, counted as four full planes */
@@ -803,7 +804,16 @@ TC_EXPORT int32_t tcg_frame_encode_sized_batch(const topos_frame_config* cfgs, c
         const uint64_t px = (uint64_t)cfgs[0].visible_width * cfgs[0].visible_height;
         const uint64_t samples = px * 4u, cblocks = px / 16u;
         const uint64_t per = (uint64_t)sized_window(cap, samples, cblocks) * ((uint64_t)cap + samples * 2u + cblocks * 2048u);
-        const uint64_t fit = per > 0u ? SIZED_BATCH_BYTES / per : workers;
+        uint64_t free_b = 0, total_b = 0;
+        tcg_mem_info(&free_b, &total_b);
+        if (total_b > 0u && free_b / 4u * 3u < (uint64_t)workers * per) {
+            /* idle contexts' buffers from earlier calls are worth more as probe windows */
+            tcg_trim_idle();
+            tcg_mem_info(&free_b, &total_b);
+        }
+        uint64_t budget = SIZED_BATCH_BYTES;
+        if (total_b > 0u && free_b / 4u * 3u < budget) { budget = free_b / 4u * 3u; }
+        const uint64_t fit = per > 0u ? budget / per : workers;
         if (fit < workers) { workers = fit < 1u ? 1u : (uint32_t)fit; }
     }
     pthread_t th[SIZED_BATCH_WORKERS];
@@ -813,8 +823,16 @@ TC_EXPORT int32_t tcg_frame_encode_sized_batch(const topos_frame_config* cfgs, c
     }
     sized_worker(&b);
     for (uint32_t w = 0; w < started; ++w) { pthread_join(th[w], NULL); }
+    /* a search that ran out of device memory beside the others runs again alone */
     for (uint32_t i = 0; i < count; ++i) {
-        if (rcs[i] != TC_OK) { return rcs[i]; }
+        if (rcs[i] != TC_ERR_OUT_OF_MEMORY) { continue; }
+        uint8_t q = 0;
+        rcs[i] = sized_one(&cfgs[i], &inputs[i], target_bytes[i], qp_min, qp_max, &q, outs[i],
+                           outs[i] == NULL ? 0u : out_caps[i], stats != NULL ? &stats[i] : NULL, 0);
+        if (qp_used != NULL) { qp_used[i] = q; }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        if (rcs[i] != TC_OK) { return tc_fail(rcs[i], "sized batch: frame %u failed with status %d", i, (int)rcs[i]); }
     }
     return TC_OK;
 }

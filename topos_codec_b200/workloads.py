@@ -13,6 +13,8 @@
 * Size-targeted encode: 3840x2160 10-bit 4:2:2 HQ frames from host memory,
   one tc_frame_encode_sized call per frame with a byte target, beside the
   reference library on the host cores.
+* Preview decode: the bench batch's packets decoded at half size
+  (tc_frame_decode_batch_reduced), beside the reference library.
 
 The first two are coded as one batched call and as one plain call per frame
 on the same device-resident inputs; device time comes from the library's own
@@ -229,6 +231,70 @@ def sized_batch_vs_reference(product, reference, cfg: B.FrameConfig, frames, tar
         r["speedup_vs_reference"] = r["gpu_fps"] / r["reference_fps"]
         r["parity"] = all(rr[0] == 0 and (rr[1], rr[2]) == g for rr, g in zip(ref, got))
     return r
+
+
+def preview_vs_reference(product, reference, pkts: List[bytes], scale: int = 1, repeats: int = 2,
+                         ref_frames: int = 8) -> Dict:
+    """Reduced-size (preview) decode of a batch: tc_frame_decode_batch_reduced
+    on device-resident packets into device planes (device time from the
+    library's stream events), against the reference library decoding a
+    sample of the same packets frame-parallel on the host cores with
+    tc_frame_decode_reduced; the sampled frames must agree sample for sample."""
+    import os
+    import time
+
+    import torch
+    n = len(pkts)
+    L = product._lib
+    L.tc_frame_decode_batch_reduced.restype = ctypes.c_int32
+    dev = [torch.from_numpy(np.frombuffer(p, dtype=np.uint8).copy()).cuda() for p in pkts]
+    arr = (B.BatchPacket * n)()
+    for i, t in enumerate(dev):
+        arr[i].data, arr[i].size = t.data_ptr(), len(pkts[i])
+    infos = (B.FrameOutput * n)()
+    rc = int(L.tc_frame_decode_batch_reduced(arr, n, scale, None, None, infos))
+    if rc != 0:
+        raise RuntimeError(f"preview query failed [{rc}]: {product.last_error()}")
+    shapes = [B.ToposCodec.geometry(infos[i]) for i in range(n)]
+    out = [[torch.empty(s, dtype=torch.uint16, device="cuda") for s in shapes[i]] for i in range(n)]
+    ptrs = (ctypes.c_void_p * (4 * n))()
+    for i in range(n):
+        for p, t in enumerate(out[i]):
+            ptrs[4 * i + p] = t.data_ptr()
+
+    def run() -> float:
+        r = int(L.tc_frame_decode_batch_reduced(arr, n, scale, ptrs, None, infos))
+        if r not in (B.TC_OK, B.TC_WARN_CONCEALED):
+            raise RuntimeError(f"preview decode failed [{r}]: {product.last_error()}")
+        return L.tcg_last_device_ms()
+
+    run()
+    ms = min(run() for _ in range(repeats))
+    res = {"frames": n, "scale": scale, "target": f"{infos[0].visible_width}x{infos[0].visible_height}",
+           "gpu_ms": ms, "gpu_fps": n / (ms / 1e3)}
+    if reference is not None:
+        k = min(ref_frames, n)
+        R = reference._lib
+        R.tc_frame_decode_reduced.restype = ctypes.c_int32
+
+        def one(i):
+            planes = [np.empty(s, dtype=np.uint16) for s in shapes[i]]
+            pp = (ctypes.c_void_p * 4)(*[a.ctypes.data for a in planes])
+            buf = np.frombuffer(pkts[i], np.uint8)
+            info = B.FrameOutput()
+            r = int(R.tc_frame_decode_reduced(ctypes.c_void_p(buf.ctypes.data), ctypes.c_size_t(len(pkts[i])),
+                                              ctypes.c_int32(scale), pp, None, ctypes.byref(info)))
+            return r, planes
+        threads = min(k, os.cpu_count() or 1)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            ref = list(ex.map(one, range(k)))
+        el = time.perf_counter() - t0
+        res["reference_fps"] = k / el
+        res["reference_sample"] = f"{k} frames, {threads} threads"
+        res["parity"] = all(r == 0 and all(np.array_equal(a, b.cpu().numpy()) for a, b in zip(planes, out[i]))
+                            for i, (r, planes) in enumerate(ref))
+    return res
 
 
 def slice_spans(pkt: bytes):
