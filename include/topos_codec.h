@@ -433,6 +433,99 @@ int32_t tc_decoder_decode_surface_request(tc_decoder* dec, const uint8_t* packet
                                           const topos_decode_request* request, const topos_decode_surface* surface,
                                           topos_frame_output* info);
 
+/* ---------------- MOV read path and its hand-off to the batched decoder ----------------
+ * Reference: native/include/topos_codec.h:655-770 (io, movie information) and
+ * 880-1014 (reader calls); behaviour native/src/mov/mov.c:2260-2760 (atoms and
+ * sample tables), 3642-4182 (open, information), 4419-4770 (packets, timing,
+ * sync). The video track of a QuickTime file written by the reference muxer:
+ * open indexes the sample table without reading samples; packet and batch
+ * reads check every packet's header against the track's tpcC configuration.
+ * Audio and timecode tracks are skipped unparsed. tcg_movie_decode_batch
+ * (extension) reads samples [start, start + count) with one read when they lie
+ * back to back and decodes them as one tc_frame_decode_batch. */
+typedef int32_t (*tc_io_read_fn)(void* ctx, uint64_t offset, void* buf, size_t len);
+typedef int32_t (*tc_io_write_fn)(void* ctx, const void* data, size_t len);
+typedef int32_t (*tc_io_seek_write_fn)(void* ctx, uint64_t offset, const void* data, size_t len);
+
+typedef struct topos_io {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    void* ctx;
+    tc_io_read_fn read;
+    tc_io_write_fn write;
+    tc_io_seek_write_fn seek_write;
+    uint64_t length;           /* reader: bytes of the source */
+    uint32_t reserved[4];
+} topos_io;
+
+#define TC_MOVIE_MAX_SAMPLES 67108864u
+
+typedef struct topos_movie_info {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint16_t visible_width;
+    uint16_t visible_height;
+    uint8_t profile;
+    uint8_t pixel_format;
+    uint8_t bit_depth;
+    uint8_t qmatrix_id;
+    uint8_t qp_base;
+    int8_t qp_delta_luma;
+    int8_t qp_delta_chroma;
+    uint8_t alpha_mode;
+    uint8_t alpha_bit_depth;
+    uint8_t alpha_premultiplied;
+    uint8_t color_range;
+    uint8_t color_primaries;
+    uint8_t color_transfer;
+    uint8_t color_matrix;
+    uint8_t chroma_siting;
+    uint16_t sar_num;
+    uint16_t sar_den;
+    uint32_t timescale;
+    uint32_t sample_count;
+    uint32_t faststart;        /* 1 = moov before mdat */
+    uint32_t index_bytes;
+    uint32_t reserved[8];      /* [0] tpcC bitstream major, [1] tpcD tier */
+} topos_movie_info;
+
+typedef struct topos_alpha_budget_info {
+    uint32_t struct_size;
+    uint32_t abi_version;
+    uint16_t target_ratio_bp;
+    uint16_t actual_ratio_bp;
+    uint16_t max_abs_error;
+    uint16_t flags;
+    uint32_t frame_count;
+    uint32_t reserved[4];
+} topos_alpha_budget_info;
+
+typedef struct topos_movie topos_movie;
+
+int32_t tc_movie_open(const topos_io* io, topos_movie** out);
+int32_t tc_movie_open_fd(int fd, uint64_t length, topos_movie** out);
+int32_t tc_movie_info(const topos_movie* movie, topos_movie_info* info);
+int32_t tc_movie_alpha_budget(const topos_movie* movie, topos_alpha_budget_info* info);
+int32_t tc_movie_packet(const topos_movie* movie, uint32_t sample_index, uint8_t* buf, size_t cap, size_t* need_size);
+int32_t tc_movie_packet_base(const topos_movie* movie, uint32_t sample_index, uint8_t* buf, size_t cap,
+                             size_t* need_size);
+int32_t tc_movie_packet_batch(const topos_movie* movie, uint32_t start, uint32_t count, uint8_t* arena, size_t cap,
+                              size_t* offsets_out, size_t* sizes_out, size_t* need_total);
+int32_t tc_movie_packet_base_batch(const topos_movie* movie, uint32_t start, uint32_t count, uint8_t* arena,
+                                   size_t cap, size_t* offsets_out, size_t* sizes_out, uint8_t* base_flags_out,
+                                   size_t* need_total);
+int32_t tc_movie_packet_pts(const topos_movie* movie, uint32_t sample_index, uint64_t* pts_tick, uint32_t* dur_tick);
+int32_t tc_movie_packet_sync(const topos_movie* movie, uint32_t sample_index, uint8_t* is_sync);
+int32_t tc_movie_prev_sync(const topos_movie* movie, uint32_t sample_index, uint32_t* sync_index);
+void tc_movie_close(topos_movie* movie);
+
+/* Decodes movie samples [start, start + count) as one batch: planes_out,
+ * strides and infos as in tc_frame_decode_batch (planes_out NULL = frame
+ * information only). Returns the first failing status of the sample reads
+ * (no frame decoded) or of the decode. */
+int32_t tcg_movie_decode_batch(const topos_movie* movie, uint32_t start, uint32_t count, uint16_t* const* planes_out,
+                               const size_t* strides, topos_frame_output* infos);
+
 /* Decode-chain tiling chosen for batches of the given number of colour slices:
  * one lane per slice with 8 (0), 4 (2), 2 (3) or 1 (4) slices per warp, one
  * warp per slice (1), or a split (5: the largest slices, half of the blocks,

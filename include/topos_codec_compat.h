@@ -18,15 +18,11 @@ extern "C" {
 
 typedef struct topos_gop_context topos_gop_context;
 typedef struct topos_mux topos_mux;
-typedef struct topos_movie topos_movie;
 typedef struct topos_gop_frame_info topos_gop_frame_info;
 typedef struct topos_movie_config topos_movie_config;
-typedef struct topos_io topos_io;
-typedef struct topos_alpha_budget_info topos_alpha_budget_info;
 typedef struct topos_timecode_info topos_timecode_info;
 typedef struct topos_audio_track_config topos_audio_track_config;
 typedef struct topos_audio_track_info topos_audio_track_info;
-typedef struct topos_movie_info topos_movie_info;
 
 /* reference: native/include/topos_codec.h:122. Implemented: "experimental",
  * "reference", "eligible", "default" for 0..3, "unknown" otherwise. */
@@ -103,9 +99,6 @@ int32_t tc_mux_add_audio_to(topos_mux* mux, uint32_t track, const uint8_t* data,
 
 /* reference: native/include/topos_codec.h:880-1014 (MOV reader) */
 int32_t tc_movie_faststart(const topos_io* src, const topos_io* dst);
-int32_t tc_movie_open(const topos_io* io, topos_movie** out);
-int32_t tc_movie_info(const topos_movie* movie, topos_movie_info* info);
-int32_t tc_movie_alpha_budget(const topos_movie* movie, topos_alpha_budget_info* info);
 int32_t tc_movie_audio_info(const topos_movie* movie, topos_audio_track_info* info);
 int32_t tc_movie_audio_track_count(const topos_movie* movie, uint32_t* out_count);
 int32_t tc_movie_audio_info_at(const topos_movie* movie, uint32_t track, topos_audio_track_info* info);
@@ -114,13 +107,6 @@ int32_t tc_movie_read_audio_at(const topos_movie* movie, uint32_t track, uint64_
 int32_t tc_movie_timecode(const topos_movie* movie, topos_timecode_info* out);
 int32_t tc_movie_read_audio(const topos_movie* movie, uint64_t start_chunk, uint32_t chunk_count, uint8_t* buf,
                             size_t cap, size_t* need_size);
-int32_t tc_movie_packet(const topos_movie* movie, uint32_t sample_index, uint8_t* buf, size_t cap, size_t* need_size);
-int32_t tc_movie_packet_base_batch(const topos_movie* movie, uint32_t start, uint32_t count, uint8_t* arena,
-                                   size_t cap, size_t* offsets_out, size_t* sizes_out, uint8_t* base_flags_out,
-                                   size_t* need_total);
-int32_t tc_movie_packet_pts(const topos_movie* movie, uint32_t sample_index, uint64_t* pts_tick, uint32_t* dur_tick);
-int32_t tc_movie_packet_sync(const topos_movie* movie, uint32_t sample_index, uint8_t* is_sync);
-void tc_movie_close(topos_movie* movie);
 
 #ifdef __cplusplus
 }

@@ -157,24 +157,8 @@ TC_EXPORT int32_t tc_movie_faststart(const topos_io* src, const topos_io* dst)
     return NOT_PATH("tc_movie_faststart");
 }
 
-TC_EXPORT int32_t tc_movie_open(const topos_io* io, topos_movie** out)
-{
-    (void)io;
-    if (out != NULL) { *out = NULL; }
-    return NOT_PATH("tc_movie_open");
-}
 
-TC_EXPORT int32_t tc_movie_info(const topos_movie* movie, topos_movie_info* info)
-{
-    (void)movie; (void)info;
-    return NOT_PATH("tc_movie_info");
-}
 
-TC_EXPORT int32_t tc_movie_alpha_budget(const topos_movie* movie, topos_alpha_budget_info* info)
-{
-    (void)movie; (void)info;
-    return NOT_PATH("tc_movie_alpha_budget");
-}
 
 TC_EXPORT int32_t tc_movie_audio_info(const topos_movie* movie, topos_audio_track_info* info)
 {
@@ -214,33 +198,7 @@ TC_EXPORT int32_t tc_movie_read_audio(const topos_movie* movie, uint64_t start_c
     return NOT_PATH("tc_movie_read_audio");
 }
 
-TC_EXPORT int32_t tc_movie_packet(const topos_movie* movie, uint32_t sample_index, uint8_t* buf, size_t cap,
-                                  size_t* need_size)
-{
-    (void)movie; (void)sample_index; (void)buf; (void)cap; (void)need_size;
-    return NOT_PATH("tc_movie_packet");
-}
 
-TC_EXPORT int32_t tc_movie_packet_base_batch(const topos_movie* movie, uint32_t start, uint32_t count,
-                                             uint8_t* arena, size_t cap, size_t* offsets_out, size_t* sizes_out,
-                                             uint8_t* base_flags_out, size_t* need_total)
-{
-    (void)movie; (void)start; (void)count; (void)arena; (void)cap; (void)offsets_out; (void)sizes_out;
-    (void)base_flags_out; (void)need_total;
-    return NOT_PATH("tc_movie_packet_base_batch");
-}
 
-TC_EXPORT int32_t tc_movie_packet_pts(const topos_movie* movie, uint32_t sample_index, uint64_t* pts_tick,
-                                      uint32_t* dur_tick)
-{
-    (void)movie; (void)sample_index; (void)pts_tick; (void)dur_tick;
-    return NOT_PATH("tc_movie_packet_pts");
-}
 
-TC_EXPORT int32_t tc_movie_packet_sync(const topos_movie* movie, uint32_t sample_index, uint8_t* is_sync)
-{
-    (void)movie; (void)sample_index; (void)is_sync;
-    return NOT_PATH("tc_movie_packet_sync");
-}
 
-TC_EXPORT void tc_movie_close(topos_movie* movie) { (void)movie; }
