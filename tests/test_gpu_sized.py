@@ -144,3 +144,29 @@ def test_sized_batch_vs_reference_single_calls(libs):
         assert iters == reference._lib.tc_dev_sized_iters() - ri0
     finally:
         reference._lib.tc_dev_set_qp_hint_model(0)
+
+
+def test_sized_device_resident_input_equals_host(product, libs):
+    """Sample planes in device memory give the host-memory call's packet and qp."""
+    import ctypes
+
+    import torch
+    for c in libs:
+        c._lib.tc_dev_set_sized_mode(0)
+        c._lib.tc_dev_set_qp_hint(1)
+    cfg, planes = _frame(320, 192, seed=21)
+    target = len(product.encode(cfg, planes)) * 2 // 3
+    rc, pkt, st, qp, _ = product.encode_sized_status(cfg, planes, target, 0, 63)
+    assert rc == 0
+    dev = [torch.from_numpy(p.astype(np.int32)).cuda().to(torch.uint16) for p in planes]
+    fi = B.FrameInput()
+    fi.struct_size, fi.abi_version = ctypes.sizeof(B.FrameInput), 2
+    for i, t in enumerate(dev):
+        fi.planes[i], fi.strides[i] = t.data_ptr(), t.shape[1]
+    cap = product.packet_bound(cfg)
+    out = np.empty(cap, np.uint8)
+    st2 = B.FrameStats()
+    q2 = ctypes.c_uint8()
+    rc2 = product._lib.tc_frame_encode_sized(ctypes.byref(cfg), ctypes.byref(fi), target, 0, 63, ctypes.byref(q2),
+                                             out.ctypes.data, cap, ctypes.byref(st2))
+    assert rc2 == 0 and q2.value == qp and out[: st2.packet_size].tobytes() == pkt
