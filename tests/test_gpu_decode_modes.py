@@ -190,3 +190,27 @@ def test_batch_reduced_and_decoder_contexts_vs_reference(product, reference, pac
     for x, y in zip(a[2], b[2]):
         assert all(np.array_equal(p, q) for p, q in zip(x, y))
     assert all(np.array_equal(p, q) for p, q in zip(a[5], b[5]))
+
+
+def test_exact_half_edge_blocks_vs_reference(product, reference):
+    """Exact-half delivery of planes whose last block column is narrower than 8
+    pixels (the reference's 4x4 block store reads entries past the block's
+    computed prefix): wide planes, planes one block wide with the partial last
+    block row in its own slice band or sharing one, 10/12/16-bit, deblocked."""
+    cases = [(115, 58, dict(qp=30, qmatrix_id=3, features=2, qp_delta_chroma=3), {}),
+             (12, 40, dict(qp=8), {}), (12, 40, dict(qp=8, slice_rows=1), {}),
+             (6, 44, dict(qp=8, slice_rows=2), {}), (6, 44, dict(qp=8, slice_rows=1), {}),
+             (4, 28, dict(qp=8, slice_rows=3), {}), (6, 12, dict(qp=8), {}), (2, 6, dict(qp=8), {}),
+             (44, 30, dict(qp=6, features=1, qmatrix_id=4), {}),
+             (90, 22, dict(qp=10, bit_depth=12, qmatrix_id=1), dict(bit_depth=12)),
+             (38, 26, dict(qp=40, bit_depth=16), dict(bit_depth=16, limited=False)),
+             (30, 14, dict(qp=3, bit_depth=12, pixel_format=2, profile=5, color_range=1),
+              dict(bit_depth=12, pixel_format=2, limited=False))]
+    for k, (w, h, ck, kw) in enumerate(cases):
+        planes = synth.make_frame_np(w, h, seed=300 + k, **kw)
+        pkt = reference.encode(B.make_config(w, h, **ck), planes)
+        for rl, req in [("half", B.make_request(1, target=((w + 1) // 2, (h + 1) // 2))),
+                        ("reduced half", B.make_request(2, scale=1))]:
+            a = B.decode_request(product, pkt, req, fill=7)
+            b = B.decode_request(reference, pkt, req, fill=7)
+            _same(a, b, (w, h, ck, rl))

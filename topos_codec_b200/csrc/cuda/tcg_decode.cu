@@ -886,9 +886,24 @@ __global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices
 // codec.c:7955-7964 alpha, 7987-8000 concealment): target sample (x, y) of a
 // plane is the reconstruction at (x * vis_w / dst_w, y * vis_h / dst_h),
 // rounded down. One thread per target sample; grid.y = plane.
+//
+// Exact-half colour planes (dst = vis / 2 on both axes) follow the reference's
+// 4x4 block store (color_store.h:538-559, transform_avx2.c:528-570): a block
+// of nx x ny target samples computes only the first nx*ny entries of a 4-wide
+// row-major sample array and then reads entry iy*4 + ix, so in a right-edge
+// block narrower than 8 source pixels (nx < 4) the entries at or past nx*ny
+// still hold the previous block's samples, the same (ix, iy) one block to the
+// left (`half_edge` 1: planes wider than one block, whose edge blocks follow
+// their left neighbour in the same slice band). In a plane one block wide the
+// previous block is the one above in the same band: its entries below 4 * nx
+// were written, so a partial last block row whose band also holds the row
+// above reads those (`half_edge` 2), and every entry no block of the band
+// wrote is delivered as a zero residual, the mid-level sample (`half_edge` 3:
+// the last block row starts its own band).
 struct DecimPlane {
     uint64_t src_off, dst_off;
     uint32_t vis_w, vis_h, dst_w, dst_h;
+    uint32_t half_edge, mid;
 };
 
 __global__ void __launch_bounds__(256) k_decimate(const DecimPlane* __restrict__ dp, uint16_t* __restrict__ out)
@@ -897,8 +912,24 @@ __global__ void __launch_bounds__(256) k_decimate(const DecimPlane* __restrict__
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (uint64_t)P.dst_w * P.dst_h) { return; }
     const uint32_t ty = (uint32_t)(i / P.dst_w), tx = (uint32_t)(i % P.dst_w);
-    const uint32_t sx = (uint32_t)(((uint64_t)tx * P.vis_w) / P.dst_w);
-    const uint32_t sy = (uint32_t)(((uint64_t)ty * P.vis_h) / P.dst_h);
+    uint32_t sx = (uint32_t)(((uint64_t)tx * P.vis_w) / P.dst_w);
+    uint32_t sy = (uint32_t)(((uint64_t)ty * P.vis_h) / P.dst_h);
+    if (P.half_edge != 0u) {
+        const uint32_t px0 = (tx >> 2) * 8u, py0 = (ty >> 2) * 8u;
+        const uint32_t nx = min(8u, P.vis_w - px0) / 2u;
+        const uint32_t ny = min(8u, P.vis_h - py0) / 2u;
+        const uint32_t k = (ty & 3u) * 4u + (tx & 3u);
+        if (nx < 4u && k >= nx * ny) {
+            if (P.half_edge == 1u) {
+                sx -= 8u;               // px0 >= 8: not the first block column
+            } else if (P.half_edge == 2u && ny < 4u && k < 4u * nx) {
+                sy -= 8u;               // the partial last row, below row 0
+            } else {
+                out[P.dst_off + i] = (uint16_t)P.mid;
+                return;
+            }
+        }
+    }
     out[P.dst_off + i] = out[P.src_off + (uint64_t)sy * P.vis_w + sx];
 }
 
@@ -1245,7 +1276,19 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 P.dst_w = F.dst_w[p];
                 P.dst_h = F.dst_h[p];
                 out_elems = align_up(out_elems + (uint64_t)P.dst_w * P.dst_h, 64);
-                DecimPlane dm = {P.out_off, P.dst_off, P.vis_w, P.vis_h, P.dst_w, P.dst_h};
+                const bool half = P.kind == TCG_PLANE_COLOR && (uint64_t)P.dst_w * 2u == P.vis_w &&
+                                  (uint64_t)P.dst_h * 2u == P.vis_h;
+                uint32_t half_edge = half ? (P.vis_w > 8u ? 1u : 2u) : 0u;
+                if (half_edge == 2u) {
+                    const uint32_t last = (P.vis_h - 1u) / 8u;  // last block row
+                    bool own = last == 0u;
+                    for (uint32_t i = 0; i < F.slices && !own; ++i) {
+                        own = F.slice[i].plane == p && F.slice[i].y0 == last;
+                    }
+                    half_edge = own ? 3u : 2u;
+                }
+                DecimPlane dm = {P.out_off, P.dst_off, P.vis_w, P.vis_h, P.dst_w, P.dst_h, half_edge,
+                                 1u << (P.bd - 1u)};
                 if (P.dst_w > 0u && P.dst_h > 0u) { decim.push_back(dm); }
             } else {
                 P.dst_off = P.out_off;
