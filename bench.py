@@ -10,6 +10,7 @@ the plain per-frame GPU path on the same frames for comparison.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--serve-seconds S] [--no-serve] [--no-extra]
+    python bench.py --case 3840x2160 --frames 2 [--repeat R] [--case-qp Q] [--case-gbr]
 
 Beside the headline the line reports (key `workloads`) a 64-frame mixed batch
 (720p..8K, four tiers, qp 2..16) and a 32-frame 4096x2160 12-bit GBR 4:4:4 +
@@ -30,6 +31,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -57,10 +59,10 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="tc_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -99,6 +101,10 @@ class ClockSampler:
             for n, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
@@ -140,6 +146,71 @@ def reference_rate(frames_np, cfg, budget_s=10.0, threads=None):
     return done[0] / el, cores, done[0], el
 
 
+# ------------------------------------------------------------------ profiling case
+
+def kernel_case(args):
+    """One batched encode + decode of a small case (device-resident samples,
+    packets and planes; the same library path as the bench), repeated
+    --repeat times; prints the per-kernel device times of the last repetition.
+    Sized for a profiler capture: --case 3840x2160 --frames 2."""
+    import torch
+    from topos_codec_b200 import binding as B, synth
+    w, h = (int(v) for v in args.case.split("x"))
+    n = args.frames
+    gpu = B.ToposCodec(B.PRODUCT_LIBRARY)
+    L = gpu._lib
+    L.tcg_profile_read.argtypes = [ctypes.c_uint32, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_uint64)]
+    if args.case_gbr:
+        from topos_codec_b200.workloads import gbr_config
+        cfg = gbr_config(w, h)
+        kw = dict(bit_depth=12, pixel_format=2, limited=False, alpha=True, sigma=12)
+    else:
+        cfg = B.make_config(w, h, qp=args.case_qp, qmatrix_id=0 if w >= 3840 else 4, features=3 if w >= 3840 else 1)
+        kw = {}
+    frames = [[p.to(torch.uint16) for p in synth.make_frame(w, h, seed=0, frame=i, device="cuda", **kw)]
+              for i in range(n)]
+    cap = gpu.packet_bound(cfg)
+    outs = [torch.empty(cap, dtype=torch.uint8, device="cuda") for _ in range(n)]
+    dec = [[torch.empty(sh, dtype=torch.uint16, device="cuda") for sh in B.plane_shapes(cfg)] for _ in range(n)]
+    cfgs = (B.FrameConfig * n)(*[cfg] * n)
+    ins = (B.FrameInput * n)()
+    for i, fr in enumerate(frames):
+        ins[i].struct_size, ins[i].abi_version = ctypes.sizeof(B.FrameInput), 2
+        for p, t in enumerate(fr):
+            ins[i].planes[p], ins[i].strides[p] = t.data_ptr(), t.shape[1]
+    optr = (ctypes.c_void_p * n)(*[t.data_ptr() for t in outs])
+    caps = (ctypes.c_size_t * n)(*[cap] * n)
+    st = (B.FrameStats * n)()
+    rcs = (ctypes.c_int32 * n)()
+    dptr = (ctypes.c_void_p * (4 * n))()
+    for i in range(n):
+        for p, t in enumerate(dec[i]):
+            dptr[4 * i + p] = t.data_ptr()
+    infos = (B.FrameOutput * n)()
+    for r in range(args.repeat):
+        if r == args.repeat - 1:
+            L.tcg_profile_reset()
+            L.tcg_profile_enable(1)
+        rc = L.tcg_frame_encode_batch(cfgs, ins, n, optr, caps, st, rcs)
+        assert rc == 0, gpu.last_error()
+        pk = (B.BatchPacket * n)()
+        for i in range(n):
+            pk[i].data, pk[i].size = outs[i].data_ptr(), st[i].packet_size
+        rc = L.tc_frame_decode_batch(pk, n, dptr, None, infos)
+        assert rc == 0, gpu.last_error()
+    L.tcg_profile_enable(0)
+    res = {}
+    for k in range(64):
+        name, ms, cnt = ctypes.c_char_p(), ctypes.c_double(), ctypes.c_uint64()
+        if L.tcg_profile_read(k, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(cnt)) != 0:
+            break
+        if cnt.value:
+            res[name.value.decode()] = round(ms.value, 3)
+    print(json.dumps({"case": args.case, "frames": n, "packet_bytes": sum(s.packet_size for s in st),
+                      "kernels_ms": res}))
+
+
 # ------------------------------------------------------------------ GPU path
 
 def main():
@@ -152,7 +223,15 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed-batch and GBR 4:4:4 + alpha workloads")
+    ap.add_argument("--case", default=None, help="WxH: run one small batched round trip for a profiler capture "
+                                                   "(with --frames, --repeat, --case-qp, --case-gbr) instead of the bench")
+    ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--case-qp", type=int, default=4)
+    ap.add_argument("--case-gbr", action="store_true", help="12-bit GBR 4:4:4 + 16-bit alpha at qp 2")
     args = ap.parse_args()
+    if args.case:
+        kernel_case(args)
+        return
     args.warmup = max(3, args.warmup)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -284,8 +284,10 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
  *    records; each call clears the records it uses before writing them, but
  *    calls that overlap on the GPU (from several host threads at once) race on
  *    it, so serialise them;
- *  - the call runs on the default stream and returns when its device work has
- *    finished. */
+ *  - the call runs on the default stream of the calling thread's current
+ *    device and returns when its device work has finished; a packet in the
+ *    memory of another device is rejected with TC_ERR_INVALID_ARGUMENT (make
+ *    the packets' device current first). */
 #define TCG_NOALLOC_MAX_PACKETS 64u
 int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                       topos_frame_output* infos);

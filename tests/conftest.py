@@ -12,6 +12,28 @@ REF_LIB = os.path.join(REF_DIR, "libtopos_codec_ref.so")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def _reference_dir():
+    """The reference checkout (CPU tests only): TOPOS_REFERENCE_DIR, else the
+    directory the oracle recipe built oracle/_ref from; None when neither."""
+    env = os.environ.get("TOPOS_REFERENCE_DIR")
+    if env:
+        return env
+    rec = os.path.join(REF_DIR, "SOURCE_DIR")
+    if os.path.exists(rec):
+        with open(rec) as f:
+            d = f.read().strip()
+        return d or None
+    return None
+
+
+REFERENCE_DIR = _reference_dir()
+
+
+def reference_path(*parts):
+    """A file of the reference checkout, or a path that does not exist."""
+    return os.path.join(REFERENCE_DIR, *parts) if REFERENCE_DIR else os.path.join(REF_DIR, "missing", *parts)
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); parity tests through the C-ABI")
 

@@ -12,12 +12,12 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, ROOT, reference_path
 from topos_codec_b200 import binding as B
 
 HEADER = os.path.join(ROOT, "include", "topos_codec.h")
 HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include"))) if f.endswith(".h")]
-REF_HEADER = "/root/reference/native/include/topos_codec.h"
+REF_HEADER = reference_path("native", "include", "topos_codec.h")
 
 
 def _declared_functions():
@@ -145,7 +145,7 @@ def test_structural_parse_matches_oracle(product, oracle):
                 assert bytes(ia) == bytes(ib)
 
 
-REF_PY = "/root/reference/python"
+REF_PY = reference_path("python")
 
 
 def test_reference_python_binding_loads_this_library(built):

@@ -12,10 +12,10 @@ import zlib
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, REF_DIR, ROOT
+from conftest import GOLDEN, REF_DIR, ROOT, reference_path
 from topos_codec_b200 import binding as B, synth
 
-REF_GOLDEN = "/root/reference/native/tests/conformance/golden_codec_v7r2_intra.bin"
+REF_GOLDEN = reference_path("native", "tests", "conformance", "golden_codec_v7r2_intra.bin")
 
 
 def _cases():

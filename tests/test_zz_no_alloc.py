@@ -83,6 +83,28 @@ def test_noalloc_query_matches_batch_query_twice(product, packets):
         assert got[0].slice_count > 0
 
 
+def test_noalloc_query_allocates_nothing(product, packets):
+    """After one warm-up call (which may look up the scratch address and load
+    device code), further calls change neither the library's allocation count
+    nor the device's free memory."""
+    import torch
+    (a, da), (b, db), (c, dc) = packets
+    host_c = ctypes.create_string_buffer(c, len(c))
+    items = [(da.data_ptr(), len(a)), (ctypes.addressof(host_c), len(c)), (db.data_ptr(), len(b))]
+    fn = _bind(product._lib)
+    count = product._lib.tcg_allocation_count
+    count.restype = ctypes.c_uint64
+    infos = (B.FrameOutput * len(items))()
+    torch.cuda.synchronize()
+    assert int(fn(_packets(items), len(items), infos)) == 0
+    allocs0 = int(count())
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert int(fn(_packets(items), len(items), infos)) == 0
+    assert int(count()) == allocs0
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_query_damaged_and_truncated(product, packets):
     import torch
     (a, _), (b, _), _ = packets

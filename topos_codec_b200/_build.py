@@ -84,8 +84,9 @@ def build_oracle() -> None:
     """The CPU checker (test infrastructure): oracle restatement, and - where the
     reference sources are present - the reference library and golden driver."""
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
-    if os.path.isdir("/root/reference/native"):
-        _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    ref = os.environ.get("TOPOS_REFERENCE_DIR", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "native")):
+        _run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref", f"TOPOS_REFERENCE_DIR={ref}"])
 
 
 if __name__ == "__main__":

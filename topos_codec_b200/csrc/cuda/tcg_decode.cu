@@ -20,6 +20,7 @@
 //   k_dconceal  damaged slices: neutral fill of the visible band rows
 //                                               (codec.c:7975-7985)
 //   k_deblock_v / k_deblock_h  frame-level output filter (deblock.c:71-341)
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1742,20 +1743,55 @@ static __device__ __align__(256) uint8_t g_walk_scratch[NA_BYTES];
 constexpr int NA_MAX_DEVICES = 64;
 static std::mutex g_na_mu;
 static uint8_t* g_na_base[NA_MAX_DEVICES];
+static unsigned long long g_na_ctx[NA_MAX_DEVICES];  // context the address belongs to
 
-static int32_t noalloc_base(uint8_t** base)
+// Unique id of the calling thread's current context (0 when unknown). A
+// context destroyed and created again (cudaDeviceReset, a released primary
+// context) gets a new id, so an address looked up in the old one is not reused.
+static unsigned long long current_ctx_id()
 {
-    int dev = 0;
-    TCG_CHECK(cudaGetDevice(&dev));
+    using get_cur_t = int (*)(void**);
+    using get_id_t = int (*)(void*, unsigned long long*);
+    static get_cur_t get_cur = nullptr;
+    static get_id_t get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            get_cur = reinterpret_cast<get_cur_t>(f);
+        }
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            get_id = reinterpret_cast<get_id_t>(f);
+        }
+        cudaGetLastError();
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (get_cur == nullptr || get_id == nullptr || get_cur(&ctx) != 0 || ctx == nullptr || get_id(ctx, &id) != 0) {
+        return 0;
+    }
+    return id;
+}
+
+// Device address of the static scratch on the current device, looked up once
+// per device and context (the lookup may load the library's device code).
+static int32_t noalloc_base(int dev, uint8_t** base)
+{
     if (dev < 0 || dev >= NA_MAX_DEVICES) {
         tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: device ordinal beyond 63");
         return TCG_ERR_LIMIT_EXCEEDED;
     }
+    const unsigned long long ctx = current_ctx_id();
     std::lock_guard<std::mutex> g(g_na_mu);
-    if (g_na_base[dev] == nullptr) {
+    if (g_na_base[dev] == nullptr || ctx == 0 || g_na_ctx[dev] != ctx) {
         void* p = nullptr;
         TCG_CHECK(cudaGetSymbolAddress(&p, g_walk_scratch));
         g_na_base[dev] = static_cast<uint8_t*>(p);
+        g_na_ctx[dev] = ctx;
     }
     *base = g_na_base[dev];
     return 0;
@@ -1803,8 +1839,28 @@ extern "C" int32_t tcg_walk_packets_noalloc(const uint8_t* const* pkts, const si
         tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: more than 64 packets in one call");
         return TCG_ERR_LIMIT_EXCEEDED;
     }
+    int dev = 0;
+    TCG_CHECK(cudaGetDevice(&dev));
+    // the walk runs on the calling thread's current device: a packet on another
+    // device would be read through a peer pointer, so it is refused up front
+    for (uint32_t i = 0; i < n; ++i) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, pkts[i]) != cudaSuccess) {
+            cudaGetLastError();
+            tcg_host_set_error(TCG_ERR_INVALID_ARGUMENT, "allocation-free walk: packet pointer not known to CUDA");
+            return TCG_ERR_INVALID_ARGUMENT;
+        }
+        if (a.type == cudaMemoryTypeDevice && a.device != dev) {
+            char msg[160];
+            snprintf(msg, sizeof(msg),
+                     "allocation-free walk: packet %u is on device %d, the calling thread's current device is %d", i,
+                     a.device, dev);
+            tcg_host_set_error(TCG_ERR_INVALID_ARGUMENT, msg);
+            return TCG_ERR_INVALID_ARGUMENT;
+        }
+    }
     uint8_t* base = nullptr;
-    const int32_t rc = tcg::noalloc_base(&base);
+    const int32_t rc = tcg::noalloc_base(dev, &base);
     if (rc != 0) { return rc; }
     uint64_t tab[2u * TCG_NOALLOC_MAX_PACKETS];
     for (uint32_t i = 0; i < n; ++i) {
@@ -1829,8 +1885,10 @@ extern "C" int32_t tcg_walk_record_noalloc(uint32_t i, uint8_t* host_rec)
         tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "allocation-free walk: record index beyond 63");
         return TCG_ERR_LIMIT_EXCEEDED;
     }
+    int dev = 0;
+    TCG_CHECK(cudaGetDevice(&dev));
     uint8_t* base = nullptr;
-    const int32_t rc = tcg::noalloc_base(&base);
+    const int32_t rc = tcg::noalloc_base(dev, &base);
     if (rc != 0) { return rc; }
     TCG_CHECK(cudaMemcpy(host_rec, base + 2u * tcg::NA_TABLE + (size_t)i * tcg::WALK_REC, tcg::WALK_REC,
                          cudaMemcpyDeviceToHost));

@@ -16,6 +16,7 @@ static bool g_init = false;
 static int g_device = -1;
 static DevTables g_tab;
 static std::atomic<uint64_t> g_launches{0};
+static std::atomic<uint64_t> g_allocs{0};  // device and pinned host allocations made
 static std::atomic<int> g_prof_on{0};
 static double g_prof_ms[K_COUNT];
 static uint64_t g_prof_n[K_COUNT];
@@ -255,6 +256,7 @@ static bool init_locked(int device)
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "device table allocation failed");
         return false;
     }
+    g_allocs.fetch_add(1, std::memory_order_relaxed);
     uint32_t* m = (uint32_t*)(h + om);
     uint8_t* l = h + ol;
     double* lg = (double*)(h + olg);
@@ -362,6 +364,7 @@ bool dreserve(Ctx* c, BufId id, size_t bytes)
         b.p = nullptr;
         trim_idle();
         if (cudaMalloc(&b.p, want) == cudaSuccess) {
+            g_allocs.fetch_add(1, std::memory_order_relaxed);
             b.cap = want;
             return true;
         }
@@ -372,6 +375,7 @@ bool dreserve(Ctx* c, BufId id, size_t bytes)
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, msg);
         return false;
     }
+    g_allocs.fetch_add(1, std::memory_order_relaxed);
     b.cap = want;
     return true;
 }
@@ -393,6 +397,7 @@ bool hreserve(Ctx* c, int id, size_t bytes)
         tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "pinned host allocation failed");
         return false;
     }
+    g_allocs.fetch_add(1, std::memory_order_relaxed);
     b.cap = want;
     return true;
 }
@@ -433,6 +438,14 @@ extern "C" void tcg_shutdown(void)
 extern "C" uint64_t tcg_launch_count(void)
 {
     return tcg::g_launches.load(std::memory_order_relaxed);
+}
+
+// Device (cudaMalloc) and pinned host (cudaMallocHost) allocations the library
+// has made since it was loaded; a test of an allocation-free call reads it
+// before and after.
+extern "C" __attribute__((visibility("default"))) uint64_t tcg_allocation_count(void)
+{
+    return tcg::g_allocs.load(std::memory_order_relaxed);
 }
 
 extern "C" double tcg_last_ms(void) { return tcg::t_last_ms; }

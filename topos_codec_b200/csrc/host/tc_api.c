@@ -551,8 +551,7 @@ TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* co
 /* Allocation-free form of tc_frame_decode_batch's query mode (no reference
  * counterpart). Every buffer is on the stack or in the device library's static
  * scratch; packets in device memory are walked with the static-scratch walk
- * and parsed from their records one at a time. The packets are parsed twice -
- * once to find the first failing status, then to fill infos - so that, like
+ * and parsed from their records one at a time, each record copied once. Like
  * the batch query, infos is left untouched when any packet fails. */
 TC_EXPORT int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                                 topos_frame_output* infos)
@@ -581,29 +580,31 @@ TC_EXPORT int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packet
         const int32_t rc = tcg_walk_packets_noalloc(dptrs, dsizes, ndev);
         if (rc != TC_OK) { return rc; }
     }
+    /* each record is copied and parsed once; only the frame headers are kept
+     * until every packet has parsed, so infos stays untouched on a failure */
     uint8_t rec[TCG_WALK_REC];
     tc_view v;
-    for (int pass = 0; pass < 2; ++pass) {
-        for (uint32_t i = 0; i < count; ++i) {
-            const int dev = slot[i] != UINT32_MAX;
-            if (dev) {
-                const int32_t rc = tcg_walk_record_noalloc(slot[i], rec);
-                if (rc != TC_OK) { return rc; }
-            }
-            const uint8_t* head = dev ? rec : packets[i].data;
-            int32_t rc = tc_probe_generation(head, packets[i].size);
-            if (rc == 0) {
-                rc = dev ? tc_parse_compact(head, packets[i].size, &v) : tc_parse_structure(packets[i].data, packets[i].size, &v);
-            }
+    tc_hdr hdrs[TCG_NOALLOC_MAX_PACKETS];
+    for (uint32_t i = 0; i < count; ++i) {
+        const int dev = slot[i] != UINT32_MAX;
+        if (dev) {
+            const int32_t rc = tcg_walk_record_noalloc(slot[i], rec);
             if (rc != TC_OK) { return rc; }
-            if (pass == 1) {
-                topos_frame_output* o = &infos[i];
-                memset(o, 0, sizeof(*o));
-                o->struct_size = (uint32_t)sizeof(topos_frame_output);
-                o->abi_version = TOPOS_CODEC_ABI_VERSION;
-                tc_fill_info(&v.h, o);
-            }
         }
+        const uint8_t* head = dev ? rec : packets[i].data;
+        int32_t rc = tc_probe_generation(head, packets[i].size);
+        if (rc == 0) {
+            rc = dev ? tc_parse_compact(head, packets[i].size, &v) : tc_parse_structure(packets[i].data, packets[i].size, &v);
+        }
+        if (rc != TC_OK) { return rc; }
+        hdrs[i] = v.h;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        topos_frame_output* o = &infos[i];
+        memset(o, 0, sizeof(*o));
+        o->struct_size = (uint32_t)sizeof(topos_frame_output);
+        o->abi_version = TOPOS_CODEC_ABI_VERSION;
+        tc_fill_info(&hdrs[i], o);
     }
     return TC_OK;
 }
