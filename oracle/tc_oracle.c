@@ -1015,6 +1015,89 @@ static int32_t band_tokens(const hdr* h, const uint16_t* coded, uint32_t p, cons
     return TC_OK;
 }
 
+/* joint histograms of a token set, added to the rows (codec.c:2116-2151):
+ * level by zigzag position, level by the previous level's category in the
+ * block, DC category by the previous block's DC category */
+static void tok_joints(const band_tok* t, uint32_t jpos[POS_CTX * LVL_SYMS], uint32_t jprev[PREV_CTX * LVL_SYMS],
+                       uint32_t jdc[DCP_CTX * DC_SYMS])
+{
+    size_t pi = 0;
+    uint32_t prev_dcc = 0;
+    for (uint32_t b = 0; b < t->blocks; ++b) {
+        const uint32_t dcc = bitlen(t->dc_m[b]);
+        jdc[(b == 0u ? 0u : dcp_ctx(prev_dcc, 1)) * DC_SYMS + dcc]++;
+        prev_dcc = dcc;
+        uint32_t ppos = 0, pcat = 0;
+        for (uint32_t k = 0; k < t->np[b]; ++k, ++pi) {
+            const uint32_t cat = bitlen(t->lvl_m[pi]);
+            const uint32_t pos = ppos + t->run[pi] + 1u;
+            jpos[pos_ctx(pos) * LVL_SYMS + cat]++;
+            jprev[prev_ctx(pcat, k != 0u) * LVL_SYMS + cat]++;
+            pcat = cat;
+            ppos = pos;
+        }
+    }
+}
+
+/* model choice by the candidates' costs in bits, strict < in candidate order
+ * (codec.c:2300-2326; the V8 tile choice codec.c:2672-2709 is the same) */
+static void pick_models(const uint32_t* dch, const uint32_t* lvlh, const uint32_t* jpos, const uint32_t* jprev,
+                        const uint32_t* jdc, uint32_t* lvl_model, uint32_t* dc_model)
+{
+    uint32_t lm = 0;
+    double best = rows_cost(lvlh, 1u, LVL_SYMS) + 8.0 * (double)LVL_SYMS;
+    const double pc = rows_cost(jpos, POS_CTX, LVL_SYMS) + 8.0 * (double)(POS_CTX * LVL_SYMS);
+    if (pc < best) { best = pc; lm = 1; }
+    const double prc = rows_cost(jprev, PREV_CTX, LVL_SYMS) + 8.0 * (double)(PREV_CTX * LVL_SYMS);
+    if (prc < best) { lm = 2; }
+    const double dn = rows_cost(dch, 1u, DC_SYMS) + 8.0 * (double)DC_SYMS;
+    const double dp = rows_cost(jdc, DCP_CTX, DC_SYMS) + 8.0 * (double)(DCP_CTX * DC_SYMS);
+    *lvl_model = lm;
+    *dc_model = dp < dn ? 1u : 0u;
+}
+
+/* backward rANS walk of a token set with given models (codec.c:2410-2492;
+ * the V8 segment form codec.c:2528-2640 is the same walk) */
+static void tok_stream(const band_tok* t, uint32_t lvl_model, uint32_t dc_model, const model* dcm,
+                       const model* rnm, const model* lvm, renc* e)
+{
+    size_t pi = t->pairs;
+    for (uint32_t b = t->blocks; b-- > 0u;) {
+        const uint32_t np = t->np[b];
+        pi -= np;
+        put_sym(e, rnm->freq[63], rnm->cum[63]);
+        for (uint32_t k = np; k-- > 0u;) {
+            const uint32_t lm = t->lvl_m[pi + k];
+            const uint32_t ls = bitlen(lm);
+            put_suffix(e, ls, lm);
+            uint32_t lc = 0;
+            if (lvl_model == 1) {
+                uint32_t pos = 0;
+                for (uint32_t j = 0; j <= k; ++j) { pos += t->run[pi + j] + 1u; }
+                lc = pos_ctx(pos);
+            } else if (lvl_model == 2) {
+                lc = prev_ctx(k != 0u ? bitlen(t->lvl_m[pi + k - 1u]) : 0u, k != 0u);
+            }
+            put_sym(e, lvm[lc].freq[ls], lvm[lc].cum[ls]);
+            const uint32_t r = t->run[pi + k];
+            put_sym(e, rnm->freq[r], rnm->cum[r]);
+        }
+        const uint32_t dm = t->dc_m[b];
+        const uint32_t ds = bitlen(dm);
+        put_suffix(e, ds, dm);
+        const uint32_t dctx = dc_model == 1 ? dcp_ctx(b != 0u ? bitlen(t->dc_m[b - 1u]) : 0u, b != 0u) : 0u;
+        put_sym(e, dcm[dctx].freq[ds], dcm[dctx].cum[ds]);
+    }
+}
+
+/* stream bytes as the decoder reads them: final state big-endian, then the
+ * emitted bytes in reverse (rans.c:165-228) */
+static void stream_out(const renc* e, uint8_t* dst)
+{
+    be32(dst, e->x);
+    for (size_t i = 0; i < e->pos; ++i) { dst[4u + i] = e->buf[e->pos - 1u - i]; }
+}
+
 /* V7-R2 slice entropy coding (codec.c:2116-2515): joint histograms, per-slice
  * model choice, prefix tables, backward rANS walk, flush. Output payload is
  * appended to *out (malloc'd). */
@@ -1022,34 +1105,9 @@ static int32_t band_rans2(const band_tok* t, const uint32_t dch[DC_SYMS], const 
                           const uint32_t lvlh[LVL_SYMS], uint8_t** out, size_t* out_n)
 {
     uint32_t jpos[POS_CTX * LVL_SYMS] = {0}, jprev[PREV_CTX * LVL_SYMS] = {0}, jdc[DCP_CTX * DC_SYMS] = {0};
-    {
-        size_t pi = 0;
-        uint32_t prev_dcc = 0;
-        for (uint32_t b = 0; b < t->blocks; ++b) {
-            const uint32_t dcc = bitlen(t->dc_m[b]);
-            jdc[(b == 0u ? 0u : dcp_ctx(prev_dcc, 1)) * DC_SYMS + dcc]++;
-            prev_dcc = dcc;
-            uint32_t ppos = 0, pcat = 0;
-            for (uint32_t k = 0; k < t->np[b]; ++k, ++pi) {
-                const uint32_t cat = bitlen(t->lvl_m[pi]);
-                const uint32_t pos = ppos + t->run[pi] + 1u;
-                jpos[pos_ctx(pos) * LVL_SYMS + cat]++;
-                jprev[prev_ctx(pcat, k != 0u) * LVL_SYMS + cat]++;
-                pcat = cat;
-                ppos = pos;
-            }
-        }
-    }
-    uint32_t lvl_model = 0;
-    double best = rows_cost(lvlh, 1u, LVL_SYMS) + 8.0 * (double)LVL_SYMS;
-    const double pc = rows_cost(jpos, POS_CTX, LVL_SYMS) + 8.0 * (double)(POS_CTX * LVL_SYMS);
-    if (pc < best) { best = pc; lvl_model = 1; }
-    const double prc = rows_cost(jprev, PREV_CTX, LVL_SYMS) + 8.0 * (double)(PREV_CTX * LVL_SYMS);
-    if (prc < best) { lvl_model = 2; }
-    uint32_t dc_model = 0;
-    const double dn = rows_cost(dch, 1u, DC_SYMS) + 8.0 * (double)DC_SYMS;
-    const double dp = rows_cost(jdc, DCP_CTX, DC_SYMS) + 8.0 * (double)(DCP_CTX * DC_SYMS);
-    if (dp < dn) { dc_model = 1; }
+    tok_joints(t, jpos, jprev, jdc);
+    uint32_t lvl_model, dc_model;
+    pick_models(dch, lvlh, jpos, jprev, jdc, &lvl_model, &dc_model);
 
     const uint32_t nl = lvl_model == 1 ? POS_CTX : lvl_model == 2 ? PREV_CTX : 1u;
     const uint32_t nd = dc_model == 1 ? DCP_CTX : 1u;
@@ -1074,40 +1132,12 @@ static int32_t band_rans2(const band_tok* t, const uint32_t dch[DC_SYMS], const 
     }
 
     renc e = {RANS_L, NULL, 0, 0};
-    size_t pi = t->pairs;
-    for (uint32_t b = t->blocks; b-- > 0u;) {
-        const uint32_t np = t->np[b];
-        pi -= np;
-        put_sym(&e, rnm.freq[63], rnm.cum[63]);
-        for (uint32_t k = np; k-- > 0u;) {
-            const uint32_t lm = t->lvl_m[pi + k];
-            const uint32_t ls = bitlen(lm);
-            put_suffix(&e, ls, lm);
-            uint32_t lc = 0;
-            if (lvl_model == 1) {
-                uint32_t pos = 0;
-                for (uint32_t j = 0; j <= k; ++j) { pos += t->run[pi + j] + 1u; }
-                lc = pos_ctx(pos);
-            } else if (lvl_model == 2) {
-                lc = prev_ctx(k != 0u ? bitlen(t->lvl_m[pi + k - 1u]) : 0u, k != 0u);
-            }
-            put_sym(&e, lvm[lc].freq[ls], lvm[lc].cum[ls]);
-            const uint32_t r = t->run[pi + k];
-            put_sym(&e, rnm.freq[r], rnm.cum[r]);
-        }
-        const uint32_t dm = t->dc_m[b];
-        const uint32_t ds = bitlen(dm);
-        put_suffix(&e, ds, dm);
-        const uint32_t dctx = dc_model == 1 ? dcp_ctx(b != 0u ? bitlen(t->dc_m[b - 1u]) : 0u, b != 0u) : 0u;
-        put_sym(&e, dcm[dctx].freq[ds], dcm[dctx].cum[ds]);
-    }
-    /* payload = prefix | final state (big-endian) | bytes in consumption order
-     * (rans.c:165-228) */
+    tok_stream(t, lvl_model, dc_model, dcm, &rnm, lvm, &e);
+    /* payload = prefix | final state (big-endian) | bytes in consumption order */
     const size_t total = off + 4u + e.pos;
     uint8_t* pay = (uint8_t*)malloc(total);
     memcpy(pay, prefix, off);
-    be32(pay + off, e.x);
-    for (size_t i = 0; i < e.pos; ++i) { pay[off + 4u + i] = e.buf[e.pos - 1u - i]; }
+    stream_out(&e, pay + off);
     free(e.buf);
     *out = pay;
     *out_n = total;
@@ -1272,6 +1302,9 @@ typedef struct slice_out {
     int alpha;
 } slice_out;
 
+static int32_t v8_encode_frame(const topos_frame_config* cfg, hdr* h, const topos_frame_input* in, uint8_t** pkt_out,
+                               size_t* pkt_n, topos_frame_stats* st);
+
 static int32_t encode_frame(const topos_frame_config* cfg, const topos_frame_input* in,
                             uint8_t** pkt_out, size_t* pkt_n, topos_frame_stats* st)
 {
@@ -1293,8 +1326,9 @@ static int32_t encode_frame(const topos_frame_config* cfg, const topos_frame_inp
             return fail(TC_ERR_INVALID_ARGUMENT, "input stride[%u] < visible width", p);
         }
     }
+    if (h.major == 8u && h.em == 8u) { return v8_encode_frame(cfg, &h, in, pkt_out, pkt_n, st); }
     if (h.major != 7u || h.em != 7u) {
-        return fail(TC_ERR_NOT_IMPLEMENTED, "oracle encodes only the V7-R2 generation");
+        return fail(TC_ERR_NOT_IMPLEMENTED, "oracle encodes only the V7-R2 and V8 generations");
     }
     uint16_t qmL[64], qmC[64];
     if (!qm_lookup(h.qm, 0, qmL) || !qm_lookup(h.qm, 1, qmC)) {
@@ -1413,6 +1447,318 @@ static int32_t encode_frame(const topos_frame_config* cfg, const topos_frame_inp
     st->slice_count = (uint16_t)total;
     st->qp_base = h.qp;
     st->alpha_max_abs_error = alpha_err;
+    *pkt_out = pkt;
+    *pkt_n = (size_t)size;
+    return TC_OK;
+}
+
+/* ============================ V8 segmented rANS encode ============================ */
+/* reference: codec.c:3817-4320 (v8_tokenize_segment, v8_write_table,
+ * v8_encode_plane, v8_frame_encode_ready), packet.h:36-82 (layout).
+ * Per colour plane: [segment directory S x 12][tile tables T x 350]
+ * [segment streams][tile CRCs T x 4]. A segment is sb consecutive blocks in
+ * raster order with its own rANS chain; a tile is tile_rows block rows and
+ * owns the segments whose first block it holds; its model is chosen from the
+ * summed counts of its segments. */
+#define V8_EXT 8u
+#define V8_TABLE 350u
+#define V8_DIR 12u
+#define V8_MAXSEG 32u
+
+static uint32_t crc_update(uint32_t crc, const uint8_t* p, size_t n)
+{
+    (void)tco_crc32(p, 0u);  /* table */
+    uint32_t c = crc ^ 0xFFFFFFFFu;
+    for (size_t i = 0; i < n; ++i) { c = g_crc_tab[(c ^ p[i]) & 0xFFu] ^ (c >> 8); }
+    return c ^ 0xFFFFFFFFu;
+}
+
+typedef struct v8tile {
+    uint32_t plane, seg_first, seg_count, table_off, stream_off, stream_bytes, crc_stored, crc_ok;
+} v8tile;
+
+typedef struct v8view {
+    hdr h;
+    uint32_t sb, tile_rows;
+    uint32_t segs[4], tiles[4], dir_off[4], table_off[4], stream_off[4], crc_off[4];
+    uint32_t ntiles;
+    v8tile t[MAX_SLICES];
+} v8view;
+
+static int32_t v8_scan(const uint8_t* d, size_t n, v8view* v, int verify_crc);
+
+typedef struct v8seg {
+    uint32_t dc_m[V8_MAXSEG];
+    uint8_t np[V8_MAXSEG];
+    uint8_t run[V8_MAXSEG * 63u];
+    uint32_t lvl_m[V8_MAXSEG * 63u];
+    band_tok t;
+} v8seg;
+
+/* tokens of one segment (codec.c:3882-3947): DC predicted inside the segment
+ * only (left = the segment's previous block, top = the block one row up when
+ * the segment reaches that far), AC run/level pairs in zigzag order */
+static int32_t v8_seg_tokens(const int32_t* qplane, uint32_t cols, uint32_t b0, uint32_t nb, v8seg* g,
+                             uint32_t dch[DC_SYMS], uint32_t runh[RUN_SYMS], uint32_t lvlh[LVL_SYMS])
+{
+    int viol = 0;
+    uint32_t pi = 0;
+    int32_t sdc[V8_MAXSEG];
+    for (uint32_t i = 0; i < nb; ++i) {
+        const int32_t* q = qplane + (size_t)(b0 + i) * 64u;
+        sdc[i] = q[0];
+        const int32_t pred = dc_pred(i != 0u, i != 0u ? sdc[i - 1u] : 0, i >= cols, sdc[i >= cols ? i - cols : 0u]);
+        uint32_t dcm = map_s(q[0] - pred);
+        if (dcm > M_MAX_DC_BD16) { dcm = M_MAX_DC_BD16; viol = 1; }
+        g->dc_m[i] = dcm;
+        dch[bitlen(dcm)]++;
+        uint32_t prev = 0, np = 0;
+        for (uint32_t pos = 1; pos < 64u; ++pos) {
+            const int32_t v = q[ZZ[pos]];
+            if (v == 0) { continue; }
+            uint32_t lm = map_s(v);
+            if (lm > M_MAX_LVL_BD16) { lm = M_MAX_LVL_BD16; viol = 1; }
+            const uint32_t r = pos - prev - 1u;
+            g->run[pi] = (uint8_t)r;
+            g->lvl_m[pi] = lm;
+            pi++; np++;
+            runh[r]++;
+            lvlh[bitlen(lm)]++;
+            prev = pos;
+        }
+        g->np[i] = (uint8_t)np;
+        runh[63]++;
+    }
+    g->t.blocks = nb;
+    g->t.pairs = pi;
+    g->t.dc_m = g->dc_m;
+    g->t.np = g->np;
+    g->t.run = g->run;
+    g->t.lvl_m = g->lvl_m;
+    if (viol) { return fail(TC_ERR_INVALID_ARGUMENT, "token domain violated (bit_depth 16 qp too low): raise qp"); }
+    return TC_OK;
+}
+
+/* segments of tile t: [floor(first block / sb), floor(next tile's first block / sb)) */
+static void v8_tile_segs(uint32_t t, uint32_t tile_rows, uint32_t cols, uint32_t blocks, uint32_t sb, uint32_t S,
+                         uint32_t* sf, uint32_t* sn)
+{
+    const uint64_t fb = tile_rows == 0u ? 0u : (uint64_t)t * tile_rows * cols;
+    const uint64_t fn = tile_rows == 0u ? (uint64_t)blocks : (uint64_t)(t + 1u) * tile_rows * cols;
+    uint32_t a = (uint32_t)(fb / sb), b = (uint32_t)(fn / sb);
+    if (a > S) { a = S; }
+    if (b > S) { b = S; }
+    if (b < a) { b = a; }
+    *sf = a;
+    *sn = b;
+}
+
+/* one colour plane's V8 payload (codec.c:3974-4200) */
+static int32_t v8_encode_plane(const hdr* h, uint32_t p, const uint16_t* coded, const qctx* q, uint32_t qdb,
+                               uint32_t sb, uint32_t tile_rows, uint8_t** out, size_t* out_n, uint32_t* tiles)
+{
+    const uint32_t cols = h->bcols[p], rows = h->brows[p], blocks = rows * cols;
+    const uint32_t S = (blocks + sb - 1u) / sb;
+    const uint32_t T = tile_rows == 0u ? 1u : (rows + tile_rows - 1u) / tile_rows;
+    *tiles = T;
+    /* quantised coefficients of the whole plane, natural order */
+    const uint32_t stride = cols * 8u;
+    const int32_t mid = (int32_t)(1u << (h->bd - 1u));
+    const int wide = h->bd > 12u;
+    int32_t* qp = (int32_t*)malloc((size_t)blocks * 64u * sizeof(int32_t) + 1u);
+    for (uint32_t b = 0; b < blocks; ++b) {
+        const uint32_t bx = b % cols, by = b / cols;
+        int32_t x[64], F[64];
+        const uint16_t* src = coded + (size_t)by * 8u * stride + (size_t)bx * 8u;
+        for (int yy = 0; yy < 8; ++yy) {
+            for (int xx = 0; xx < 8; ++xx) {
+                const int32_t d = (int32_t)src[(size_t)yy * stride + xx] - mid;
+                x[yy * 8 + xx] = wide ? d : (int32_t)(int16_t)d;
+            }
+        }
+        tco_forward_8x8(x, F, wide);
+        quantize(q, F, qp + (size_t)b * 64u);
+    }
+    uint8_t* dir = (uint8_t*)calloc((size_t)S * V8_DIR + 1u, 1);
+    uint8_t* tabs = (uint8_t*)calloc((size_t)T * V8_TABLE, 1);
+    uint8_t* streams = NULL;
+    size_t slen = 0, scap = 0;
+    v8seg* g = (v8seg*)malloc(sizeof(v8seg));
+    int32_t rc = TC_OK;
+    static const uint32_t zeros[64];
+    for (uint32_t t = 0; t < T && rc == TC_OK; ++t) {
+        uint32_t sf, sn;
+        v8_tile_segs(t, tile_rows, cols, blocks, sb, S, &sf, &sn);
+        uint32_t dch[DC_SYMS] = {0}, runh[RUN_SYMS] = {0}, lvlh[LVL_SYMS] = {0};
+        uint32_t jpos[POS_CTX * LVL_SYMS] = {0}, jprev[PREV_CTX * LVL_SYMS] = {0}, jdc[DCP_CTX * DC_SYMS] = {0};
+        for (uint32_t k = sf; k < sn && rc == TC_OK; ++k) {
+            const uint32_t b0 = k * sb, nb = blocks - b0 < sb ? blocks - b0 : sb;
+            rc = v8_seg_tokens(qp, cols, b0, nb, g, dch, runh, lvlh);
+            if (rc == TC_OK) { tok_joints(&g->t, jpos, jprev, jdc); }
+        }
+        if (rc != TC_OK) { break; }
+        uint32_t lm, dm;
+        pick_models(dch, lvlh, jpos, jprev, jdc, &lm, &dm);
+        const uint32_t nl = lm == 1 ? POS_CTX : lm == 2 ? PREV_CTX : 1u;
+        const uint32_t nd = dm == 1 ? DCP_CTX : 1u;
+        const uint32_t* drows = dm == 1 ? jdc : dch;
+        const uint32_t* lrows = lm == 1 ? jpos : lm == 2 ? jprev : lvlh;
+        /* 350-byte table: flags, 5 DC rows, run row, 5 level rows; rows past the
+         * model's contexts hold the all-zero row {1, 0, ...} (codec.c:3949-3971) */
+        uint8_t* tb = tabs + (size_t)t * V8_TABLE;
+        tb[0] = (uint8_t)(lm | (dm << 2));
+        for (uint32_t c = 0; c < DCP_CTX; ++c) { row_encode(tb + 1u + c * DC_SYMS, DC_SYMS, c < nd ? drows + c * DC_SYMS : zeros); }
+        row_encode(tb + 1u + DCP_CTX * DC_SYMS, RUN_SYMS, runh);
+        for (uint32_t c = 0; c < PREV_CTX; ++c) {
+            row_encode(tb + 1u + DCP_CTX * DC_SYMS + RUN_SYMS + c * LVL_SYMS, LVL_SYMS, c < nl ? lrows + c * LVL_SYMS : zeros);
+        }
+        model dcm[DCP_CTX], lvm[PREV_CTX], rnm;
+        for (uint32_t c = 0; c < nd && rc == TC_OK; ++c) {
+            if (row_decode(tb + 1u + c * DC_SYMS, DC_SYMS, &dcm[c]) != TC_OK) { rc = TC_ERR_INVALID_ARGUMENT; }
+        }
+        if (rc == TC_OK && row_decode(tb + 1u + DCP_CTX * DC_SYMS, RUN_SYMS, &rnm) != TC_OK) { rc = TC_ERR_INVALID_ARGUMENT; }
+        for (uint32_t c = 0; c < nl && rc == TC_OK; ++c) {
+            if (row_decode(tb + 1u + DCP_CTX * DC_SYMS + RUN_SYMS + c * LVL_SYMS, LVL_SYMS, &lvm[c]) != TC_OK) {
+                rc = TC_ERR_INVALID_ARGUMENT;
+            }
+        }
+        for (uint32_t k = sf; k < sn && rc == TC_OK; ++k) {
+            const uint32_t b0 = k * sb, nb = blocks - b0 < sb ? blocks - b0 : sb;
+            uint32_t d0[DC_SYMS] = {0}, r0[RUN_SYMS] = {0}, l0[LVL_SYMS] = {0};
+            rc = v8_seg_tokens(qp, cols, b0, nb, g, d0, r0, l0);
+            if (rc != TC_OK) { break; }
+            renc e = {RANS_L, NULL, 0, 0};
+            tok_stream(&g->t, lm, dm, dcm, &rnm, lvm, &e);
+            const size_t n = 4u + e.pos;
+            if (slen + n > scap) {
+                scap = (slen + n) * 2u + 4096u;
+                streams = (uint8_t*)realloc(streams, scap);
+            }
+            stream_out(&e, streams + slen);
+            free(e.buf);
+            uint8_t* de = dir + (size_t)k * V8_DIR;
+            be32(de, (uint32_t)slen);
+            be32(de + 4, (uint32_t)n);
+            de[8] = (uint8_t)qdb;
+            slen += n;
+        }
+    }
+    free(g);
+    free(qp);
+    if (rc != TC_OK) { free(dir); free(tabs); free(streams); return rc; }
+    const size_t total = (size_t)S * V8_DIR + (size_t)T * V8_TABLE + slen + (size_t)T * 4u;
+    uint8_t* pay = (uint8_t*)malloc(total + 1u);
+    memcpy(pay, dir, (size_t)S * V8_DIR);
+    memcpy(pay + (size_t)S * V8_DIR, tabs, (size_t)T * V8_TABLE);
+    const size_t sbase = (size_t)S * V8_DIR + (size_t)T * V8_TABLE;
+    if (slen) { memcpy(pay + sbase, streams, slen); }
+    for (uint32_t t = 0; t < T; ++t) {
+        uint32_t sf, sn;
+        v8_tile_segs(t, tile_rows, cols, blocks, sb, S, &sf, &sn);
+        const uint32_t soff = sf < S ? ld32(dir + (size_t)sf * V8_DIR) : 0u;
+        uint32_t sbytes = 0;
+        for (uint32_t k = sf; k < sn; ++k) { sbytes += ld32(dir + (size_t)k * V8_DIR + 4u); }
+        uint32_t crc = crc_update(0u, tabs + (size_t)t * V8_TABLE, V8_TABLE);
+        crc = crc_update(crc, pay + sbase + soff, sbytes);
+        be32(pay + sbase + slen + (size_t)t * 4u, crc);
+    }
+    free(dir);
+    free(tabs);
+    free(streams);
+    *out = pay;
+    *out_n = total;
+    return TC_OK;
+}
+
+/* V8 frame (codec.c:4204-4319): colour planes only; the packet is the frame
+ * header (slice count = tiles of all planes), the 8-byte extension
+ * (segment blocks log2, tile rows log2, zeros) and the plane payloads */
+static int32_t v8_encode_frame(const topos_frame_config* cfg, hdr* h, const topos_frame_input* in, uint8_t** pkt_out,
+                               size_t* pkt_n, topos_frame_stats* st)
+{
+    const uint32_t sb_log2 = cfg->reserved[3] != 0u ? cfg->reserved[3] : 4u;
+    const uint32_t tile_log2 = cfg->reserved[4] != 0u ? cfg->reserved[4] : 5u;
+    if (sb_log2 < 3u || sb_log2 > 5u) { return fail(TC_ERR_INVALID_ARGUMENT, "v8 reserved[3] sb_log2 %u not in {3,4,5}", sb_log2); }
+    if (tile_log2 != 0u && (tile_log2 < 4u || tile_log2 > 6u)) {
+        return fail(TC_ERR_INVALID_ARGUMENT, "v8 reserved[4] tile_log2 %u not in {0,4,5,6}", tile_log2);
+    }
+    if (h->amode != 0u) { return fail(TC_ERR_NOT_IMPLEMENTED, "v8 alpha pending"); }
+    if (h->pf == 3u) { return fail(TC_ERR_NOT_IMPLEMENTED, "v8 does not carry CFA (TRAW uses rans2)"); }
+    uint16_t qmL[64], qmC[64];
+    if (!qm_lookup(h->qm, 0, qmL) || !qm_lookup(h->qm, 1, qmC)) {
+        return fail(TC_ERR_UNSUPPORTED_MATRIX, "qmatrix_id %u", h->qm);
+    }
+    const uint32_t refined = (h->flags & 0x8u) != 0u;
+    uint8_t* pay[3] = {NULL, NULL, NULL};
+    size_t pn[3] = {0, 0, 0};
+    uint32_t tiles[3] = {0, 0, 0};
+    int32_t rc = TC_OK;
+    for (uint32_t p = 0; p < 3u && rc == TC_OK; ++p) {
+        const uint32_t cw = h->pcw[p], ch = h->pch[p], vw = h->pvw[p], vh = h->pvh[p];
+        const size_t sstride = in->strides[p] ? in->strides[p] : vw;
+        uint16_t* coded = (uint16_t*)malloc((size_t)cw * ch * sizeof(uint16_t));
+        for (uint32_t y = 0; y < ch; ++y) {
+            const uint16_t* sr = in->planes[p] + (size_t)(y < vh ? y : vh - 1u) * sstride;
+            for (uint32_t x = 0; x < cw; ++x) { coded[(size_t)y * cw + x] = sr[x < vw ? x : vw - 1u]; }
+        }
+        const int chroma = p == 1u || p == 2u;
+        const int32_t delta = chroma ? cfg->qp_delta_chroma : cfg->qp_delta_luma;
+        int32_t qe = (int32_t)h->qp + delta + (h->bd >= 12u ? 2 * ((int32_t)h->bd - 10) : 0);
+        if (qe < 0) { qe = 0; }
+        const int32_t ceil = h->qp >= QP_V15_MIN ? (int32_t)QP_MAX : 63;
+        if (qe > ceil) { qe = ceil; }
+        qctx q;
+        qctx_init(&q, chroma ? qmC : qmL, (uint32_t)qe, h->bd, refined);
+        rc = v8_encode_plane(h, p, coded, &q, (uint32_t)(64 + qe - (int32_t)h->qp), 1u << sb_log2,
+                             tile_log2 == 0u ? 0u : 1u << tile_log2, &pay[p], &pn[p], &tiles[p]);
+        free(coded);
+    }
+    const uint32_t nt = tiles[0] + tiles[1] + tiles[2];
+    if (rc == TC_OK && (nt < 3u || nt > MAX_SLICES)) { rc = fail(TC_ERR_LIMIT_EXCEEDED, "v8 tile count %u out of [3,512]", nt); }
+    uint64_t size = HDR_SIZE + V8_EXT;
+    for (uint32_t p = 0; p < 3u; ++p) { size += pn[p]; }
+    if (rc == TC_OK && size > MAX_PACKET) { rc = fail(TC_ERR_LIMIT_EXCEEDED, "frame packet exceeds 256 MiB"); }
+    uint8_t* pkt = NULL;
+    if (rc == TC_OK) {
+        pkt = (uint8_t*)calloc((size_t)size, 1);
+        pkt[HDR_SIZE] = (uint8_t)sb_log2;
+        pkt[HDR_SIZE + 1u] = (uint8_t)tile_log2;
+        size_t off = HDR_SIZE + V8_EXT;
+        for (uint32_t p = 0; p < 3u; ++p) {
+            memcpy(pkt + off, pay[p], pn[p]);
+            off += pn[p];
+        }
+        h->slices = (uint16_t)nt;
+        h->size = (uint32_t)size;
+        rc = hdr_validate(h);
+        if (rc == TC_OK) { hdr_pack(h, pkt); }
+    }
+    for (uint32_t p = 0; p < 3u; ++p) { free(pay[p]); }
+    if (rc == TC_OK) {
+        /* self-check (codec.c:4289-4304): a structure scan with tile CRCs.
+         * It fails where a plane's last segment lies past the last tile's
+         * nominal block range (no tile owns it, its directory entry stays
+         * zero): the reference rejects such frames as MALFORMED. */
+        v8view* v = (v8view*)malloc(sizeof(v8view));
+        const int32_t src = v8_scan(pkt, (size_t)size, v, 1);
+        if (src != TC_OK) {
+            rc = fail(TC_ERR_MALFORMED, "v8 self-check scan failed");
+        } else {
+            for (uint32_t t = 0; t < v->ntiles; ++t) {
+                if (!v->t[t].crc_ok) { rc = fail(TC_ERR_MALFORMED, "v8 self-check: tile %u crc", t); break; }
+            }
+        }
+        free(v);
+    }
+    if (rc != TC_OK) { free(pkt); return rc; }
+    st->packet_size = (uint32_t)size;
+    st->color_payload_bytes = (uint32_t)(pn[0] + pn[1] + pn[2]);
+    st->alpha_payload_bytes = 0;
+    st->color_header_bytes = HDR_SIZE + V8_EXT;
+    st->alpha_header_bytes = 0;
+    st->slice_count = (uint16_t)nt;
+    st->qp_base = h->qp;
+    st->alpha_max_abs_error = 0;
     *pkt_out = pkt;
     *pkt_n = (size_t)size;
     return TC_OK;
@@ -1894,6 +2240,236 @@ static int32_t decode_view(const pview* v, uint16_t* const planes[4], const size
     return TC_OK;
 }
 
+/* ============================ V8 segmented rANS decode ============================ */
+/* reference: packet.c:103-266 (tc_packet_scan_v8_ex), codec.c:4349-4475
+ * (v8_tile_dec_build, v8_decode_segment_q), 4772-4975 (v8_frame_decode).
+ * A tile whose CRC (table + member streams) mismatches is concealed whole;
+ * a segment whose stream fails is concealed alone; concealment reconstructs
+ * the segment's blocks from zero coefficients (the mid level). The call
+ * returns TC_OK even when it concealed (concealed_slices and per-tile status
+ * tell), and no deblocking runs. */
+static int32_t v8_scan(const uint8_t* d, size_t n, v8view* v, int verify_crc)
+{
+    memset(v, 0, sizeof(*v));
+    int32_t rc = hdr_decode(d, n, &v->h);
+    if (rc != TC_OK) { return rc; }
+    if (v->h.major != 8u && v->h.major != 9u) { return vf(TC_ERR_UNSUPPORTED_VERSION, "version_major(not v8/v9)", v->h.major); }
+    if ((uint64_t)v->h.size != (uint64_t)n) { return fail(TC_ERR_MALFORMED, "frame_packet_size %u != actual %zu", v->h.size, n); }
+    if (n < HDR_SIZE + V8_EXT) { return fail(TC_ERR_TRUNCATED, "v8 ext header out of packet"); }
+    const uint8_t* ext = d + HDR_SIZE;
+    if (ext[0] < 3u || ext[0] > 5u) { return vf(TC_ERR_MALFORMED, "segment_blocks_log2", ext[0]); }
+    if (ext[1] != 0u && (ext[1] < 4u || ext[1] > 6u)) { return vf(TC_ERR_MALFORMED, "tile_rows_log2", ext[1]); }
+    for (uint32_t i = 2; i < V8_EXT; ++i) {
+        if (ext[i] != 0u) { return vf(TC_ERR_MALFORMED, "ext reserved(!=0)", ext[i]); }
+    }
+    v->sb = 1u << ext[0];
+    v->tile_rows = ext[1] == 0u ? 0u : 1u << ext[1];
+    size_t off = HDR_SIZE + V8_EXT;
+    uint32_t nt = 0;
+    for (uint32_t p = 0; p < v->h.planes; ++p) {
+        const uint32_t rows = v->h.brows[p], cols = v->h.bcols[p], blocks = rows * cols;
+        const uint32_t S = (blocks + v->sb - 1u) / v->sb;
+        const uint32_t T = (v->tile_rows == 0u || rows == 0u) ? 1u : (rows + v->tile_rows - 1u) / v->tile_rows;
+        v->segs[p] = S;
+        v->tiles[p] = T;
+        v->dir_off[p] = (uint32_t)off;
+        if (off > n || (size_t)S * V8_DIR > n - off) { return fail(TC_ERR_TRUNCATED, "v8 plane %u dir out of packet", p); }
+        off += (size_t)S * V8_DIR;
+        v->table_off[p] = (uint32_t)off;
+        if (off > n || (size_t)T * V8_TABLE > n - off) { return fail(TC_ERR_TRUNCATED, "v8 plane %u tables out of packet", p); }
+        off += (size_t)T * V8_TABLE;
+        v->stream_off[p] = (uint32_t)off;
+        const uint8_t* dir = d + v->dir_off[p];
+        uint64_t sl = 0;
+        for (uint32_t k = 0; k < S; ++k) {
+            const uint32_t so = ld32(dir + (size_t)k * V8_DIR), ln = ld32(dir + (size_t)k * V8_DIR + 4u);
+            if (ln < 4u) { return vf(TC_ERR_MALFORMED, "segment stream_len(<state)", ln); }
+            if (k == 0u) {
+                if (so != 0u) { return vf(TC_ERR_MALFORMED, "seg0 stream_off", so); }
+            } else if (so != ld32(dir + (size_t)(k - 1u) * V8_DIR) + ld32(dir + (size_t)(k - 1u) * V8_DIR + 4u)) {
+                return vf(TC_ERR_MALFORMED, "segment dir gap/off", so);
+            }
+            sl += ln;
+            if (sl > MAX_PACKET) { return vf(TC_ERR_LIMIT_EXCEEDED, "plane stream bytes", sl); }
+        }
+        if (off > n || sl > n - off) { return fail(TC_ERR_TRUNCATED, "v8 plane %u stream out of packet", p); }
+        off += (size_t)sl;
+        v->crc_off[p] = (uint32_t)off;
+        if (off > n || (size_t)T * 4u > n - off) { return fail(TC_ERR_TRUNCATED, "v8 plane %u crc out of packet", p); }
+        for (uint32_t t = 0; t < T; ++t) {
+            if (nt + t >= MAX_SLICES) { return vf(TC_ERR_MALFORMED, "slice_count(!= tile total)", nt + t); }
+            v8tile* ti = &v->t[nt + t];
+            uint32_t sf, sn;
+            v8_tile_segs(t, v->tile_rows, cols, blocks, v->sb, S, &sf, &sn);
+            ti->plane = p;
+            ti->seg_first = sf;
+            ti->seg_count = sn - sf;
+            ti->table_off = v->table_off[p] + t * V8_TABLE;
+        }
+        nt += T;
+        off += (size_t)T * 4u;
+    }
+    if (off != n) { return fail(TC_ERR_MALFORMED, "v8 packet has %zu trailing bytes", n - off); }
+    if (nt != v->h.slices) { return vf(TC_ERR_MALFORMED, "slice_count(!= tile total)", ((unsigned long long)v->h.slices << 16) | nt); }
+    v->ntiles = nt;
+    uint32_t tbase = 0;
+    for (uint32_t p = 0; p < v->h.planes; ++p) {
+        for (uint32_t t = 0; t < v->tiles[p]; ++t) {
+            v8tile* ti = &v->t[tbase + t];
+            const uint8_t* e0 = d + v->dir_off[p] + (size_t)ti->seg_first * V8_DIR;
+            ti->stream_off = ti->seg_count ? v->stream_off[p] + ld32(e0) : v->stream_off[p] + (ti->seg_first < v->segs[p] ? ld32(e0) : 0u);
+            ti->stream_bytes = 0;
+            for (uint32_t k = 0; k < ti->seg_count; ++k) { ti->stream_bytes += ld32(e0 + (size_t)k * V8_DIR + 4u); }
+            ti->crc_stored = ld32(d + v->crc_off[p] + (size_t)t * 4u);
+            if (verify_crc) {
+                uint32_t crc = crc_update(0u, d + ti->table_off, V8_TABLE);
+                crc = crc_update(crc, d + ti->stream_off, ti->stream_bytes);
+                ti->crc_ok = crc == ti->crc_stored;
+            }
+        }
+        tbase += v->tiles[p];
+    }
+    return TC_OK;
+}
+
+/* one segment: forward decode with the tile's models, blocks reconstructed
+ * into the plane as they decode (codec.c:4382-4475); DC and level magnitudes
+ * and the DC domain use the 12-bit limits at every bit depth */
+static int32_t v8_segment_decode(const uint8_t* s, size_t n, uint32_t lm, uint32_t dm, const model* dcm,
+                                 const model* rnm, const model* lvm, uint32_t nb, uint32_t cols, uint32_t b0,
+                                 const qctx* q, const store* st)
+{
+    if (n < 4u) { return TC_ERR_TRUNCATED; }
+    rdec d;
+    d.b = s;
+    d.n = n;
+    d.x = ld32(s);
+    d.pos = 4u;
+    if (d.x < RANS_L) { return TC_ERR_MALFORMED; }
+    int32_t sdc[V8_MAXSEG];
+    uint32_t prev_dcc = 0;
+    for (uint32_t i = 0; i < nb; ++i) {
+        int32_t blk[64] = {0};
+        const model* dmv = &dcm[(i == 0u || dm != 1u) ? 0u : dcp_ctx(prev_dcc, 1)];
+        uint32_t cat, m;
+        int32_t rc;
+        if ((rc = rd_sym(&d, dmv, &cat)) != TC_OK) { return rc; }
+        if ((rc = rd_suffix(&d, cat, &m)) != TC_OK) { return rc; }
+        if (m > M_MAX_DC) { return TC_ERR_MALFORMED; }
+        const int32_t pred = dc_pred(i != 0u, i != 0u ? sdc[i - 1u] : 0, i >= cols, sdc[i >= cols ? i - cols : 0u]);
+        const int64_t dcv = (int64_t)pred + unmap_s(m);
+        if (dcv > DC_DOMAIN || dcv < -DC_DOMAIN) { return TC_ERR_MALFORMED; }
+        blk[0] = (int32_t)dcv;
+        sdc[i] = blk[0];
+        prev_dcc = cat;
+        uint32_t pos = 1, pcat = 0;
+        int has = 0;
+        for (;;) {
+            uint32_t r;
+            if ((rc = rd_sym(&d, rnm, &r)) != TC_OK) { return rc; }
+            if (r == 63u) { break; }
+            const uint32_t idx = pos + r;
+            if (idx > 63u) { return TC_ERR_MALFORMED; }
+            const uint32_t lc = lm == 1u ? pos_ctx(idx) : lm == 2u ? prev_ctx(pcat, has) : 0u;
+            if ((rc = rd_sym(&d, &lvm[lc], &cat)) != TC_OK) { return rc; }
+            if ((rc = rd_suffix(&d, cat, &m)) != TC_OK) { return rc; }
+            if (m > M_MAX_LVL) { return TC_ERR_MALFORMED; }
+            blk[ZZ[idx]] = unmap_s(m);
+            pcat = cat;
+            has = 1;
+            pos = idx + 1u;
+        }
+        const uint32_t ab = b0 + i;
+        store_block(st, q, ab % cols, ab / cols, blk);
+    }
+    return d.pos == d.n ? TC_OK : TC_ERR_MALFORMED;
+}
+
+static int32_t v8_decode(const uint8_t* data, size_t size, uint16_t* const planes[4], const size_t* strides,
+                         topos_frame_output* o)
+{
+    v8view* v = (v8view*)malloc(sizeof(v8view));
+    int32_t rc = v8_scan(data, size, v, 0);
+    if (rc != TC_OK) { free(v); return rc; }
+    const hdr* h = &v->h;
+    if (h->pf == 3u) { free(v); return fail(TC_ERR_UNSUPPORTED_PIXEL_FORMAT, "v8 does not carry CFA (TRAW uses rans2)"); }
+    fill_info(h, o);
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        if (planes[p] == NULL) { free(v); return fail(TC_ERR_INVALID_ARGUMENT, "v8 planes_out[%u] == NULL", p); }
+    }
+    /* tile models first: a malformed table rejects the frame */
+    typedef struct tmod { uint32_t lm, dm; model dcm[DCP_CTX], rnm, lvm[PREV_CTX]; } tmod;
+    tmod* tm = (tmod*)malloc(sizeof(tmod) * (v->ntiles ? v->ntiles : 1u));
+    for (uint32_t t = 0; t < v->ntiles && rc == TC_OK; ++t) {
+        const uint8_t* tb = data + v->t[t].table_off;
+        const uint32_t lm = tb[0] & 3u, dm = (tb[0] >> 2) & 1u;
+        if ((tb[0] & 0xF8u) != 0u || lm > 2u) { rc = fail(TC_ERR_MALFORMED, "v8 tile flags %u", tb[0]); break; }
+        tm[t].lm = lm;
+        tm[t].dm = dm;
+        const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+        for (uint32_t c = 0; c < nd && rc == TC_OK; ++c) {
+            if (row_decode(tb + 1u + c * DC_SYMS, DC_SYMS, &tm[t].dcm[c]) != TC_OK) { rc = fail(TC_ERR_MALFORMED, "v8 tile dc row %u", c); }
+        }
+        if (rc == TC_OK && row_decode(tb + 1u + DCP_CTX * DC_SYMS, RUN_SYMS, &tm[t].rnm) != TC_OK) {
+            rc = fail(TC_ERR_MALFORMED, "v8 tile run row");
+        }
+        for (uint32_t c = 0; c < nl && rc == TC_OK; ++c) {
+            if (row_decode(tb + 1u + DCP_CTX * DC_SYMS + RUN_SYMS + c * LVL_SYMS, LVL_SYMS, &tm[t].lvm[c]) != TC_OK) {
+                rc = fail(TC_ERR_MALFORMED, "v8 tile lvl row %u", c);
+            }
+        }
+    }
+    uint16_t qmL[64], qmC[64];
+    if (rc == TC_OK && (!qm_lookup(h->qm, 0, qmL) || !qm_lookup(h->qm, 1, qmC))) {
+        rc = fail(TC_ERR_UNSUPPORTED_MATRIX, "qmatrix_id %u", h->qm);
+    }
+    if (rc != TC_OK) { free(tm); free(v); return rc; }
+    const uint32_t refined = (h->flags & 0x8u) != 0u;
+    uint32_t concealed = 0, tbase = 0;
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        const size_t str = (strides && strides[p]) ? strides[p] : h->pvw[p];
+        const uint32_t cols = h->bcols[p], blocks = h->brows[p] * cols;
+        const int chroma = p == 1u || p == 2u;
+        store st = {planes[p], str, h->pvw[p], h->pvh[p], (int32_t)(1u << (h->bd - 1u)), (int32_t)((1u << h->bd) - 1u)};
+        for (uint32_t t = 0; t < v->tiles[p]; ++t) {
+            v8tile* ti = &v->t[tbase + t];
+            uint32_t crc = crc_update(0u, data + ti->table_off, V8_TABLE);
+            crc = crc_update(crc, data + ti->stream_off, ti->stream_bytes);
+            ti->crc_ok = crc == ti->crc_stored;
+            uint32_t tile_conc = 0;
+            for (uint32_t k = ti->seg_first; k < ti->seg_first + ti->seg_count; ++k) {
+                const uint32_t b0 = k * v->sb, nb = blocks - b0 < v->sb ? blocks - b0 : v->sb;
+                const uint8_t* de = data + v->dir_off[p] + (size_t)k * V8_DIR;
+                int32_t qe = (int32_t)h->qp + (int32_t)de[8] - 64;
+                if (qe < 0) { qe = 0; }
+                const int32_t ceil = h->qp >= QP_V15_MIN ? (int32_t)QP_MAX : 63;
+                if (qe > ceil) { qe = ceil; }
+                qctx q;
+                qctx_init(&q, chroma ? qmC : qmL, (uint32_t)qe, h->bd, refined);
+                int32_t drc = TC_ERR_CHECKSUM_MISMATCH;
+                if (ti->crc_ok) {
+                    drc = v8_segment_decode(data + v->stream_off[p] + ld32(de), ld32(de + 4u), tm[tbase + t].lm,
+                                            tm[tbase + t].dm, tm[tbase + t].dcm, &tm[tbase + t].rnm, tm[tbase + t].lvm,
+                                            nb, cols, b0, &q, &st);
+                    if (drc != TC_OK) { tile_conc++; }
+                }
+                if (drc != TC_OK) {
+                    static const int32_t zero[64];
+                    for (uint32_t i = 0; i < nb; ++i) { store_block(&st, &q, (b0 + i) % cols, (b0 + i) / cols, zero); }
+                }
+            }
+            const int bad = tile_conc != 0u || !ti->crc_ok;
+            o->slice_status[tbase + t] = bad ? TC_FRAME_SLICE_CONCEALED : TC_FRAME_SLICE_OK;
+            concealed += bad ? 1u : 0u;
+        }
+        tbase += v->tiles[p];
+    }
+    o->concealed_slices = (uint16_t)concealed;
+    free(tm);
+    free(v);
+    return TC_OK;
+}
+
 /* Generation probe ahead of the V7 structural parse (codec.c:9016-9077):
  * V7-A is retired (UNSUPPORTED_VERSION); V7-B/V8/V9 exist in the reference but
  * are outside this path (NOT_IMPLEMENTED). Returns 0 to continue. */
@@ -1906,8 +2482,8 @@ static int32_t probe_generation(const uint8_t* d, size_t n)
     if (n > 45u && memcmp(d, "TPIC", 4u) == 0 && d[6] == 7u && d[45] == 5u) {
         return fail(TC_ERR_UNSUPPORTED_VERSION, "generation 7 (V7-A band decode) retired");
     }
-    if (n >= HDR_SIZE && memcmp(d, "TPIC", 4u) == 0 && (d[6] == 8u || d[6] == 9u)) {
-        return fail(TC_ERR_NOT_IMPLEMENTED, "V8/V9 packets are not implemented");
+    if (n >= HDR_SIZE && memcmp(d, "TPIC", 4u) == 0 && d[6] == 9u) {
+        return fail(TC_ERR_NOT_IMPLEMENTED, "V9 packets are not implemented");
     }
     return 0;
 }
@@ -1922,6 +2498,17 @@ EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* const
     if (data == NULL) { return fail(TC_ERR_INVALID_ARGUMENT, "data == NULL"); }
     int32_t rc = probe_generation(data, size);
     if (rc != 0) { return rc; }
+    if (size >= HDR_SIZE && memcmp(data, "TPIC", 4u) == 0 && data[6] == 8u) {
+        /* V8 (codec.c:9039-9049): query = full scan with tile CRCs + info */
+        if (planes_out == NULL) {
+            v8view* v8 = (v8view*)malloc(sizeof(v8view));
+            rc = v8_scan(data, size, v8, 1);
+            if (rc == TC_OK) { fill_info(&v8->h, o); }
+            free(v8);
+            return rc;
+        }
+        return v8_decode(data, size, planes_out, strides, o);
+    }
     pview* v = (pview*)malloc(sizeof(pview));
     rc = parse_structure(data, size, v);
     if (rc != TC_OK) { free(v); return rc; }

@@ -129,3 +129,88 @@ def test_oracle_concealment_vs_reference(oracle, reference):
         assert da.status == db.status
         assert da.slice_status == db.slice_status
         assert all(np.array_equal(x, y) for x, y in zip(da.planes, db.planes))
+
+
+def _random_v8_config(rng):
+    """A random V8 configuration: colour only (V8 carries no alpha and no CFA),
+    segment granularity 8/16/32 blocks (reserved[3]) and tile heights whole
+    plane / 16 / 32 / 64 block rows (reserved[4])."""
+    w, h = rng.randint(1, 200), rng.randint(1, 120)
+    pf = rng.choice([0, 0, 1, 2])
+    bd = rng.choice([10, 10, 12, 16])
+    ck = dict(qp=rng.choice([0, 2, 4, 8, 16, 30, 45, 63, 80]), pixel_format=pf, bit_depth=bd,
+              profile=3 if pf == 0 else 5, qmatrix_id=rng.choice([0, 1, 2, 3]) if bd == 10 else 0)
+    if bd == 16:
+        ck["qp"] = rng.choice([30, 60, 80])
+    if pf == 2:
+        ck.update(color_range=1)
+    kw = dict(bit_depth=bd, pixel_format=pf, limited=pf != 2)
+    return w, h, kw, ck, rng.choice([0, 3, 4, 5]), rng.choice([0, 4, 5, 6])
+
+
+def _v8(cfg, sb, tl):
+    cfg.reserved[0] = 9
+    cfg.reserved[3] = sb
+    cfg.reserved[4] = tl
+    return cfg
+
+
+def _same_decode(a, b):
+    return (a.status == b.status and a.slice_status == b.slice_status
+            and a.info.concealed_slices == b.info.concealed_slices
+            and all(np.array_equal(x, y) for x, y in zip(a.planes, b.planes)))
+
+
+def test_oracle_v8_differential_vs_reference(oracle, reference):
+    """V8 segmented rANS (reserved[0] = 9): packets, statistics and decoded
+    planes equal the reference library's on random geometry, formats, QPs,
+    segment sizes and tile heights."""
+    rng = random.Random(8008)
+    coded = 0
+    for i in range(60):
+        w, h, kw, ck, sb, tl = _random_v8_config(rng)
+        planes = synth.make_frame_np(w, h, seed=100 + i, **kw)
+        cfg = _v8(B.make_config(w, h, **ck), sb, tl)
+        ra, pa, sa = reference.encode_status(cfg, planes)
+        rb, pb, sbb = oracle.encode_status(cfg, planes)
+        assert ra == rb, (w, h, ck, sb, tl)
+        if ra != 0:
+            continue
+        coded += 1
+        assert pa == pb, (w, h, ck, sb, tl)
+        assert sa.as_dict() == sbb.as_dict()
+        assert _same_decode(reference.decode_status(pa), oracle.decode_status(pa))
+        ia, ib = reference.query(pa), oracle.query(pa)
+        assert ia[0] == ib[0] and bytes(ia[1]) == bytes(ib[1])
+    assert coded >= 40
+
+
+def test_oracle_v8_concealment_vs_reference(oracle, reference):
+    """Damaged V8 packets: bytes changed in a segment stream with the tile CRC
+    re-sealed (the segment's own decode fails: that segment is concealed), with
+    the CRC left stale (the whole tile is concealed), and in the directory or
+    tables (structural rejects or tile-level failures): same status, per-tile
+    status, concealed count and planes as the reference."""
+    from v8_packets import layout, plane_blocks, reseal_tile
+    rng = random.Random(88)
+    w, h = 160, 96
+    cfg = _v8(B.make_config(w, h, qp=4, qmatrix_id=4), 3, 4)
+    pkt = reference.encode(cfg, synth.make_frame_np(w, h, seed=9))
+    lay = layout(pkt, plane_blocks(w, h, 0))
+    for trial in range(90):
+        p = bytearray(pkt)
+        pl = lay[rng.randrange(3)]
+        kind = trial % 3
+        if kind < 2:
+            t = rng.randrange(len(pl["tiles"]))
+            sf, sn = pl["tiles"][t]
+            if sn == sf:
+                continue
+            so, ln = pl["segs"][rng.randrange(sf, sn)]
+            p[pl["streams"] + so + rng.randrange(ln)] ^= 1 + rng.randrange(255)
+            if kind == 0:
+                reseal_tile(p, pl, t)
+        else:
+            p[rng.randrange(53, len(p))] ^= 1 + rng.randrange(255)
+        p = bytes(p)
+        assert _same_decode(reference.decode_status(p), oracle.decode_status(p)), trial

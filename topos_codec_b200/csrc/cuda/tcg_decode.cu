@@ -306,6 +306,22 @@ __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool u
     return s;
 }
 
+// One level symbol through a bucket table in the fast layout (category - 1 in
+// bits 12-17), otherwise as dl_sym<true>.
+__device__ __forceinline__ uint32_t dl_sym_lvl(DLane& L, const uint32_t* lut, const uint16_t* cum)
+{
+    const uint32_t x = L.x, slot = x & 4095u;
+    const uint32_t e = lut[slot >> 4];
+    uint32_t s = ((e >> 12) + 1u) & 63u, c0 = e & 0xFFFu, c1 = cum[s + 1u];
+    while (slot >= c1 && s < CUM_LEN - 2u) {
+        ++s;
+        c0 = c1;
+        c1 = cum[s + 1u];
+    }
+    dl_renorm<true>(L, (c1 - c0) * (x >> 12) + slot - c0);
+    return s;
+}
+
 // raw chunk of w bits (w <= 23; 0 leaves the state unchanged)
 __device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
 {
@@ -528,6 +544,246 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
 #undef DCH_FINISH
     if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
+}
+
+// ------------------------------------------------------------------ chain, one slice per warp
+//
+// The one-lane decode again, built for the slices that set a batch's time
+// (one per warp). Same stream semantics and results as k_dchain<1>; the fast
+// iteration is shaped for a short dependent path:
+//  * it is one straight-line block: the stream window's refill is predicated
+//    (a load and selects instead of a branch), so the compiler can place the
+//    refill, the store and the next position's context read in the cycles the
+//    state chain spends waiting;
+//  * the loop is unrolled twice with two state sets, the second step reading
+//    what the first wrote, so a committed fast step moves no registers (only a
+//    general step after the second fast step copies the state back);
+//  * level bucket entries hold fields the step uses as they are: cumulative
+//    start (bits 0-11), category - 1 (bits 12-17), read by wrap-mode shifts
+//    that use the low five bits of their amount), frequency (bits 19-31);
+//  * the level tables sit first in shared memory, each 1 KB aligned, so a
+//    bucket's address is one shift and one and-or of the state.
+// The general iteration (end of block and next DC, other runs, bucket walks,
+// wide categories, damaged streams) is k_dchain's.
+
+constexpr uint32_t DCF_LVL = 0u;                             // level bucket tables, ctx * 1 KB (5)
+constexpr uint32_t DCF_RUN = 5u * LUT_BYTES;                 // run bucket table
+constexpr uint32_t DCF_DC = DCF_RUN + LUT_BYTES;             // DC bucket tables (when they fit: 1)
+constexpr uint32_t DCF_CUM = DCF_DC + LUT_BYTES;             // cumulative tables, 11 x 66 u16
+constexpr uint32_t DCF_CTX = DCF_CUM + DCH_CUM_BYTES;        // context rows, 3 x 80 u16 (byte offsets)
+constexpr uint32_t DCF_SMEM = DCF_CTX + DCH_HEAD;
+
+struct FState {
+    uint32_t x, whi, wlo, wbits, nxt, wi;
+    uint32_t pos;   // zigzag position of the next coefficient
+    uint32_t lcb;   // byte offset of its level table if the next run is 0
+};
+
+// One fast iteration from A into B; true when it applies (B and the store are
+// then valid). LM: the slice's level model (0 single, 1 by position, 2 by the
+// previous category).
+template <uint32_t LM>
+__device__ __forceinline__ bool dcf_step(const FState& A, FState& B, uint32_t f0, const uint8_t* __restrict__ sm,
+                                         const uint32_t* __restrict__ wb, uint32_t wlast, int32_t* __restrict__ blk)
+{
+    const uint16_t* ctx = reinterpret_cast<const uint16_t*>(sm + DCF_CTX);
+    const uint32_t x = A.x, slot = x & 4095u;
+    const uint32_t x1 = f0 * (x >> 12) + slot;
+    const uint32_t e = *reinterpret_cast<const uint32_t*>(sm + (((x1 >> 2) & 0x3FCu) | A.lcb));
+    // next position's level table (by position: known before the symbol)
+    const uint32_t lcb_pos = LM == 1u ? (uint32_t)ctx[DCH_CTX_ROW + A.pos + 1u] : 0u;
+    // refill: a window of 32 bits or fewer takes the next stream word below its valid bits
+    const bool need = A.wbits <= 32u;
+    const uint32_t w = need ? __byte_perm(A.nxt, 0u, 0x0123u) : 0u;
+    const uint32_t whi = A.whi | __funnelshift_rc(w, 0u, A.wbits);
+    const uint32_t wlo = A.wlo | __funnelshift_rc(0u, w, A.wbits);
+    const uint32_t wbits = A.wbits + (need ? 32u : 0u);
+    B.wi = A.wi + (need ? 1u : 0u);
+    B.nxt = ldg_nc_if(wb + min(B.wi, wlast), A.nxt, need);
+    // level symbol at pos and its suffix (one chunk of cat - 1 <= 23 bits)
+    const uint32_t c0 = e & 0xFFFu, fq = e >> 19;
+    const uint32_t d = (x1 & 4095u) - c0;
+    const uint32_t xn = fq * (x1 >> 12) + d;
+    const uint32_t lzm = (uint32_t)__clz((int32_t)xn) - 1u;
+    const uint32_t n8 = lzm & 0x18u;
+    const uint32_t x2 = __funnelshift_l(whi, xn, n8);
+    const uint32_t whi2 = __funnelshift_l(wlo, whi, n8);
+    const uint32_t wlo2 = wlo << n8;
+    const uint32_t bw = e >> 12;                              // low five bits: category - 1
+    const uint32_t x3 = __funnelshift_r(x2, 0u, bw);          // x2 >> bw
+    const uint32_t n8s = (lzm - n8 + bw) & 0x18u;
+    B.x = __funnelshift_l(whi2, x3, n8s);
+    B.whi = __funnelshift_l(wlo2, whi2, n8s);
+    B.wlo = wlo2 << n8s;
+    B.wbits = wbits - n8 - n8s;
+    const uint32_t hb = __funnelshift_l(0u, 1u, bw);          // 1 << bw
+    const uint32_t mk = __funnelshift_l(0xFFFFFFFFu, 0u, bw); // (1 << bw) - 1
+    B.pos = A.pos + 1u;
+    B.lcb = LM == 1u ? lcb_pos : (LM == 2u ? (uint32_t)ctx[2u * DCH_CTX_ROW + (bw & 31u) + 1u] : 0u);
+    const bool ok = slot < f0 && x1 >= RANS_L && A.pos < 64u && wbits >= 40u && d < fq;
+    if (ok) { blk[A.pos] = (int32_t)((x2 & mk) | hb); }
+    return ok;
+}
+
+template <uint32_t LM>
+__device__ __forceinline__ void dcf_run(const DSlice& S, const DPlane& P, const uint8_t* __restrict__ sm,
+                                        uint32_t dm, bool dc_lut, const uint8_t* stream, uint32_t nbytes,
+                                        int32_t* __restrict__ coef, int32_t* __restrict__ status_out)
+{
+    const uint32_t* lut_run = reinterpret_cast<const uint32_t*>(sm + DCF_RUN);
+    const uint32_t* lut_dc = dc_lut ? reinterpret_cast<const uint32_t*>(sm + DCF_DC) : lut_run;
+    const uint16_t* cums = reinterpret_cast<const uint16_t*>(sm + DCF_CUM);
+    const uint16_t* cum_run = cums + 5u * CUM_LEN;
+    const uint16_t* cum_lvl = cums + 6u * CUM_LEN;
+    const uint16_t* cum_dc = cums;
+    const uint16_t* ctab = reinterpret_cast<const uint16_t*>(sm + DCF_CTX);
+    const uint16_t* ctl = ctab + LM * DCH_CTX_ROW;
+
+    DLane L;
+    dl_init(L, stream, nbytes);
+    uint32_t err = L.x < RANS_L ? 1u : 0u;
+    const bool wide = P.bd > 12u;
+    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
+    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
+    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
+    const uint32_t cols = S.cols, nblk = S.nblk;
+    int32_t* blk = coef + (size_t)S.blk0 * 64u;
+
+    uint32_t dcat = dl_sym<true>(L, lut_dc, dc_lut, cum_dc);
+    uint32_t m = dl_suffix(L, dcat);
+    err |= m > mdc ? 1u : 0u;
+    int64_t dcv = unmap_s(m);
+    err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+    int32_t left = (int32_t)dcv;
+    blk[0] = left;
+    int32_t top_next = (1u < nblk && 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
+    uint32_t prev_dcc = dcat;
+    uint32_t b = 0, bx = 0;
+    const bool x_ok = L.x < 0x80000000u;
+    const uint32_t f0 = x_ok ? cum_run[1] : 0u;
+
+    FState s0, s1;
+    s0.x = L.x; s0.whi = L.whi; s0.wlo = L.wlo; s0.wbits = L.wbits; s0.nxt = L.nxt; s0.wi = L.wi;
+    s0.pos = 1u;
+    s0.lcb = (uint32_t)ctl[LM == 1u ? 1u : 79u];
+    // general iteration on state s (the old state of a fast step that did not apply)
+    auto general = [&](FState& s) -> bool {
+        if (err != 0u) { return true; }
+        L.x = s.x; L.whi = s.whi; L.wlo = s.wlo; L.wbits = s.wbits; L.nxt = s.nxt; L.wi = s.wi;
+        // a fast step takes at most 16 bits per symbol; refill before the general step as k_dchain does
+        if (L.wbits <= 32u) { dl_take_word(L); }
+        const uint32_t pos = s.pos;
+        const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
+        const bool geob = r == 63u;
+        const uint32_t idx = pos + r;
+        if (!geob && idx > 63u) {
+            err = 1u;
+            return true;
+        }
+        if (geob && b + 1u >= nblk) { return true; }
+        // level context: by position, else the table the state already names
+        // (previous category's bucket, or the single model)
+        const uint32_t lc = LM == 1u ? pos_ctx(idx & 63u) : s.lcb / LUT_BYTES;
+        const uint32_t dctx = dm ? dcp_ctx(prev_dcc, true) : 0u;
+        uint32_t sc;
+        if (!geob) {
+            sc = dl_sym_lvl(L, reinterpret_cast<const uint32_t*>(sm + DCF_LVL) + lc * LUT_BUCKETS, cum_lvl + lc * CUM_LEN);
+        } else {
+            sc = dl_sym<true>(L, dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run, dc_lut, cum_dc + dctx * CUM_LEN);
+        }
+        m = dl_suffix(L, sc);
+        if (!geob) {
+            err |= m > mlv ? 1u : 0u;
+            blk[idx] = (int32_t)m;
+            s.pos = idx + 1u;
+            s.lcb = (uint32_t)ctl[LM == 1u ? s.pos : sc];
+        } else {
+            ++b;
+            blk += 64;
+            bx = bx + 1u == cols ? 0u : bx + 1u;
+            const bool ht = b >= cols;
+            err |= m > mdc ? 1u : 0u;
+            dcv = (int64_t)dc_pred(bx != 0u, left, ht, top_next) + unmap_s(m);
+            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
+            left = (int32_t)dcv;
+            blk[0] = left;
+            top_next = (b + 1u < nblk && b + 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
+            prev_dcc = sc;
+            s.pos = 1u;
+            s.lcb = (uint32_t)ctl[LM == 1u ? 1u : 79u];
+        }
+        s.x = L.x; s.whi = L.whi; s.wlo = L.wlo; s.wbits = L.wbits; s.nxt = L.nxt; s.wi = L.wi;
+        return false;
+    };
+    const uint32_t* wb = L.wb;
+    const uint32_t wlast = L.wlast;
+    for (;;) {
+        if (!dcf_step<LM>(s0, s1, f0, sm, wb, wlast, blk)) {
+            if (general(s0)) { break; }
+            continue;
+        }
+        if (!dcf_step<LM>(s1, s0, f0, sm, wb, wlast, blk)) {
+            s0 = s1;
+            if (general(s0)) { break; }
+            continue;
+        }
+    }
+    L.x = s0.x; L.whi = s0.whi; L.wlo = s0.wlo; L.wbits = s0.wbits; L.nxt = s0.nxt; L.wi = s0.wi;
+    if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
+    *status_out = err != 0u ? TCG_ERR_MALFORMED : 0;
+}
+
+// One colour slice per block: the warp stages the slice's tables, lane 0 decodes.
+__global__ void __launch_bounds__(32) k_dchain_f(const DSlice* __restrict__ slices, const uint32_t* __restrict__ order,
+                                                 uint32_t nc, const uint32_t* __restrict__ slice_tab,
+                                                 const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
+                                                 const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
+                                                 int32_t* __restrict__ status)
+{
+    extern __shared__ __align__(16) uint8_t dsm[];
+    const uint32_t t = threadIdx.x;
+    if (blockIdx.x >= nc) { return; }
+    const uint32_t si = order[blockIdx.x];
+    if (status[si] != 0) { return; }
+    // context rows as byte offsets of level tables: row 1 by the next position
+    // (1..64), row 2 by the previous level's category (79 = none in the block), row 0 zero
+    uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm + DCF_CTX);
+    for (uint32_t i = t; i < 3u * DCH_CTX_ROW; i += 32u) {
+        const uint32_t row = i / DCH_CTX_ROW, k = i % DCH_CTX_ROW;
+        const uint32_t ctx = row == 1u ? pos_ctx(k) : (row == 2u ? (k < 64u ? cat_bucket(k) : 4u) : 0u);
+        ctab[i] = (uint16_t)(ctx * LUT_BYTES);
+    }
+    const uint8_t* tb = tabs + (size_t)slice_tab[si] * DTAB_BYTES;
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
+    const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
+    const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+    const bool dc_lut = dm == 0u;
+    // level tables re-laid for the fast step: cumulative start, category - 1, frequency
+    for (uint32_t k = t; k < nl * LUT_BUCKETS; k += 32u) {
+        const uint32_t eo = reinterpret_cast<const uint32_t*>(tb + TAB_LUT + 6u * LUT_BYTES)[k];
+        const uint32_t sy = (eo >> 12) & 63u, fq = eo >> 18;
+        reinterpret_cast<uint32_t*>(dsm + DCF_LVL)[k] = (eo & 0xFFFu) | (((sy - 1u) & 63u) << 12) | (fq << 19);
+    }
+    for (uint32_t k = t; k < LUT_BYTES / 16u; k += 32u) {
+        reinterpret_cast<uint4*>(dsm + DCF_RUN)[k] = reinterpret_cast<const uint4*>(tb + TAB_LUT + 5u * LUT_BYTES)[k];
+        if (dc_lut) { reinterpret_cast<uint4*>(dsm + DCF_DC)[k] = reinterpret_cast<const uint4*>(tb + TAB_LUT)[k]; }
+    }
+    for (uint32_t k = t; k < DCH_CUM_BYTES / 16u; k += 32u) {
+        reinterpret_cast<uint4*>(dsm + DCF_CUM)[k] = reinterpret_cast<const uint4*>(tb + TAB_CUM)[k];
+    }
+    __syncthreads();
+    if (t != 0u) { return; }
+    const DSlice& S = slices[si];
+    const DPlane& P = planes[S.plane];
+    const uint8_t* stream = pkt + S.pay + plen;
+    const uint32_t nb = S.size - plen;
+    if (lm == 1u) {
+        dcf_run<1>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
+    } else if (lm == 2u) {
+        dcf_run<2>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
+    } else {
+        dcf_run<0>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
+    }
 }
 
 // ------------------------------------------------------------------ chain, warp tiling
@@ -1193,7 +1449,7 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 // slots from the long ones that set the batch time.
 // TCG_DCHAIN=lane|lane4|lane2|lane1|warp|split forces any one ("lane" is 8).
 enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4,
-                    DCH_TILE_SPLIT = 5 };
+                    DCH_TILE_SPLIT = 5, DCH_TILE_SPLITF = 6, DCH_TILE_LANE1F = 7 };
 
 static std::mutex g_tune_mu;
 static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
@@ -1209,6 +1465,8 @@ static int dchain_forced()
     if (strcmp(v, "lane1") == 0) { return DCH_TILE_LANE1; }
     if (strcmp(v, "warp") == 0) { return DCH_TILE_WARP; }
     if (strcmp(v, "split") == 0) { return DCH_TILE_SPLIT; }
+    if (strcmp(v, "splitf") == 0) { return DCH_TILE_SPLITF; }
+    if (strcmp(v, "lane1f") == 0) { return DCH_TILE_LANE1F; }
     return -1;
 }
 
@@ -1444,6 +1702,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
         }
         auto run = [&](int tiling) -> int32_t {
             switch (tiling) {
+            case DCH_TILE_SPLITF:
             case DCH_TILE_SPLIT: {
                 cudaStream_t sd = side_stream(C);
                 if (sd == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
@@ -1451,8 +1710,13 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 tcg::kern_begin(C, K_DCHAIN);
                 TCG_CHECK(cudaEventRecord(C->fork, st));
                 TCG_CHECK(cudaStreamWaitEvent(sd, C->fork, 0));
-                k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
-                                                               d_status);
+                if (tiling == DCH_TILE_SPLITF) {
+                    k_dchain_f<<<nsplit, 32, DCF_SMEM, st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
+                                                             d_status);
+                } else {
+                    k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
+                                                                   d_status);
+                }
                 if (nc > nsplit) {
                     k_dchain<4><<<(nc - nsplit + 3u) / 4u, 32, dch_smem(4), sd>>>(
                         d_sl, d_ord + nsplit, nc - nsplit, d_st, d_pl, d_pkt, d_tab, d_coef, d_status);
@@ -1478,6 +1742,11 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
                 TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L2, (nc + 1u) / 2u, 32, dch_smem(2), d_sl, d_ord, nc, d_st, d_pl,
                            d_pkt, d_tab, d_coef, d_status);
+                return TCG_OK;
+            case DCH_TILE_LANE1F:
+                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+                TCG_LAUNCH(C, K_DCHAIN, k_dchain_f, nc, 32, DCF_SMEM, d_sl, d_ord, nc, d_st, d_pl, d_pkt, d_tab, d_coef,
+                           d_status);
                 return TCG_OK;
             case DCH_TILE_LANE1:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
