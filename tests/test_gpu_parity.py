@@ -230,7 +230,7 @@ def test_strided_io_and_buffer_too_small(product):
     assert rc == B.TC_ERR_BUFFER_TOO_SMALL and st.packet_size == len(tight)
 
 
-@pytest.mark.parametrize("tiling", ["lane", "lane4", "lane2", "lane1", "warp", "split", "splitf", "lane1f"])
+@pytest.mark.parametrize("tiling", ["lane", "lane4", "lane2", "lane1", "warp", "split"])
 def test_decode_tilings_vs_oracle(product, oracle, monkeypatch, tiling):
     """Every decode-chain tiling (lane per slice with 8/4/2/1 slices per warp,
     warp per slice, the two-stream split) decodes random configurations and

@@ -306,22 +306,6 @@ __device__ __forceinline__ uint32_t dl_sym(DLane& L, const uint32_t* lut, bool u
     return s;
 }
 
-// One level symbol through a bucket table in the fast layout (category - 1 in
-// bits 12-17), otherwise as dl_sym<true>.
-__device__ __forceinline__ uint32_t dl_sym_lvl(DLane& L, const uint32_t* lut, const uint16_t* cum)
-{
-    const uint32_t x = L.x, slot = x & 4095u;
-    const uint32_t e = lut[slot >> 4];
-    uint32_t s = ((e >> 12) + 1u) & 63u, c0 = e & 0xFFFu, c1 = cum[s + 1u];
-    while (slot >= c1 && s < CUM_LEN - 2u) {
-        ++s;
-        c0 = c1;
-        c1 = cum[s + 1u];
-    }
-    dl_renorm<true>(L, (c1 - c0) * (x >> 12) + slot - c0);
-    return s;
-}
-
 // raw chunk of w bits (w <= 23; 0 leaves the state unchanged)
 __device__ __forceinline__ uint32_t dl_chunk(DLane& L, uint32_t w)
 {
@@ -546,243 +530,196 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
-// ------------------------------------------------------------------ chain, one slice per warp
+// ------------------------------------------------------------------ V8 segments
 //
-// The one-lane decode again, built for the slices that set a batch's time
-// (one per warp). Same stream semantics and results as k_dchain<1>; the fast
-// iteration is shaped for a short dependent path:
-//  * it is one straight-line block: the stream window's refill is predicated
-//    (a load and selects instead of a branch), so the compiler can place the
-//    refill, the store and the next position's context read in the cycles the
-//    state chain spends waiting;
-//  * the loop is unrolled twice with two state sets, the second step reading
-//    what the first wrote, so a committed fast step moves no registers (only a
-//    general step after the second fast step copies the state back);
-//  * level bucket entries hold fields the step uses as they are: cumulative
-//    start (bits 0-11), category - 1 (bits 12-17), read by wrap-mode shifts
-//    that use the low five bits of their amount), frequency (bits 19-31);
-//  * the level tables sit first in shared memory, each 1 KB aligned, so a
-//    bucket's address is one shift and one and-or of the state.
-// The general iteration (end of block and next DC, other runs, bucket walks,
-// wide categories, damaged streams) is k_dchain's.
+// V8 (reference codec.c:4321-4475 segment decode, 4772-4975 frame decode).
+// Tile tables hold every row at a fixed place (flags, DC rows 0..4, run row,
+// level rows 0..4: 350 bytes), so k_v8_dtab builds the same decode-table
+// layout as k_dtables from them. A warp decodes up to 32 segments of one
+// tile, one lane each, with the tile's eleven bucket tables and cumulative
+// tables in shared memory (12.5 KB). DC prediction and the DC context stay
+// inside the segment (left = the segment's previous block in raster order,
+// top = the block one plane row up when the segment reaches back that far).
+// Magnitude and DC-domain checks use the 12-bit limits at every bit depth,
+// as the reference's segment decoder does. A segment that fails is zeroed,
+// so it reconstructs at the mid level, the reference's concealment.
 
-constexpr uint32_t DCF_LVL = 0u;                             // level bucket tables, ctx * 1 KB (5)
-constexpr uint32_t DCF_RUN = 5u * LUT_BYTES;                 // run bucket table
-constexpr uint32_t DCF_DC = DCF_RUN + LUT_BYTES;             // DC bucket tables (when they fit: 1)
-constexpr uint32_t DCF_CUM = DCF_DC + LUT_BYTES;             // cumulative tables, 11 x 66 u16
-constexpr uint32_t DCF_CTX = DCF_CUM + DCH_CUM_BYTES;        // context rows, 3 x 80 u16 (byte offsets)
-constexpr uint32_t DCF_SMEM = DCF_CTX + DCH_HEAD;
+constexpr uint32_t V8_TABLE_BYTES = 350u;
+constexpr uint32_t V8D_LUT = 0u;                                  // 11 x 1 KB bucket tables
+constexpr uint32_t V8D_CUM = MAX_CTX * LUT_BYTES;                 // 11 x 66 u16
+constexpr uint32_t V8D_SMEM = V8D_CUM + DCH_CUM_BYTES;
 
-struct FState {
-    uint32_t x, whi, wlo, wbits, nxt, wi;
-    uint32_t pos;   // zigzag position of the next coefficient
-    uint32_t lcb;   // byte offset of its level table if the next run is 0
-};
-
-// One fast iteration from A into B; true when it applies (B and the store are
-// then valid). LM: the slice's level model (0 single, 1 by position, 2 by the
-// previous category).
-template <uint32_t LM>
-__device__ __forceinline__ bool dcf_step(const FState& A, FState& B, uint32_t f0, const uint8_t* __restrict__ sm,
-                                         const uint32_t* __restrict__ wb, uint32_t wlast, int32_t* __restrict__ blk)
+// one block per tile: CRC of the table and the member streams against the stored one
+__global__ void __launch_bounds__(256) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
+                                                 const uint32_t* __restrict__ crctab, uint8_t* __restrict__ ok)
 {
-    const uint16_t* ctx = reinterpret_cast<const uint16_t*>(sm + DCF_CTX);
-    const uint32_t x = A.x, slot = x & 4095u;
-    const uint32_t x1 = f0 * (x >> 12) + slot;
-    const uint32_t e = *reinterpret_cast<const uint32_t*>(sm + (((x1 >> 2) & 0x3FCu) | A.lcb));
-    // next position's level table (by position: known before the symbol)
-    const uint32_t lcb_pos = LM == 1u ? (uint32_t)ctx[DCH_CTX_ROW + A.pos + 1u] : 0u;
-    // refill: a window of 32 bits or fewer takes the next stream word below its valid bits
-    const bool need = A.wbits <= 32u;
-    const uint32_t w = need ? __byte_perm(A.nxt, 0u, 0x0123u) : 0u;
-    const uint32_t whi = A.whi | __funnelshift_rc(w, 0u, A.wbits);
-    const uint32_t wlo = A.wlo | __funnelshift_rc(0u, w, A.wbits);
-    const uint32_t wbits = A.wbits + (need ? 32u : 0u);
-    B.wi = A.wi + (need ? 1u : 0u);
-    B.nxt = ldg_nc_if(wb + min(B.wi, wlast), A.nxt, need);
-    // level symbol at pos and its suffix (one chunk of cat - 1 <= 23 bits)
-    const uint32_t c0 = e & 0xFFFu, fq = e >> 19;
-    const uint32_t d = (x1 & 4095u) - c0;
-    const uint32_t xn = fq * (x1 >> 12) + d;
-    const uint32_t lzm = (uint32_t)__clz((int32_t)xn) - 1u;
-    const uint32_t n8 = lzm & 0x18u;
-    const uint32_t x2 = __funnelshift_l(whi, xn, n8);
-    const uint32_t whi2 = __funnelshift_l(wlo, whi, n8);
-    const uint32_t wlo2 = wlo << n8;
-    const uint32_t bw = e >> 12;                              // low five bits: category - 1
-    const uint32_t x3 = __funnelshift_r(x2, 0u, bw);          // x2 >> bw
-    const uint32_t n8s = (lzm - n8 + bw) & 0x18u;
-    B.x = __funnelshift_l(whi2, x3, n8s);
-    B.whi = __funnelshift_l(wlo2, whi2, n8s);
-    B.wlo = wlo2 << n8s;
-    B.wbits = wbits - n8 - n8s;
-    const uint32_t hb = __funnelshift_l(0u, 1u, bw);          // 1 << bw
-    const uint32_t mk = __funnelshift_l(0xFFFFFFFFu, 0u, bw); // (1 << bw) - 1
-    B.pos = A.pos + 1u;
-    B.lcb = LM == 1u ? lcb_pos : (LM == 2u ? (uint32_t)ctx[2u * DCH_CTX_ROW + (bw & 31u) + 1u] : 0u);
-    const bool ok = slot < f0 && x1 >= RANS_L && A.pos < 64u && wbits >= 40u && d < fq;
-    if (ok) { blk[A.pos] = (int32_t)((x2 & mk) | hb); }
-    return ok;
-}
-
-template <uint32_t LM>
-__device__ __forceinline__ void dcf_run(const DSlice& S, const DPlane& P, const uint8_t* __restrict__ sm,
-                                        uint32_t dm, bool dc_lut, const uint8_t* stream, uint32_t nbytes,
-                                        int32_t* __restrict__ coef, int32_t* __restrict__ status_out)
-{
-    const uint32_t* lut_run = reinterpret_cast<const uint32_t*>(sm + DCF_RUN);
-    const uint32_t* lut_dc = dc_lut ? reinterpret_cast<const uint32_t*>(sm + DCF_DC) : lut_run;
-    const uint16_t* cums = reinterpret_cast<const uint16_t*>(sm + DCF_CUM);
-    const uint16_t* cum_run = cums + 5u * CUM_LEN;
-    const uint16_t* cum_lvl = cums + 6u * CUM_LEN;
-    const uint16_t* cum_dc = cums;
-    const uint16_t* ctab = reinterpret_cast<const uint16_t*>(sm + DCF_CTX);
-    const uint16_t* ctl = ctab + LM * DCH_CTX_ROW;
-
-    DLane L;
-    dl_init(L, stream, nbytes);
-    uint32_t err = L.x < RANS_L ? 1u : 0u;
-    const bool wide = P.bd > 12u;
-    const uint32_t mdc = wide ? 0x0FFFFFFFu : 0x08000000u;
-    const uint32_t mlv = wide ? 0x07FFFFFFu : 0x04000000u;
-    const int64_t dlim = wide ? ((int64_t)1 << 27) : ((int64_t)1 << 25);
-    const uint32_t cols = S.cols, nblk = S.nblk;
-    int32_t* blk = coef + (size_t)S.blk0 * 64u;
-
-    uint32_t dcat = dl_sym<true>(L, lut_dc, dc_lut, cum_dc);
-    uint32_t m = dl_suffix(L, dcat);
-    err |= m > mdc ? 1u : 0u;
-    int64_t dcv = unmap_s(m);
-    err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
-    int32_t left = (int32_t)dcv;
-    blk[0] = left;
-    int32_t top_next = (1u < nblk && 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
-    uint32_t prev_dcc = dcat;
-    uint32_t b = 0, bx = 0;
-    const bool x_ok = L.x < 0x80000000u;
-    const uint32_t f0 = x_ok ? cum_run[1] : 0u;
-
-    FState s0, s1;
-    s0.x = L.x; s0.whi = L.whi; s0.wlo = L.wlo; s0.wbits = L.wbits; s0.nxt = L.nxt; s0.wi = L.wi;
-    s0.pos = 1u;
-    s0.lcb = (uint32_t)ctl[LM == 1u ? 1u : 79u];
-    // general iteration on state s (the old state of a fast step that did not apply)
-    auto general = [&](FState& s) -> bool {
-        if (err != 0u) { return true; }
-        L.x = s.x; L.whi = s.whi; L.wlo = s.wlo; L.wbits = s.wbits; L.nxt = s.nxt; L.wi = s.wi;
-        // a fast step takes at most 16 bits per symbol; refill before the general step as k_dchain does
-        if (L.wbits <= 32u) { dl_take_word(L); }
-        const uint32_t pos = s.pos;
-        const uint32_t r = dl_sym<false>(L, lut_run, true, cum_run);
-        const bool geob = r == 63u;
-        const uint32_t idx = pos + r;
-        if (!geob && idx > 63u) {
-            err = 1u;
-            return true;
-        }
-        if (geob && b + 1u >= nblk) { return true; }
-        // level context: by position, else the table the state already names
-        // (previous category's bucket, or the single model)
-        const uint32_t lc = LM == 1u ? pos_ctx(idx & 63u) : s.lcb / LUT_BYTES;
-        const uint32_t dctx = dm ? dcp_ctx(prev_dcc, true) : 0u;
-        uint32_t sc;
-        if (!geob) {
-            sc = dl_sym_lvl(L, reinterpret_cast<const uint32_t*>(sm + DCF_LVL) + lc * LUT_BUCKETS, cum_lvl + lc * CUM_LEN);
-        } else {
-            sc = dl_sym<true>(L, dc_lut ? lut_dc + dctx * LUT_BUCKETS : lut_run, dc_lut, cum_dc + dctx * CUM_LEN);
-        }
-        m = dl_suffix(L, sc);
-        if (!geob) {
-            err |= m > mlv ? 1u : 0u;
-            blk[idx] = (int32_t)m;
-            s.pos = idx + 1u;
-            s.lcb = (uint32_t)ctl[LM == 1u ? s.pos : sc];
-        } else {
-            ++b;
-            blk += 64;
-            bx = bx + 1u == cols ? 0u : bx + 1u;
-            const bool ht = b >= cols;
-            err |= m > mdc ? 1u : 0u;
-            dcv = (int64_t)dc_pred(bx != 0u, left, ht, top_next) + unmap_s(m);
-            err |= (dcv > dlim || dcv < -dlim) ? 1u : 0u;
-            left = (int32_t)dcv;
-            blk[0] = left;
-            top_next = (b + 1u < nblk && b + 1u >= cols) ? blk[64 - (int64_t)cols * 64] : 0;
-            prev_dcc = sc;
-            s.pos = 1u;
-            s.lcb = (uint32_t)ctl[LM == 1u ? 1u : 79u];
-        }
-        s.x = L.x; s.whi = L.whi; s.wlo = L.wlo; s.wbits = L.wbits; s.nxt = L.nxt; s.wi = L.wi;
-        return false;
-    };
-    const uint32_t* wb = L.wb;
-    const uint32_t wlast = L.wlast;
-    for (;;) {
-        if (!dcf_step<LM>(s0, s1, f0, sm, wb, wlast, blk)) {
-            if (general(s0)) { break; }
-            continue;
-        }
-        if (!dcf_step<LM>(s1, s0, f0, sm, wb, wlast, blk)) {
-            s0 = s1;
-            if (general(s0)) { break; }
-            continue;
-        }
-    }
-    L.x = s0.x; L.whi = s0.whi; L.wlo = s0.wlo; L.wbits = s0.wbits; L.nxt = s0.nxt; L.wi = s0.wi;
-    if (err == 0u && dl_consumed(L) != nbytes) { err = 1u; }
-    *status_out = err != 0u ? TCG_ERR_MALFORMED : 0;
-}
-
-// One colour slice per block: the warp stages the slice's tables, lane 0 decodes.
-__global__ void __launch_bounds__(32) k_dchain_f(const DSlice* __restrict__ slices, const uint32_t* __restrict__ order,
-                                                 uint32_t nc, const uint32_t* __restrict__ slice_tab,
-                                                 const DPlane* __restrict__ planes, const uint8_t* __restrict__ pkt,
-                                                 const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
-                                                 int32_t* __restrict__ status)
-{
-    extern __shared__ __align__(16) uint8_t dsm[];
-    const uint32_t t = threadIdx.x;
-    if (blockIdx.x >= nc) { return; }
-    const uint32_t si = order[blockIdx.x];
-    if (status[si] != 0) { return; }
-    // context rows as byte offsets of level tables: row 1 by the next position
-    // (1..64), row 2 by the previous level's category (79 = none in the block), row 0 zero
-    uint16_t* ctab = reinterpret_cast<uint16_t*>(dsm + DCF_CTX);
-    for (uint32_t i = t; i < 3u * DCH_CTX_ROW; i += 32u) {
-        const uint32_t row = i / DCH_CTX_ROW, k = i % DCH_CTX_ROW;
-        const uint32_t ctx = row == 1u ? pos_ctx(k) : (row == 2u ? (k < 64u ? cat_bucket(k) : 4u) : 0u);
-        ctab[i] = (uint16_t)(ctx * LUT_BYTES);
-    }
-    const uint8_t* tb = tabs + (size_t)slice_tab[si] * DTAB_BYTES;
-    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
-    const uint32_t lm = hdr[0], dm = hdr[1], plen = hdr[2];
-    const uint32_t nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
-    const bool dc_lut = dm == 0u;
-    // level tables re-laid for the fast step: cumulative start, category - 1, frequency
-    for (uint32_t k = t; k < nl * LUT_BUCKETS; k += 32u) {
-        const uint32_t eo = reinterpret_cast<const uint32_t*>(tb + TAB_LUT + 6u * LUT_BYTES)[k];
-        const uint32_t sy = (eo >> 12) & 63u, fq = eo >> 18;
-        reinterpret_cast<uint32_t*>(dsm + DCF_LVL)[k] = (eo & 0xFFFu) | (((sy - 1u) & 63u) << 12) | (fq << 19);
-    }
-    for (uint32_t k = t; k < LUT_BYTES / 16u; k += 32u) {
-        reinterpret_cast<uint4*>(dsm + DCF_RUN)[k] = reinterpret_cast<const uint4*>(tb + TAB_LUT + 5u * LUT_BYTES)[k];
-        if (dc_lut) { reinterpret_cast<uint4*>(dsm + DCF_DC)[k] = reinterpret_cast<const uint4*>(tb + TAB_LUT)[k]; }
-    }
-    for (uint32_t k = t; k < DCH_CUM_BYTES / 16u; k += 32u) {
-        reinterpret_cast<uint4*>(dsm + DCF_CUM)[k] = reinterpret_cast<const uint4*>(tb + TAB_CUM)[k];
-    }
+    __shared__ uint32_t t[8 * 256];
+    __shared__ uint32_t scratch[512];
+    __shared__ uint32_t c_tab;
+    for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
     __syncthreads();
-    if (t != 0u) { return; }
-    const DSlice& S = slices[si];
-    const DPlane& P = planes[S.plane];
-    const uint8_t* stream = pkt + S.pay + plen;
-    const uint32_t nb = S.size - plen;
-    if (lm == 1u) {
-        dcf_run<1>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
-    } else if (lm == 2u) {
-        dcf_run<2>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
-    } else {
-        dcf_run<0>(S, P, dsm, dm, dc_lut, stream, nb, coef, status + si);
+    const tcg_v8_tile& T = tiles[blockIdx.x];
+    const uint32_t c1 = crc32_block(pkt + T.table_off, V8_TABLE_BYTES, t, scratch);
+    if (threadIdx.x == 0) { c_tab = c1; }
+    __syncthreads();
+    const uint32_t c2 = crc32_block(pkt + T.stream_off, T.stream_bytes, t, scratch);
+    if (threadIdx.x == 0) {
+        const uint32_t c = T.stream_bytes == 0u ? c_tab : crc_combine(c_tab, c2, gf2_xpow8n(T.stream_bytes));
+        ok[blockIdx.x] = c == T.crc ? 1u : 0u;
+    }
+}
+
+// one warp per tile: decode tables in k_dtables' layout from the fixed rows
+// (the host has checked the flags and that every used row normalises)
+__global__ void __launch_bounds__(32) k_v8_dtab(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
+                                                uint8_t* __restrict__ tabs)
+{
+    const tcg_v8_tile& T = tiles[blockIdx.x];
+    const uint8_t* tb350 = pkt + T.table_off;
+    uint8_t* tb = tabs + (size_t)blockIdx.x * DTAB_BYTES;
+    const uint32_t t = threadIdx.x;
+    const uint32_t fl = tb350[0], lm = fl & 3u, dm = (fl >> 2) & 1u;
+    const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+    const uint32_t nrows = nd + 1u + nl;
+    if (t < nrows) {
+        uint32_t ctx, off, n;
+        if (t < nd) { ctx = t; off = 1u + t * DC_SYMS; n = DC_SYMS; }
+        else if (t == nd) { ctx = 5u; off = 1u + DCP_CTX * DC_SYMS; n = RUN_SYMS; }
+        else { ctx = 6u + (t - nd - 1u); off = 1u + DCP_CTX * DC_SYMS + RUN_SYMS + (t - nd - 1u) * LVL_SYMS; n = LVL_SYMS; }
+        uint8_t bytes[64];
+        for (uint32_t k = 0; k < n; ++k) { bytes[k] = tb350[off + k]; }
+        uint16_t fr[64], cu[64];
+        if (model_from_bytes(bytes, n, fr, cu)) {
+            uint16_t* cd = reinterpret_cast<uint16_t*>(tb + TAB_CUM + (size_t)ctx * CUM_BYTES);
+            for (uint32_t k = 0; k < CUM_LEN; ++k) { cd[k] = k < n ? cu[k] : (uint16_t)4096u; }
+            uint32_t* lut = reinterpret_cast<uint32_t*>(tb + TAB_LUT + (size_t)ctx * LUT_BYTES);
+            for (uint32_t sy = 0; sy < n; ++sy) {
+                const uint32_t c0 = cu[sy], c1 = c0 + fr[sy];
+                for (uint32_t bk = (c0 + 15u) >> 4; bk < LUT_BUCKETS && (bk << 4) < c1; ++bk) { lut[bk] = c0 | (sy << 12); }
+            }
+        }
+    }
+    if (t == 0) {
+        uint32_t* hdr = reinterpret_cast<uint32_t*>(tb + TAB_HDR);
+        hdr[0] = lm; hdr[1] = dm; hdr[2] = 0u;
+    }
+}
+
+// one lane per segment, up to 32 segments of one tile per warp
+__global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ wtile,
+                                                  const int32_t* __restrict__ wsegs, const uint32_t* __restrict__ pinfo,
+                                                  const uint8_t* __restrict__ tile_ok, const uint8_t* __restrict__ pkt,
+                                                  const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
+                                                  uint8_t* __restrict__ seg_fail)
+{
+    extern __shared__ __align__(16) uint8_t vsm[];
+    const uint32_t lane = threadIdx.x;
+    const uint32_t ti = wtile[blockIdx.x];
+    if (tile_ok[ti] == 0u) { return; }  // concealed whole: coefficients stay zero
+    const uint8_t* tb = tabs + (size_t)ti * DTAB_BYTES;
+    for (uint32_t k = lane; k < V8D_SMEM / 16u; k += 32u) {
+        reinterpret_cast<uint4*>(vsm)[k] = reinterpret_cast<const uint4*>(tb)[k];
+    }
+    __syncwarp();
+    const int32_t si = wsegs[blockIdx.x * 32u + lane];
+    if (si < 0) { return; }
+    const tcg_v8_seg& S = segs[si];
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
+    const uint32_t lm = hdr[0], dm = hdr[1];
+    const uint32_t* luts = reinterpret_cast<const uint32_t*>(vsm + V8D_LUT);
+    const uint16_t* cums = reinterpret_cast<const uint16_t*>(vsm + V8D_CUM);
+    const uint32_t cols = pinfo[6u * S.plane + 2u];
+    int32_t* blk = coef + ((size_t)pinfo[6u * S.plane] + S.blk0) * 64u;
+    DLane L;
+    dl_init(L, pkt + S.off, S.len);
+    uint32_t err = L.x < RANS_L ? 1u : 0u;
+    uint32_t prev_dcc = 0u;
+    int32_t left = 0;
+    for (uint32_t i = 0; i < S.nblk && err == 0u; ++i) {
+        const uint32_t dctx = (i == 0u || dm == 0u) ? 0u : dcp_ctx(prev_dcc, true);
+        const uint32_t dcat = dl_sym<true>(L, luts + dctx * LUT_BUCKETS, true, cums + dctx * CUM_LEN);
+        uint32_t m = dl_suffix(L, dcat);
+        err |= m > 0x08000000u ? 1u : 0u;
+        const int32_t top = i >= cols ? blk[(size_t)(i - cols) * 64u] : 0;
+        const int64_t dcv = (int64_t)dc_pred(i != 0u, left, i >= cols, top) + unmap_s(m);
+        err |= (dcv > ((int64_t)1 << 25) || dcv < -((int64_t)1 << 25)) ? 1u : 0u;
+        int32_t* b = blk + (size_t)i * 64u;
+        b[0] = (int32_t)dcv;
+        left = (int32_t)dcv;
+        prev_dcc = dcat;
+        uint32_t pos = 1u, pcat = 0u;
+        bool has = false;
+        while (err == 0u) {
+            const uint32_t r = dl_sym<false>(L, luts + 5u * LUT_BUCKETS, true, cums + 5u * CUM_LEN);
+            if (r == 63u) { break; }
+            const uint32_t idx = pos + r;
+            if (idx > 63u) { err = 1u; break; }
+            const uint32_t lc = 6u + (lm == 1u ? pos_ctx(idx) : (lm == 2u ? prev_ctx(pcat, has) : 0u));
+            const uint32_t cat = dl_sym<true>(L, luts + lc * LUT_BUCKETS, true, cums + lc * CUM_LEN);
+            m = dl_suffix(L, cat);
+            err |= m > 0x04000000u ? 1u : 0u;
+            b[idx] = (int32_t)m;  // zigzag-mapped level at zigzag position idx
+            pcat = cat;
+            has = true;
+            pos = idx + 1u;
+        }
+    }
+    if (err == 0u && dl_consumed(L) != S.len) { err = 1u; }
+    if (err != 0u) {
+        for (uint32_t k = 0; k < S.nblk * 64u; ++k) { blk[k] = 0; }
+    }
+    seg_fail[si] = err != 0u ? 1u : 0u;
+}
+
+// Reconstruction of every block of the three planes (k_didct's arithmetic):
+// the block's segment gives its quantiser steps.
+__global__ void __launch_bounds__(128) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
+                                                  const uint32_t* __restrict__ q, const int32_t* __restrict__ coef,
+                                                  uint32_t total, uint32_t bd, uint32_t sb_log2, uint16_t* __restrict__ out)
+{
+    const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gb >= total) { return; }
+    // pinfo per plane: blk0, seg0, cols, vis_w, vis_h, out_off (u32 element offset / 64)
+    uint32_t p = 0;
+    if (gb >= pinfo[6]) { p = 1; }
+    if (gb >= pinfo[12]) { p = 2; }
+    const uint32_t* I = pinfo + 6u * p;
+    const uint32_t lb = gb - I[0];
+    const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4];
+    const tcg_v8_seg& S = segs[I[1] + (lb >> sb_log2)];
+    const uint32_t* Q = q + (size_t)S.qidx * 64u;
+    const uint32_t bx = lb % cols, by = lb / cols;
+    const int64_t fc = bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (bd - 1u)) - 1u)) / 2047;
+    int32_t c[64], xh[64];
+    const int4* src = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const int4 v = src[i];
+        const int32_t vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
+            const int nat = k_zigzag[i * 4 + j];
+            int64_t f = (int64_t)lv * __ldg(Q + nat);
+            f = f > fc ? fc : (f < -fc ? -fc : f);
+            c[nat] = (int32_t)f;
+        }
+    }
+    idct8x8(c, xh);
+    const int32_t mid = 1 << (bd - 1u), maxv = (1 << bd) - 1;
+    const uint32_t px = bx * 8u, py = by * 8u;
+    if (px >= vis_w || py >= vis_h) { return; }
+    const uint32_t cw = min(8u, vis_w - px), ch = min(8u, vis_h - py);
+    uint16_t* dst = out + (size_t)I[5] * 64u + (size_t)py * vis_w + px;
+#pragma unroll
+    for (int y = 0; y < 8; ++y) {
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            if ((uint32_t)y < ch && (uint32_t)x < cw) {
+                const int32_t v = xh[y * 8 + x] + mid;
+                dst[(size_t)y * vis_w + x] = (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
+            }
+        }
     }
 }
 
@@ -1449,7 +1386,7 @@ static uint32_t host_qp_scale(uint32_t refined, uint32_t qp)
 // slots from the long ones that set the batch time.
 // TCG_DCHAIN=lane|lane4|lane2|lane1|warp|split forces any one ("lane" is 8).
 enum DchainTiling { DCH_TILE_LANE = 0, DCH_TILE_WARP = 1, DCH_TILE_LANE4 = 2, DCH_TILE_LANE2 = 3, DCH_TILE_LANE1 = 4,
-                    DCH_TILE_SPLIT = 5, DCH_TILE_SPLITF = 6, DCH_TILE_LANE1F = 7 };
+                    DCH_TILE_SPLIT = 5 };
 
 static std::mutex g_tune_mu;
 static int8_t g_tune[33] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
@@ -1465,8 +1402,6 @@ static int dchain_forced()
     if (strcmp(v, "lane1") == 0) { return DCH_TILE_LANE1; }
     if (strcmp(v, "warp") == 0) { return DCH_TILE_WARP; }
     if (strcmp(v, "split") == 0) { return DCH_TILE_SPLIT; }
-    if (strcmp(v, "splitf") == 0) { return DCH_TILE_SPLITF; }
-    if (strcmp(v, "lane1f") == 0) { return DCH_TILE_LANE1F; }
     return -1;
 }
 
@@ -1702,7 +1637,6 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
         }
         auto run = [&](int tiling) -> int32_t {
             switch (tiling) {
-            case DCH_TILE_SPLITF:
             case DCH_TILE_SPLIT: {
                 cudaStream_t sd = side_stream(C);
                 if (sd == nullptr) { return TCG_ERR_OUT_OF_MEMORY; }
@@ -1710,13 +1644,8 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 tcg::kern_begin(C, K_DCHAIN);
                 TCG_CHECK(cudaEventRecord(C->fork, st));
                 TCG_CHECK(cudaStreamWaitEvent(sd, C->fork, 0));
-                if (tiling == DCH_TILE_SPLITF) {
-                    k_dchain_f<<<nsplit, 32, DCF_SMEM, st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
-                                                             d_status);
-                } else {
-                    k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
-                                                                   d_status);
-                }
+                k_dchain<1><<<nsplit, 32, dch_smem(1), st>>>(d_sl, d_ord, nsplit, d_st, d_pl, d_pkt, d_tab, d_coef,
+                                                               d_status);
                 if (nc > nsplit) {
                     k_dchain<4><<<(nc - nsplit + 3u) / 4u, 32, dch_smem(4), sd>>>(
                         d_sl, d_ord + nsplit, nc - nsplit, d_st, d_pl, d_pkt, d_tab, d_coef, d_status);
@@ -1742,11 +1671,6 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
                 TCG_LAUNCH(C, K_DCHAIN, K_DCHAIN_L2, (nc + 1u) / 2u, 32, dch_smem(2), d_sl, d_ord, nc, d_st, d_pl,
                            d_pkt, d_tab, d_coef, d_status);
-                return TCG_OK;
-            case DCH_TILE_LANE1F:
-                TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
-                TCG_LAUNCH(C, K_DCHAIN, k_dchain_f, nc, 32, DCF_SMEM, d_sl, d_ord, nc, d_st, d_pl, d_pkt, d_tab, d_coef,
-                           d_status);
                 return TCG_OK;
             case DCH_TILE_LANE1:
                 TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
@@ -2066,6 +1990,109 @@ static int32_t noalloc_base(int dev, uint8_t** base)
     return 0;
 }
 
+// V8 frame decode: descriptors and the packet up, CRCs, tables, chains,
+// reconstruction, planes and per-segment / per-tile results back.
+static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J)
+{
+    std::vector<uint32_t> wtile;
+    std::vector<int32_t> wsegs;
+    for (uint32_t t = 0; t < J->ntile; ++t) {
+        const tcg_v8_tile& T = J->tile[t];
+        for (uint32_t k = 0; k < T.nseg; k += 32u) {
+            wtile.push_back(t);
+            for (uint32_t l = 0; l < 32u; ++l) { wsegs.push_back(k + l < T.nseg ? (int32_t)(T.seg0 + k + l) : -1); }
+        }
+    }
+    // per plane: first block, first segment, block columns, visible size, output offset / 64
+    uint32_t pinfo[18];
+    uint64_t nblk = 0, out_elems = 0;
+    uint32_t seg0 = 0;
+    const uint32_t sb = 1u << J->sb_log2;
+    for (uint32_t p = 0; p < 3u; ++p) {
+        const uint32_t blocks = J->cols[p] * J->rows[p];
+        pinfo[6 * p + 0] = (uint32_t)nblk;
+        pinfo[6 * p + 1] = seg0;
+        pinfo[6 * p + 2] = J->cols[p];
+        pinfo[6 * p + 3] = J->vis_w[p];
+        pinfo[6 * p + 4] = J->vis_h[p];
+        pinfo[6 * p + 5] = (uint32_t)(out_elems / 64u);
+        nblk += blocks;
+        seg0 += (blocks + sb - 1u) / sb;
+        out_elems = align_up(out_elems + (uint64_t)J->vis_w[p] * J->vis_h[p], 64);
+    }
+    const size_t desc = align_up((size_t)J->nseg * sizeof(tcg_v8_seg), 256) +
+                        align_up((size_t)J->ntile * sizeof(tcg_v8_tile), 256) + align_up((size_t)J->nq * 256u, 256) +
+                        align_up(wtile.size() * 4u + 16u, 256) + align_up(wsegs.size() * 4u + 16u, 256) + 256u;
+    const size_t resb = align_up((size_t)J->nseg + 16u, 256) + align_up((size_t)J->ntile + 16u, 256);
+    if (!dreserve(C, B_DEC_PKT, J->size + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_DEC_TAB, (size_t)J->ntile * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
+        !dreserve(C, B_DEC_RES, resb) || !dreserve(C, B_DESC, desc) || !hreserve(C, 0, desc) || !hreserve(C, 1, resb)) {
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    cudaStream_t st = C->stream;
+    uint8_t* hd = (uint8_t*)C->h[0].p;
+    uint8_t* dd = dptr<uint8_t>(C, B_DESC);
+    size_t o = 0;
+    auto put = [&](const void* src, size_t n) -> size_t {
+        const size_t at = o;
+        if (n) { memcpy(hd + o, src, n); }
+        o = align_up(o + n, 256);
+        return at;
+    };
+    const size_t o_sg = put(J->seg, (size_t)J->nseg * sizeof(tcg_v8_seg));
+    const size_t o_tl = put(J->tile, (size_t)J->ntile * sizeof(tcg_v8_tile));
+    const size_t o_q = put(J->q, (size_t)J->nq * 256u);
+    const size_t o_wt = put(wtile.data(), wtile.size() * 4u);
+    const size_t o_ws = put(wsegs.data(), wsegs.size() * 4u);
+    const size_t o_pi = put(pinfo, sizeof(pinfo));
+    call_begin(C);
+    TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
+    const tcg_v8_seg* d_sg = (const tcg_v8_seg*)(dd + o_sg);
+    const tcg_v8_tile* d_tl = (const tcg_v8_tile*)(dd + o_tl);
+    const uint32_t* d_q = (const uint32_t*)(dd + o_q);
+    const uint32_t* d_wt = (const uint32_t*)(dd + o_wt);
+    const int32_t* d_ws = (const int32_t*)(dd + o_ws);
+    const uint32_t* d_pi = (const uint32_t*)(dd + o_pi);
+    uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
+    TCG_CHECK(cudaMemcpyAsync(d_pkt, J->packet, J->size, cudaMemcpyDefault, st));
+    int32_t* d_coef = dptr<int32_t>(C, B_DEC_COEF);
+    uint8_t* d_tab = dptr<uint8_t>(C, B_DEC_TAB);
+    uint16_t* d_out = dptr<uint16_t>(C, B_DEC_OUT);
+    uint8_t* d_res = dptr<uint8_t>(C, B_DEC_RES);
+    uint8_t* d_fail = d_res;
+    uint8_t* d_ok = d_res + align_up((size_t)J->nseg + 16u, 256);
+    TCG_CHECK(cudaMemsetAsync(d_res, 0, resb, st));
+    TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
+    const DevTables& T = tables();
+    if (J->ntile > 0u) {
+        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, J->ntile, 256, 0, d_tl, d_pkt, T.crc, d_ok);
+        TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, J->ntile, 32, 0, d_tl, d_pkt, d_tab);
+    }
+    if (!wtile.empty()) {
+        TCG_LAUNCH(C, K_DCHAIN, k_v8_dchain, (uint32_t)wtile.size(), 32, V8D_SMEM, d_sg, d_wt, d_ws, d_pi, d_ok, d_pkt,
+                   d_tab, d_coef, d_fail);
+    }
+    if (nblk > 0u) {
+        TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sg, d_pi, d_q, d_coef,
+                   (uint32_t)nblk, J->bit_depth, J->sb_log2, d_out);
+    }
+    for (uint32_t p = 0; p < 3u; ++p) {
+        const size_t w = J->vis_w[p], h = J->vis_h[p];
+        if (w == 0u || h == 0u) { continue; }
+        const size_t pitch = (J->dst_stride[p] ? J->dst_stride[p] : w) * 2u;
+        TCG_CHECK(cudaMemcpy2DAsync(J->dst[p], pitch, d_out + (size_t)pinfo[6 * p + 5] * 64u, w * 2u, w * 2u, h,
+                                    cudaMemcpyDefault, st));
+    }
+    uint8_t* hr = (uint8_t*)C->h[1].p;
+    TCG_CHECK(cudaMemcpyAsync(hr, d_res, resb, cudaMemcpyDeviceToHost, st));
+    TCG_CHECK(cudaGetLastError());
+    TCG_CHECK(cudaStreamSynchronize(st));
+    call_end(C);
+    memcpy(J->seg_fail, hr, J->nseg);
+    memcpy(J->tile_ok, hr + align_up((size_t)J->nseg + 16u, 256), J->ntile);
+    return 0;
+}
+
 }  // namespace tcg
 
 extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
@@ -2088,6 +2115,15 @@ extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
     tcg::Ctx* c = tcg::ctx_acquire();
     if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
     const int32_t rc = tcg::decode_impl(c, frames, count);
+    tcg::ctx_release(c);
+    return rc;
+}
+
+extern "C" int32_t tcg_decode_v8(const tcg_v8_job* job)
+{
+    tcg::Ctx* c = tcg::ctx_acquire();
+    if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
+    const int32_t rc = tcg::decode_v8_impl(c, job);
     tcg::ctx_release(c);
     return rc;
 }

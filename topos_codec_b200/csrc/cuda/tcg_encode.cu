@@ -17,6 +17,7 @@
 //   k_pack_*    payload sizes, prefix sums into packet offsets, payload copy,
 //               slice CRC-32 + 17-byte headers, frame header size + CRC
 //               (codec.c:5203-5225, 5660-5693; frame_header.c:590-631)
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -34,6 +35,8 @@ struct EPlane {
     uint32_t blk0;       // first global colour block
     uint32_t Q[64];
     int64_t fclamp;
+    uint32_t seg0;       // V8: first global segment of the plane
+    uint32_t sb_log2;    // V8: segment blocks log2 (0 for V7-R2 planes)
 };
 
 struct ESlice {
@@ -941,9 +944,443 @@ __global__ void k_pack_header(const EFrame* __restrict__ frames, uint32_t nf, co
     h[49] = (uint8_t)(c >> 24); h[50] = (uint8_t)(c >> 16); h[51] = (uint8_t)(c >> 8); h[52] = (uint8_t)c;
 }
 
+// ============================ V8 segmented rANS ============================
+//
+// V8 (reference codec.c:3817-4320, layout packet.h:36-82) codes each colour
+// plane as segments of sb = 8/16/32 consecutive blocks, each an independent
+// rANS chain (DC predicted and DC context taken inside the segment only),
+// grouped into tiles of tile_rows block rows that share one model chosen from
+// their segments' summed counts. Per plane the packet holds
+// [directory S x 12][tables T x 350][segment streams][tile CRCs T x 4].
+// A 3840x2160 4:2:2 frame has 16,200 segments of ~3 K operations, so the
+// chains run one lane each, 32 segments of a tile per warp sharing the
+// tile's coding table in shared memory: the chains are short and many, and
+// the encode is bound by issue and bandwidth instead of one long chain.
+//
+// Segments whose first block lies past the last tile's nominal block range
+// belong to no tile; the reference leaves them unwritten and its self-check
+// rejects the frame, and so does the host here (MALFORMED).
+
+constexpr uint32_t V8_EXT = 8u, V8_DIR = 12u, V8_TABLE = 350u;
+
+struct VSeg {
+    uint32_t frame, plane, tile, nblk;   // tile = UINT32_MAX: in no tile (not coded)
+    uint32_t blk0;                       // first global block
+    uint32_t sidx;                       // index within the plane (directory entry)
+    uint32_t qdb, pad;
+    uint64_t op_base, stage_base, stage_cap;
+};
+
+struct VSegRes {
+    uint32_t nops, nbytes, xfin, len;    // len: 4 + nbytes (0 when not coded)
+    uint32_t rel;                        // stream offset from the plane's stream base
+    uint32_t pad;
+    uint64_t pkt_off;                    // stream offset from the packet start
+};
+
+struct VTile {
+    uint32_t frame, plane, tidx, seg0, nseg, blk0, nblk, pad;
+    uint64_t tab_off, str_off, str_bytes, crc_off;   // from the packet start (k_v8_sizes)
+};
+
+struct VPlaneD {
+    uint32_t seg0, nseg, tile0, ntile;
+    uint64_t dir_off, tab_off, str_off, crc_off;      // from the packet start (k_v8_sizes)
+};
+
+__device__ __forceinline__ uint32_t v8_block_dcm(const int32_t* coef, uint32_t gb, uint32_t i, uint32_t cols, bool* viol)
+{
+    const int32_t q0 = coef[(size_t)gb * 64u];
+    const int32_t l = i > 0u ? coef[(size_t)(gb - 1u) * 64u] : 0;
+    const int32_t t = i >= cols ? coef[(size_t)(gb - cols) * 64u] : 0;
+    uint32_t dcm = map_s(q0 - dc_pred(i > 0u, l, i >= cols, t));
+    if (dcm > 0x0FFFFFFFu) { dcm = 0x0FFFFFFFu; *viol = true; }
+    return dcm;
+}
+
+// Tokens and tile histograms (codec.c:3882-3947, 2116-2151): a work item is a
+// run of up to 256 blocks of one tile's segments; DC residuals and the DC
+// context use the segment's own previous blocks only.
+__global__ void __launch_bounds__(256) k_v8_tokens(const EWork* __restrict__ work, const VTile* __restrict__ tiles,
+                                                   const EPlane* __restrict__ planes, const int32_t* __restrict__ coef,
+                                                   const uint64_t* __restrict__ mask, uint32_t* __restrict__ dcm_out,
+                                                   uint32_t* __restrict__ nops_out, uint32_t* __restrict__ hist,
+                                                   ESliceRes* __restrict__ tres)
+{
+    extern __shared__ uint32_t sh[];  // [H_BINS][32] lane-replicated counters
+    const EWork w = work[blockIdx.x];
+    const VTile& T = tiles[w.slice];
+    const EPlane& P = planes[T.plane];
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t i = threadIdx.x; i < H_BINS * 32u; i += blockDim.x) { sh[i] = 0u; }
+    __syncthreads();
+    bool viol = false;
+    if (threadIdx.x < w.n) {
+        const uint32_t gb = T.blk0 + w.lb0 + threadIdx.x;
+        const uint32_t i = (gb - P.blk0) & ((1u << P.sb_log2) - 1u);
+        const uint32_t dcm = v8_block_dcm(coef, gb, i, P.cols, &viol);
+        const uint32_t dcc = bitlen32(dcm);
+        uint32_t ctx = 0u;
+        if (i > 0u) {
+            bool dummy = false;
+            ctx = dcp_ctx(bitlen32(v8_block_dcm(coef, gb - 1u, i - 1u, P.cols, &dummy)), true);
+        }
+        atomicAdd(&sh[(H_DC + dcc) * 32u + lane], 1u);
+        atomicAdd(&sh[(H_JDC + ctx * DC_SYMS + dcc) * 32u + lane], 1u);
+        uint32_t nops = 2u + suffix_chunks(dcc);
+        const uint64_t m = mask[gb];
+        uint32_t prev = 0u, pcat = 0u;
+        bool has = false;
+        int32_t cv[64];
+        const int4* c4 = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            const int4 v = c4[k];
+            cv[4 * k] = v.x; cv[4 * k + 1] = v.y; cv[4 * k + 2] = v.z; cv[4 * k + 3] = v.w;
+        }
+#pragma unroll
+        for (uint32_t p = 1; p < 64u; ++p) {
+            if (((m >> p) & 1u) == 0u) { continue; }
+            uint32_t lm = map_s(cv[p]);
+            if (lm > 0x07FFFFFFu) { lm = 0x07FFFFFFu; viol = true; }
+            const uint32_t cat = bitlen32(lm);
+            const uint32_t run = p - prev - 1u;
+            atomicAdd(&sh[(H_RUN + run) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_LVL + cat) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_JPOS + pos_ctx(p) * LVL_SYMS + cat) * 32u + lane], 1u);
+            atomicAdd(&sh[(H_JPREV + prev_ctx(pcat, has) * LVL_SYMS + cat) * 32u + lane], 1u);
+            nops += 2u + suffix_chunks(cat);
+            prev = p;
+            pcat = cat;
+            has = true;
+        }
+        atomicAdd(&sh[(H_RUN + 63u) * 32u + lane], 1u);
+        dcm_out[gb] = dcm;
+        nops_out[gb] = nops;
+    }
+    if (__syncthreads_or(viol) && threadIdx.x == 0) { atomicOr(&tres[w.slice].err, 1u); }
+    uint32_t* g = hist + (size_t)w.slice * H_BINS;
+    for (uint32_t b = threadIdx.x; b < H_BINS; b += blockDim.x) {
+        uint32_t s = 0;
+#pragma unroll 8
+        for (uint32_t r = 0; r < 32u; ++r) { s += sh[b * 32u + ((r + b) & 31u)]; }
+        if (s != 0u) { atomicAdd(&g[b], s); }
+    }
+}
+
+// One warp per coded segment: operation offsets of its blocks in coding
+// (reverse) order, the segment's count, identity padding to a multiple of 32.
+__global__ void __launch_bounds__(256) k_v8_opscan(const VSeg* __restrict__ segs, const uint32_t* __restrict__ coded,
+                                                   uint32_t ncoded, const uint32_t* __restrict__ nops,
+                                                   uint32_t* __restrict__ opoff, uint32_t* __restrict__ ops,
+                                                   VSegRes* __restrict__ sres)
+{
+    const uint32_t k = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    if (k >= ncoded) { return; }
+    const uint32_t s = coded[k];
+    const VSeg& S = segs[s];
+    const uint32_t v = lane < S.nblk ? nops[S.blk0 + S.nblk - 1u - lane] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (uint32_t d = 1; d < 32u; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= d) { x += y; }
+    }
+    if (lane < S.nblk) { opoff[S.blk0 + S.nblk - 1u - lane] = x - v; }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (lane == 0u) { sres[s].nops = total; }
+    if (total + lane < ((total + 31u) & ~31u)) { ops[S.op_base + total + lane] = 0u; }
+}
+
+// One warp per block (k_opgen's scheme), with the tile's models and the
+// segment's own previous block as the DC context.
+__global__ void __launch_bounds__(256) k_v8_opgen(const EWork* __restrict__ work, const VTile* __restrict__ tiles,
+                                                  const EPlane* __restrict__ planes, const VSeg* __restrict__ segs,
+                                                  const int32_t* __restrict__ coef, const uint64_t* __restrict__ mask,
+                                                  const uint32_t* __restrict__ dcm, const uint32_t* __restrict__ opoff,
+                                                  const ESliceRes* __restrict__ tres, uint32_t* __restrict__ ops)
+{
+    __shared__ uint8_t cats[8][64];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const EWork w = work[blockIdx.x];
+    const uint32_t k = blockIdx.y * 8u + warp;
+    if (k >= w.n) { return; }
+    const VTile& T = tiles[w.slice];
+    const EPlane& P = planes[T.plane];
+    const uint32_t gb = T.blk0 + w.lb0 + k;
+    const uint32_t lb = gb - P.blk0;
+    const uint32_t i = lb & ((1u << P.sb_log2) - 1u);
+    const VSeg& S = segs[P.seg0 + (lb >> P.sb_log2)];
+    const uint32_t pl = tres[w.slice].plen;
+    const uint32_t lmod = (pl >> 16) & 3u, dmod = (pl >> 20) & 1u;
+    uint32_t* o = ops + S.op_base + opoff[gb];
+    const int32_t* c = coef + (size_t)gb * 64u;
+    const uint64_t m = mask[gb];
+    uint32_t lmv[2], cat[2], cnt[2];
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        const uint32_t p = lane + 32u * h;
+        const bool nz = ((m >> p) & 1u) != 0u;
+        const uint32_t lv = nz ? map_s(c[p]) : 0u;
+        lmv[h] = lv > 0x07FFFFFFu ? 0x07FFFFFFu : lv;
+        cat[h] = nz ? bitlen32(lmv[h]) : 0u;
+        cnt[h] = nz ? 2u + suffix_chunks(cat[h]) : 0u;
+        cats[warp][p] = (uint8_t)cat[h];
+    }
+    const uint32_t packed = cnt[0] | (cnt[1] << 16);
+    uint32_t incl = packed;
+#pragma unroll
+    for (uint32_t d = 1; d < 32u; d <<= 1) {
+        const uint32_t t = __shfl_down_sync(0xFFFFFFFFu, incl, d);
+        if (lane + d < 32u) { incl += t; }
+    }
+    const uint32_t above = incl - packed;
+    const uint32_t all = __shfl_sync(0xFFFFFFFFu, incl, 0);
+    const uint32_t hi_total = all >> 16, total = (all & 0xFFFFu) + hi_total;
+    __syncwarp();
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        if (cnt[h] == 0u) { continue; }
+        const uint32_t p = lane + 32u * h;
+        uint32_t* q = o + 1u + (h ? (above >> 16) : hi_total + (above & 0xFFFFu));
+        const uint64_t lower = m & ((1ull << p) - 1ull);
+        const uint32_t below = lower != 0u ? 63u - (uint32_t)__clzll((long long)lower) : 0u;
+        put_suffix_ops(q, cat[h], lmv[h]);
+        uint32_t ctx = 0u;
+        if (lmod == 1u) {
+            ctx = pos_ctx(p);
+        } else if (lmod == 2u) {
+            ctx = prev_ctx(lower != 0u ? cats[warp][below] : 0u, lower != 0u);
+        }
+        *q++ = op_sym(T_LVL + ctx * LVL_SYMS + cat[h]);
+        *q = op_sym(T_RUN + (p - below - 1u));
+    }
+    if (lane == 0u) {
+        o[0] = op_sym(T_RUN + 63u);
+        uint32_t* q = o + 1u + total;
+        const uint32_t dm = dcm[gb];
+        const uint32_t ds = bitlen32(dm);
+        put_suffix_ops(q, ds, dm);
+        const uint32_t dctx = dmod ? dcp_ctx(i > 0u ? bitlen32(dcm[gb - 1u]) : 0u, i > 0u) : 0u;
+        *q = op_sym(T_DC + dctx * DC_SYMS + ds);
+    }
+}
+
+// One lane per segment, 32 segments of one tile per warp: the warp expands
+// the tile's coding table into shared memory once, then every lane runs its
+// segment's backward chain as k_chain does.
+constexpr size_t V8CH_SMEM = (size_t)OP_ENTRIES * sizeof(uint4);
+
+__global__ void __launch_bounds__(32) k_v8_chain(const VSeg* __restrict__ segs, const int32_t* __restrict__ lanes,
+                                                 const uint32_t* __restrict__ ctile, const uint32_t* __restrict__ ops,
+                                                 const uint32_t* __restrict__ stab, const uint32_t* __restrict__ div_m,
+                                                 const uint8_t* __restrict__ div_l, uint8_t* __restrict__ stage,
+                                                 VSegRes* __restrict__ sres)
+{
+    extern __shared__ uint4 chain_tab[];
+    const uint32_t lane = threadIdx.x;
+    const uint32_t* st = stab + (size_t)ctile[blockIdx.x] * T_SIZE;
+    for (uint32_t w = lane; w < OP_ENTRIES; w += 32u) {
+        chain_tab[w] = w < OP_CHUNKS ? chunk_entry(w) : symbol_entry(__ldg(st + (w - OP_CHUNKS)), div_m, div_l);
+    }
+    __syncwarp();
+    const int32_t si = lanes[blockIdx.x * 32u + lane];
+    if (si < 0) { return; }
+    const uint4* tab = chain_tab;
+    const VSeg& S = segs[si];
+    const uint32_t nops = sres[si].nops;
+    const uint4* op4 = reinterpret_cast<const uint4*>(ops + S.op_base);
+    uint8_t* const end = stage + S.stage_base + S.stage_cap;
+    uint8_t* p = end;
+    uint32_t x = RANS_L;
+    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops);
+    uint4 q2 = op_group(op4, 2u, nops), q3 = op_group(op4, 3u, nops);
+    uint4 q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
+    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops);
+    for (uint32_t g = 0; 4u * g < nops; g += 8u) {
+        ENC_GROUP(q0); q0 = op_group(op4, g + 8u, nops);
+        ENC_GROUP(q1); q1 = op_group(op4, g + 9u, nops);
+        ENC_GROUP(q2); q2 = op_group(op4, g + 10u, nops);
+        ENC_GROUP(q3); q3 = op_group(op4, g + 11u, nops);
+        ENC_GROUP(q4); q4 = op_group(op4, g + 12u, nops);
+        ENC_GROUP(q5); q5 = op_group(op4, g + 13u, nops);
+        ENC_GROUP(q6); q6 = op_group(op4, g + 14u, nops);
+        ENC_GROUP(q7); q7 = op_group(op4, g + 15u, nops);
+    }
+    sres[si].nbytes = (uint32_t)(end - p);
+    sres[si].xfin = x;
+}
+
+// One block per frame: segment stream offsets (a block-wide scan per plane),
+// plane section offsets, tile table / stream / CRC ranges, the packet size,
+// the 8-byte extension header; token-domain errors of its tiles.
+__global__ void __launch_bounds__(1024) k_v8_sizes(const EFrame* __restrict__ frames, VPlaneD* __restrict__ vp,
+                                                   const VSeg* __restrict__ segs, VSegRes* __restrict__ sres,
+                                                   VTile* __restrict__ tiles, const ESliceRes* __restrict__ tres,
+                                                   EFrameRes* __restrict__ fres, uint8_t* __restrict__ pkt,
+                                                   const uint8_t* __restrict__ ext)
+{
+    __shared__ unsigned long long sm[32];
+    const EFrame& F = frames[blockIdx.x];
+    uint64_t off = 53u + V8_EXT;
+    uint32_t err = 0u;
+    for (uint32_t pi = 0; pi < F.nslices; ++pi) {
+        VPlaneD& P = vp[F.slice0 + pi];
+        const uint64_t dir = off, tab = dir + (uint64_t)P.nseg * V8_DIR, str = tab + (uint64_t)P.ntile * V8_TABLE;
+        unsigned long long carry = 0;
+        for (uint32_t b = 0; b < P.nseg; b += blockDim.x) {
+            const uint32_t k = b + threadIdx.x;
+            const uint32_t s = P.seg0 + k;
+            const uint32_t len = k < P.nseg && segs[s].tile != 0xFFFFFFFFu ? 4u + sres[s].nbytes : 0u;
+            unsigned long long tot;
+            const unsigned long long pre = block_exscan<unsigned long long>(len, &tot, sm);
+            if (k < P.nseg) {
+                sres[s].len = len;
+                sres[s].rel = (uint32_t)(carry + pre);
+                sres[s].pkt_off = str + carry + pre;
+            }
+            carry += tot;
+        }
+        const uint64_t crc = str + carry;
+        __syncthreads();
+        for (uint32_t t = threadIdx.x; t < P.ntile; t += blockDim.x) {
+            VTile& T = tiles[P.tile0 + t];
+            T.tab_off = tab + (uint64_t)t * V8_TABLE;
+            T.crc_off = crc + 4u * t;
+            if (T.nseg != 0u) {
+                const VSegRes& a = sres[T.seg0];
+                const VSegRes& z = sres[T.seg0 + T.nseg - 1u];
+                T.str_off = a.pkt_off;
+                T.str_bytes = z.pkt_off + z.len - a.pkt_off;
+            } else {
+                T.str_off = str;
+                T.str_bytes = 0u;
+            }
+            err |= tres[P.tile0 + t].err;
+        }
+        if (threadIdx.x == 0) {
+            P.dir_off = dir;
+            P.tab_off = tab;
+            P.str_off = str;
+            P.crc_off = crc;
+        }
+        off = crc + 4u * P.ntile;
+    }
+    err = __syncthreads_or(err != 0u) ? 1u : 0u;
+    if (threadIdx.x == 0) {
+        fres[blockIdx.x].size = off > 0x10000000ull ? 0xFFFFFFFFu : (uint32_t)off;
+        fres[blockIdx.x].color_payload = (uint32_t)(off - 53u - V8_EXT);
+        fres[blockIdx.x].alpha_payload = 0u;
+        fres[blockIdx.x].err = err;
+        fres[blockIdx.x].color_slices = 0u;
+        fres[blockIdx.x].alpha_slices = 0u;
+    }
+    if (threadIdx.x < V8_EXT) { pkt[F.pkt_base + 53u + threadIdx.x] = ext[blockIdx.x * V8_EXT + threadIdx.x]; }
+}
+
+// One warp per segment: its directory entry and its stream (final state
+// big-endian, then the bytes the chain emitted) at the offsets k_v8_sizes set.
+__global__ void __launch_bounds__(256) k_v8_copy(const EFrame* __restrict__ frames, const VPlaneD* __restrict__ vp,
+                                                 const VSeg* __restrict__ segs, uint32_t nseg,
+                                                 const VSegRes* __restrict__ sres, const uint8_t* __restrict__ stage,
+                                                 uint8_t* __restrict__ pkt)
+{
+    const uint32_t s = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    if (s >= nseg) { return; }
+    const VSeg& S = segs[s];
+    const VSegRes& R = sres[s];
+    const EFrame& F = frames[S.frame];
+    const VPlaneD& P = vp[S.plane];
+    uint8_t* de = pkt + F.pkt_base + P.dir_off + (uint64_t)S.sidx * V8_DIR;
+    if (lane < V8_DIR) {
+        const bool coded = S.tile != 0xFFFFFFFFu;
+        uint32_t b = 0u;
+        if (coded) {
+            if (lane < 4u) { b = (R.rel >> (8u * (3u - lane))) & 0xFFu; }
+            else if (lane < 8u) { b = (R.len >> (8u * (7u - lane))) & 0xFFu; }
+            else if (lane == 8u) { b = S.qdb; }
+        }
+        de[lane] = (uint8_t)b;
+    }
+    if (S.tile == 0xFFFFFFFFu) { return; }
+    uint8_t* dst = pkt + F.pkt_base + R.pkt_off;
+    const uint8_t* stream = stage + S.stage_base + S.stage_cap - R.nbytes;
+    const uint32_t total = R.len, xfin = R.xfin;
+    auto byte_at = [&](uint32_t i) -> uint8_t {
+        return i < 4u ? (uint8_t)(xfin >> (8u * (3u - i))) : stream[i - 4u];
+    };
+    const uint32_t lead = (uint32_t)((4u - ((uintptr_t)dst & 3u)) & 3u);
+    const uint32_t nw = total > lead ? (total - lead) / 4u : 0u;
+    const uint32_t tail0 = lead + 4u * nw;
+    if (lane < lead && lane < total) { dst[lane] = byte_at(lane); }
+    if (tail0 + lane < total) { dst[tail0 + lane] = byte_at(tail0 + lane); }
+    uint32_t* dw = reinterpret_cast<uint32_t*>(dst + lead);
+    for (uint32_t w = lane; w < nw; w += 32u) {
+        const uint32_t i = lead + 4u * w;
+        uint32_t word;
+        if (i >= 4u) {
+            const uintptr_t sa = (uintptr_t)(stream + (i - 4u));
+            const uint32_t* sw = reinterpret_cast<const uint32_t*>(sa & ~(uintptr_t)3);
+            const uint32_t sh = (uint32_t)(sa & 3u);
+            word = __byte_perm(sw[0], sh != 0u ? sw[1] : 0u, 0x3210u + sh * 0x1111u);
+        } else {
+            word = (uint32_t)byte_at(i) | ((uint32_t)byte_at(i + 1u) << 8) | ((uint32_t)byte_at(i + 2u) << 16) |
+                   ((uint32_t)byte_at(i + 3u) << 24);
+        }
+        dw[w] = word;
+    }
+}
+
+// One block per tile: the 350-byte table (flags, five DC rows, run row, five
+// level rows; rows past the model's contexts are the all-zero row {1, 0, ...},
+// codec.c:3949-3971), then the CRC of the table and the member streams.
+__global__ void __launch_bounds__(256) k_v8_tiles(const EFrame* __restrict__ frames, const VTile* __restrict__ tiles,
+                                                  const ESliceRes* __restrict__ tres, const uint8_t* __restrict__ prefix,
+                                                  const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
+{
+    __shared__ uint32_t t[8 * 256];
+    __shared__ uint32_t scratch[512];
+    __shared__ uint32_t crc_tab;
+    for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
+    const uint32_t ti = blockIdx.x;
+    const VTile& T = tiles[ti];
+    uint8_t* base = pkt + frames[T.frame].pkt_base;
+    const uint32_t pl = tres[ti].plen;
+    const uint32_t lm = (pl >> 16) & 3u, dm = (pl >> 20) & 1u;
+    const uint32_t nd = dm ? DCP_CTX : 1u, nl = lm == 1u ? POS_CTX : lm == 2u ? PREV_CTX : 1u;
+    const uint8_t* pre = prefix + (size_t)ti * PREFIX_MAX;
+    uint8_t* tb = base + T.tab_off;
+    for (uint32_t k = threadIdx.x; k < V8_TABLE; k += blockDim.x) {
+        uint8_t v;
+        if (k == 0u) {
+            v = pre[0];
+        } else if (k < 1u + DCP_CTX * DC_SYMS) {
+            const uint32_t c = (k - 1u) / DC_SYMS, j = (k - 1u) % DC_SYMS;
+            v = c < nd ? pre[1u + c * DC_SYMS + j] : (uint8_t)(j == 0u);
+        } else if (k < 1u + DCP_CTX * DC_SYMS + RUN_SYMS) {
+            v = pre[1u + nd * DC_SYMS + (k - 1u - DCP_CTX * DC_SYMS)];
+        } else {
+            const uint32_t r = k - 1u - DCP_CTX * DC_SYMS - RUN_SYMS, c = r / LVL_SYMS, j = r % LVL_SYMS;
+            v = c < nl ? pre[1u + nd * DC_SYMS + RUN_SYMS + c * LVL_SYMS + j] : (uint8_t)(j == 0u);
+        }
+        tb[k] = v;
+    }
+    __syncthreads();
+    const uint32_t c1 = crc32_block(tb, V8_TABLE, t, scratch);
+    if (threadIdx.x == 0) { crc_tab = c1; }
+    __syncthreads();
+    const uint32_t c2 = crc32_block(base + T.str_off, T.str_bytes, t, scratch);
+    if (threadIdx.x == 0) {
+        const uint32_t c = T.str_bytes == 0u ? crc_tab : crc_combine(crc_tab, c2, gf2_xpow8n(T.str_bytes));
+        uint8_t* h = base + T.crc_off;
+        h[0] = (uint8_t)(c >> 24); h[1] = (uint8_t)(c >> 16); h[2] = (uint8_t)(c >> 8); h[3] = (uint8_t)c;
+    }
+}
+
 // ================================== driver ==================================
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1u) / a * a; }
+
 
 // Enqueue one batch on the context's streams: descriptors, sample copies,
 // kernels and the copy of the per-frame results to pinned host memory. The
@@ -1167,6 +1604,229 @@ static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count
     return 0;
 }
 
+// V8 batch: every frame of the call is V8 (tcg_encode splits mixed batches).
+// Host planning lays out planes, segments, tiles, token work items and the
+// chain warps (32 segments of one tile each); the device does the rest.
+static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t count, std::vector<EFrame>& ef)
+{
+    std::vector<EPlane> planes;
+    std::vector<VSeg> segs;
+    std::vector<VTile> tiles;
+    std::vector<VPlaneD> vps;
+    std::vector<EWork> work;
+    std::vector<uint32_t> coded, tile_ids, ctile;
+    std::vector<int32_t> lanes;
+    std::vector<uint8_t> ext((size_t)count * V8_EXT, 0);
+    ef.assign(count, EFrame());
+    uint64_t pix_elems = 0, nblk = 0, ops_words = 0, stage_bytes = 0, pkt_bytes = 0;
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_enc_frame& F = frames[f];
+        ef[f].slice0 = (uint32_t)vps.size();
+        ef[f].nslices = 3u;
+        memset(ef[f].hdr, 0, sizeof(ef[f].hdr));
+        memcpy(ef[f].hdr, F.header, 53);
+        ext[(size_t)f * V8_EXT] = (uint8_t)F.v8_sb_log2;
+        ext[(size_t)f * V8_EXT + 1u] = (uint8_t)F.v8_tile_log2;
+        const uint32_t sb = 1u << F.v8_sb_log2;
+        uint64_t fbound = 53u + V8_EXT;
+        for (uint32_t p = 0; p < 3u; ++p) {
+            const tcg_enc_plane& I = F.plane[p];
+            EPlane P;
+            memset(&P, 0, sizeof(P));
+            P.pix_off = pix_elems;
+            pix_elems = align_up(pix_elems + (uint64_t)I.vis_w * I.vis_h, 64);
+            P.vis_w = I.vis_w; P.vis_h = I.vis_h; P.coded_w = I.coded_w; P.coded_h = I.coded_h;
+            P.cols = I.cols; P.rows = I.rows; P.kind = TCG_PLANE_COLOR;
+            P.bd = F.bit_depth;
+            P.blk0 = (uint32_t)nblk;
+            P.fclamp = I.fclamp;
+            P.q_is_one = 1u;
+            for (int i = 0; i < 64; ++i) { P.Q[i] = I.Q[i]; if (I.Q[i] != 1u) { P.q_is_one = 0u; } }
+            P.seg0 = (uint32_t)segs.size();
+            P.sb_log2 = F.v8_sb_log2;
+            const uint32_t pg = (uint32_t)planes.size();
+            const uint32_t blocks = I.cols * I.rows;
+            const uint32_t S = (blocks + sb - 1u) / sb;
+            const uint32_t tr = F.v8_tile_log2 == 0u ? 0u : 1u << F.v8_tile_log2;
+            const uint32_t T = (tr == 0u || I.rows == 0u) ? 1u : (I.rows + tr - 1u) / tr;
+            VPlaneD D;
+            memset(&D, 0, sizeof(D));
+            D.seg0 = P.seg0; D.nseg = S; D.tile0 = (uint32_t)tiles.size(); D.ntile = T;
+            const uint32_t vpi = (uint32_t)vps.size();
+            for (uint32_t k = 0; k < S; ++k) {
+                VSeg G;
+                memset(&G, 0, sizeof(G));
+                G.frame = f; G.plane = vpi; G.tile = 0xFFFFFFFFu;
+                G.blk0 = P.blk0 + k * sb;
+                G.nblk = std::min(sb, blocks - k * sb);
+                G.sidx = k;
+                G.qdb = I.qdb;
+                G.op_base = ops_words;
+                ops_words += (uint64_t)G.nblk * 256u + 256u;
+                G.stage_cap = (uint64_t)G.nblk * 512u + 64u;
+                G.stage_base = stage_bytes;
+                stage_bytes = align_up(stage_bytes + G.stage_cap, 256);
+                fbound += V8_DIR + 4u + G.stage_cap;
+                segs.push_back(G);
+            }
+            for (uint32_t t = 0; t < T; ++t) {
+                const uint64_t fb = tr == 0u ? 0u : (uint64_t)t * tr * I.cols;
+                const uint64_t fn = tr == 0u ? (uint64_t)blocks : (uint64_t)(t + 1u) * tr * I.cols;
+                uint32_t sf = (uint32_t)std::min<uint64_t>(fb / sb, S), sn = (uint32_t)std::min<uint64_t>(fn / sb, S);
+                sn = std::max(sn, sf);
+                VTile V;
+                memset(&V, 0, sizeof(V));
+                V.frame = f; V.plane = pg; V.tidx = t; V.seg0 = P.seg0 + sf; V.nseg = sn - sf;
+                V.blk0 = P.blk0 + sf * sb;
+                V.nblk = sn > sf ? std::min(sn * sb, blocks) - sf * sb : 0u;
+                const uint32_t ti = (uint32_t)tiles.size();
+                for (uint32_t k = sf; k < sn; ++k) {
+                    segs[P.seg0 + k].tile = ti;
+                    coded.push_back(P.seg0 + k);
+                }
+                for (uint32_t lb = 0; lb < V.nblk; lb += 256u) {
+                    EWork w = {ti, lb, std::min(256u, V.nblk - lb), 0u};
+                    work.push_back(w);
+                }
+                for (uint32_t k = sf; k < sn; k += 32u) {
+                    ctile.push_back(ti);
+                    for (uint32_t l = 0; l < 32u; ++l) { lanes.push_back(k + l < sn ? (int32_t)(P.seg0 + k + l) : -1); }
+                }
+                tile_ids.push_back(ti);
+                tiles.push_back(V);
+                fbound += V8_TABLE + 4u;
+            }
+            nblk += blocks;
+            planes.push_back(P);
+            vps.push_back(D);
+        }
+        ef[f].pkt_base = pkt_bytes;
+        pkt_bytes = align_up(pkt_bytes + fbound, 256);
+    }
+    const uint32_t nseg = (uint32_t)segs.size(), nt = (uint32_t)tiles.size(), ncoded = (uint32_t)coded.size();
+    const uint32_t nwarps = (uint32_t)ctile.size();
+    const size_t desc_bytes = align_up(planes.size() * sizeof(EPlane), 256) + align_up(segs.size() * sizeof(VSeg), 256) +
+                              align_up(tiles.size() * sizeof(VTile), 256) + align_up(vps.size() * sizeof(VPlaneD), 256) +
+                              align_up(count * sizeof(EFrame), 256) + align_up(work.size() * sizeof(EWork) + 16, 256) +
+                              align_up((planes.size() + coded.size() + tile_ids.size() + ctile.size()) * 4u + 16u, 256) +
+                              align_up(lanes.size() * 4u + 16u, 256) + align_up(ext.size() + 16u, 256);
+    const size_t res_bytes = align_up((size_t)nseg * sizeof(VSegRes), 256) + align_up((size_t)nt * sizeof(ESliceRes), 256);
+    if (!dreserve(C, B_PIX, pix_elems * 2u + 256) || !dreserve(C, B_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_MASK, nblk * 8u + 256) || !dreserve(C, B_DCM, nblk * 4u + 256) ||
+        !dreserve(C, B_NOPS, nblk * 4u + 256) || !dreserve(C, B_OPOFF, nblk * 4u + 256) ||
+        !dreserve(C, B_HIST, (size_t)nt * H_BINS * 4u + 256) || !dreserve(C, B_STAB, (size_t)nt * T_SIZE * 4u + 256) ||
+        !dreserve(C, B_TMP0, (size_t)nt * PREFIX_MAX + 256) || !dreserve(C, B_OPS, ops_words * 4u + 256) ||
+        !dreserve(C, B_STAGE, stage_bytes + 256) || !dreserve(C, B_SRES, res_bytes + 256) ||
+        !dreserve(C, B_FRES, (size_t)count * (sizeof(EFrameRes) + 4u) + 256) || !dreserve(C, B_PKT, pkt_bytes + 256) ||
+        !dreserve(C, B_DESC, desc_bytes) || !hreserve(C, 0, desc_bytes) ||
+        !hreserve(C, 1, (size_t)count * sizeof(EFrameRes) + 4096)) {
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    cudaStream_t st = C->stream;
+    uint8_t* hd = (uint8_t*)C->h[0].p;
+    uint8_t* dd = dptr<uint8_t>(C, B_DESC);
+    size_t o = 0;
+    auto put = [&](const void* src, size_t n) -> size_t {
+        const size_t at = o;
+        if (n) { memcpy(hd + o, src, n); }
+        o = align_up(o + n, 256);
+        return at;
+    };
+    std::vector<uint32_t> cplanes(planes.size());
+    for (uint32_t i = 0; i < (uint32_t)planes.size(); ++i) { cplanes[i] = i; }
+    const size_t o_pl = put(planes.data(), planes.size() * sizeof(EPlane));
+    const size_t o_sg = put(segs.data(), segs.size() * sizeof(VSeg));
+    const size_t o_tl = put(tiles.data(), tiles.size() * sizeof(VTile));
+    const size_t o_vp = put(vps.data(), vps.size() * sizeof(VPlaneD));
+    const size_t o_fr = put(ef.data(), count * sizeof(EFrame));
+    const size_t o_wk = put(work.data(), work.size() * sizeof(EWork));
+    const size_t o_cp = put(cplanes.data(), cplanes.size() * 4u);
+    const size_t o_cd = put(coded.data(), coded.size() * 4u);
+    const size_t o_ti = put(tile_ids.data(), tile_ids.size() * 4u);
+    const size_t o_ct = put(ctile.data(), ctile.size() * 4u);
+    const size_t o_ln = put(lanes.data(), lanes.size() * 4u);
+    const size_t o_ex = put(ext.data(), ext.size());
+    call_begin(C);
+    TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
+    const EPlane* d_pl = (const EPlane*)(dd + o_pl);
+    const VSeg* d_sg = (const VSeg*)(dd + o_sg);
+    VTile* d_tl = (VTile*)(dd + o_tl);
+    VPlaneD* d_vp = (VPlaneD*)(dd + o_vp);
+    const EFrame* d_fr = (const EFrame*)(dd + o_fr);
+    const EWork* d_wk = (const EWork*)(dd + o_wk);
+    const uint32_t* d_cp = (const uint32_t*)(dd + o_cp);
+    const uint32_t* d_cd = (const uint32_t*)(dd + o_cd);
+    const uint32_t* d_ti = (const uint32_t*)(dd + o_ti);
+    const uint32_t* d_ct = (const uint32_t*)(dd + o_ct);
+    const int32_t* d_ln = (const int32_t*)(dd + o_ln);
+    const uint8_t* d_ex = dd + o_ex;
+    uint16_t* d_pix = dptr<uint16_t>(C, B_PIX);
+    for (uint32_t f = 0, pg = 0; f < count; ++f) {
+        for (uint32_t p = 0; p < 3u; ++p, ++pg) {
+            const tcg_enc_plane& I = frames[f].plane[p];
+            if (I.stride == I.vis_w) {
+                TCG_CHECK(cudaMemcpyAsync(d_pix + planes[pg].pix_off, I.src, (size_t)I.vis_w * I.vis_h * 2u,
+                                          cudaMemcpyDefault, st));
+            } else {
+                TCG_CHECK(cudaMemcpy2DAsync(d_pix + planes[pg].pix_off, (size_t)I.vis_w * 2u, I.src, I.stride * 2u,
+                                            (size_t)I.vis_w * 2u, I.vis_h, cudaMemcpyDefault, st));
+            }
+        }
+    }
+    TCG_CHECK(cudaEventRecord(C->gate, st));
+    uint8_t* d_res = dptr<uint8_t>(C, B_SRES);
+    VSegRes* d_sres = (VSegRes*)d_res;
+    ESliceRes* d_tres = (ESliceRes*)(d_res + align_up((size_t)nseg * sizeof(VSegRes), 256));
+    EFrameRes* d_fres = dptr<EFrameRes>(C, B_FRES);
+    uint32_t* d_aerr = reinterpret_cast<uint32_t*>(dptr<uint8_t>(C, B_FRES) + align_up(count * sizeof(EFrameRes), 16));
+    TCG_CHECK(cudaMemsetAsync(d_res, 0, res_bytes, st));
+    TCG_CHECK(cudaMemsetAsync(d_aerr, 0, (size_t)count * 4u, st));
+    TCG_CHECK(cudaMemsetAsync(dptr<uint32_t>(C, B_HIST), 0, (size_t)nt * H_BINS * 4u, st));
+    const DevTables& Tb = tables();
+    int32_t* d_coef = dptr<int32_t>(C, B_COEF);
+    uint64_t* d_mask = dptr<uint64_t>(C, B_MASK);
+    uint32_t* d_dcm = dptr<uint32_t>(C, B_DCM);
+    uint32_t* d_nops = dptr<uint32_t>(C, B_NOPS);
+    uint32_t* d_opoff = dptr<uint32_t>(C, B_OPOFF);
+    uint32_t* d_hist = dptr<uint32_t>(C, B_HIST);
+    uint32_t* d_stab = dptr<uint32_t>(C, B_STAB);
+    uint8_t* d_prefix = dptr<uint8_t>(C, B_TMP0);
+    uint32_t* d_ops = dptr<uint32_t>(C, B_OPS);
+    uint8_t* d_stage = dptr<uint8_t>(C, B_STAGE);
+    uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
+    TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)planes.size(),
+               (uint32_t)nblk, d_pix, d_coef, d_mask);
+    const size_t tok_smem = H_BINS * 32u * 4u;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_v8_tokens, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tok_smem);
+        attr_set = true;
+    }
+    if (!work.empty()) {
+        TCG_LAUNCH(C, K_TOKENS, k_v8_tokens, (uint32_t)work.size(), 256, tok_smem, d_wk, d_tl, d_pl, d_coef, d_mask,
+                   d_dcm, d_nops, d_hist, d_tres);
+    }
+    TCG_LAUNCH(C, K_SELECT, k_select, nt, 32, 0, nullptr, d_ti, d_hist, Tb.log2, d_stab, d_prefix, d_tres);
+    if (ncoded > 0u) {
+        TCG_LAUNCH(C, K_OPSCAN, k_v8_opscan, (ncoded + 7u) / 8u, 256, 0, d_sg, d_cd, ncoded, d_nops, d_opoff, d_ops,
+                   d_sres);
+        TCG_LAUNCH(C, K_OPGEN, k_v8_opgen, dim3((uint32_t)work.size(), 32), 256, 0, d_wk, d_tl, d_pl, d_sg, d_coef,
+                   d_mask, d_dcm, d_opoff, d_tres, d_ops);
+        TCG_LAUNCH(C, K_CHAIN, k_v8_chain, nwarps, 32, V8CH_SMEM, d_sg, d_ln, d_ct, d_ops, d_stab, Tb.div_m, Tb.div_l,
+                   d_stage, d_sres);
+    }
+    TCG_LAUNCH(C, K_PACK_SIZES, k_v8_sizes, count, 1024, 0, d_fr, d_vp, d_sg, d_sres, d_tl, d_tres, d_fres, d_pkt, d_ex);
+    TCG_LAUNCH(C, K_PACK_COPY, k_v8_copy, (nseg + 7u) / 8u, 256, 0, d_fr, d_vp, d_sg, nseg, d_sres, d_stage, d_pkt);
+    TCG_LAUNCH(C, K_PACK_CRC, k_v8_tiles, nt, 256, 0, d_fr, d_tl, d_tres, d_prefix, Tb.crc, d_pkt);
+    TCG_LAUNCH(C, K_PACK_HEADER, k_pack_header, (count + 127u) / 128u, 128, 0, d_fr, count, d_fres, Tb.crc, d_pkt);
+    TCG_CHECK(cudaGetLastError());
+    EFrameRes* hf = (EFrameRes*)C->h[1].p;
+    uint32_t* ha = (uint32_t*)((uint8_t*)C->h[1].p + align_up(count * sizeof(EFrameRes), 16));
+    TCG_CHECK(cudaMemcpyAsync(hf, d_fres, count * sizeof(EFrameRes), cudaMemcpyDeviceToHost, st));
+    TCG_CHECK(cudaMemcpyAsync(ha, d_aerr, count * 4u, cudaMemcpyDeviceToHost, st));
+    return 0;
+}
+
 // Wait for a launched batch's per-frame results, fill res and enqueue the copy
 // of every packet that fits its buffer (the caller synchronises the stream).
 static int32_t encode_results(Ctx* C, const std::vector<EFrame>& ef, uint8_t* const* outs, const size_t* caps,
@@ -1211,7 +1871,8 @@ static int32_t encode_impl(Ctx* C, const tcg_enc_frame* frames, uint32_t count, 
                            const size_t* caps, tcg_enc_result* res)
 {
     std::vector<EFrame> ef;
-    int32_t rc = encode_launch(C, frames, count, nullptr, ef);
+    int32_t rc = count > 0u && frames[0].v8_sb_log2 != 0u ? encode_launch_v8(C, frames, count, ef)
+                                                          : encode_launch(C, frames, count, nullptr, ef);
     if (rc == 0) { rc = encode_results(C, ef, outs, caps, res); }
     if (rc != 0) { return rc; }
     TCG_CHECK(cudaStreamSynchronize(C->stream));
@@ -1375,7 +2036,33 @@ extern "C" void tcg_sized_close(tcg_sized* s)
 extern "C" int32_t tcg_encode(const tcg_enc_frame* frames, uint32_t count, uint8_t* const* outs, const size_t* caps,
                               tcg_enc_result* res)
 {
-    if (count >= 2u && tcg::host_memory(frames[0].plane[0].src)) {
+    uint32_t n8 = 0;
+    for (uint32_t f = 0; f < count; ++f) { n8 += frames[f].v8_sb_log2 != 0u ? 1u : 0u; }
+    if (n8 != 0u && n8 != count) {
+        // V7-R2 and V8 frames run as two launch sequences, each in call order
+        double ms = 0.0;
+        for (int v8 = 0; v8 < 2; ++v8) {
+            std::vector<tcg_enc_frame> fr;
+            std::vector<uint8_t*> o;
+            std::vector<size_t> c;
+            std::vector<uint32_t> at;
+            for (uint32_t f = 0; f < count; ++f) {
+                if ((frames[f].v8_sb_log2 != 0u) != (v8 != 0)) { continue; }
+                fr.push_back(frames[f]);
+                o.push_back(outs[f]);
+                c.push_back(caps[f]);
+                at.push_back(f);
+            }
+            std::vector<tcg_enc_result> r(fr.size());
+            const int32_t rc = tcg_encode(fr.data(), (uint32_t)fr.size(), o.data(), c.data(), r.data());
+            if (rc != 0) { return rc; }
+            ms += tcg_last_ms();
+            for (size_t k = 0; k < at.size(); ++k) { res[at[k]] = r[k]; }
+        }
+        tcg::set_last_ms(ms);
+        return 0;
+    }
+    if (count >= 2u && n8 == 0u && tcg::host_memory(frames[0].plane[0].src)) {
         std::vector<uint64_t> bytes(count, 0);
         for (uint32_t f = 0; f < count; ++f) {
             for (uint32_t p = 0; p < frames[f].planes; ++p) {

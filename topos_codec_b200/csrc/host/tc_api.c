@@ -223,8 +223,25 @@ int32_t tc_prepare_encode(const topos_frame_config* cfg, const topos_frame_input
     if (cfg->reserved[1] == 1u || cfg->reserved[2] == 1u) {
         return tc_fail(TC_ERR_NOT_IMPLEMENTED, "adaptive quantisation / RDO encode is not implemented by the GPU library");
     }
-    if (!(h.major == 7u && h.em == 7u)) {
-        return tc_fail(TC_ERR_NOT_IMPLEMENTED, "the GPU library encodes the V7-R2 generation only (reserved[0] = 8)");
+    const int v8 = h.major == 8u && h.em == 8u;
+    uint32_t sb_log2 = 0u, tile_log2 = 0u;
+    if (v8) {
+        /* V8 segmented rANS (reference codec.c:5749-5770 granularity, 4204-4215
+         * format limits): reserved[3] = segment blocks log2 (0 = 4),
+         * reserved[4] = tile rows log2 (0 = 5) */
+        sb_log2 = cfg->reserved[3] != 0u ? cfg->reserved[3] : 4u;
+        tile_log2 = cfg->reserved[4] != 0u ? cfg->reserved[4] : 5u;
+        if (sb_log2 < 3u || sb_log2 > 5u) {
+            return tc_fail(TC_ERR_INVALID_ARGUMENT, "v8 reserved[3] sb_log2 %u not in {3,4,5}", sb_log2);
+        }
+        if (tile_log2 != 0u && (tile_log2 < 4u || tile_log2 > 6u)) {
+            return tc_fail(TC_ERR_INVALID_ARGUMENT, "v8 reserved[4] tile_log2 %u not in {0,4,5,6}", tile_log2);
+        }
+        if (h.amode != 0u) { return tc_fail(TC_ERR_NOT_IMPLEMENTED, "v8 alpha pending (format-plan batch 5)"); }
+        if (h.pf == 3u) { return tc_fail(TC_ERR_NOT_IMPLEMENTED, "v8 does not carry CFA (TRAW uses rans2)"); }
+    } else if (!(h.major == 7u && h.em == 7u)) {
+        return tc_fail(TC_ERR_NOT_IMPLEMENTED,
+                       "the GPU library encodes the V7-R2 and V8 generations only (reserved[0] = 8 or 9)");
     }
     uint16_t qmL[64], qmC[64];
     if (!tc_qmatrix(h.qm, 0, qmL) || !tc_qmatrix(h.qm, 1, qmC)) {
@@ -261,10 +278,40 @@ int32_t tc_prepare_encode(const topos_frame_config* cfg, const topos_frame_input
             P->qdb = (uint32_t)(64 + qe - (int32_t)h.qp);
         }
     }
+    if (v8) {
+        /* the packet's slice count is the tiles of the three colour planes */
+        const uint32_t tr = tile_log2 == 0u ? 0u : 1u << tile_log2;
+        uint32_t tiles = 0;
+        for (uint32_t p = 0; p < 3u; ++p) { tiles += (tr == 0u || h.brows[p] == 0u) ? 1u : (h.brows[p] + tr - 1u) / tr; }
+        if (tiles < 3u || tiles > TC_MAX_SLICE_COUNT) {
+            return tc_fail(TC_ERR_LIMIT_EXCEEDED, "v8 tile count %u out of [3,512]", tiles);
+        }
+        jf->v8_sb_log2 = sb_log2;
+        jf->v8_tile_log2 = tile_log2;
+        total = tiles;
+        h.slices = (uint16_t)tiles;
+    }
     tc_hdr_pack(&h, jf->header);
     *slice_count = total;
     *qp_base = h.qp;
     return TC_OK;
+}
+
+/* A V8 plane whose last segment starts past the last tile's nominal block
+ * range has a segment no tile owns: the reference never codes it and its
+ * post-encode self-check rejects the frame (codec.c:4289-4304). */
+int tc_v8_orphans(const tcg_enc_frame* jf)
+{
+    if (jf->v8_sb_log2 == 0u) { return 0; }
+    const uint32_t sb = 1u << jf->v8_sb_log2, tr = jf->v8_tile_log2 == 0u ? 0u : 1u << jf->v8_tile_log2;
+    for (uint32_t p = 0; p < 3u; ++p) {
+        const uint32_t cols = jf->plane[p].cols, rows = jf->plane[p].rows, blocks = cols * rows;
+        const uint32_t S = (blocks + sb - 1u) / sb;
+        const uint32_t T = (tr == 0u || rows == 0u) ? 1u : (rows + tr - 1u) / tr;
+        const uint64_t fn = tr == 0u ? (uint64_t)blocks : (uint64_t)T * tr * cols;
+        if (fn / sb < S) { return 1; }
+    }
+    return 0;
 }
 
 void tc_fill_enc_stats(topos_frame_stats* st, const tcg_enc_result* r, uint32_t slices, uint8_t qp)
@@ -272,7 +319,8 @@ void tc_fill_enc_stats(topos_frame_stats* st, const tcg_enc_result* r, uint32_t 
     st->packet_size = r->packet_size;
     st->color_payload_bytes = r->color_payload;
     st->alpha_payload_bytes = r->alpha_payload;
-    st->color_header_bytes = TC_HDR_SIZE + TC_SH_SIZE * r->color_slices;
+    /* V8 (no slice headers): the frame header and the 8-byte extension */
+    st->color_header_bytes = r->v8 ? TC_HDR_SIZE + 8u : TC_HDR_SIZE + TC_SH_SIZE * r->color_slices;
     st->alpha_header_bytes = TC_SH_SIZE * r->alpha_slices;
     st->slice_count = (uint16_t)slices;
     st->qp_base = qp;
@@ -311,8 +359,25 @@ TC_EXPORT int32_t tc_frame_encode(const topos_frame_config* cfg, const topos_fra
     const size_t caps[1] = {out == NULL ? 0u : out_cap};
     rc = tcg_encode(&jf, 1u, outs, caps, &r);
     if (rc != TC_OK) { return rc; }
-    if (r.rc == TC_OK || r.rc == TC_ERR_BUFFER_TOO_SMALL) { tc_fill_enc_stats(stats, &r, slices, qp); }
-    return tc_enc_result_status(r.rc, r.packet_size, out_cap);
+    return tc_finish_encode(&jf, &r, stats, slices, qp, out_cap);
+}
+
+/* Status and statistics of one encoded frame. V8 fills the statistics only on
+ * success and reports a frame with an unowned segment after its packet was
+ * written, as the reference's self-check does (codec.c:4268-4317). */
+int32_t tc_finish_encode(const tcg_enc_frame* jf, tcg_enc_result* r, topos_frame_stats* stats, uint32_t slices,
+                         uint8_t qp, size_t out_cap)
+{
+    r->v8 = jf->v8_sb_log2 != 0u;
+    if (r->v8) {
+        if (r->rc == TC_OK && tc_v8_orphans(jf)) {
+            return tc_fail(TC_ERR_MALFORMED, "v8 self-check scan failed: a segment lies past the last tile");
+        }
+        if (r->rc == TC_OK) { tc_fill_enc_stats(stats, r, slices, qp); }
+        return tc_enc_result_status(r->rc, r->packet_size, out_cap);
+    }
+    if (r->rc == TC_OK || r->rc == TC_ERR_BUFFER_TOO_SMALL) { tc_fill_enc_stats(stats, r, slices, qp); }
+    return tc_enc_result_status(r->rc, r->packet_size, out_cap);
 }
 
 /* extension: many frames in one device launch sequence */
@@ -356,10 +421,9 @@ TC_EXPORT int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs, const t
     int32_t first = TC_OK;
     for (uint32_t k = 0; k < n && call == TC_OK; ++k) {
         const uint32_t i = idx[k];
-        if (stats != NULL && (res[k].rc == TC_OK || res[k].rc == TC_ERR_BUFFER_TOO_SMALL)) {
-            tc_fill_enc_stats(&stats[i], &res[k], nsl[i], qps[i]);
-        }
-        rcs[i] = tc_enc_result_status(res[k].rc, res[k].packet_size, c2[k]);
+        topos_frame_stats scratch;
+        memset(&scratch, 0, sizeof(scratch));
+        rcs[i] = tc_finish_encode(&jobs[k], &res[k], stats != NULL ? &stats[i] : &scratch, nsl[i], qps[i], c2[k]);
     }
     for (uint32_t i = 0; i < count; ++i) {
         if (call != TC_OK && rcs[i] == TC_OK) { rcs[i] = call; }

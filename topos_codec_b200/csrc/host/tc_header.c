@@ -218,6 +218,8 @@ void tc_hdr_pack(const tc_hdr* h, uint8_t o[TC_HDR_SIZE])
     be32(o + 49, tc_crc32(o, 49u));
 }
 
+int32_t tc_hdr_decode(const uint8_t* d, size_t n, tc_hdr* h);
+
 static int32_t hdr_decode(const uint8_t* d, size_t n, tc_hdr* h)
 {
     if (n < TC_HDR_SIZE) { return tc_fail(TC_ERR_TRUNCATED, "frame header needs 53 bytes, got %zu", n); }
@@ -322,6 +324,10 @@ int32_t tc_band_plan(const tc_hdr* h, uint32_t rows_per, uint32_t* total)
     return TC_OK;
 }
 
+int32_t tc_hdr_decode(const uint8_t* d, size_t n, tc_hdr* h) { return hdr_decode(d, n, h); }
+
+/* V8 (major 8) is not intercepted: the single-frame decode routes it to the V8
+ * decoder first, and the V7 scanner rejects it elsewhere (packet.c:19-26). */
 int32_t tc_probe_generation(const uint8_t* d, size_t n)
 {
     if (n >= TC_HDR_SIZE + 8u && memcmp(d, "TPIC", 4u) == 0 && d[6] == 7u &&
@@ -331,8 +337,8 @@ int32_t tc_probe_generation(const uint8_t* d, size_t n)
     if (n > 45u && memcmp(d, "TPIC", 4u) == 0 && d[6] == 7u && d[45] == 5u) {
         return tc_fail(TC_ERR_UNSUPPORTED_VERSION, "generation 7 (V7-A band decode) retired");
     }
-    if (n >= TC_HDR_SIZE && memcmp(d, "TPIC", 4u) == 0 && (d[6] == 8u || d[6] == 9u)) {
-        return tc_fail(TC_ERR_NOT_IMPLEMENTED, "V8/V9 packets are not implemented by this library");
+    if (n >= TC_HDR_SIZE && memcmp(d, "TPIC", 4u) == 0 && d[6] == 9u) {
+        return tc_fail(TC_ERR_NOT_IMPLEMENTED, "V9 packets are not implemented by this library");
     }
     return 0;
 }

@@ -58,6 +58,13 @@ typedef struct tc_view {
     uint32_t off[TC_MAX_SLICE_COUNT]; /* payload offset within the packet */
 } tc_view;
 
+int32_t tc_hdr_decode(const uint8_t* d, size_t n, tc_hdr* h);
+
+/* ---- V8 segmented rANS packets (tc_v8.c) ---- */
+/* single-frame decode or query (planes_out NULL) of a V8 packet, host or device memory */
+int32_t tc_v8_frame_decode(const uint8_t* data, size_t size, uint16_t* const planes_out[4], const size_t strides[4],
+                           topos_frame_output* o);
+
 /* ---- errors (tc_error.c) ---- */
 int32_t tc_fail(int32_t status, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 
@@ -117,5 +124,10 @@ int32_t tc_prepare_encode(const topos_frame_config* cfg, const topos_frame_input
                           uint32_t* slice_count, uint8_t* qp_base);
 void tc_fill_enc_stats(topos_frame_stats* st, const struct tcg_enc_result* r, uint32_t slices, uint8_t qp);
 int32_t tc_enc_result_status(int32_t rc, size_t need, size_t cap);
+/* public status (and statistics on success) of one encoded frame, V7-R2 or V8 */
+int32_t tc_finish_encode(const struct tcg_enc_frame* jf, struct tcg_enc_result* r, topos_frame_stats* stats,
+                         uint32_t slices, uint8_t qp, size_t out_cap);
+/* a V8 frame with a segment no tile owns (the reference's self-check rejects it) */
+int tc_v8_orphans(const struct tcg_enc_frame* jf);
 
 #endif /* TC_INTERNAL_H */

@@ -39,6 +39,10 @@ typedef struct tcg_enc_frame {
     uint32_t slices;        /* total slices (all planes) */
     tcg_enc_plane plane[4];
     uint8_t header[53];     /* frame header; packet size and header CRC are patched on the device */
+    /* V8 segmented rANS: 0 for a V7-R2 frame, else the segment size log2
+     * (3..5: 8/16/32 blocks per independent rANS chain) */
+    uint32_t v8_sb_log2;
+    uint32_t v8_tile_log2;  /* V8 tile height log2 in block rows (4..6), 0 = the whole plane */
 } tcg_enc_frame;
 
 typedef struct tcg_enc_result {
@@ -47,6 +51,7 @@ typedef struct tcg_enc_result {
     uint32_t color_payload, alpha_payload;
     uint32_t color_slices, alpha_slices;
     uint32_t alpha_max_err;
+    uint32_t v8;            /* host side: the frame is V8 */
 } tcg_enc_result;
 
 /* Encodes count frames in one device launch sequence. For each frame whose
@@ -156,6 +161,41 @@ int32_t tcg_walk_packets(const uint8_t* const* pkts, const size_t* sizes, uint32
  * the last walk on the current device to host_rec (TCG_WALK_REC bytes). */
 int32_t tcg_walk_packets_noalloc(const uint8_t* const* pkts, const size_t* sizes, uint32_t n);
 int32_t tcg_walk_record_noalloc(uint32_t i, uint8_t* host_rec);
+
+/* ------------------------------- V8 decode ------------------------------- */
+
+/* One V8 frame (segmented multi-chain rANS): the host has scanned the
+ * structure and checked the tile tables; the device checks the tile CRCs,
+ * decodes every segment whose tile matched, reconstructs all blocks (a segment
+ * that is not decoded, or fails, reconstructs from zero coefficients: the mid
+ * level) and writes the three colour planes. */
+typedef struct tcg_v8_seg {
+    uint32_t plane, blk0, nblk, tile;   /* blk0: first block within the plane */
+    uint32_t off, len;                  /* stream bytes from the packet start */
+    uint32_t qidx, pad;                 /* quantiser steps: q[qidx * 64 ..] */
+} tcg_v8_seg;
+
+typedef struct tcg_v8_tile {
+    uint32_t plane, seg0, nseg, table_off;
+    uint32_t stream_off, stream_bytes, crc, pad;
+} tcg_v8_tile;
+
+typedef struct tcg_v8_job {
+    const uint8_t* packet;              /* host or device memory */
+    size_t size;
+    uint32_t bit_depth, sb_log2;
+    uint32_t vis_w[3], vis_h[3], cols[3], rows[3];
+    uint16_t* dst[3];                   /* host or device memory */
+    size_t dst_stride[3];               /* uint16 elements */
+    uint32_t nseg, ntile, nq;
+    const tcg_v8_seg* seg;              /* plane-major, segment order */
+    const tcg_v8_tile* tile;
+    const uint32_t* q;                  /* nq x 64 steps, natural order */
+    uint8_t* seg_fail;                  /* out, per segment: decode failed */
+    uint8_t* tile_ok;                   /* out, per tile: CRC matched */
+} tcg_v8_job;
+
+int32_t tcg_decode_v8(const tcg_v8_job* job);
 
 /* provided by the host library: thread-local error detail */
 void tcg_host_set_error(int32_t status, const char* text);
