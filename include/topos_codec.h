@@ -292,21 +292,28 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
 int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                       topos_frame_output* infos);
 
-/* Continuous-batching request server. Encode and decode requests of single
- * frames (any mix of sizes and configurations; buffers owned by the caller,
+/* Continuous-batching request server (no counterpart in the reference).
+ * Encode and decode requests of single frames (any mix of sizes,
+ * configurations and generations, V7-R2 or V8; buffers owned by the caller,
  * host or device memory, valid until the request completes) enter two
- * queues; a worker per direction codes everything that has arrived in one
- * batched call, while requests arriving meanwhile wait for its next batch.
- * The two workers run concurrently on their own streams. A batch admits
- * requests while their estimated device bytes fit max_bytes_in_flight (0 =
- * no limit) and the device's free memory, up to max_batch_frames (1..64).
+ * queues. Each direction has a pool of workers, each on its own CUDA stream:
+ * an idle worker codes the requests that have arrived (an even share when
+ * other workers are idle too, at most max_batch_frames, 1..64) in one batched
+ * call, and requests arriving while batches run are taken by the next idle
+ * worker at once, so their work overlaps the batches already on the GPU.
+ * A batch admits requests while the estimated device bytes of all batches in
+ * flight fit max_bytes_in_flight (0 = no limit) and the device's free memory.
  * Every result equals the single-frame call's. tcg_server_wait blocks until
  * the ticket's request is done and returns its status (as tc_frame_encode /
  * tc_frame_decode would), its stats or frame information, and its latency
  * from submission to completion. Decode requests are validated on
- * submission: an invalid packet returns its error there. */
+ * submission: an invalid packet returns its error there.
+ * tcg_server_create uses 4 workers per direction; tcg_server_create_ex takes
+ * the count (1..16). */
 typedef struct tcg_server tcg_server;
 int32_t tcg_server_create(uint64_t max_bytes_in_flight, uint32_t max_batch_frames, tcg_server** out);
+int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t max_batch_frames, uint32_t workers,
+                             tcg_server** out);
 void tcg_server_destroy(tcg_server* server);
 int32_t tcg_server_submit_encode(tcg_server* server, const topos_frame_config* cfg, const topos_frame_input* input,
                                  uint8_t* out, size_t out_cap, uint64_t* ticket);

@@ -57,3 +57,88 @@ def test_v8_batch_beside_v7_equals_single_calls(product):
     assert rc == 0 and rcs == [0] * len(specs)
     for cfg, planes, p in zip(cfgs, frames, pk):
         assert product.encode(cfg, planes) == p
+
+
+def _same_decode(a, b):
+    return (a.status == b.status and a.slice_status == b.slice_status
+            and a.info.concealed_slices == b.info.concealed_slices
+            and all(np.array_equal(x, y) for x, y in zip(a.planes, b.planes)))
+
+
+def test_v8_decode_random_vs_reference(product, reference):
+    """Reference V8 packets of random configurations decode to the same
+    planes, statuses and frame information on the GPU."""
+    rng = random.Random(4242)
+    n = 0
+    for i in range(60):
+        w, h, kw, ck, sb, tl = _random_v8_config(rng)
+        cfg = _v8(B.make_config(w, h, **ck), sb, tl)
+        rc, pkt, _ = reference.encode_status(cfg, synth.make_frame_np(w, h, seed=500 + i, **kw))
+        if rc != 0:
+            continue
+        n += 1
+        a, b = reference.decode_status(pkt), product.decode_status(pkt)
+        assert _same_decode(a, b), (w, h, ck, sb, tl)
+        qa, qb = reference.query(pkt), product.query(pkt)
+        assert qa[0] == qb[0] and bytes(qa[1]) == bytes(qb[1])
+    assert n >= 40
+
+
+def test_v8_decode_damaged_vs_reference(product, reference):
+    """Segment streams changed with the tile CRC re-sealed (that segment alone
+    is concealed), with the CRC stale (the tile is concealed), and bytes
+    changed anywhere (structural rejects, bad tables, concealment)."""
+    from v8_packets import layout, plane_blocks, reseal_tile
+    rng = random.Random(77)
+    for (w, h, sb, tl) in [(320, 180, 3, 4), (256, 144, 5, 0), (1920, 1080, 0, 0)]:
+        cfg = _v8(B.make_config(w, h, qp=6, qmatrix_id=4), sb, tl)
+        pkt = reference.encode(cfg, synth.make_frame_np(w, h, seed=12))
+        lay = layout(pkt, plane_blocks(w, h, 0))
+        for trial in range(30):
+            p = bytearray(pkt)
+            pl = lay[rng.randrange(3)]
+            kind = trial % 3
+            if kind < 2:
+                t = rng.randrange(len(pl["tiles"]))
+                sf, sn = pl["tiles"][t]
+                if sn == sf:
+                    continue
+                for _ in range(rng.randint(1, 2)):
+                    so, ln = pl["segs"][rng.randrange(sf, sn)]
+                    p[pl["streams"] + so + rng.randrange(ln)] ^= 1 + rng.randrange(255)
+                if kind == 0:
+                    reseal_tile(p, pl, t)
+            else:
+                p[rng.randrange(53, len(p))] ^= 1 + rng.randrange(255)
+            p = bytes(p)
+            assert _same_decode(reference.decode_status(p), product.decode_status(p)), (w, h, trial)
+
+
+def test_v8_decode_full_size_and_device_resident(product, reference):
+    """3840x2160 HQ-like V8 frame: host packet and device-resident packet and
+    planes decode like the reference."""
+    import torch
+    w, h = 3840, 2160
+    cfg = _v8(B.make_config(w, h, qp=4, qmatrix_id=0), 0, 0)
+    pkt = reference.encode(cfg, synth.make_frame_np(w, h, seed=3, frame=1))
+    a, b = reference.decode_status(pkt), product.decode_status(pkt)
+    assert _same_decode(a, b)
+    dpkt = torch.from_numpy(np.frombuffer(pkt, dtype=np.uint8).copy()).cuda()
+    planes = [torch.zeros(s, dtype=torch.int16, device="cuda") for s in B.plane_shapes(cfg)]
+    import ctypes
+    ptrs = (ctypes.c_void_p * 4)(*[t.data_ptr() for t in planes], None)
+    info = B.FrameOutput()
+    rc = product._lib.tc_frame_decode(ctypes.c_void_p(dpkt.data_ptr()), len(pkt), ptrs, None, ctypes.byref(info))
+    assert rc == 0 and info.concealed_slices == 0
+    for x, y in zip(a.planes, planes):
+        assert np.array_equal(x, y.cpu().numpy().view(np.uint16))
+
+
+def test_v8_in_batch_decode_is_rejected_like_reference(product, reference):
+    """tc_frame_decode_batch takes V7 packets only; a V8 packet fails the batch
+    with the reference's status (its V7 scanner rejects major 8)."""
+    cfg = _v8(B.make_config(128, 64, qp=8), 0, 0)
+    pkt = reference.encode(cfg, synth.make_frame_np(128, 64, seed=1))
+    ra, _ = reference.decode_batch([pkt])
+    rb, _ = product.decode_batch([pkt])
+    assert ra == rb == B.TC_ERR_UNSUPPORTED_VERSION

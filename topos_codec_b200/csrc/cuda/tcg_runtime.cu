@@ -499,3 +499,11 @@ extern "C" int32_t tcg_is_device_ptr(const void* p)
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
+
+extern "C" int32_t tcg_read_device(void* dst, const void* src, size_t n)
+{
+    if (n == 0u) { return 0; }
+    if (!tcg::ensure_init()) { return TCG_ERR_NOT_IMPLEMENTED; }
+    TCG_CHECK(cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost));
+    return 0;
+}

@@ -577,6 +577,19 @@ static int32_t finish_frame(const tc_hdr* h, topos_frame_output* o)
     return TC_OK;
 }
 
+/* version_major of a packet in host or device memory (-1: no TPIC header) */
+int tc_packet_major(const uint8_t* data, size_t size)
+{
+    uint8_t head[8] = {0};
+    if (data == NULL || size < TC_HDR_SIZE) { return -1; }
+    if (tcg_is_device_ptr(data)) {
+        if (tcg_read_device(head, data, 8u) != TC_OK) { return -1; }
+    } else {
+        memcpy(head, data, 8u);
+    }
+    return memcmp(head, "TPIC", 4u) == 0 ? (int)head[6] : -1;
+}
+
 /* reference: native/src/codec/codec.c:9005-9098 */
 TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* const planes_out[TC_FRAME_MAX_PLANES],
                                   const size_t strides[TC_FRAME_MAX_PLANES], topos_frame_output* o)
@@ -586,6 +599,8 @@ TC_EXPORT int32_t tc_frame_decode(const uint8_t* data, size_t size, uint16_t* co
     o->struct_size = (uint32_t)sizeof(topos_frame_output);
     o->abi_version = TOPOS_CODEC_ABI_VERSION;
     if (data == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "data == NULL"); }
+    /* V8 packets take their own decoder (reference codec.c:9039-9049) */
+    if (tc_packet_major(data, size) == 8) { return tc_v8_frame_decode(data, size, planes_out, strides, o); }
     tc_view* v = (tc_view*)malloc(sizeof(tc_view));
     if (v == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "decode view"); }
     const topos_batch_packet one = {data, size};

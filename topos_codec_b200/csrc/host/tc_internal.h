@@ -60,6 +60,9 @@ typedef struct tc_view {
 
 int32_t tc_hdr_decode(const uint8_t* d, size_t n, tc_hdr* h);
 
+/* version_major of a packet in host or device memory (-1: no TPIC header) */
+int tc_packet_major(const uint8_t* data, size_t size);
+
 /* ---- V8 segmented rANS packets (tc_v8.c) ---- */
 /* single-frame decode or query (planes_out NULL) of a V8 packet, host or device memory */
 int32_t tc_v8_frame_decode(const uint8_t* data, size_t size, uint16_t* const planes_out[4], const size_t strides[4],

@@ -2,14 +2,19 @@
 // calls (extension; the reference has no server).
 //
 // Requests (encode or decode of one frame, caller-owned buffers in host or
-// device memory) enter two queues. One worker per direction takes every
-// request that has arrived, up to a frame count and a byte budget, and codes
-// them in one batched call; requests that arrive meanwhile wait for the next
-// batch. The two workers run at the same time on their own call contexts
-// (their own CUDA streams), so encode and decode batches overlap on the GPU.
-// Admission: a batch only takes requests while the estimated device bytes of
-// the batch fit both the server's budget and the device's free memory.
-// Each request's latency is measured from submission to completion.
+// device memory) enter two queues. Each direction has a pool of workers, each
+// coding through its own call context (its own CUDA stream): an idle worker
+// takes the requests that have arrived - an even share of them when other
+// workers are idle too, at most max_batch_frames - and codes them in one
+// batched call. Requests that arrive while batches run are picked up by the
+// next idle worker at once, so their work overlaps the batches already on the
+// GPU instead of waiting for them. Admission: a batch takes requests while
+// the estimated device bytes of everything in flight fit the server's budget
+// and the device's free memory (the first request of a batch always goes, so
+// one large request cannot stall the queue). V8 decodes run through the
+// single-frame V8 decoder (the batched decode takes V7 packets only, as the
+// reference's does). Each request's latency is measured from submission to
+// completion.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -43,6 +48,7 @@ struct Request {
     uint16_t* planes[TC_FRAME_MAX_PLANES] = {nullptr, nullptr, nullptr, nullptr};
     size_t strides[TC_FRAME_MAX_PLANES] = {0, 0, 0, 0};
     uint64_t bytes = 0;  // estimated device footprint
+    bool v8 = false;     // decode of a V8 packet
     Clock::time_point t_submit;
 };
 
@@ -62,9 +68,11 @@ struct tcg_server {
     std::unordered_map<uint64_t, Result> done;
     uint64_t next_ticket = 1;
     uint64_t budget = 0;
+    uint64_t inflight = 0;       // estimated device bytes of the batches running
     uint32_t max_frames = 64;
+    uint32_t idle[2] = {0, 0};   // idle workers per direction (0 decode, 1 encode)
     bool stop = false;
-    std::thread w_enc, w_dec;
+    std::vector<std::thread> workers;
     int device = 0;
 };
 
@@ -125,10 +133,34 @@ void run_batch(tcg_server* s, std::vector<Request>& batch, bool encode)
                 strides[(size_t)i * TC_FRAME_MAX_PLANES + p] = batch[i].strides[p];
             }
         }
-        const int32_t rc = tc_frame_decode_batch(pk.data(), n, planes.data(), strides.data(), infos.data());
+        // V7 packets in one batched call, V8 packets one by one
+        std::vector<uint32_t> v7;
         for (uint32_t i = 0; i < n; ++i) {
-            res[i].info = infos[i];
-            res[i].status = rc < 0 ? rc : (infos[i].concealed_slices != 0 ? TC_WARN_CONCEALED : TC_OK);
+            if (!batch[i].v8) {
+                v7.push_back(i);
+                continue;
+            }
+            res[i].status = tc_frame_decode(pk[i].data, pk[i].size, &planes[(size_t)i * TC_FRAME_MAX_PLANES],
+                                            &strides[(size_t)i * TC_FRAME_MAX_PLANES], &res[i].info);
+        }
+        if (!v7.empty()) {
+            const uint32_t m = (uint32_t)v7.size();
+            std::vector<topos_batch_packet> pk7(m);
+            std::vector<uint16_t*> pl7((size_t)m * TC_FRAME_MAX_PLANES);
+            std::vector<size_t> st7((size_t)m * TC_FRAME_MAX_PLANES);
+            for (uint32_t k = 0; k < m; ++k) {
+                pk7[k] = pk[v7[k]];
+                for (uint32_t p = 0; p < TC_FRAME_MAX_PLANES; ++p) {
+                    pl7[(size_t)k * TC_FRAME_MAX_PLANES + p] = planes[(size_t)v7[k] * TC_FRAME_MAX_PLANES + p];
+                    st7[(size_t)k * TC_FRAME_MAX_PLANES + p] = strides[(size_t)v7[k] * TC_FRAME_MAX_PLANES + p];
+                }
+            }
+            const int32_t rc = tc_frame_decode_batch(pk7.data(), m, pl7.data(), st7.data(), infos.data());
+            for (uint32_t k = 0; k < m; ++k) {
+                Result& r = res[v7[k]];
+                r.info = infos[k];
+                r.status = rc < 0 ? rc : (infos[k].concealed_slices != 0 ? TC_WARN_CONCEALED : TC_OK);
+            }
         }
     }
     const Clock::time_point t_end = Clock::now();
@@ -144,25 +176,36 @@ void worker(tcg_server* s, bool encode)
 {
     cudaSetDevice(s->device);
     std::deque<Request>& q = encode ? s->q_enc : s->q_dec;
+    uint32_t& idle = s->idle[encode ? 1 : 0];
     for (;;) {
         std::vector<Request> batch;
+        uint64_t used = 0;
         {
             std::unique_lock<std::mutex> lk(s->mu);
+            idle++;
             s->cv_work.wait(lk, [&] { return s->stop || !q.empty(); });
+            idle--;
             if (s->stop && q.empty()) { return; }
+            // an even share of what has arrived when other workers are idle too
+            const size_t share = (q.size() + idle) / (idle + 1u);
+            const size_t take = std::min<size_t>(std::max<size_t>(share, 1u), s->max_frames);
             const uint64_t free_b = device_free();
-            const uint64_t cap = free_b == 0 ? s->budget : std::min<uint64_t>(s->budget, free_b - free_b / 8);
-            uint64_t used = 0;
-            while (!q.empty() && batch.size() < s->max_frames) {
+            const uint64_t room = s->budget > s->inflight ? s->budget - s->inflight : 0u;
+            const uint64_t cap = free_b == 0 ? room : std::min<uint64_t>(room, free_b - free_b / 8);
+            while (!q.empty() && batch.size() < take) {
                 const uint64_t b = q.front().bytes;
-                // the first request always goes, so an oversized one cannot stall the queue
                 if (!batch.empty() && used + b > cap) { break; }
                 used += b;
                 batch.push_back(q.front());
                 q.pop_front();
             }
+            s->inflight += used;
+            if (!q.empty()) { s->cv_work.notify_all(); }  // more for the next idle worker
         }
         run_batch(s, batch, encode);
+        std::lock_guard<std::mutex> g(s->mu);
+        s->inflight -= used;
+        if (!q.empty()) { s->cv_work.notify_all(); }
     }
 }
 
@@ -184,11 +227,20 @@ extern "C" {
 
 TC_EXPORT int32_t tcg_server_create(uint64_t max_bytes_in_flight, uint32_t max_batch_frames, tcg_server** out)
 {
+    return tcg_server_create_ex(max_bytes_in_flight, max_batch_frames, 4u, out);
+}
+
+TC_EXPORT int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t max_batch_frames, uint32_t workers,
+                                       tcg_server** out)
+{
     if (out == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "tcg_server_create: out is NULL"); }
     *out = NULL;
     if (max_batch_frames == 0u || max_batch_frames > TC_BATCH_MAX_FRAMES) {
         return tc_fail(TC_ERR_INVALID_ARGUMENT, "tcg_server_create: max_batch_frames %u outside 1..%u",
                        max_batch_frames, (unsigned)TC_BATCH_MAX_FRAMES);
+    }
+    if (workers == 0u || workers > 16u) {
+        return tc_fail(TC_ERR_INVALID_ARGUMENT, "tcg_server_create: workers %u outside 1..16", workers);
     }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
@@ -200,8 +252,10 @@ TC_EXPORT int32_t tcg_server_create(uint64_t max_bytes_in_flight, uint32_t max_b
     s->budget = max_bytes_in_flight == 0u ? UINT64_MAX : max_bytes_in_flight;
     s->max_frames = max_batch_frames;
     s->device = dev;
-    s->w_enc = std::thread(worker, s, true);
-    s->w_dec = std::thread(worker, s, false);
+    for (uint32_t i = 0; i < workers; ++i) {
+        s->workers.emplace_back(worker, s, true);
+        s->workers.emplace_back(worker, s, false);
+    }
     *out = s;
     return TC_OK;
 }
@@ -214,8 +268,7 @@ TC_EXPORT void tcg_server_destroy(tcg_server* s)
         s->stop = true;
         s->cv_work.notify_all();
     }
-    s->w_enc.join();
-    s->w_dec.join();
+    for (std::thread& t : s->workers) { t.join(); }
     delete s;
 }
 
@@ -254,6 +307,7 @@ TC_EXPORT int32_t tcg_server_submit_decode(tcg_server* s, const uint8_t* packet,
         r.strides[p] = strides != NULL ? strides[p] : 0u;
     }
     r.bytes = frame_bytes(info.visible_width, info.visible_height, false);
+    r.v8 = tc_packet_major(packet, size) == 8;
     *ticket = submit(s, std::move(r), false);
     return TC_OK;
 }

@@ -139,6 +139,8 @@ void tcg_prof_reset(void);
 int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uint64_t* launches);
 /* nonzero when p is device (or managed) memory */
 int32_t tcg_is_device_ptr(const void* p);
+/* n bytes of device memory at src into host memory at dst (synchronous) */
+int32_t tcg_read_device(void* dst, const void* src, size_t n);
 /* free and total device memory of the library's device (0 and 0 without one) */
 void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes);
 /* gives back the device buffers idle call contexts keep from earlier calls */
