@@ -111,6 +111,78 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ reference CPU path
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def ref_simd_backend(lib):
+    """The reference library's SIMD dispatch choice (dispatch.c:213)."""
+    fn = lib._lib.tc_dev_simd_backend
+    fn.restype = ctypes.c_char_p
+    v = fn()
+    return v.decode() if v else None
+
+
+def cpu_mode_main(mode, seconds, nframes):
+    """One as-is mode of the reference CPU path, run in its own process so its
+    slice pool takes the thread count set for it (TOPOS_SLICE_THREADS is read
+    once per process): prints one JSON line.
+      slice  - tc_frame_encode then tc_frame_decode per frame, slice pool of
+               min(cores, 16) threads (the reference's per-frame path)
+      batch  - tc_frame_decode_batch over the frame set, same pool"""
+    from topos_codec_b200 import binding as B, synth
+    ref = B.ToposCodec(REF_LIB)
+    cfg = B.make_config(W, H, **CFG)
+    frames = [synth.make_frame_np(W, H, seed=0, frame=i) for i in range(nframes)]
+    pkts = [ref.encode(cfg, f) for f in frames[:1]]  # warm-up (pool start, tables)
+    ref.decode(pkts[0])
+    out = {"mode": mode, "threads": int(os.environ.get("TOPOS_SLICE_THREADS", "0")), "frames": nframes,
+           "simd_backend": ref_simd_backend(ref), "cpu_model": cpu_model()}
+    if mode == "slice":
+        t0 = time.perf_counter()
+        n, pkts = 0, []
+        while time.perf_counter() - t0 < seconds or n < 2:
+            pkts.append(ref.encode(cfg, frames[n % nframes]))
+            n += 1
+        enc_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        m = 0
+        while time.perf_counter() - t0 < seconds or m < 2:
+            ref.decode(pkts[m % len(pkts)])
+            m += 1
+        dec_s = time.perf_counter() - t0
+        out.update(encode_fps=n / enc_s, decode_fps=m / dec_s, encoded=n, decoded=m)
+    else:
+        pkts = [ref.encode(cfg, f) for f in frames]
+        t0 = time.perf_counter()
+        calls = 0
+        while time.perf_counter() - t0 < seconds or calls < 1:
+            rc, _ = ref.decode_batch(pkts)
+            assert rc == 0
+            calls += 1
+        out.update(decode_fps=calls * len(pkts) / (time.perf_counter() - t0), batches=calls)
+    print(json.dumps(out))
+
+
+def cpu_modes(seconds=6.0, nframes=8):
+    """The reference's as-is CPU modes, each in a subprocess of this script."""
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, TOPOS_SLICE_THREADS=str(min(cores, 16)))
+    res = {}
+    for mode in ("slice", "batch"):
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--cpu-mode", mode, "--cpu-seconds", str(seconds),
+                            "--frames", str(nframes)], capture_output=True, text=True, env=env)
+        lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+        res[mode] = json.loads(lines[-1]) if r.returncode == 0 and lines else {"error": (r.stderr or r.stdout)[-300:]}
+    return res
+
+
 def reference_rate(frames_np, cfg, budget_s=10.0, threads=None):
     """Round-trip frames/s of the reference CPU library (built from its own
     sources into oracle/_ref) on the host cores: frame-parallel, one frame per
@@ -220,7 +292,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=FRAMES)
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="seconds per offered load (config: 60)")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the mixed-batch and GBR 4:4:4 + alpha workloads")
     ap.add_argument("--case", default=None, help="WxH: run one small batched round trip for a profiler capture "
@@ -228,7 +300,12 @@ def main():
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--case-qp", type=int, default=4)
     ap.add_argument("--case-gbr", action="store_true", help="12-bit GBR 4:4:4 + 16-bit alpha at qp 2")
+    ap.add_argument("--cpu-mode", default=None, choices=["slice", "batch"], help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-seconds", type=float, default=6.0, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.cpu_mode:
+        cpu_mode_main(args.cpu_mode, args.cpu_seconds, args.frames if args.frames != FRAMES else 8)
+        return
     if args.case:
         kernel_case(args)
         return
@@ -252,7 +329,7 @@ def main():
         if not os.path.exists(REF_LIB):
             print(json.dumps({"impl": "reference", "unavailable": "reference library not built (oracle/_ref)"}))
             return
-        frames = [synth.make_frame_np(W, H, seed=0, frame=i) for i in range(4)]
+        frames = [synth.make_frame_np(W, H, seed=0, frame=i) for i in range(16)]
         for _ in range(args.warmup):
             reference_rate(frames[:1], cfg, budget_s=0.0, threads=1)
         rates = []
@@ -266,7 +343,9 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/int32",
             "data": "synthetic", "config": config_desc,
             "cpu_baseline": {"value": value, "unit": "frames/s", "cores": cores, "kind": "reference",
-                             "sample": f"each step: frame-parallel encode+decode on {cores} threads for ~10 s"},
+                             "sample": f"each step: frame-parallel encode+decode of 16 distinct frames on {cores} "
+                                       "threads (slice pool 1 thread per call) for ~10 s",
+                             "cpu_model": cpu_model()},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -483,8 +562,13 @@ def main():
     if rank == 0 and world == 1 and os.path.exists(REF_LIB):
         f_np = [[p.cpu().numpy() for p in frames_d[i]] for i in range(min(nf, 8))]
         r, cores, n, el = reference_rate(f_np, cfg, budget_s=12.0)
+        modes = cpu_modes()
         cpu = {"value": r, "unit": "frames/s", "cores": cores, "kind": "reference",
-               "sample": f"{n} frames encoded+decoded frame-parallel in {el:.1f} s"}
+               "sample": f"{n} frames encoded+decoded frame-parallel (one slice thread per call) in {el:.1f} s",
+               "cpu_model": cpu_model(), "simd_backend": modes.get("slice", {}).get("simd_backend"),
+               "modes": {"frame_parallel_round_trip_fps": r,
+                         "per_frame_slice_parallel": modes.get("slice"),
+                         "decode_batch": modes.get("batch")}}
 
     # ---------------- further workloads: mixed batch, GBR 4:4:4 + alpha ----------------
     extra = {}
@@ -519,6 +603,22 @@ def main():
             r["damaged_decode_vs_reference"]["corruption"] = "1 % of the slices of 8 reference packets, one payload byte each"
         extra["gbr4444_alpha"] = r
         del gframes
+        # the bench batch coded as V8 (segmented rANS: 16-block segments, 32-row tiles; no deblocking or
+        # refined qp table in V8): batched encode and batched decode beside the per-frame calls, and the
+        # packets of two frames against the reference library's
+        v8cfg = B.make_config(W, H, qp=4, qmatrix_id=0)
+        v8cfg.reserved[0] = 9
+        r = WL.batched_vs_plain(gpu, [v8cfg] * nf, frames_d, v8=True)
+        v8pk = r.pop("packets")
+        r["workload"] = f"the {nf} 3840x2160 10-bit 4:2:2 frames as V8 packets (qp 4, flat matrix), device-resident"
+        r["encode_fps"] = nf / (r["batched_encode_ms"] / 1000.0)
+        r["decode_fps"] = nf / (r["batched_decode_ms"] / 1000.0)
+        if rank == 0 and os.path.exists(REF_LIB):
+            ref = B.ToposCodec(REF_LIB)
+            r["reference_packets_equal_2_frames"] = all(
+                ref.encode(v8cfg, [p.cpu().numpy() for p in frames_d[i]]) == v8pk[i] for i in (0, nf - 1))
+        extra["v8_batch"] = r
+        del v8pk
         # size-targeted encode: 8 frames of the bench workload from host memory, target = the
         # first frame's packet at qp 24, qp searched over 0..63 (strict search, hints on)
         sframes = [[p.cpu().numpy() for p in frames_d[i]] for i in range(min(nf, 8))]
@@ -541,26 +641,43 @@ def main():
     served = None
     if world == 1 and not args.no_serve:
         from topos_codec_b200 import serving
-        sat = serving.saturation_rps(gpu)
+        floors = [serving.single_frame_floor(gpu, 1920, 1080, "422", g) for g in ("v7", "v8")]
+        kinds = serving._kinds(gpu, torch, dev, 0, "v7")
+        sat = serving.saturation_rps(gpu, kinds=kinds)
         # a short discarded trace first: the decode-tiling tuner times the tilings
         # on the first batch of each batch-size class
-        serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=3.0, seed=7)
+        serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=3.0, seed=7, kinds=kinds)
         loads = {}
         for ld in (0.25, 0.5, 0.75, 1.0):
-            loads[ld] = serving.run_trace(gpu, rate_rps=ld * sat, duration_s=args.serve_seconds, seed=int(ld * 100))
+            loads[ld] = serving.run_trace(gpu, rate_rps=ld * sat, duration_s=args.serve_seconds, seed=int(ld * 100),
+                                          kinds=kinds)
         served = dict(loads[0.5])
-        psat = serving.plain_saturation_rps(gpu)
+        psat = serving.plain_saturation_rps(gpu, kinds=kinds)
+        plain_s = min(30.0, args.serve_seconds)
         plain = {"saturation_rps": psat,
-                 "at_half_batched_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * sat,
-                                                                       duration_s=args.serve_seconds),
-                 "at_half_plain_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * psat,
-                                                                     duration_s=args.serve_seconds)}
+                 "at_quarter_batched_saturation": serving.run_trace_plain(gpu, rate_rps=0.25 * sat,
+                                                                          duration_s=plain_s, kinds=kinds),
+                 "at_half_plain_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * psat, duration_s=plain_s,
+                                                                     kinds=kinds)}
+        del kinds
+        # the same stream coded as V8 (segmented rANS): many short chains per frame
+        k8 = serving._kinds(gpu, torch, dev, 0, "v8")
+        sat8 = serving.saturation_rps(gpu, generation="v8", kinds=k8)
+        serving.run_trace(gpu, rate_rps=0.5 * sat8, duration_s=3.0, seed=7, generation="v8", kinds=k8)
+        v8_half = serving.run_trace(gpu, rate_rps=0.5 * sat8, duration_s=args.serve_seconds, seed=50,
+                                    generation="v8", kinds=k8)
+        del k8
+        keys = ("offered_rps", "throughput_rps", "p50_ms", "p99_ms", "p999_ms", "errors", "by_resolution")
         served.update({"load": 0.5, "saturation_rps": sat,
                        "mix": "50/50 encode/decode; 1080p 40 %, 2160p 40 %, 720p 20 %; 10-bit 4:2:2 tiers 422/HQ",
-                       "latency": "server-side, submission to completion",
-                       "loads": {str(k): {x: v[x] for x in ("offered_rps", "throughput_rps", "p50_ms", "p99_ms",
-                                                            "p999_ms", "errors")} for k, v in loads.items()},
-                       "plain_per_request": plain})
+                       "latency": "client side, from each request's scheduled (open-loop Poisson) arrival to its "
+                                  "completion; server_side: submission to completion",
+                       "seconds_per_load": args.serve_seconds,
+                       "loads": {str(k): {x: v[x] for x in keys} for k, v in loads.items()},
+                       "plain_per_request": plain,
+                       "single_frame_floor_1080p": floors,
+                       "v8_at_half_saturation": dict({x: v8_half[x] for x in keys}, saturation_rps=sat8,
+                                                     by_direction=v8_half["by_direction"])})
 
     if rank == 0:
         line = {

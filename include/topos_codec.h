@@ -292,6 +292,16 @@ int32_t tcg_frame_encode_batch(const topos_frame_config* cfgs,
 int32_t tcg_frame_query_batch_noalloc(const topos_batch_packet* packets, uint32_t count,
                                       topos_frame_output* infos);
 
+/* Batched V8 decode. No counterpart in the reference, whose
+ * tc_frame_decode_batch takes V7 packets only: count V8 packets (host or
+ * device memory) decoded in one device launch sequence, each frame with the
+ * result tc_frame_decode gives it (planes, per-tile slice_status,
+ * concealed_slices). Every packet is scanned and checked before any decode;
+ * a failing packet fails the call with its status. planes_out (count x 4) NULL
+ * = query only; strides (count x 4) NULL = tight rows. */
+int32_t tcg_frame_decode_v8_batch(const topos_batch_packet* packets, uint32_t count, uint16_t* const* planes_out,
+                                  const size_t* strides, topos_frame_output* infos);
+
 /* Continuous-batching request server (no counterpart in the reference).
  * Encode and decode requests of single frames (any mix of sizes,
  * configurations and generations, V7-R2 or V8; buffers owned by the caller,

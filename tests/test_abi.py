@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN, ROOT, reference_path
-from topos_codec_b200 import binding as B
+from topos_codec_b200 import binding as B, synth
 
 HEADER = os.path.join(ROOT, "include", "topos_codec.h")
 HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include"))) if f.endswith(".h")]
@@ -275,7 +275,7 @@ def test_decode_request_query_matches_reference(product, reference):
     """tc_frame_decode_request and tc_decoder_prepare_request in query mode
     (no output planes): status and frame information equal the reference
     library's for every mode, scale, flag and invalid request on the fixture
-    packets (4:2:2, 4:4:4 + alpha, 1x1)."""
+    packets (4:2:2, 4:4:4 + alpha, 1x1) and a V8 packet."""
     names = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
     for lib in (product._lib, reference._lib):
         lib.tc_frame_decode_request.restype = ctypes.c_int32
@@ -286,9 +286,12 @@ def test_decode_request_query_matches_reference(product, reference):
         d = ctypes.c_void_p()
         assert lib.tc_decoder_create(None, ctypes.byref(d)) == 0
         decs.append(d)
+    pkts = [(name, bytes(np.load(os.path.join(GOLDEN, name + ".npz"))["packet"])) for name in names]
+    v8 = B.make_config(96, 64, qp=9, qmatrix_id=4)
+    v8.reserved[0], v8.reserved[3], v8.reserved[4] = 9, 4, 5
+    pkts.append(("v8", reference.encode(v8, synth.make_frame_np(96, 64, seed=5))))
     try:
-        for name in names:
-            pkt = bytes(np.load(os.path.join(GOLDEN, name + ".npz"))["packet"])
+        for name, pkt in pkts:
             buf = np.frombuffer(pkt, np.uint8)
             for req, label in _request_cases():
                 got = []

@@ -142,3 +142,82 @@ def test_v8_in_batch_decode_is_rejected_like_reference(product, reference):
     ra, _ = reference.decode_batch([pkt])
     rb, _ = product.decode_batch([pkt])
     assert ra == rb == B.TC_ERR_UNSUPPORTED_VERSION
+
+
+def test_v8_batch_decode_equals_single_calls(product, reference):
+    """tcg_frame_decode_v8_batch: frames of several sizes and segment / tile
+    layouts, one of them damaged, decode in one launch sequence exactly as
+    tc_frame_decode (and the reference) decodes each alone; a V7 packet in the
+    batch fails the call."""
+    import ctypes
+    from v8_packets import layout, plane_blocks
+    specs = [(320, 180, 3, 4), (640, 360, 4, 5), (257, 131, 5, 0), (1920, 1080, 0, 0)]
+    pkts = []
+    for i, (w, h, sb, tl) in enumerate(specs):
+        cfg = _v8(B.make_config(w, h, qp=5 + i, qmatrix_id=4), sb, tl)
+        rc, pkt, _ = reference.encode_status(cfg, synth.make_frame_np(w, h, seed=900 + i))
+        assert rc == 0
+        pkts.append(pkt)
+    bad = bytearray(pkts[1])
+    pl = layout(pkts[1], plane_blocks(640, 360, 0))[0]
+    so, ln = pl["segs"][3]
+    bad[pl["streams"] + so + ln // 2] ^= 0x5A
+    pkts[1] = bytes(bad)
+    want = [reference.decode_status(p) for p in pkts]
+    fn = product._lib.tcg_frame_decode_v8_batch
+    fn.restype = ctypes.c_int32
+    n = len(pkts)
+    bufs = [np.frombuffer(p, dtype=np.uint8) for p in pkts]
+    arr = (B.BatchPacket * n)()
+    for i, b in enumerate(bufs):
+        arr[i].data, arr[i].size = b.ctypes.data, b.size
+    planes = [[np.zeros(x.shape, dtype=np.uint16) for x in wd.planes] for wd in want]
+    ptrs = (ctypes.c_void_p * (4 * n))()
+    for i in range(n):
+        for p, a in enumerate(planes[i]):
+            ptrs[4 * i + p] = a.ctypes.data
+    infos = (B.FrameOutput * n)()
+    assert fn(arr, n, ptrs, None, infos) == 0
+    for i in range(n):
+        assert infos[i].concealed_slices == want[i].info.concealed_slices
+        assert list(infos[i].slice_status[:infos[i].slice_count]) == want[i].slice_status
+        for a, b in zip(planes[i], want[i].planes):
+            assert np.array_equal(a, b)
+    assert want[1].info.concealed_slices > 0
+    v7 = product.encode(B.make_config(64, 48, qp=8), synth.make_frame_np(64, 48, seed=1))
+    b7 = np.frombuffer(v7, dtype=np.uint8)
+    arr[0].data, arr[0].size = b7.ctypes.data, b7.size
+    assert fn(arr, n, None, None, infos) == B.TC_ERR_UNSUPPORTED_VERSION
+
+
+def test_v8_request_scaled_and_reduced_entries_vs_reference(product, reference):
+    """A V8 packet through tc_frame_decode_request (every mode),
+    tc_frame_decode_scaled and tc_frame_decode_reduced: the full decode where
+    the reference has one, and otherwise its status and frame information."""
+    import ctypes
+    from test_gpu_decode_modes import _call_planes, _requests, _same
+    cfg = _v8(B.make_config(320, 180, qp=7, qmatrix_id=4), 4, 5)
+    pkt = reference.encode(cfg, synth.make_frame_np(320, 180, seed=77))
+    rc, info = reference.query(pkt)
+    assert rc == 0
+    w, h = info.visible_width, info.visible_height
+    for rl, req in _requests(w, h):
+        _same(B.decode_request(product, pkt, req, fill=7), B.decode_request(reference, pkt, req, fill=7), rl)
+    for tw, th in [((w + 1) // 2, (h + 1) // 2), (w, h)]:
+        got = []
+        for c in (product, reference):
+            c._lib.tc_frame_decode_scaled.restype = ctypes.c_int32
+            i2 = B.FrameOutput()
+            i2.visible_width, i2.visible_height, i2.plane_count, i2.pixel_format = tw, th, info.plane_count, \
+                info.pixel_format
+            got.append(_call_planes(c._lib.tc_frame_decode_scaled, pkt, B.ToposCodec.geometry(i2),
+                                    ctypes.c_uint32(tw), ctypes.c_uint32(th)))
+        _same(got[0], got[1], ("scaled", tw, th))
+        assert got[0].status == B.TC_ERR_NOT_IMPLEMENTED
+    for s in range(0, 5):
+        got = []
+        for c in (product, reference):
+            c._lib.tc_frame_decode_reduced.restype = ctypes.c_int32
+            got.append(_call_planes(c._lib.tc_frame_decode_reduced, pkt, B.ToposCodec.geometry(info),
+                                    ctypes.c_int32(s)))
+        _same(got[0], got[1], ("reduced", s))

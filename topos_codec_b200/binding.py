@@ -397,11 +397,13 @@ class Server:
     pointers; the caller keeps the buffers alive until wait() returns.
     """
 
-    def __init__(self, codec: "ToposCodec", max_bytes_in_flight: int = 0, max_batch_frames: int = 64):
+    def __init__(self, codec: "ToposCodec", max_bytes_in_flight: int = 0, max_batch_frames: int = 64,
+                 workers: int = 4):
         L = codec._lib
         self._codec, self._lib = codec, L
-        L.tcg_server_create.restype = ctypes.c_int32
-        L.tcg_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)]
+        L.tcg_server_create_ex.restype = ctypes.c_int32
+        L.tcg_server_create_ex.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_void_p)]
         L.tcg_server_destroy.restype = None
         L.tcg_server_destroy.argtypes = [ctypes.c_void_p]
         L.tcg_server_submit_encode.restype = ctypes.c_int32
@@ -415,7 +417,7 @@ class Server:
                                       ctypes.POINTER(FrameStats), ctypes.POINTER(FrameOutput),
                                       ctypes.POINTER(ctypes.c_double)]
         h = ctypes.c_void_p()
-        rc = int(L.tcg_server_create(max_bytes_in_flight, max_batch_frames, ctypes.byref(h)))
+        rc = int(L.tcg_server_create_ex(max_bytes_in_flight, max_batch_frames, workers, ctypes.byref(h)))
         if rc != TC_OK:
             raise ToposCodecError(f"tcg_server_create failed [{rc}]: {codec.last_error()}", rc)
         self._h = h

@@ -548,6 +548,9 @@ constexpr uint32_t V8_TABLE_BYTES = 350u;
 constexpr uint32_t V8D_LUT = 0u;                                  // 11 x 1 KB bucket tables
 constexpr uint32_t V8D_CUM = MAX_CTX * LUT_BYTES;                 // 11 x 66 u16
 constexpr uint32_t V8D_SMEM = V8D_CUM + DCH_CUM_BYTES;
+// per plane of a batch: first block, first segment, block columns, visible
+// width and height, output offset / 64, segment blocks log2, bit depth
+constexpr uint32_t V8_PINFO = 8u;
 
 // one block per tile: CRC of the table and the member streams against the stored one
 __global__ void __launch_bounds__(256) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
@@ -628,8 +631,8 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
     const uint32_t lm = hdr[0], dm = hdr[1];
     const uint32_t* luts = reinterpret_cast<const uint32_t*>(vsm + V8D_LUT);
     const uint16_t* cums = reinterpret_cast<const uint16_t*>(vsm + V8D_CUM);
-    const uint32_t cols = pinfo[6u * S.plane + 2u];
-    int32_t* blk = coef + ((size_t)pinfo[6u * S.plane] + S.blk0) * 64u;
+    const uint32_t cols = pinfo[V8_PINFO * S.plane + 2u];
+    int32_t* blk = coef + ((size_t)pinfo[V8_PINFO * S.plane] + S.blk0) * 64u;
     DLane L;
     dl_init(L, pkt + S.off, S.len);
     uint32_t err = L.x < RANS_L ? 1u : 0u;
@@ -671,21 +674,25 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
     seg_fail[si] = err != 0u ? 1u : 0u;
 }
 
-// Reconstruction of every block of the three planes (k_didct's arithmetic):
-// the block's segment gives its quantiser steps.
+// Reconstruction of every block of the batch's planes (k_didct's
+// arithmetic): the block's plane by a binary search over the planes' first
+// blocks, its segment by the plane's segment size, its quantiser steps by the
+// segment.
 __global__ void __launch_bounds__(128) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
-                                                  const uint32_t* __restrict__ q, const int32_t* __restrict__ coef,
-                                                  uint32_t total, uint32_t bd, uint32_t sb_log2, uint16_t* __restrict__ out)
+                                                  uint32_t nplanes, const uint32_t* __restrict__ q,
+                                                  const int32_t* __restrict__ coef, uint32_t total,
+                                                  uint16_t* __restrict__ out)
 {
     const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
     if (gb >= total) { return; }
-    // pinfo per plane: blk0, seg0, cols, vis_w, vis_h, out_off (u32 element offset / 64)
-    uint32_t p = 0;
-    if (gb >= pinfo[6]) { p = 1; }
-    if (gb >= pinfo[12]) { p = 2; }
-    const uint32_t* I = pinfo + 6u * p;
+    uint32_t lo = 0, hi = nplanes - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (pinfo[V8_PINFO * mid] <= gb) { lo = mid; } else { hi = mid - 1u; }
+    }
+    const uint32_t* I = pinfo + V8_PINFO * lo;
     const uint32_t lb = gb - I[0];
-    const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4];
+    const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4], sb_log2 = I[6], bd = I[7];
     const tcg_v8_seg& S = segs[I[1] + (lb >> sb_log2)];
     const uint32_t* Q = q + (size_t)S.qidx * 64u;
     const uint32_t bx = lb % cols, by = lb / cols;
@@ -1990,42 +1997,75 @@ static int32_t noalloc_base(int dev, uint8_t** base)
     return 0;
 }
 
-// V8 frame decode: descriptors and the packet up, CRCs, tables, chains,
-// reconstruction, planes and per-segment / per-tile results back.
-static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J)
+// V8 batch decode: the frames' descriptors are concatenated (segments,
+// tiles, quantiser steps and planes renumbered into one index space) and
+// decoded in one launch sequence: packets and descriptors up, tile CRCs,
+// tile tables, chains, reconstruction, planes and per-segment / per-tile
+// results back.
+static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
 {
+    std::vector<tcg_v8_seg> segs;
+    std::vector<tcg_v8_tile> tiles;
+    std::vector<uint32_t> q, pinfo;
+    std::vector<uint64_t> pkt_off(count), out_off;
+    uint64_t pkt_bytes = 0, nblk = 0, out_elems = 0;
+    for (uint32_t f = 0; f < count; ++f) {
+        const tcg_v8_job& F = J[f];
+        pkt_off[f] = pkt_bytes;
+        pkt_bytes = align_up(pkt_bytes + F.size, 256);
+        const uint32_t seg_base = (uint32_t)segs.size(), tile_base = (uint32_t)tiles.size();
+        const uint32_t q_base = (uint32_t)(q.size() / 64u), plane_base = (uint32_t)(pinfo.size() / V8_PINFO);
+        const uint32_t sb = 1u << F.sb_log2;
+        uint32_t seg0 = seg_base;
+        for (uint32_t p = 0; p < 3u; ++p) {
+            const uint32_t blocks = F.cols[p] * F.rows[p];
+            const uint32_t pi[V8_PINFO] = {(uint32_t)nblk, seg0, F.cols[p], F.vis_w[p], F.vis_h[p],
+                                           (uint32_t)(out_elems / 64u), F.sb_log2, F.bit_depth};
+            pinfo.insert(pinfo.end(), pi, pi + V8_PINFO);
+            out_off.push_back(out_elems);
+            nblk += blocks;
+            seg0 += (blocks + sb - 1u) / sb;
+            out_elems = align_up(out_elems + (uint64_t)F.vis_w[p] * F.vis_h[p], 64);
+        }
+        for (uint32_t k = 0; k < F.nseg; ++k) {
+            tcg_v8_seg g = F.seg[k];
+            g.plane += plane_base;
+            g.off += (uint32_t)pkt_off[f];
+            g.tile = g.tile == UINT32_MAX ? UINT32_MAX : g.tile + tile_base;
+            g.qidx += q_base;
+            segs.push_back(g);
+        }
+        for (uint32_t t = 0; t < F.ntile; ++t) {
+            tcg_v8_tile T = F.tile[t];
+            T.plane += plane_base;
+            T.seg0 += seg_base;
+            T.table_off += (uint32_t)pkt_off[f];
+            T.stream_off += (uint32_t)pkt_off[f];
+            tiles.push_back(T);
+        }
+        q.insert(q.end(), F.q, F.q + (size_t)F.nq * 64u);
+    }
+    if (pkt_bytes > 0xFFFFFFFFull) {
+        tcg_host_set_error(TCG_ERR_LIMIT_EXCEEDED, "V8 batch packets exceed 4 GB: decode fewer frames per call");
+        return TCG_ERR_LIMIT_EXCEEDED;
+    }
+    const uint32_t nseg = (uint32_t)segs.size(), ntile = (uint32_t)tiles.size();
+    const uint32_t nplanes = (uint32_t)(pinfo.size() / V8_PINFO);
     std::vector<uint32_t> wtile;
     std::vector<int32_t> wsegs;
-    for (uint32_t t = 0; t < J->ntile; ++t) {
-        const tcg_v8_tile& T = J->tile[t];
-        for (uint32_t k = 0; k < T.nseg; k += 32u) {
+    for (uint32_t t = 0; t < ntile; ++t) {
+        for (uint32_t k = 0; k < tiles[t].nseg; k += 32u) {
             wtile.push_back(t);
-            for (uint32_t l = 0; l < 32u; ++l) { wsegs.push_back(k + l < T.nseg ? (int32_t)(T.seg0 + k + l) : -1); }
+            for (uint32_t l = 0; l < 32u; ++l) { wsegs.push_back(k + l < tiles[t].nseg ? (int32_t)(tiles[t].seg0 + k + l) : -1); }
         }
     }
-    // per plane: first block, first segment, block columns, visible size, output offset / 64
-    uint32_t pinfo[18];
-    uint64_t nblk = 0, out_elems = 0;
-    uint32_t seg0 = 0;
-    const uint32_t sb = 1u << J->sb_log2;
-    for (uint32_t p = 0; p < 3u; ++p) {
-        const uint32_t blocks = J->cols[p] * J->rows[p];
-        pinfo[6 * p + 0] = (uint32_t)nblk;
-        pinfo[6 * p + 1] = seg0;
-        pinfo[6 * p + 2] = J->cols[p];
-        pinfo[6 * p + 3] = J->vis_w[p];
-        pinfo[6 * p + 4] = J->vis_h[p];
-        pinfo[6 * p + 5] = (uint32_t)(out_elems / 64u);
-        nblk += blocks;
-        seg0 += (blocks + sb - 1u) / sb;
-        out_elems = align_up(out_elems + (uint64_t)J->vis_w[p] * J->vis_h[p], 64);
-    }
-    const size_t desc = align_up((size_t)J->nseg * sizeof(tcg_v8_seg), 256) +
-                        align_up((size_t)J->ntile * sizeof(tcg_v8_tile), 256) + align_up((size_t)J->nq * 256u, 256) +
-                        align_up(wtile.size() * 4u + 16u, 256) + align_up(wsegs.size() * 4u + 16u, 256) + 256u;
-    const size_t resb = align_up((size_t)J->nseg + 16u, 256) + align_up((size_t)J->ntile + 16u, 256);
-    if (!dreserve(C, B_DEC_PKT, J->size + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
-        !dreserve(C, B_DEC_TAB, (size_t)J->ntile * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
+    const size_t desc = align_up((size_t)nseg * sizeof(tcg_v8_seg) + 16u, 256) +
+                        align_up((size_t)ntile * sizeof(tcg_v8_tile) + 16u, 256) + align_up(q.size() * 4u + 16u, 256) +
+                        align_up(wtile.size() * 4u + 16u, 256) + align_up(wsegs.size() * 4u + 16u, 256) +
+                        align_up(pinfo.size() * 4u + 16u, 256);
+    const size_t resb = align_up((size_t)nseg + 16u, 256) + align_up((size_t)ntile + 16u, 256);
+    if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_DEC_TAB, (size_t)ntile * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
         !dreserve(C, B_DEC_RES, resb) || !dreserve(C, B_DESC, desc) || !hreserve(C, 0, desc) || !hreserve(C, 1, resb)) {
         return TCG_ERR_OUT_OF_MEMORY;
     }
@@ -2039,12 +2079,12 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J)
         o = align_up(o + n, 256);
         return at;
     };
-    const size_t o_sg = put(J->seg, (size_t)J->nseg * sizeof(tcg_v8_seg));
-    const size_t o_tl = put(J->tile, (size_t)J->ntile * sizeof(tcg_v8_tile));
-    const size_t o_q = put(J->q, (size_t)J->nq * 256u);
+    const size_t o_sg = put(segs.data(), (size_t)nseg * sizeof(tcg_v8_seg));
+    const size_t o_tl = put(tiles.data(), (size_t)ntile * sizeof(tcg_v8_tile));
+    const size_t o_q = put(q.data(), q.size() * 4u);
     const size_t o_wt = put(wtile.data(), wtile.size() * 4u);
     const size_t o_ws = put(wsegs.data(), wsegs.size() * 4u);
-    const size_t o_pi = put(pinfo, sizeof(pinfo));
+    const size_t o_pi = put(pinfo.data(), pinfo.size() * 4u);
     call_begin(C);
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
     const tcg_v8_seg* d_sg = (const tcg_v8_seg*)(dd + o_sg);
@@ -2054,42 +2094,51 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J)
     const int32_t* d_ws = (const int32_t*)(dd + o_ws);
     const uint32_t* d_pi = (const uint32_t*)(dd + o_pi);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
-    TCG_CHECK(cudaMemcpyAsync(d_pkt, J->packet, J->size, cudaMemcpyDefault, st));
+    for (uint32_t f = 0; f < count; ++f) {
+        TCG_CHECK(cudaMemcpyAsync(d_pkt + pkt_off[f], J[f].packet, J[f].size, cudaMemcpyDefault, st));
+    }
     int32_t* d_coef = dptr<int32_t>(C, B_DEC_COEF);
     uint8_t* d_tab = dptr<uint8_t>(C, B_DEC_TAB);
     uint16_t* d_out = dptr<uint16_t>(C, B_DEC_OUT);
     uint8_t* d_res = dptr<uint8_t>(C, B_DEC_RES);
     uint8_t* d_fail = d_res;
-    uint8_t* d_ok = d_res + align_up((size_t)J->nseg + 16u, 256);
+    uint8_t* d_ok = d_res + align_up((size_t)nseg + 16u, 256);
     TCG_CHECK(cudaMemsetAsync(d_res, 0, resb, st));
     TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
     const DevTables& T = tables();
-    if (J->ntile > 0u) {
-        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, J->ntile, 256, 0, d_tl, d_pkt, T.crc, d_ok);
-        TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, J->ntile, 32, 0, d_tl, d_pkt, d_tab);
+    if (ntile > 0u) {
+        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, ntile, 256, 0, d_tl, d_pkt, T.crc, d_ok);
+        TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, ntile, 32, 0, d_tl, d_pkt, d_tab);
     }
     if (!wtile.empty()) {
         TCG_LAUNCH(C, K_DCHAIN, k_v8_dchain, (uint32_t)wtile.size(), 32, V8D_SMEM, d_sg, d_wt, d_ws, d_pi, d_ok, d_pkt,
                    d_tab, d_coef, d_fail);
     }
     if (nblk > 0u) {
-        TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sg, d_pi, d_q, d_coef,
-                   (uint32_t)nblk, J->bit_depth, J->sb_log2, d_out);
+        TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sg, d_pi, nplanes, d_q, d_coef,
+                   (uint32_t)nblk, d_out);
     }
-    for (uint32_t p = 0; p < 3u; ++p) {
-        const size_t w = J->vis_w[p], h = J->vis_h[p];
-        if (w == 0u || h == 0u) { continue; }
-        const size_t pitch = (J->dst_stride[p] ? J->dst_stride[p] : w) * 2u;
-        TCG_CHECK(cudaMemcpy2DAsync(J->dst[p], pitch, d_out + (size_t)pinfo[6 * p + 5] * 64u, w * 2u, w * 2u, h,
-                                    cudaMemcpyDefault, st));
+    for (uint32_t f = 0; f < count; ++f) {
+        for (uint32_t p = 0; p < 3u; ++p) {
+            const size_t w = J[f].vis_w[p], h = J[f].vis_h[p];
+            if (w == 0u || h == 0u) { continue; }
+            const size_t pitch = (J[f].dst_stride[p] ? J[f].dst_stride[p] : w) * 2u;
+            TCG_CHECK(cudaMemcpy2DAsync(J[f].dst[p], pitch, d_out + out_off[3u * f + p], w * 2u, w * 2u, h,
+                                        cudaMemcpyDefault, st));
+        }
     }
     uint8_t* hr = (uint8_t*)C->h[1].p;
     TCG_CHECK(cudaMemcpyAsync(hr, d_res, resb, cudaMemcpyDeviceToHost, st));
     TCG_CHECK(cudaGetLastError());
     TCG_CHECK(cudaStreamSynchronize(st));
     call_end(C);
-    memcpy(J->seg_fail, hr, J->nseg);
-    memcpy(J->tile_ok, hr + align_up((size_t)J->nseg + 16u, 256), J->ntile);
+    uint32_t sb0 = 0, tb0 = 0;
+    for (uint32_t f = 0; f < count; ++f) {
+        memcpy(J[f].seg_fail, hr + sb0, J[f].nseg);
+        memcpy(J[f].tile_ok, hr + align_up((size_t)nseg + 16u, 256) + tb0, J[f].ntile);
+        sb0 += J[f].nseg;
+        tb0 += J[f].ntile;
+    }
     return 0;
 }
 
@@ -2119,11 +2168,12 @@ extern "C" int32_t tcg_decode(const tcg_dec_frame* frames, uint32_t count)
     return rc;
 }
 
-extern "C" int32_t tcg_decode_v8(const tcg_v8_job* job)
+extern "C" int32_t tcg_decode_v8(const tcg_v8_job* jobs, uint32_t count)
 {
+    if (count == 0u) { return 0; }
     tcg::Ctx* c = tcg::ctx_acquire();
     if (c == nullptr) { return TCG_ERR_NOT_IMPLEMENTED; }
-    const int32_t rc = tcg::decode_v8_impl(c, job);
+    const int32_t rc = tcg::decode_v8_impl(c, jobs, count);
     tcg::ctx_release(c);
     return rc;
 }

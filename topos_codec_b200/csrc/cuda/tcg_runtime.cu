@@ -15,6 +15,13 @@ static Ctx* g_free = nullptr;
 static bool g_init = false;
 static int g_device = -1;
 static DevTables g_tab;
+// Stream-ordered pool for the call contexts' grow-only buffers. Growing a
+// buffer frees and allocates in the order of the context's own stream, so it
+// never synchronises the device (cudaMalloc / cudaFree do, and with several
+// calls in flight - the request server's workers - that stalls all of them).
+// The pool keeps what is freed (release threshold at the maximum) until
+// trim_idle returns idle contexts' memory.
+static cudaMemPool_t g_pool = nullptr;
 static std::atomic<uint64_t> g_launches{0};
 static std::atomic<uint64_t> g_allocs{0};  // device and pinned host allocations made
 static std::atomic<int> g_prof_on{0};
@@ -275,6 +282,20 @@ static bool init_locked(int device)
         cuda_fail(e, "table upload");
         return false;
     }
+    {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        if (cudaMemPoolCreate(&g_pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "device memory pool creation failed");
+            return false;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(g_pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     g_tab.div_m = (const uint32_t*)(d + om);
     g_tab.div_l = d + ol;
     g_tab.log2 = (const double*)(d + olg);
@@ -339,31 +360,35 @@ void trim_idle()
             if (s != nullptr) { cudaStreamSynchronize(s); }
         }
         for (auto& b : c->d) {
-            if (b.p != nullptr) { cudaFree(b.p); }
+            if (b.p != nullptr) { cudaFreeAsync(b.p, c->stream); }
             b.p = nullptr;
             b.cap = 0;
         }
+        cudaStreamSynchronize(c->stream);
     }
+    if (g_pool != nullptr) { cudaMemPoolTrimTo(g_pool, 0); }
 }
 
+// A context's buffers are used only by its own calls, which have finished
+// (or are ordered behind it by call_begin) when the next call reserves, so
+// freeing on the context's stream is enough.
 bool dreserve(Ctx* c, BufId id, size_t bytes)
 {
     DBuf& b = c->d[id];
     if (bytes <= b.cap) { return true; }
     if (b.p != nullptr) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(b.p);
+        cudaFreeAsync(b.p, c->stream);
         b.p = nullptr;
         b.cap = 0;
     }
-    size_t want = bytes + bytes / 8 + 4096;
-    if (cudaMalloc(&b.p, want) != cudaSuccess) {
+    size_t want = bytes + bytes / 4 + 4096;
+    if (cudaMallocFromPoolAsync(&b.p, want, g_pool, c->stream) != cudaSuccess) {
         // idle contexts keep the buffers of their largest call: give those
         // back and try once more
         cudaGetLastError();
         b.p = nullptr;
         trim_idle();
-        if (cudaMalloc(&b.p, want) == cudaSuccess) {
+        if (cudaMallocFromPoolAsync(&b.p, want, g_pool, c->stream) == cudaSuccess) {
             g_allocs.fetch_add(1, std::memory_order_relaxed);
             b.cap = want;
             return true;
@@ -390,7 +415,7 @@ bool hreserve(Ctx* c, int id, size_t bytes)
         b.p = nullptr;
         b.cap = 0;
     }
-    size_t want = bytes + bytes / 8 + 4096;
+    size_t want = bytes + bytes / 4 + 4096;
     if (cudaMallocHost(&b.p, want) != cudaSuccess) {
         cudaGetLastError();
         b.p = nullptr;
@@ -420,7 +445,8 @@ extern "C" void tcg_shutdown(void)
         for (cudaStream_t s : {c->stream, c->side, c->aux}) {
             if (s != nullptr) { cudaStreamSynchronize(s); }
         }
-        for (auto& b : c->d) { if (b.p) { cudaFree(b.p); } }
+        for (auto& b : c->d) { if (b.p) { cudaFreeAsync(b.p, c->stream); } }
+        if (c->stream != nullptr) { cudaStreamSynchronize(c->stream); }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
         for (cudaEvent_t e : {c->fork, c->join, c->afork, c->ajoin, c->gate, c->t0, c->t1}) {
             if (e != nullptr) { cudaEventDestroy(e); }

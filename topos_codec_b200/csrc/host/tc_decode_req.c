@@ -212,6 +212,14 @@ TC_EXPORT int32_t tc_frame_decode_request(const uint8_t* data, size_t size, cons
     if (data == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "data == NULL"); }
     rc = request_validate(request);
     if (rc != TC_OK) { return rc; }
+    if (tc_packet_major(data, size) == 8) {
+        /* V8 (codec.c:9469-9482): the query and FULL decode; no scaled path */
+        if (planes_out != NULL && request->mode != TC_DECODE_MODE_FULL) {
+            rc = tc_v8_frame_decode(data, size, NULL, NULL, out_info);
+            return rc != TC_OK ? rc : tc_fail(TC_ERR_NOT_IMPLEMENTED, "v8 reduced/auto2k path not defined");
+        }
+        return tc_v8_frame_decode(data, size, planes_out, strides, out_info);
+    }
     return decode_one(data, size, planes_out, strides, out_info, request_resolve, request);
 }
 
@@ -224,6 +232,11 @@ TC_EXPORT int32_t tc_frame_decode_scaled(const uint8_t* data, size_t size, uint3
     if (rc != TC_OK) { return rc; }
     if (data == NULL || target_width == 0u || target_height == 0u) {
         return tc_fail(TC_ERR_INVALID_ARGUMENT, "scaled decode invalid arguments");
+    }
+    if (tc_packet_major(data, size) == 8) {
+        /* V8 (codec.c:9123-9130): structure and information, no scaled path */
+        rc = tc_v8_frame_decode(data, size, NULL, NULL, out_info);
+        return rc != TC_OK ? rc : tc_fail(TC_ERR_NOT_IMPLEMENTED, "v8 scaled decode lands in format-plan batch 3");
     }
     const fixed_plan f = {1u, target_width, target_height, 63u, 0u};
     return decode_one(data, size, planes_out, strides, out_info, scaled_resolve, &f);

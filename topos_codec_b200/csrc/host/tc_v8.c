@@ -177,6 +177,161 @@ static int32_t check_tables(const uint8_t* d, const v8_view* v, uint32_t p, uint
     return TC_OK;
 }
 
+/* One frame prepared for the device: its view, the job and the job's arrays. */
+typedef struct v8_prep {
+    v8_src src;
+    v8_view* v;
+    tcg_v8_seg* seg;
+    tcg_v8_tile* tile;
+    uint8_t* fail;
+    uint32_t* q;
+    tcg_v8_job job;
+} v8_prep;
+
+static void v8_release(v8_prep* P)
+{
+    free(P->v);
+    free(P->src.skel);
+    free(P->seg);
+    free(P->tile);
+    free(P->fail);
+    free(P->q);
+    memset(P, 0, sizeof(*P));
+}
+
+/* Scan, checks in the reference's order and the device job of one frame
+ * (reference codec.c:4772-4870). planes_out NULL: the query only (structure
+ * and frame information), *query set. */
+static int32_t v8_prepare(const uint8_t* data, size_t size, uint16_t* const planes_out[4], const size_t* strides,
+                          topos_frame_output* o, v8_prep* P, int* query)
+{
+    memset(P, 0, sizeof(*P));
+    *query = 0;
+    const uint8_t* d = data;
+    if (tcg_is_device_ptr(data)) {
+        P->src.dev = data;
+        P->src.skel = (uint8_t*)malloc(size > 0u ? size : 1u);
+        if (P->src.skel == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 packet structure copy"); }
+        const int32_t rc = fetch(&P->src, 0u, size < TC_HDR_SIZE + V8_EXT ? size : TC_HDR_SIZE + V8_EXT);
+        if (rc != TC_OK) { return rc; }
+        d = P->src.skel;
+    }
+    P->v = (v8_view*)malloc(sizeof(v8_view));
+    if (P->v == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 view"); }
+    v8_view* v = P->v;
+    int32_t rc = v8_scan(&P->src, d, size, v);
+    if (rc != TC_OK) { return rc; }
+    if (planes_out == NULL) {
+        tc_fill_info(&v->h, o);
+        *query = 1;
+        return TC_OK;
+    }
+    if (v->h.major == 9u) { return tc_fail(TC_ERR_NOT_IMPLEMENTED, "V9 packets are not implemented by this library"); }
+    if (v->h.pf == 3u) { return tc_fail(TC_ERR_UNSUPPORTED_PIXEL_FORMAT, "v8 does not carry CFA (TRAW uses rans2)"); }
+    tc_fill_info(&v->h, o);
+    const tc_hdr* h = &v->h;
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        if (planes_out[p] == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "v8 planes_out[%u] == NULL", p); }
+    }
+    uint16_t qm[2][64];
+    uint32_t t0 = 0;
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        if ((rc = check_tables(d, v, p, t0)) != TC_OK) { return rc; }
+        t0 += v->tiles[p];
+        if (!tc_qmatrix(h->qm, 0, qm[0]) || !tc_qmatrix(h->qm, 1, qm[1])) {
+            return tc_fail(TC_ERR_UNSUPPORTED_MATRIX, "qmatrix_id %u", h->qm);
+        }
+    }
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        const size_t s = strides != NULL ? strides[p] : 0u;
+        if (s != 0u && s < (size_t)h->pvw[p]) {
+            return tc_fail(TC_ERR_INVALID_ARGUMENT, "plane %u stride %zu < visible width %u", p, s, h->pvw[p]);
+        }
+    }
+    uint32_t nseg = 0;
+    for (uint32_t p = 0; p < h->planes; ++p) { nseg += v->segs[p]; }
+    P->seg = (tcg_v8_seg*)calloc(nseg ? nseg : 1u, sizeof(tcg_v8_seg));
+    P->tile = (tcg_v8_tile*)calloc(v->ntiles ? v->ntiles : 1u, sizeof(tcg_v8_tile));
+    P->fail = (uint8_t*)calloc(nseg + v->ntiles + 1u, 1);
+    P->q = (uint32_t*)malloc(2u * 96u * 64u * sizeof(uint32_t));
+    if (P->seg == NULL || P->tile == NULL || P->fail == NULL || P->q == NULL) {
+        return tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 decode job");
+    }
+    tcg_v8_seg* seg = P->seg;
+    tcg_v8_tile* tile = P->tile;
+    /* quantiser steps per (matrix, effective qp) that a segment uses */
+    int32_t qslot[2][96];
+    memset(qslot, 0xFF, sizeof(qslot));
+    uint32_t nq = 0, k = 0, tg = 0;
+    const int32_t ceil = h->qp >= TC_QP_V15_MIN ? (int32_t)TC_QP_MAX : 63;
+    const uint32_t refined = (h->flags & 0x8u) != 0u;
+    for (uint32_t p = 0; p < h->planes; ++p) {
+        const uint32_t blocks = h->brows[p] * h->bcols[p];
+        const uint8_t* dir = d + v->dir_off[p];
+        const int chroma = p == 1u || p == 2u;
+        for (uint32_t s = 0; s < v->segs[p]; ++s, ++k) {
+            int32_t qe = (int32_t)h->qp + (int32_t)dir[(size_t)s * V8_DIR + 8u] - 64;
+            qe = qe < 0 ? 0 : (qe > ceil ? ceil : qe);
+            if (qslot[chroma][qe] < 0) {
+                qslot[chroma][qe] = (int32_t)nq;
+                tc_quant_steps(qm[chroma], (uint32_t)qe, refined, P->q + (size_t)nq * 64u);
+                nq++;
+            }
+            seg[k].plane = p;
+            seg[k].blk0 = s * v->sb;
+            seg[k].nblk = blocks - s * v->sb < v->sb ? blocks - s * v->sb : v->sb;
+            seg[k].tile = UINT32_MAX;
+            seg[k].off = v->stream_off[p] + ld32(dir + (size_t)s * V8_DIR);
+            seg[k].len = ld32(dir + (size_t)s * V8_DIR + 4u);
+            seg[k].qidx = (uint32_t)qslot[chroma][qe];
+        }
+        for (uint32_t t = 0; t < v->tiles[p]; ++t, ++tg) {
+            const v8_tile* ti = &v->t[tg];
+            tile[tg].plane = p;
+            tile[tg].seg0 = k - v->segs[p] + ti->seg_first;
+            tile[tg].nseg = ti->seg_count;
+            tile[tg].table_off = ti->table_off;
+            tile[tg].stream_off = ti->stream_off;
+            tile[tg].stream_bytes = ti->stream_bytes;
+            tile[tg].crc = ti->crc;
+            for (uint32_t x = 0; x < ti->seg_count; ++x) { seg[tile[tg].seg0 + x].tile = tg; }
+        }
+    }
+    tcg_v8_job* J = &P->job;
+    J->packet = data;
+    J->size = size;
+    J->bit_depth = h->bd;
+    J->sb_log2 = v->sb_log2;
+    for (uint32_t p = 0; p < 3u; ++p) {
+        J->vis_w[p] = h->pvw[p]; J->vis_h[p] = h->pvh[p];
+        J->cols[p] = h->bcols[p]; J->rows[p] = h->brows[p];
+        J->dst[p] = planes_out[p];
+        J->dst_stride[p] = strides != NULL ? strides[p] : 0u;
+    }
+    J->nseg = nseg;
+    J->ntile = v->ntiles;
+    J->nq = nq;
+    J->seg = seg;
+    J->tile = tile;
+    J->q = P->q;
+    J->seg_fail = P->fail;
+    J->tile_ok = P->fail + nseg;
+    return TC_OK;
+}
+
+/* per-tile status: concealed when its CRC failed or a member segment failed */
+static void v8_status(const v8_prep* P, topos_frame_output* o)
+{
+    uint32_t concealed = 0;
+    for (uint32_t t = 0; t < P->job.ntile; ++t) {
+        uint32_t bad = P->job.tile_ok[t] == 0u;
+        for (uint32_t s = 0; s < P->tile[t].nseg && !bad; ++s) { bad = P->job.seg_fail[P->tile[t].seg0 + s]; }
+        o->slice_status[t] = bad ? TC_FRAME_SLICE_CONCEALED : TC_FRAME_SLICE_OK;
+        concealed += bad;
+    }
+    o->concealed_slices = (uint16_t)concealed;
+}
+
 /* reference: codec.c:9039-9049 (tc_frame_decode's V8 branch), 4772-4975
  * (v8_frame_decode). Concealed tiles are reported per tile and counted, and
  * the call still returns TC_OK, as the reference's does; V8 has no
@@ -186,129 +341,62 @@ static int32_t check_tables(const uint8_t* d, const v8_view* v, uint32_t p, uint
 int32_t tc_v8_frame_decode(const uint8_t* data, size_t size, uint16_t* const planes_out[4], const size_t strides[4],
                            topos_frame_output* o)
 {
-    v8_src src = {NULL, NULL};
-    const uint8_t* d = data;
-    if (tcg_is_device_ptr(data)) {
-        src.dev = data;
-        src.skel = (uint8_t*)malloc(size > 0u ? size : 1u);
-        if (src.skel == NULL) { return tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 packet structure copy"); }
-        const int32_t rc = fetch(&src, 0u, size < TC_HDR_SIZE + V8_EXT ? size : TC_HDR_SIZE + V8_EXT);
-        if (rc != TC_OK) { free(src.skel); return rc; }
-        d = src.skel;
+    v8_prep P;
+    int query = 0;
+    int32_t rc = v8_prepare(data, size, planes_out, strides, o, &P, &query);
+    if (rc == TC_OK && !query) {
+        rc = tcg_decode_v8(&P.job, 1u);
+        if (rc == TC_OK) { v8_status(&P, o); }
     }
-    v8_view* v = (v8_view*)malloc(sizeof(v8_view));
-    int32_t rc = v == NULL ? tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 view") : v8_scan(&src, d, size, v);
-    if (rc == TC_OK && planes_out == NULL) {
-        tc_fill_info(&v->h, o);  /* query: structure and frame information */
-    } else if (rc == TC_OK && v->h.major == 9u) {
-        rc = tc_fail(TC_ERR_NOT_IMPLEMENTED, "V9 packets are not implemented by this library");
-    } else if (rc == TC_OK && v->h.pf == 3u) {
-        rc = tc_fail(TC_ERR_UNSUPPORTED_PIXEL_FORMAT, "v8 does not carry CFA (TRAW uses rans2)");
-    } else if (rc == TC_OK) {
-        tc_fill_info(&v->h, o);
-        const tc_hdr* h = &v->h;
-        for (uint32_t p = 0; p < h->planes && rc == TC_OK; ++p) {
-            if (planes_out[p] == NULL) { rc = tc_fail(TC_ERR_INVALID_ARGUMENT, "v8 planes_out[%u] == NULL", p); }
-        }
-        uint16_t qm[2][64];
-        uint32_t t0 = 0;
-        for (uint32_t p = 0; p < h->planes && rc == TC_OK; ++p) {
-            rc = check_tables(d, v, p, t0);
-            t0 += v->tiles[p];
-            if (rc == TC_OK && (!tc_qmatrix(h->qm, 0, qm[0]) || !tc_qmatrix(h->qm, 1, qm[1]))) {
-                rc = tc_fail(TC_ERR_UNSUPPORTED_MATRIX, "qmatrix_id %u", h->qm);
-            }
-        }
-        for (uint32_t p = 0; p < h->planes && rc == TC_OK; ++p) {
-            const size_t s = strides != NULL ? strides[p] : 0u;
-            if (s != 0u && s < (size_t)h->pvw[p]) { rc = tc_fail(TC_ERR_INVALID_ARGUMENT, "plane %u stride %zu < visible width %u", p, s, h->pvw[p]); }
-        }
-        uint32_t nseg = 0;
-        for (uint32_t p = 0; p < h->planes; ++p) { nseg += v->segs[p]; }
-        tcg_v8_seg* seg = rc == TC_OK ? (tcg_v8_seg*)calloc(nseg ? nseg : 1u, sizeof(tcg_v8_seg)) : NULL;
-        tcg_v8_tile* tile = rc == TC_OK ? (tcg_v8_tile*)calloc(v->ntiles ? v->ntiles : 1u, sizeof(tcg_v8_tile)) : NULL;
-        uint8_t* fail = rc == TC_OK ? (uint8_t*)calloc(nseg + v->ntiles + 1u, 1) : NULL;
-        uint32_t* q = rc == TC_OK ? (uint32_t*)malloc(2u * 96u * 64u * sizeof(uint32_t)) : NULL;
-        if (rc == TC_OK && (seg == NULL || tile == NULL || fail == NULL || q == NULL)) {
-            rc = tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 decode job");
-        }
-        if (rc == TC_OK) {
-            /* quantiser steps per (matrix, effective qp) that a segment uses */
-            int32_t qslot[2][96];
-            memset(qslot, 0xFF, sizeof(qslot));
-            uint32_t nq = 0, k = 0, tg = 0;
-            const int32_t ceil = h->qp >= TC_QP_V15_MIN ? (int32_t)TC_QP_MAX : 63;
-            const uint32_t refined = (h->flags & 0x8u) != 0u;
-            for (uint32_t p = 0; p < h->planes; ++p) {
-                const uint32_t blocks = h->brows[p] * h->bcols[p];
-                const uint8_t* dir = d + v->dir_off[p];
-                const int chroma = p == 1u || p == 2u;
-                for (uint32_t s = 0; s < v->segs[p]; ++s, ++k) {
-                    int32_t qe = (int32_t)h->qp + (int32_t)dir[(size_t)s * V8_DIR + 8u] - 64;
-                    qe = qe < 0 ? 0 : (qe > ceil ? ceil : qe);
-                    if (qslot[chroma][qe] < 0) {
-                        qslot[chroma][qe] = (int32_t)nq;
-                        tc_quant_steps(qm[chroma], (uint32_t)qe, refined, q + (size_t)nq * 64u);
-                        nq++;
-                    }
-                    seg[k].plane = p;
-                    seg[k].blk0 = s * v->sb;
-                    seg[k].nblk = blocks - s * v->sb < v->sb ? blocks - s * v->sb : v->sb;
-                    seg[k].tile = UINT32_MAX;
-                    seg[k].off = v->stream_off[p] + ld32(dir + (size_t)s * V8_DIR);
-                    seg[k].len = ld32(dir + (size_t)s * V8_DIR + 4u);
-                    seg[k].qidx = (uint32_t)qslot[chroma][qe];
-                }
-                for (uint32_t t = 0; t < v->tiles[p]; ++t, ++tg) {
-                    const v8_tile* ti = &v->t[tg];
-                    tile[tg].plane = p;
-                    tile[tg].seg0 = k - v->segs[p] + ti->seg_first;
-                    tile[tg].nseg = ti->seg_count;
-                    tile[tg].table_off = ti->table_off;
-                    tile[tg].stream_off = ti->stream_off;
-                    tile[tg].stream_bytes = ti->stream_bytes;
-                    tile[tg].crc = ti->crc;
-                    for (uint32_t s = 0; s < ti->seg_count; ++s) { seg[tile[tg].seg0 + s].tile = tg; }
-                }
-            }
-            tcg_v8_job J;
-            memset(&J, 0, sizeof(J));
-            J.packet = data;
-            J.size = size;
-            J.bit_depth = h->bd;
-            J.sb_log2 = v->sb_log2;
-            for (uint32_t p = 0; p < 3u; ++p) {
-                J.vis_w[p] = h->pvw[p]; J.vis_h[p] = h->pvh[p];
-                J.cols[p] = h->bcols[p]; J.rows[p] = h->brows[p];
-                J.dst[p] = planes_out[p];
-                J.dst_stride[p] = strides != NULL ? strides[p] : 0u;
-            }
-            J.nseg = nseg;
-            J.ntile = v->ntiles;
-            J.nq = nq;
-            J.seg = seg;
-            J.tile = tile;
-            J.q = q;
-            J.seg_fail = fail;
-            J.tile_ok = fail + nseg;
-            rc = tcg_decode_v8(&J);
-            if (rc == TC_OK) {
-                uint32_t concealed = 0;
-                for (uint32_t t = 0; t < v->ntiles; ++t) {
-                    uint32_t bad = J.tile_ok[t] == 0u;
-                    for (uint32_t s = 0; s < tile[t].nseg && !bad; ++s) { bad = fail[tile[t].seg0 + s]; }
-                    o->slice_status[t] = bad ? TC_FRAME_SLICE_CONCEALED : TC_FRAME_SLICE_OK;
-                    concealed += bad;
-                }
-                o->concealed_slices = (uint16_t)concealed;
-            }
-        }
-        free(seg);
-        free(tile);
-        free(fail);
-        free(q);
+    v8_release(&P);
+    return rc;
+}
+
+/* Extension (no reference counterpart; the reference's batch decode takes V7
+ * packets only): count V8 packets decoded in one launch sequence. Every
+ * packet is scanned and checked first, and any failure fails the call
+ * (like tc_frame_decode_batch); planes_out NULL = query only. Returns TC_OK
+ * or the first failing packet's status; concealment is reported per tile. */
+TC_EXPORT int32_t tcg_frame_decode_v8_batch(const topos_batch_packet* packets, uint32_t count,
+                                            uint16_t* const* planes_out, const size_t* strides,
+                                            topos_frame_output* infos)
+{
+    if (count == 0u) { return TC_OK; }
+    if (count > TC_BATCH_MAX_FRAMES) { return tc_fail(TC_ERR_LIMIT_EXCEEDED, "batch count %u", count); }
+    if (packets == NULL || infos == NULL) { return tc_fail(TC_ERR_INVALID_ARGUMENT, "batch arguments NULL"); }
+    v8_prep* P = (v8_prep*)calloc(count, sizeof(v8_prep));
+    tcg_v8_job* jobs = (tcg_v8_job*)calloc(count, sizeof(tcg_v8_job));
+    if (P == NULL || jobs == NULL) {
+        free(P);
+        free(jobs);
+        return tc_fail(TC_ERR_OUT_OF_MEMORY, "v8 batch staging");
     }
-    free(v);
-    free(src.skel);
+    int32_t rc = TC_OK;
+    uint32_t prepared = 0;
+    for (uint32_t i = 0; i < count && rc == TC_OK; ++i) {
+        topos_frame_output* o = &infos[i];
+        memset(o, 0, sizeof(*o));
+        o->struct_size = (uint32_t)sizeof(topos_frame_output);
+        o->abi_version = TOPOS_CODEC_ABI_VERSION;
+        int query = 0;
+        if (packets[i].data == NULL) {
+            rc = tc_fail(TC_ERR_INVALID_ARGUMENT, "packets[%u].data == NULL", i);
+        } else if (tc_packet_major(packets[i].data, packets[i].size) != 8) {
+            rc = tc_fail(TC_ERR_UNSUPPORTED_VERSION, "packets[%u] is not a V8 packet", i);
+        } else {
+            rc = v8_prepare(packets[i].data, packets[i].size,
+                            planes_out != NULL ? planes_out + (size_t)i * TC_FRAME_MAX_PLANES : NULL,
+                            strides != NULL ? strides + (size_t)i * TC_FRAME_MAX_PLANES : NULL, o, &P[i], &query);
+        }
+        prepared = i + 1u;
+        jobs[i] = P[i].job;
+    }
+    if (rc == TC_OK && planes_out != NULL) {
+        rc = tcg_decode_v8(jobs, count);
+        for (uint32_t i = 0; i < count && rc == TC_OK; ++i) { v8_status(&P[i], &infos[i]); }
+    }
+    for (uint32_t i = 0; i < prepared; ++i) { v8_release(&P[i]); }
+    free(P);
+    free(jobs);
     return rc;
 }

@@ -197,7 +197,8 @@ typedef struct tcg_v8_job {
     uint8_t* tile_ok;                   /* out, per tile: CRC matched */
 } tcg_v8_job;
 
-int32_t tcg_decode_v8(const tcg_v8_job* job);
+/* count frames in one launch sequence */
+int32_t tcg_decode_v8(const tcg_v8_job* jobs, uint32_t count);
 
 /* provided by the host library: thread-local error detail */
 void tcg_host_set_error(int32_t status, const char* text);

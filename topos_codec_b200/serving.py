@@ -3,9 +3,19 @@
 Requests arrive as a Poisson process: half encodes, half decodes; frames of
 1920x1080 (40 %), 3840x2160 (40 %) and 1280x720 (20 %), 10-bit 4:2:2, tiers
 422 (qp 8, quant matrix 4) and HQ (qp 4; flat matrix and refined qp table at
-3840 wide), chosen from a seeded generator. Sample planes and packets stay
-resident in device memory; each request codes into its own output buffer.
-The server measures each request's latency from submission to completion.
+3840 wide), chosen from a seeded generator. generation="v8" codes the same
+stream as V8 segmented-rANS packets (16-block segments, 32-row tiles; V8 has
+no deblocking or refined qp table, so those features are off).
+
+The load generator is open-loop: arrivals follow their schedule whatever the
+server does. Input planes and packets are shared, read-only, per (resolution,
+tier); every request gets its own output buffer from a pool that is provisioned
+before the stream for half a second of arrivals and grows when all are in
+use, so a busy server never delays the next arrival. Latency runs
+from a request's scheduled arrival to the moment its completion is seen
+(the generator's lag before submitting it plus the server's own
+submission-to-completion time, which is also reported alone). Percentiles are given for the whole stream and per resolution and
+direction.
 """
 from __future__ import annotations
 
@@ -20,65 +30,112 @@ RESOLUTIONS = [((1920, 1080), 0.4), ((3840, 2160), 0.4), ((1280, 720), 0.2)]
 TIERS = ["422", "hq"]
 
 
-def tier_config(w: int, h: int, tier: str) -> B.FrameConfig:
+def tier_config(w: int, h: int, tier: str, generation: str = "v7") -> B.FrameConfig:
+    if generation == "v8":
+        cfg = B.make_config(w, h, qp=4 if tier == "hq" else 8, qmatrix_id=0 if (tier == "hq" and w >= 3840) else 4)
+        cfg.reserved[0] = 9
+        return cfg
     if tier == "hq":
         big = w >= 3840
         return B.make_config(w, h, qp=4, qmatrix_id=0 if big else 4, features=3 if big else 1)
     return B.make_config(w, h, qp=8, qmatrix_id=4, features=1)
 
 
-class _Slot:
-    """Device buffers for one request of one (resolution, tier, direction)."""
+class _Kind:
+    """Shared inputs of one (resolution, tier): sample planes and a packet in
+    device memory; output buffers are handed out per request."""
 
-    def __init__(self, codec, torch, dev, w, h, tier, seed):
-        self.cfg = tier_config(w, h, tier)
+    def __init__(self, codec, torch, dev, w, h, tier, seed, generation):
+        self.cfg = tier_config(w, h, tier, generation)
         self.w, self.h = w, h
+        self.torch, self.dev = torch, dev
         planes = synth.make_frame(w, h, seed=seed, frame=0, device=dev)
         self.planes = [p.to(torch.uint16).contiguous() for p in planes]
         self.cap = codec.packet_bound(self.cfg)
-        self.out = torch.empty(self.cap, dtype=torch.uint8, device=dev)
         pkt = codec.encode(self.cfg, [p.cpu().numpy() for p in self.planes])
         self.pkt = torch.frombuffer(bytearray(pkt), dtype=torch.uint8).to(dev)
-        self.dec = [torch.empty_like(p) for p in self.planes]
+        self.free_out: List = []
+        self.free_dec: List = []
+
+    def out(self):
+        return self.free_out.pop() if self.free_out else self.torch.empty(self.cap, dtype=self.torch.uint8,
+                                                                          device=self.dev)
+
+    def dec(self):
+        return self.free_dec.pop() if self.free_dec else [self.torch.empty_like(p) for p in self.planes]
+
+    def provision(self, n_out: int, n_dec: int):
+        """Allocate output buffers ahead of a stream, so that the device
+        allocator's synchronising calls fall outside it."""
+        while len(self.free_out) < n_out:
+            self.free_out.append(self.torch.empty(self.cap, dtype=self.torch.uint8, device=self.dev))
+        while len(self.free_dec) < n_dec:
+            self.free_dec.append([self.torch.empty_like(p) for p in self.planes])
 
 
-def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, slots_per_kind: int = 8,
-              max_batch_frames: int = 32) -> Dict:
-    """Submit a Poisson request stream at rate_rps for duration_s; returns latency percentiles."""
+def _pct(xs, p):
+    return xs[min(len(xs) - 1, int(p * len(xs)))] if xs else None
+
+
+def _summary(lat: List[float]) -> Dict:
+    lat = sorted(lat)
+    return {"n": len(lat), "p50_ms": _pct(lat, 0.50), "p99_ms": _pct(lat, 0.99), "p999_ms": _pct(lat, 0.999),
+            "max_ms": lat[-1] if lat else None}
+
+
+def _kinds(codec, torch, dev, seed, generation):
+    return {(wh, t): _Kind(codec, torch, dev, wh[0], wh[1], t, seed + i, generation)
+            for i, (wh, t) in enumerate((wh, t) for wh, _ in RESOLUTIONS for t in TIERS)}
+
+
+def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batch_frames: int = 32,
+              generation: str = "v7", workers: int = 4, kinds=None, resolutions=None) -> Dict:
+    """Submit a Poisson request stream at rate_rps for duration_s; returns the
+    latency percentiles (whole stream, per resolution, per direction)."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = random.Random(seed)
-    kinds = [(wh, t) for wh, _ in RESOLUTIONS for t in TIERS]
-    pools = {k: [_Slot(codec, torch, dev, k[0][0], k[0][1], k[1], seed + i) for i in range(slots_per_kind)]
-             for k in kinds}
-    free = {k: list(range(slots_per_kind)) for k in kinds}
-    cv = threading.Condition()
+    kinds = kinds or _kinds(codec, torch, dev, seed, generation)
+    res_mix = resolutions or RESOLUTIONS
+    # output buffers for half a second of arrivals per (resolution, tier, direction)
+    for (wh, share) in res_mix:
+        for t in TIERS:
+            if (wh, t) in kinds:
+                n = int(rate_rps * share / len(TIERS) * 0.5 * 0.5) + 2
+                kinds[(wh, t)].provision(n, n)
     torch.cuda.synchronize()
-    srv = B.Server(codec, max_batch_frames=max_batch_frames)
-    lat: List[float] = []
-    stats = {"encode": 0, "decode": 0, "errors": 0}
+    srv = B.Server(codec, max_batch_frames=max_batch_frames, workers=workers)
+    cv = threading.Condition()
     pending: List = []
-    done_evt = threading.Event()
+    records: List = []   # (resolution, encode, client ms, server ms)
+    errors = [0]
+    closing = threading.Event()
 
     def waiter():
         while True:
             with cv:
-                while not pending and not done_evt.is_set():
+                while not pending and not closing.is_set():
                     cv.wait()
                 if not pending:
                     return
-                key, idx, t = pending.pop(0)
-            st, _, _, ms = srv.wait(t)
+                kind, enc, buf, t_sched, t_sub, ticket = pending.pop(0)
+            st, _, _, ms = srv.wait(ticket)
             with cv:
-                lat.append(ms)
+                # scheduled arrival to completion: the generator's lag before
+                # submission plus the server's submission-to-completion time
+                # (completions are collected in submission order, so the time
+                # this thread sees one would add the wait for older requests)
+                records.append((kind[0], enc, (t_sub - t_sched) * 1e3 + ms, ms))
                 if st not in (0, 1):
-                    stats["errors"] += 1
-                free[key].append(idx)
-                cv.notify_all()
+                    errors[0] += 1
+                (kind_obj(kind).free_out if enc else kind_obj(kind).free_dec).append(buf)
+
+    def kind_obj(k):
+        return kinds[k]
 
     th = threading.Thread(target=waiter)
     th.start()
-    weights = [w for _, w in RESOLUTIONS]
+    weights = [w for _, w in res_mix]
     t0 = time.perf_counter()
     t_next = t0
     n = 0
@@ -87,99 +144,99 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, slots_pe
             t_next += rng.expovariate(rate_rps)
             if t_next - t0 > duration_s:
                 break
-            wh = rng.choices([r for r, _ in RESOLUTIONS], weights)[0]
+            wh = rng.choices([r for r, _ in res_mix], weights)[0]
             key = (wh, rng.choice(TIERS))
             enc = rng.random() < 0.5
             delay = t_next - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
+            k = kinds[key]
             with cv:
-                while not free[key]:
-                    cv.wait()
-                idx = free[key].pop()
-            s = pools[key][idx]
+                buf = k.out() if enc else k.dec()
+            t_sub = time.perf_counter()
             if enc:
-                t = srv.submit_encode(s.cfg, [(p.data_ptr(), p.shape[1]) for p in s.planes], s.out.data_ptr(), s.cap)
-                stats["encode"] += 1
+                ticket = srv.submit_encode(k.cfg, [(p.data_ptr(), p.shape[1]) for p in k.planes], buf.data_ptr(), k.cap)
             else:
-                t = srv.submit_decode(s.pkt.data_ptr(), s.pkt.numel(), [p.data_ptr() for p in s.dec])
-                stats["decode"] += 1
+                ticket = srv.submit_decode(k.pkt.data_ptr(), k.pkt.numel(), [p.data_ptr() for p in buf])
             n += 1
             with cv:
-                pending.append((key, idx, t))
+                pending.append((key, enc, buf, t_next, t_sub, ticket))
                 cv.notify_all()
     finally:
-        done_evt.set()
+        closing.set()
         with cv:
             cv.notify_all()
         th.join()
         srv.close()
     wall = time.perf_counter() - t0
-    lat.sort()
+    out = {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
+           "errors": errors[0], "generation": generation}
+    out.update(_summary([r[2] for r in records]))
+    out["server_side"] = _summary([r[3] for r in records])
+    out["by_resolution"] = {f"{w}x{h}": _summary([r[2] for r in records if r[0] == (w, h)]) for (w, h), _ in res_mix}
+    out["by_direction"] = {"encode": _summary([r[2] for r in records if r[1]]),
+                           "decode": _summary([r[2] for r in records if not r[1]])}
+    return out
 
-    def pct(p):
-        return lat[min(len(lat) - 1, int(p * len(lat)))] if lat else None
 
-    return {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
-            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "p999_ms": pct(0.999), "max_ms": lat[-1] if lat else None,
-            "encodes": stats["encode"], "decodes": stats["decode"], "errors": stats["errors"]}
-
-
-def saturation_rps(codec, n: int = 48, seed: int = 1, max_batch_frames: int = 32) -> float:
+def saturation_rps(codec, n: int = 96, seed: int = 1, max_batch_frames: int = 32, generation: str = "v7",
+                   workers: int = 4, kinds=None) -> float:
     """Requests per second when n requests of the mix are all submitted at once
     (the best of two passes: the first also pays for one-time per-batch-size
     tuning)."""
-    return max(_saturation_pass(codec, n, seed, max_batch_frames) for _ in range(2))
-
-
-def _saturation_pass(codec, n: int, seed: int, max_batch_frames: int) -> float:
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
+    kinds = kinds or _kinds(codec, torch, dev, seed, generation)
+    return max(_saturation_pass(codec, n, seed, max_batch_frames, workers, kinds) for _ in range(2))
+
+
+def _saturation_pass(codec, n, seed, max_batch_frames, workers, kinds) -> float:
+    import torch
     rng = random.Random(seed)
-    kinds = [(wh, t) for wh, _ in RESOLUTIONS for t in TIERS]
-    per = max(1, n // len(kinds) + 1)
-    pools = {k: [_Slot(codec, torch, dev, k[0][0], k[0][1], k[1], seed + i) for i in range(per)] for k in kinds}
     weights = [w for _, w in RESOLUTIONS]
-    used = {k: 0 for k in kinds}
     torch.cuda.synchronize()
-    srv = B.Server(codec, max_batch_frames=max_batch_frames)
+    srv = B.Server(codec, max_batch_frames=max_batch_frames, workers=workers)
+    bufs = []
     try:
         t0 = time.perf_counter()
         tickets = []
         for _ in range(n):
             wh = rng.choices([r for r, _ in RESOLUTIONS], weights)[0]
-            key = (wh, rng.choice(TIERS))
-            if used[key] >= per:
-                key = min(used, key=used.get)
-            s = pools[key][used[key]]
-            used[key] += 1
+            k = kinds[(wh, rng.choice(TIERS))]
             if rng.random() < 0.5:
-                tickets.append(srv.submit_encode(s.cfg, [(p.data_ptr(), p.shape[1]) for p in s.planes],
-                                                 s.out.data_ptr(), s.cap))
+                b = k.out()
+                tickets.append(srv.submit_encode(k.cfg, [(p.data_ptr(), p.shape[1]) for p in k.planes],
+                                                 b.data_ptr(), k.cap))
+                bufs.append((k.free_out, b))
             else:
-                tickets.append(srv.submit_decode(s.pkt.data_ptr(), s.pkt.numel(), [p.data_ptr() for p in s.dec]))
+                b = k.dec()
+                tickets.append(srv.submit_decode(k.pkt.data_ptr(), k.pkt.numel(), [p.data_ptr() for p in b]))
+                bufs.append((k.free_dec, b))
         for t in tickets:
             srv.wait(t)
         return n / (time.perf_counter() - t0)
     finally:
         srv.close()
+        for pool, b in bufs:
+            pool.append(b)
 
 
-def run_trace_plain(codec, rate_rps: float, duration_s: float, seed: int = 0) -> Dict:
+def run_trace_plain(codec, rate_rps: float, duration_s: float, seed: int = 0, generation: str = "v7",
+                    kinds=None) -> Dict:
     """The same Poisson request stream served by the plain per-frame calls, one
     request at a time in arrival order (the drop-in path without batching);
-    latency runs from each request's arrival to its completion."""
+    latency runs from each request's scheduled arrival to its completion."""
     import ctypes
     import queue
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = random.Random(seed)
-    kinds = [(wh, t) for wh, _ in RESOLUTIONS for t in TIERS]
-    slots = {k: _Slot(codec, torch, dev, k[0][0], k[0][1], k[1], seed) for k in kinds}
+    kinds = kinds or _kinds(codec, torch, dev, seed, generation)
+    outs = {k: (v.out(), v.dec()) for k, v in kinds.items()}
     L = codec._lib
     torch.cuda.synchronize()
     q: "queue.Queue" = queue.Queue()
-    lat: List[float] = []
+    records: List = []
     errors = [0]
 
     def worker():
@@ -189,22 +246,23 @@ def run_trace_plain(codec, rate_rps: float, duration_s: float, seed: int = 0) ->
             if item is None:
                 return
             key, enc, t_arr = item
-            s = slots[key]
+            k = kinds[key]
+            out, dec = outs[key]
             if enc:
                 fi = B.FrameInput()
                 fi.struct_size, fi.abi_version = ctypes.sizeof(B.FrameInput), B.TOPOS_CODEC_ABI_VERSION
-                for p, t in enumerate(s.planes):
+                for p, t in enumerate(k.planes):
                     fi.planes[p], fi.strides[p] = t.data_ptr(), t.shape[1]
-                rc = int(L.tc_frame_encode(ctypes.byref(s.cfg), ctypes.byref(fi), ctypes.c_void_p(s.out.data_ptr()),
-                                           s.cap, ctypes.byref(st)))
+                rc = int(L.tc_frame_encode(ctypes.byref(k.cfg), ctypes.byref(fi), ctypes.c_void_p(out.data_ptr()),
+                                           k.cap, ctypes.byref(st)))
             else:
-                ptrs = (ctypes.c_void_p * B.TC_FRAME_MAX_PLANES)(*[t.data_ptr() for t in s.dec])
+                ptrs = (ctypes.c_void_p * B.TC_FRAME_MAX_PLANES)(*[t.data_ptr() for t in dec])
                 info = B.FrameOutput()
-                rc = int(L.tc_frame_decode(ctypes.c_void_p(s.pkt.data_ptr()), s.pkt.numel(), ptrs, None,
+                rc = int(L.tc_frame_decode(ctypes.c_void_p(k.pkt.data_ptr()), k.pkt.numel(), ptrs, None,
                                            ctypes.byref(info)))
             if rc not in (0, 1):
                 errors[0] += 1
-            lat.append((time.perf_counter() - t_arr) * 1e3)
+            records.append((key[0], enc, (time.perf_counter() - t_arr) * 1e3))
 
     th = threading.Thread(target=worker)
     th.start()
@@ -227,18 +285,46 @@ def run_trace_plain(codec, rate_rps: float, duration_s: float, seed: int = 0) ->
     q.put(None)
     th.join()
     wall = time.perf_counter() - t0
-    lat.sort()
-
-    def pct(p):
-        return lat[min(len(lat) - 1, int(p * len(lat)))] if lat else None
-
-    return {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
-            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "p999_ms": pct(0.999), "max_ms": lat[-1] if lat else None,
-            "errors": errors[0]}
+    out = {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
+           "errors": errors[0], "generation": generation}
+    out.update(_summary([r[2] for r in records]))
+    out["by_resolution"] = {f"{w}x{h}": _summary([r[2] for r in records if r[0] == (w, h)]) for (w, h), _ in RESOLUTIONS}
+    return out
 
 
-def plain_saturation_rps(codec, n: int = 48, seed: int = 1) -> float:
+def plain_saturation_rps(codec, n: int = 48, seed: int = 1, generation: str = "v7", kinds=None) -> float:
     """Requests per second of the plain per-frame calls on n requests of the mix back to back."""
-    r = run_trace_plain(codec, rate_rps=1e6, duration_s=n / 1e6, seed=seed)
+    r = run_trace_plain(codec, rate_rps=1e6, duration_s=n / 1e6, seed=seed, generation=generation, kinds=kinds)
     return r["requests"] / max(r["duration_s"], 1e-9)
 
+
+def single_frame_floor(codec, w: int = 1920, h: int = 1080, tier: str = "422", generation: str = "v7",
+                       repeats: int = 5) -> Dict:
+    """One frame encoded and decoded alone on an idle GPU through the plain
+    calls (device-resident planes and packet): the latency floor of a request
+    of that size, best of the repeats, wall clock of the call."""
+    import ctypes
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    k = _Kind(codec, torch, dev, w, h, tier, 5, generation)
+    out, dec = k.out(), k.dec()
+    L = codec._lib
+    fi = B.FrameInput()
+    fi.struct_size, fi.abi_version = ctypes.sizeof(B.FrameInput), B.TOPOS_CODEC_ABI_VERSION
+    for p, t in enumerate(k.planes):
+        fi.planes[p], fi.strides[p] = t.data_ptr(), t.shape[1]
+    ptrs = (ctypes.c_void_p * B.TC_FRAME_MAX_PLANES)(*[t.data_ptr() for t in dec])
+    st, info = B.FrameStats(), B.FrameOutput()
+    enc_ms, dec_ms = [], []
+    torch.cuda.synchronize()
+    for _ in range(repeats + 1):
+        t0 = time.perf_counter()
+        L.tc_frame_encode(ctypes.byref(k.cfg), ctypes.byref(fi), ctypes.c_void_p(out.data_ptr()), k.cap,
+                          ctypes.byref(st))
+        t1 = time.perf_counter()
+        L.tc_frame_decode(ctypes.c_void_p(k.pkt.data_ptr()), k.pkt.numel(), ptrs, None, ctypes.byref(info))
+        t2 = time.perf_counter()
+        enc_ms.append((t1 - t0) * 1e3)
+        dec_ms.append((t2 - t1) * 1e3)
+    return {"size": f"{w}x{h}", "tier": tier, "generation": generation, "encode_ms": min(enc_ms[1:]),
+            "decode_ms": min(dec_ms[1:])}

@@ -68,10 +68,11 @@ def _inputs(frames) -> ctypes.Array:
     return arr
 
 
-def batched_vs_plain(codec, cfgs: Sequence[B.FrameConfig], frames, repeats: int = 2) -> Dict:
+def batched_vs_plain(codec, cfgs: Sequence[B.FrameConfig], frames, repeats: int = 2, v8: bool = False) -> Dict:
     """Encode and decode the frames (device-resident uint16 planes) batched and
     per frame. Returns device times, bit-exactness of the two forms and the
-    batched packets (host bytes)."""
+    batched packets (host bytes). v8: the frames are V8 packets, decoded in
+    one batch by tcg_frame_decode_v8_batch."""
     import torch
     L = _lib(codec)
     n = len(cfgs)
@@ -101,7 +102,8 @@ def batched_vs_plain(codec, cfgs: Sequence[B.FrameConfig], frames, repeats: int 
         arr = (B.BatchPacket * n)()
         for i in range(n):
             arr[i].data, arr[i].size = outs[i].data_ptr(), st[i].packet_size
-        rc = int(L.tc_frame_decode_batch(arr, n, dptr, None, infos))
+        fn = L.tcg_frame_decode_v8_batch if v8 else L.tc_frame_decode_batch
+        rc = int(fn(arr, n, dptr, None, infos))
         if rc not in (B.TC_OK, B.TC_WARN_CONCEALED):
             raise RuntimeError(f"batched decode failed [{rc}]: {codec.last_error()}")
         return L.tcg_last_device_ms()
