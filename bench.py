@@ -10,7 +10,7 @@ the plain per-frame GPU path on the same frames for comparison.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--serve-seconds S] [--no-serve] [--no-extra]
-    python bench.py --case 3840x2160 --frames 2 [--repeat R] [--case-qp Q] [--case-gbr]
+    python bench.py --case 3840x2160 --frames 2 [--repeat R] [--case-qp Q] [--case-gbr] [--case-v8]
 
 Beside the headline the line reports (key `workloads`) a 64-frame mixed batch
 (720p..8K, four tiers, qp 2..16) and a 32-frame 4096x2160 12-bit GBR 4:4:4 +
@@ -237,6 +237,10 @@ def kernel_case(args):
         from topos_codec_b200.workloads import gbr_config
         cfg = gbr_config(w, h)
         kw = dict(bit_depth=12, pixel_format=2, limited=False, alpha=True, sigma=12)
+    elif args.case_v8:
+        cfg = B.make_config(w, h, qp=args.case_qp, qmatrix_id=0 if w >= 3840 else 4)
+        cfg.reserved[0] = 9  # V8 segmented rANS, 16-block segments, 32-row tiles
+        kw = {}
     else:
         cfg = B.make_config(w, h, qp=args.case_qp, qmatrix_id=0 if w >= 3840 else 4, features=3 if w >= 3840 else 1)
         kw = {}
@@ -269,7 +273,8 @@ def kernel_case(args):
         pk = (B.BatchPacket * n)()
         for i in range(n):
             pk[i].data, pk[i].size = outs[i].data_ptr(), st[i].packet_size
-        rc = L.tc_frame_decode_batch(pk, n, dptr, None, infos)
+        dec_fn = L.tcg_frame_decode_v8_batch if args.case_v8 else L.tc_frame_decode_batch
+        rc = dec_fn(pk, n, dptr, None, infos)
         assert rc == 0, gpu.last_error()
     L.tcg_profile_enable(0)
     res = {}
@@ -279,13 +284,15 @@ def kernel_case(args):
             break
         if cnt.value:
             res[name.value.decode()] = round(ms.value, 3)
-    print(json.dumps({"case": args.case, "frames": n, "packet_bytes": sum(s.packet_size for s in st),
+    # V8 kernels are counted in the slots of the V7-R2 kernels of the same stage
+    print(json.dumps({"case": args.case, "generation": "v8" if args.case_v8 else "v7", "frames": n, "packet_bytes": sum(s.packet_size for s in st),
                       "kernels_ms": res}))
 
 
 # ------------------------------------------------------------------ GPU path
 
 def main():
+    t_main = time.perf_counter()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -300,6 +307,7 @@ def main():
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--case-qp", type=int, default=4)
     ap.add_argument("--case-gbr", action="store_true", help="12-bit GBR 4:4:4 + 16-bit alpha at qp 2")
+    ap.add_argument("--case-v8", action="store_true", help="V8 segmented rANS packets instead of V7-R2")
     ap.add_argument("--cpu-mode", default=None, choices=["slice", "batch"], help=argparse.SUPPRESS)
     ap.add_argument("--cpu-seconds", type=float, default=6.0, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -557,7 +565,9 @@ def main():
                 "note": "serial rANS state chains bound this kernel by dependent-op latency, not HBM"}
         _ = out_side
 
+    sections = {"main_s": round(time.perf_counter() - t_main, 1)}
     # ---------------- CPU baseline (rank 0, N=1 only) ----------------
+    t_sec = time.perf_counter()
     cpu = None
     if rank == 0 and world == 1 and os.path.exists(REF_LIB):
         f_np = [[p.cpu().numpy() for p in frames_d[i]] for i in range(min(nf, 8))]
@@ -570,7 +580,9 @@ def main():
                          "per_frame_slice_parallel": modes.get("slice"),
                          "decode_batch": modes.get("batch")}}
 
+    sections["cpu_baseline_s"] = round(time.perf_counter() - t_sec, 1)
     # ---------------- further workloads: mixed batch, GBR 4:4:4 + alpha ----------------
+    t_sec = time.perf_counter()
     extra = {}
     if world == 1 and not args.no_extra:
         from concurrent.futures import ThreadPoolExecutor
@@ -635,11 +647,16 @@ def main():
         r["workload"] = "the 60 3840x2160 HQ packets decoded at 1/2 size, device-resident"
         extra["preview_decode"] = r
         torch.cuda.empty_cache()
-        torch.cuda.empty_cache()
+    sections["workloads_s"] = round(time.perf_counter() - t_sec, 1)
 
     # ---------------- serving: open-loop request streams at 25/50/75/100 % of saturation ----------------
+    t_sec = time.perf_counter()
     served = None
     if world == 1 and not args.no_serve:
+        # the earlier sections' idle call contexts hold their largest buffers;
+        # the serving streams allocate their own through torch
+        gpu._lib.tcg_release_idle_memory()
+        torch.cuda.empty_cache()
         from topos_codec_b200 import serving
         floors = [serving.single_frame_floor(gpu, 1920, 1080, "422", g) for g in ("v7", "v8")]
         kinds = serving._kinds(gpu, torch, dev, 0, "v7")
@@ -679,6 +696,7 @@ def main():
                        "v8_at_half_saturation": dict({x: v8_half[x] for x in keys}, saturation_rps=sat8,
                                                      by_direction=v8_half["by_direction"])})
 
+    sections["serving_s"] = round(time.perf_counter() - t_sec, 1)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -697,6 +715,7 @@ def main():
             "cpu_baseline": cpu,
             "served": served,
             "workloads": extra,
+            "section_seconds": sections,
             "e2e": {"value": nf * world / e2e_s, "unit": "frames/s",
                     "h2d_bytes_per_step": int(in_bytes + pkt_bytes), "d2h_bytes_per_step": int(pkt_bytes + in_bytes),
                     "encode_chunks": e2e_chunks, "decode_chunks": e2e_dchunks},

@@ -591,6 +591,13 @@ uint32_t tcg_pipeline_plan(int32_t decode, const uint64_t* frame_bytes, uint32_t
 int32_t tcg_device_init(int32_t device);
 void tcg_device_release(void);
 
+/* Give back the device memory of every call context that is not in use.
+ * Contexts keep the buffers of their largest call so that the next call of
+ * that size allocates nothing; a process that shares the device with another
+ * allocator (a framework's caching allocator) calls this between phases. The
+ * next call on such a context allocates again. */
+void tcg_release_idle_memory(void);
+
 /* Number of device kernel launches issued by this library in this process
  * (diagnostics for benchmarks). */
 uint64_t tcg_kernel_launches(void);

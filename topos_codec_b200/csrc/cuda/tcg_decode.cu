@@ -11,7 +11,7 @@
 //               checks                          (slice_codec.c:626-736)
 //   k_dchain_w  the same decode with one warp per colour slice, the symbol
 //               search spread over the lanes (a second tiling; a tuner picks)
-//   k_didct     per block: dequantise, exact inverse transform, clamp, crop
+//   k_didct     32 blocks per CTA: dequantise, exact inverse transform, clamp, crop
 //                                               (color_store.h:529-711)
 //   k_dalpha    per alpha slice: Rice run/level decode -> residuals
 //                                               (block_coding.c:529-560)
@@ -530,6 +530,191 @@ __global__ void __launch_bounds__(32) k_dchain(const DSlice* __restrict__ slices
     status[si] = err != 0u ? TCG_ERR_MALFORMED : 0;
 }
 
+// ------------------------------------------------------------------ reconstruction
+//
+// Blocks are reconstructed 32 to a CTA of 256 threads (RB_BLOCKS). Lane b of
+// warp 0 first gathers block b's facts (quantiser steps, clamp, destination).
+// Then every thread loads two 16-byte pieces of the CTA's 8 KB of
+// coefficients (contiguous, so each warp reads 512 bytes in one go) and
+// dequantises them into natural order in shared memory; warp w runs the
+// 8-point row pass of row w of all 32 blocks (lane = block), then the column
+// pass of column w, and finally stores row w of every block, 16 bytes per
+// lane, so a warp writes 512 contiguous bytes of a plane row when the blocks
+// lie side by side. The arithmetic is idct8x8's, split at its passes:
+// G = c (.) W, B = G * M, xhat = round(M^T * B / 2^32).
+constexpr uint32_t RB_BLOCKS = 32u;
+constexpr uint32_t RB_CP = 65u;   // words per block in the coefficient and B arrays (odd: no bank conflicts)
+constexpr uint32_t RB_TP = 72u;   // samples per block in the output tile (144 B rows of 16-byte pieces)
+
+struct RBlock {
+    const uint32_t* Q;  // quantiser steps, natural order
+    uint16_t* dst;      // the block's top-left visible sample
+    int64_t fc;         // dequantised coefficient clamp
+    uint32_t pitch;     // plane row pitch in samples
+    uint32_t cw, ch;    // visible columns and rows of the block
+    uint32_t climit;    // highest zigzag position kept
+    uint32_t bd;
+    uint32_t ok;        // 0: nothing to write (past the batch, concealed slice, outside the plane)
+    uint32_t vec;       // whole rows of 16-byte aligned samples
+};
+
+struct RShared {
+    int32_t c[RB_BLOCKS * RB_CP];
+    int64_t B[RB_BLOCKS * RB_CP];
+    __align__(16) uint16_t t[RB_BLOCKS * RB_TP];
+    RBlock blk[RB_BLOCKS];
+    uint8_t zz[64];
+};
+
+// The transform tables as doubles (exact) for the double-precision passes.
+__device__ __constant__ double c_tmd[64] = {
+    13, 13, 13, 13, 13, 13, 13, 13, 13, 11, 7, 1, -1, -7, -11, -13,
+    12, 5, -5, -12, -12, -5, 5, 12, 11, -4, -13, -8, 8, 13, 4, -11,
+    9, -9, -9, 9, 9, -9, -9, 9, 8, -13, 4, 11, -11, -4, 13, -8,
+    5, -12, 12, -5, -5, 12, -12, 5, 1, -7, 11, -13, 13, -11, 7, -1};
+__device__ __constant__ double c_twd[64] = {
+    2350, 4672, 4699, 4293, 4902, 4293, 4699, 4672,
+    4672, 9288, 9343, 8535, 9747, 8535, 9343, 9288,
+    4699, 9343, 9399, 8586, 9805, 8586, 9399, 9343,
+    4293, 8535, 8586, 7843, 8957, 7843, 8586, 8535,
+    4902, 9747, 9805, 8957, 10228, 8957, 9805, 9747,
+    4293, 8535, 8586, 7843, 8957, 7843, 8586, 8535,
+    4699, 9343, 9399, 8586, 9805, 8586, 9399, 9343,
+    4672, 9288, 9343, 8535, 9747, 8535, 9343, 9288};
+
+// round_shift32 of an integer-valued double below 2^53 in magnitude: |v| + 2^31
+// and its scaling by 2^-32 are exact, so the floor is the integer form's
+// sign-split rounding
+__device__ __forceinline__ int32_t round_shift32_f64(double v)
+{
+    const double r = floor((fabs(v) + 2147483648.0) * 2.3283064365386962890625e-10);
+    return v >= 0.0 ? (int32_t)r : -(int32_t)r;
+}
+
+__device__ __forceinline__ int64_t recon_clamp(uint32_t bd)
+{
+    return bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (bd - 1u)) - 1u)) / 2047;
+}
+
+// Phases 1-4 above; sh.blk is filled and visible (after a barrier) on entry.
+// coef points at block gb0 and holds nvalid blocks from there.
+__device__ __forceinline__ void recon_blocks(RShared& sh, const int32_t* __restrict__ coef, uint32_t nvalid)
+{
+    const uint32_t t = threadIdx.x, w = t >> 5, lane = t & 31u;
+    // dequantise into natural order
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        const uint32_t idx = t + 256u * h;  // 16-byte piece of the CTA's coefficients
+        const uint32_t b = idx >> 4, i0 = (idx & 15u) * 4u;
+        const RBlock& R = sh.blk[b];
+        if (b < nvalid && R.ok) {
+            const int4 v = __ldg(reinterpret_cast<const int4*>(coef) + idx);
+            const int32_t vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; ++j) {
+                const uint32_t i = i0 + j;
+                int32_t lv = i == 0u ? vv[j] : unmap_s((uint32_t)vv[j]);
+                lv = i <= R.climit ? lv : 0;
+                const uint32_t nat = sh.zz[i];
+                int64_t f = (int64_t)lv * __ldg(R.Q + nat);
+                f = f > R.fc ? R.fc : (f < -R.fc ? -R.fc : f);
+                sh.c[b * RB_CP + nat] = (int32_t)f;
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t b = lane;
+    const bool live = b < nvalid && sh.blk[b].ok;
+    // Up to 12 bits the dequantised coefficients are within +-2^25, so every
+    // product and partial sum of both passes is an integer below 2^51 in
+    // magnitude (|W| < 2^14, column sums of |M| are at most 72) and double
+    // arithmetic gives the 64-bit integer results exactly, one fused
+    // multiply-add per term; wider samples take the 64-bit integer passes.
+    const bool f64 = live && sh.blk[b].bd <= 12u;
+    if (live) {  // row pass: row u = w
+        const uint32_t u = w;
+        if (f64) {
+            double g[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) { g[v] = (double)sh.c[b * RB_CP + u * 8u + v] * c_twd[u * 8u + v]; }
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                double pe = g[0] * c_tmd[x], po = g[1] * c_tmd[8 + x];
+#pragma unroll
+                for (int v = 2; v < 8; v += 2) { pe = fma(g[v], c_tmd[v * 8 + x], pe); po = fma(g[v + 1], c_tmd[(v + 1) * 8 + x], po); }
+                sh.B[b * RB_CP + u * 8u + x] = __double_as_longlong(pe + po);
+                sh.B[b * RB_CP + u * 8u + 7u - x] = __double_as_longlong(pe - po);
+            }
+        } else {
+            int64_t g[8];
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                int32_t c = sh.c[b * RB_CP + u * 8u + v];
+                c = c > (1 << 30) ? (1 << 30) : (c < -(1 << 30) ? -(1 << 30) : c);
+                g[v] = (int64_t)c * c_tw[u * 8u + v];
+            }
+#pragma unroll
+            for (int x = 0; x < 4; ++x) {
+                int64_t pe = 0, po = 0;
+#pragma unroll
+                for (int v = 0; v < 8; v += 2) { pe += g[v] * TCG_M(v, x); po += g[v + 1] * TCG_M(v + 1, x); }
+                sh.B[b * RB_CP + u * 8u + x] = pe + po;
+                sh.B[b * RB_CP + u * 8u + 7u - x] = pe - po;
+            }
+        }
+    }
+    __syncthreads();
+    if (live) {  // column pass: column x = w
+        const uint32_t x = w;
+        const int32_t mid = 1 << (sh.blk[b].bd - 1u), maxv = (1 << sh.blk[b].bd) - 1;
+        int32_t out[8];
+        if (f64) {
+            double Bc[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) { Bc[u] = __longlong_as_double(sh.B[b * RB_CP + u * 8u + x]); }
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                double qe = c_tmd[y] * Bc[0], qo = c_tmd[8 + y] * Bc[1];
+#pragma unroll
+                for (int u = 2; u < 8; u += 2) { qe = fma(c_tmd[u * 8 + y], Bc[u], qe); qo = fma(c_tmd[(u + 1) * 8 + y], Bc[u + 1], qo); }
+                out[y] = round_shift32_f64(qe + qo);
+                out[7 - y] = round_shift32_f64(qe - qo);
+            }
+        } else {
+            int64_t Bc[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) { Bc[u] = sh.B[b * RB_CP + u * 8u + x]; }
+#pragma unroll
+            for (int y = 0; y < 4; ++y) {
+                int64_t qe = 0, qo = 0;
+#pragma unroll
+                for (int u = 0; u < 8; u += 2) { qe += (int64_t)TCG_M(u, y) * Bc[u]; qo += (int64_t)TCG_M(u + 1, y) * Bc[u + 1]; }
+                out[y] = round_shift32(qe + qo);
+                out[7 - y] = round_shift32(qe - qo);
+            }
+        }
+#pragma unroll
+        for (int y = 0; y < 8; ++y) {
+            const int32_t a = out[y] + mid;
+            sh.t[b * RB_TP + y * 8u + x] = (uint16_t)(a < 0 ? 0 : (a > maxv ? maxv : a));
+        }
+    }
+    __syncthreads();
+    if (live) {  // store row y = w
+        const RBlock& R = sh.blk[b];
+        const uint32_t y = w;
+        if (y < R.ch) {
+            uint16_t* d = R.dst + (size_t)y * R.pitch;
+            const uint16_t* s = sh.t + b * RB_TP + y * 8u;
+            if (R.vec) {
+                *reinterpret_cast<uint4*>(d) = *reinterpret_cast<const uint4*>(s);
+            } else {
+                for (uint32_t x = 0; x < R.cw; ++x) { d[x] = s[x]; }
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ V8 segments
 //
 // V8 (reference codec.c:4321-4475 segment decode, 4772-4975 frame decode).
@@ -552,12 +737,13 @@ constexpr uint32_t V8D_SMEM = V8D_CUM + DCH_CUM_BYTES;
 // width and height, output offset / 64, segment blocks log2, bit depth
 constexpr uint32_t V8_PINFO = 8u;
 
-// one block per tile: CRC of the table and the member streams against the stored one
-__global__ void __launch_bounds__(256) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
-                                                 const uint32_t* __restrict__ crctab, uint8_t* __restrict__ ok)
+// one 1024-thread block per tile (a frame has few tiles, ~1 MB each at
+// 3840x2160): CRC of the table and the member streams against the stored one
+__global__ void __launch_bounds__(1024) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
+                                                  const uint32_t* __restrict__ crctab, uint8_t* __restrict__ ok)
 {
     __shared__ uint32_t t[8 * 256];
-    __shared__ uint32_t scratch[512];
+    __shared__ uint32_t scratch[2 * 1024];
     __shared__ uint32_t c_tab;
     for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
     __syncthreads();
@@ -678,56 +864,47 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
 // arithmetic): the block's plane by a binary search over the planes' first
 // blocks, its segment by the plane's segment size, its quantiser steps by the
 // segment.
-__global__ void __launch_bounds__(128) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
+__global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
                                                   uint32_t nplanes, const uint32_t* __restrict__ q,
                                                   const int32_t* __restrict__ coef, uint32_t total,
                                                   uint16_t* __restrict__ out)
 {
-    const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gb >= total) { return; }
-    uint32_t lo = 0, hi = nplanes - 1u;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1u) >> 1;
-        if (pinfo[V8_PINFO * mid] <= gb) { lo = mid; } else { hi = mid - 1u; }
-    }
-    const uint32_t* I = pinfo + V8_PINFO * lo;
-    const uint32_t lb = gb - I[0];
-    const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4], sb_log2 = I[6], bd = I[7];
-    const tcg_v8_seg& S = segs[I[1] + (lb >> sb_log2)];
-    const uint32_t* Q = q + (size_t)S.qidx * 64u;
-    const uint32_t bx = lb % cols, by = lb / cols;
-    const int64_t fc = bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (bd - 1u)) - 1u)) / 2047;
-    int32_t c[64], xh[64];
-    const int4* src = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int4 v = src[i];
-        const int32_t vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
-            const int nat = k_zigzag[i * 4 + j];
-            int64_t f = (int64_t)lv * __ldg(Q + nat);
-            f = f > fc ? fc : (f < -fc ? -fc : f);
-            c[nat] = (int32_t)f;
-        }
-    }
-    idct8x8(c, xh);
-    const int32_t mid = 1 << (bd - 1u), maxv = (1 << bd) - 1;
-    const uint32_t px = bx * 8u, py = by * 8u;
-    if (px >= vis_w || py >= vis_h) { return; }
-    const uint32_t cw = min(8u, vis_w - px), ch = min(8u, vis_h - py);
-    uint16_t* dst = out + (size_t)I[5] * 64u + (size_t)py * vis_w + px;
-#pragma unroll
-    for (int y = 0; y < 8; ++y) {
-#pragma unroll
-        for (int x = 0; x < 8; ++x) {
-            if ((uint32_t)y < ch && (uint32_t)x < cw) {
-                const int32_t v = xh[y * 8 + x] + mid;
-                dst[(size_t)y * vis_w + x] = (uint16_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
+    __shared__ RShared sh;
+    const uint32_t gb0 = blockIdx.x * RB_BLOCKS;
+    const uint32_t nvalid = min(RB_BLOCKS, total - gb0);
+    if (threadIdx.x < 64u) { sh.zz[threadIdx.x] = k_zigzag[threadIdx.x]; }
+    if (threadIdx.x < RB_BLOCKS) {
+        RBlock R;
+        R.ok = 0u;
+        const uint32_t gb = gb0 + threadIdx.x;
+        if (gb < total) {
+            uint32_t lo = 0, hi = nplanes - 1u;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (pinfo[V8_PINFO * mid] <= gb) { lo = mid; } else { hi = mid - 1u; }
+            }
+            const uint32_t* I = pinfo + V8_PINFO * lo;
+            const uint32_t lb = gb - I[0];
+            const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4], sb_log2 = I[6], bd = I[7];
+            const tcg_v8_seg& S = segs[I[1] + (lb >> sb_log2)];
+            const uint32_t px = (lb % cols) * 8u, py = (lb / cols) * 8u;
+            if (px < vis_w && py < vis_h) {
+                R.ok = 1u;
+                R.Q = q + (size_t)S.qidx * 64u;
+                R.dst = out + (size_t)I[5] * 64u + (size_t)py * vis_w + px;
+                R.fc = recon_clamp(bd);
+                R.pitch = vis_w;
+                R.cw = min(8u, vis_w - px);
+                R.ch = min(8u, vis_h - py);
+                R.climit = 63u;
+                R.bd = bd;
+                R.vec = R.cw == 8u && (vis_w & 7u) == 0u;
             }
         }
+        sh.blk[threadIdx.x] = R;
     }
+    __syncthreads();
+    recon_blocks(sh, coef + (size_t)gb0 * 64u, nvalid);
 }
 
 // ------------------------------------------------------------------ chain, warp tiling
@@ -1014,73 +1191,49 @@ __global__ void __launch_bounds__(32) k_dchain_w(const DSlice* __restrict__ slic
 
 // The block's colour slice is found by a binary search over the colour slices,
 // which are in increasing order of their first block.
-__global__ void __launch_bounds__(128) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
+__global__ void __launch_bounds__(256) k_didct(const DSlice* __restrict__ slices, const uint32_t* __restrict__ cslices,
                                                uint32_t ncs,
                                                const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
                                                const uint8_t* __restrict__ tabs, const int32_t* __restrict__ coef,
                                                const int32_t* __restrict__ status, uint32_t total,
                                                uint16_t* __restrict__ out)
 {
-    const uint32_t gb = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gb >= total) { return; }
-    uint32_t lo = 0, hi = ncs - 1u;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi + 1u) >> 1;
-        if (slices[cslices[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1u; }
-    }
-    const uint32_t si = cslices[lo];
-    if (status[si] != 0) { return; }
-    const DSlice& S = slices[si];
-    const DPlane& P = planes[S.plane];
-    const uint32_t* Q = reinterpret_cast<const uint32_t*>(tabs + (size_t)slice_tab[si] * DTAB_BYTES + TAB_Q);
-    const uint32_t lb = gb - S.blk0;
-    const uint32_t bx = lb % S.cols, by = S.y0 + lb / S.cols;
-    const int64_t fc = P.bd <= 12u ? ((int64_t)1 << 25) : (((int64_t)1 << 25) * (int64_t)((1u << (P.bd - 1u)) - 1u)) / 2047;
-    int32_t c[64], xh[64];
-    const int4* src = reinterpret_cast<const int4*>(coef + (size_t)gb * 64u);
-    const uint32_t climit = P.climit;  // reduced delivery drops the high zigzag positions
-#pragma unroll
-    for (int i = 0; i < 16; ++i) {
-        const int4 v = src[i];
-        const int32_t vv[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int32_t lv = (i | j) == 0 ? vv[j] : unmap_s((uint32_t)vv[j]);
-            lv = (uint32_t)(i * 4 + j) <= climit ? lv : 0;
-            const int nat = k_zigzag[i * 4 + j];
-            int64_t f = (int64_t)lv * __ldg(Q + nat);
-            f = f > fc ? fc : (f < -fc ? -fc : f);
-            c[nat] = (int32_t)f;
-        }
-    }
-    idct8x8(c, xh);
-    const int32_t mid = 1 << (P.bd - 1u), maxv = (1 << P.bd) - 1;
-    const uint32_t px = bx * 8u, py = by * 8u;
-    const uint32_t cw = min(8u, P.vis_w - px), ch = min(8u, P.vis_h - py);
-    uint16_t* dst = out + P.out_off + (size_t)py * P.vis_w + px;
-    uint32_t pv[64];
-#pragma unroll
-    for (int i = 0; i < 64; ++i) {
-        const int32_t v = xh[i] + mid;
-        pv[i] = (uint32_t)(v < 0 ? 0 : (v > maxv ? maxv : v));
-    }
-    if (cw == 8u && ch == 8u && (P.vis_w & 7u) == 0u) {
-        // whole block, 16-byte aligned rows (planes start on 64-sample boundaries)
-#pragma unroll
-        for (int y = 0; y < 8; ++y) {
-            const uint4 r = make_uint4(pv[y * 8] | (pv[y * 8 + 1] << 16), pv[y * 8 + 2] | (pv[y * 8 + 3] << 16),
-                                       pv[y * 8 + 4] | (pv[y * 8 + 5] << 16), pv[y * 8 + 6] | (pv[y * 8 + 7] << 16));
-            *reinterpret_cast<uint4*>(dst + (size_t)y * P.vis_w) = r;
-        }
-    } else {
-#pragma unroll
-        for (int y = 0; y < 8; ++y) {
-#pragma unroll
-            for (int x = 0; x < 8; ++x) {
-                if ((uint32_t)y < ch && (uint32_t)x < cw) { dst[(size_t)y * P.vis_w + x] = (uint16_t)pv[y * 8 + x]; }
+    __shared__ RShared sh;
+    const uint32_t gb0 = blockIdx.x * RB_BLOCKS;
+    const uint32_t nvalid = min(RB_BLOCKS, total - gb0);
+    if (threadIdx.x < 64u) { sh.zz[threadIdx.x] = k_zigzag[threadIdx.x]; }
+    if (threadIdx.x < RB_BLOCKS) {
+        RBlock R;
+        R.ok = 0u;
+        const uint32_t gb = gb0 + threadIdx.x;
+        if (gb < total) {
+            uint32_t lo = 0, hi = ncs - 1u;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi + 1u) >> 1;
+                if (slices[cslices[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1u; }
+            }
+            const uint32_t si = cslices[lo];
+            if (status[si] == 0) {
+                const DSlice& S = slices[si];
+                const DPlane& P = planes[S.plane];
+                const uint32_t lb = gb - S.blk0;
+                const uint32_t px = (lb % S.cols) * 8u, py = (S.y0 + lb / S.cols) * 8u;
+                R.ok = 1u;
+                R.Q = reinterpret_cast<const uint32_t*>(tabs + (size_t)slice_tab[si] * DTAB_BYTES + TAB_Q);
+                R.dst = out + P.out_off + (size_t)py * P.vis_w + px;
+                R.fc = recon_clamp(P.bd);
+                R.pitch = P.vis_w;
+                R.cw = min(8u, P.vis_w - px);
+                R.ch = min(8u, P.vis_h - py);
+                R.climit = P.climit;  // reduced delivery drops the high zigzag positions
+                R.bd = P.bd;
+                R.vec = R.cw == 8u && (P.vis_w & 7u) == 0u;
             }
         }
+        sh.blk[threadIdx.x] = R;
     }
+    __syncthreads();
+    recon_blocks(sh, coef + (size_t)gb0 * 64u, nvalid);
 }
 
 // Scaled delivery (reference color_store.h:223-313 scaled samples,
@@ -1733,7 +1886,8 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
             std::lock_guard<std::mutex> g(g_tune_mu);
             g_tune[cls] = (int8_t)best;
         }
-        TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sl, d_cs, nc, d_st, d_pl, d_tab, d_coef,
+        TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sl, d_cs, nc, d_st, d_pl,
+                   d_tab, d_coef,
                    d_status, (uint32_t)nblk, d_out);
     }
     if (na > 0) {
@@ -2107,7 +2261,7 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
     TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
     const DevTables& T = tables();
     if (ntile > 0u) {
-        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, ntile, 256, 0, d_tl, d_pkt, T.crc, d_ok);
+        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, ntile, 1024, 0, d_tl, d_pkt, T.crc, d_ok);
         TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, ntile, 32, 0, d_tl, d_pkt, d_tab);
     }
     if (!wtile.empty()) {
@@ -2115,7 +2269,8 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
                    d_tab, d_coef, d_fail);
     }
     if (nblk > 0u) {
-        TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_sg, d_pi, nplanes, d_q, d_coef,
+        TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sg, d_pi, nplanes,
+                   d_q, d_coef,
                    (uint32_t)nblk, d_out);
     }
     for (uint32_t f = 0; f < count; ++f) {

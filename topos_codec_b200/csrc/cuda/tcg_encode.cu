@@ -1,8 +1,9 @@
 // tcg_encode.cu - V7-R2 intra encode on the GPU (any batch of frames).
 //
 // Pipeline (one stream, no host round trip until the packets are complete):
-//   k_fdct      8x8 blocks: edge-replicated load, level shift, exact integer
-//               forward DCT, dead-zone quantisation -> zigzag coefficients +
+//   k_fdct      8x8 blocks, 32 per CTA (k_fdct_wide: planes above 12 bits):
+//               edge-replicated load, level shift, exact integer forward
+//               DCT, dead-zone quantisation -> zigzag coefficients +
 //               non-zero mask                       (reference codec.c:1702-1848)
 //   k_tokens    DC residuals, run/level categories, per-slice histograms and
 //               joint context histograms, op counts  (codec.c:1702-1848, 2116-2151)
@@ -37,7 +38,28 @@ struct EPlane {
     int64_t fclamp;
     uint32_t seg0;       // V8: first global segment of the plane
     uint32_t sb_log2;    // V8: segment blocks log2 (0 for V7-R2 planes)
+    uint32_t Qm[64];     // division by Q[i]: multiplier and shifts (div_magic)
+    uint8_t Qsh[64];
 };
+
+// Exact division by an invariant divisor (Granlund and Montgomery, "Division
+// by invariant integers using multiplication", PLDI 1994, figure 4.1): with
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, every 32-bit n gives
+// n / d = (t + ((n - t) >> s1)) >> s2, t = umulhi(m, n), s1 = min(l, 1),
+// s2 = max(l - 1, 0). sh packs s1 << 5 | s2.
+static void div_magic(uint32_t d, uint32_t* m, uint8_t* sh)
+{
+    uint32_t l = 0;
+    while (l < 32u && (1ull << l) < (uint64_t)d) { ++l; }
+    *m = (uint32_t)(((1ull << 32) * ((1ull << l) - d)) / d + 1u);
+    *sh = (uint8_t)(l == 0u ? 0u : (1u << 5) | (l - 1u));
+}
+
+__device__ __forceinline__ uint32_t div_inv(uint32_t n, uint32_t m, uint32_t sh)
+{
+    const uint32_t t = __umulhi(m, n);
+    return (t + ((n - t) >> (sh >> 5))) >> (sh & 31u);
+}
 
 struct ESlice {
     uint32_t frame, plane, kind;
@@ -73,7 +95,128 @@ struct EWork {  // token-pass work item: a run of blocks of one colour slice
 
 // ============================== forward DCT ==============================
 
-__global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes, const uint32_t* __restrict__ cplanes,
+// Forward transform and quantisation of planes up to 12 bits, 32 blocks per
+// CTA of 256 threads: lane b of warp 0 finds block b's plane and position;
+// warp w then loads row w of all 32 blocks (lane = block: a warp reads 512
+// contiguous bytes when the blocks lie side by side, edge blocks replicate
+// the last column and row), runs the 8-point row pass, and after a barrier
+// the column pass of column w with the dead-zone quantisation of its eight
+// coefficients (quant.c:310-346; the division by an invariant divisor), which
+// land in zigzag order in shared memory; finally each thread stores two
+// 16-byte pieces of the CTA's 8 KB of coefficients and 16 lanes OR their
+// pieces' non-zero flags into the block's mask. Planes above 12 bits
+// (64-bit accumulation and predistortion) go to k_fdct_wide.
+constexpr uint32_t FB_BLOCKS = 32u;
+constexpr uint32_t FB_P = 65u;  // words per block in shared memory (odd: no bank conflicts)
+
+__global__ void __launch_bounds__(256) k_fdct(const EPlane* __restrict__ planes, const uint32_t* __restrict__ cplanes,
+                                              uint32_t ncp, uint32_t total, const uint16_t* __restrict__ pix,
+                                              int32_t* __restrict__ coef, uint64_t* __restrict__ mask)
+{
+    __shared__ int32_t sa[FB_BLOCKS * FB_P];   // row-pass output, natural order
+    __shared__ int32_t sq[FB_BLOCKS * FB_P];   // quantised, zigzag order
+    __shared__ uint32_t s_pl[FB_BLOCKS], s_bx[FB_BLOCKS], s_by[FB_BLOCKS];
+    __shared__ uint8_t s_zinv[64];
+    const uint32_t t = threadIdx.x, w = t >> 5, lane = t & 31u;
+    const uint32_t gb0 = blockIdx.x * FB_BLOCKS;
+    if (t < 64u) { s_zinv[k_zigzag[t]] = (uint8_t)t; }
+    if (t < FB_BLOCKS) {
+        const uint32_t gb = gb0 + t;
+        uint32_t pl = 0xFFFFFFFFu, bx = 0, by = 0;
+        if (gb < total) {
+            int lo = 0, hi = (int)ncp - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (planes[cplanes[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1; }
+            }
+            const EPlane& P = planes[cplanes[lo]];
+            if (P.bd <= 12u) {
+                pl = cplanes[lo];
+                const uint32_t lb = gb - P.blk0;
+                bx = lb % P.cols;
+                by = lb / P.cols;
+            }
+        }
+        s_pl[t] = pl; s_bx[t] = bx; s_by[t] = by;
+    }
+    __syncthreads();
+    const uint32_t b = lane;
+    const uint32_t pl = s_pl[b];
+    if (pl != 0xFFFFFFFFu) {  // row pass: row y = w
+        const EPlane& P = planes[pl];
+        const uint32_t bx = s_bx[b], by = s_by[b], y = w;
+        const uint32_t sy = min(by * 8u + y, P.vis_h - 1u);
+        const uint16_t* row = pix + P.pix_off + (size_t)sy * P.vis_w;
+        const int32_t mid = 1 << (P.bd - 1u);
+        uint32_t u[8];
+        // planes start on 64-sample boundaries: an inner block of a plane whose
+        // width is a multiple of 8 reads its row with one 16-byte load
+        if ((P.vis_w & 7u) == 0u && bx * 8u + 8u <= P.vis_w) {
+            const uint4 r = __ldg(reinterpret_cast<const uint4*>(row + bx * 8u));
+            u[0] = r.x & 0xFFFFu; u[1] = r.x >> 16; u[2] = r.y & 0xFFFFu; u[3] = r.y >> 16;
+            u[4] = r.z & 0xFFFFu; u[5] = r.z >> 16; u[6] = r.w & 0xFFFFu; u[7] = r.w >> 16;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) { u[k] = __ldg(row + min(bx * 8u + (uint32_t)k, P.vis_w - 1u)); }
+        }
+        int32_t x[8], A[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { x[k] = (int32_t)(int16_t)((int32_t)u[k] - mid); }
+        fwd8<int32_t>(x, A);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) { sa[b * FB_P + y * 8u + v] = A[v]; }
+    }
+    __syncthreads();
+    if (pl != 0xFFFFFFFFu) {  // column pass and quantisation: column v = w
+        const EPlane& P = planes[pl];
+        const uint32_t v = w;
+        int32_t col[8], F[8];
+#pragma unroll
+        for (int y = 0; y < 8; ++y) { col[y] = sa[b * FB_P + y * 8u + v]; }
+        fwd8<int32_t>(col, F);
+        const int64_t fc = P.fclamp;
+        const bool one = P.q_is_one != 0u;
+#pragma unroll
+        for (int uu = 0; uu < 8; ++uu) {
+            const uint32_t i = (uint32_t)uu * 8u + v;  // natural position
+            int64_t c = F[uu];
+            c = c > fc ? fc : (c < -fc ? -fc : c);
+            const uint32_t mag = (uint32_t)(c < 0 ? -c : c);
+            uint32_t qm;
+            if (one) {
+                qm = mag;
+            } else {
+                const uint32_t Q = P.Q[i];
+                const uint32_t dz = i == 0u ? 0u : Q >> 2;
+                const uint32_t num = mag + (Q >> 1);
+                qm = num > dz ? div_inv(num - dz, P.Qm[i], P.Qsh[i]) : 0u;
+            }
+            sq[b * FB_P + s_zinv[i]] = c < 0 ? -(int32_t)qm : (int32_t)qm;
+        }
+    }
+    __syncthreads();
+    // coefficients out, zigzag order, and the non-zero masks
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        const uint32_t idx = t + 256u * h;  // 16-byte piece of the CTA's coefficients
+        const uint32_t bb = idx >> 4, i0 = (idx & 15u) * 4u;
+        const bool live = s_pl[bb] != 0xFFFFFFFFu;
+        uint64_t m = 0;
+        if (live) {
+            int4 q;
+            q.x = sq[bb * FB_P + i0]; q.y = sq[bb * FB_P + i0 + 1u];
+            q.z = sq[bb * FB_P + i0 + 2u]; q.w = sq[bb * FB_P + i0 + 3u];
+            reinterpret_cast<int4*>(coef + (size_t)gb0 * 64u)[idx] = q;
+            m = (uint64_t)((q.x != 0) | ((q.y != 0) << 1) | ((q.z != 0) << 2) | ((q.w != 0) << 3)) << i0;
+        }
+        // the block's 16 pieces sit in 16 neighbouring lanes
+#pragma unroll
+        for (uint32_t d = 1; d < 16u; d <<= 1) { m |= __shfl_xor_sync(0xFFFFFFFFu, m, d); }
+        if (live && (idx & 15u) == 0u) { mask[gb0 + bb] = m & ~(uint64_t)1; }
+    }
+}
+
+__global__ void __launch_bounds__(128) k_fdct_wide(const EPlane* __restrict__ planes, const uint32_t* __restrict__ cplanes,
                                               uint32_t ncp, uint32_t total, const uint16_t* __restrict__ pix,
                                               int32_t* __restrict__ coef, uint64_t* __restrict__ mask)
 {
@@ -85,11 +228,12 @@ __global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes,
         if (planes[cplanes[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1; }
     }
     const EPlane& P = planes[cplanes[lo]];
+    if (P.bd <= 12u) { return; }  // k_fdct's blocks
     const uint32_t lb = gb - P.blk0;
     const uint32_t bx = lb % P.cols, by = lb / P.cols;
     const uint16_t* src = pix + P.pix_off;
     const int32_t mid = 1 << (P.bd - 1u);
-    const bool wide = P.bd > 12u;
+    const bool wide = true;
     int32_t x[64], F[64];
     // a block inside the visible plane with 16-byte aligned rows (planes start
     // on 64-sample boundaries) reads each row with one load; edge blocks
@@ -114,7 +258,7 @@ __global__ void __launch_bounds__(128) k_fdct(const EPlane* __restrict__ planes,
             x[y * 8 + k] = wide ? d : (int32_t)(int16_t)d;
         }
     }
-    if (!wide) { fdct8x8_i32(x, F); } else { fdct8x8_wide(x, F); }
+    fdct8x8_wide(x, F);
     // dead-zone quantisation (quant.c:310-346): q = sign*((|F|+Q/2-dz)/Q), dz = Q/4 (AC)
     int32_t q[64];
     const int64_t fc = P.fclamp;
@@ -357,9 +501,9 @@ __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slic
     }
     if (threadIdx.x == 0) { sres[si].nops = carry; }
     // identity operations (word 0) from the count up to the next multiple of
-    // 32, so the chain reads whole 32-operation iterations without masking
+    // 64, so the chain reads whole 64-operation iterations without masking
     // (a slice window holds 256 words past its largest count)
-    if (threadIdx.x < 32u && carry + threadIdx.x < ((carry + 31u) & ~31u)) {
+    if (threadIdx.x < 64u && carry + threadIdx.x < ((carry + 63u) & ~63u)) {
         ops[S.op_base + carry + threadIdx.x] = 0u;
     }
 }
@@ -500,9 +644,11 @@ __device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, c
     x = xn;
 }
 
-// Four consecutive operations of a slice (group g). The slice's window holds
-// identity operations from its count to the next multiple of 32, and every
-// group the chain loads lies within the window (at most 63 words past the count).
+// Four consecutive operations of a slice or segment (group g). Its window
+// holds identity operations from its count to the next multiple of the
+// chain's iteration (64 operations for k_chain, 32 for k_v8_chain), and every
+// group a chain loads lies within the window (at most 127 words past the count;
+// a window has 256 words to spare).
 __device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t)
 {
     return __ldg(op4 + g);
@@ -547,24 +693,34 @@ __global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict_
     uint8_t* const end = stage + S.stage_base + S.stage_cap;  // emitted byte k lives at end[-1-k]
     uint8_t* p = end;
     uint32_t x = RANS_L;
-    // eight groups (32 operations) in registers, each reloaded eight groups ahead
-    // of its use, and an L1 prefetch 512 bytes ahead
-    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops);
-    uint4 q2 = op_group(op4, 2u, nops), q3 = op_group(op4, 3u, nops);
-    uint4 q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
-    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops);
-    for (uint32_t g = 0; 4u * g < nops; g += 8u) {
-        const uint32_t pf = (uint32_t)(4u * (g + 32u) < nops);
+    // sixteen groups (64 operations) in registers, each reloaded sixteen groups
+    // ahead of its use, and an L1 prefetch 1 KB ahead
+    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops), q2 = op_group(op4, 2u, nops);
+    uint4 q3 = op_group(op4, 3u, nops), q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
+    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops), q8 = op_group(op4, 8u, nops);
+    uint4 q9 = op_group(op4, 9u, nops), q10 = op_group(op4, 10u, nops), q11 = op_group(op4, 11u, nops);
+    uint4 q12 = op_group(op4, 12u, nops), q13 = op_group(op4, 13u, nops), q14 = op_group(op4, 14u, nops);
+    uint4 q15 = op_group(op4, 15u, nops);
+    for (uint32_t g = 0; 4u * g < nops; g += 16u) {
+        const uint32_t pf = (uint32_t)(4u * (g + 64u) < nops);
         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
-                     :: "l"(op4 + g + 32u), "r"(pf));
-        ENC_GROUP(q0); q0 = op_group(op4, g + 8u, nops);
-        ENC_GROUP(q1); q1 = op_group(op4, g + 9u, nops);
-        ENC_GROUP(q2); q2 = op_group(op4, g + 10u, nops);
-        ENC_GROUP(q3); q3 = op_group(op4, g + 11u, nops);
-        ENC_GROUP(q4); q4 = op_group(op4, g + 12u, nops);
-        ENC_GROUP(q5); q5 = op_group(op4, g + 13u, nops);
-        ENC_GROUP(q6); q6 = op_group(op4, g + 14u, nops);
-        ENC_GROUP(q7); q7 = op_group(op4, g + 15u, nops);
+                     :: "l"(op4 + g + 64u), "r"(pf));
+        ENC_GROUP(q0); q0 = op_group(op4, g + 16u, nops);
+        ENC_GROUP(q1); q1 = op_group(op4, g + 17u, nops);
+        ENC_GROUP(q2); q2 = op_group(op4, g + 18u, nops);
+        ENC_GROUP(q3); q3 = op_group(op4, g + 19u, nops);
+        ENC_GROUP(q4); q4 = op_group(op4, g + 20u, nops);
+        ENC_GROUP(q5); q5 = op_group(op4, g + 21u, nops);
+        ENC_GROUP(q6); q6 = op_group(op4, g + 22u, nops);
+        ENC_GROUP(q7); q7 = op_group(op4, g + 23u, nops);
+        ENC_GROUP(q8); q8 = op_group(op4, g + 24u, nops);
+        ENC_GROUP(q9); q9 = op_group(op4, g + 25u, nops);
+        ENC_GROUP(q10); q10 = op_group(op4, g + 26u, nops);
+        ENC_GROUP(q11); q11 = op_group(op4, g + 27u, nops);
+        ENC_GROUP(q12); q12 = op_group(op4, g + 28u, nops);
+        ENC_GROUP(q13); q13 = op_group(op4, g + 29u, nops);
+        ENC_GROUP(q14); q14 = op_group(op4, g + 30u, nops);
+        ENC_GROUP(q15); q15 = op_group(op4, g + 31u, nops);
     }
     sres[si].nbytes = (uint32_t)(end - p);
     sres[si].xfin = x;
@@ -1331,15 +1487,15 @@ __global__ void __launch_bounds__(256) k_v8_copy(const EFrame* __restrict__ fram
     }
 }
 
-// One block per tile: the 350-byte table (flags, five DC rows, run row, five
+// One 1024-thread block per tile: the 350-byte table (flags, five DC rows, run row, five
 // level rows; rows past the model's contexts are the all-zero row {1, 0, ...},
 // codec.c:3949-3971), then the CRC of the table and the member streams.
-__global__ void __launch_bounds__(256) k_v8_tiles(const EFrame* __restrict__ frames, const VTile* __restrict__ tiles,
-                                                  const ESliceRes* __restrict__ tres, const uint8_t* __restrict__ prefix,
-                                                  const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
+__global__ void __launch_bounds__(1024) k_v8_tiles(const EFrame* __restrict__ frames, const VTile* __restrict__ tiles,
+                                                   const ESliceRes* __restrict__ tres, const uint8_t* __restrict__ prefix,
+                                                   const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
 {
     __shared__ uint32_t t[8 * 256];
-    __shared__ uint32_t scratch[512];
+    __shared__ uint32_t scratch[2 * 1024];
     __shared__ uint32_t crc_tab;
     for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
     const uint32_t ti = blockIdx.x;
@@ -1416,7 +1572,11 @@ static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count
             P.blk0 = (uint32_t)nblk;
             P.fclamp = I.fclamp;
             P.q_is_one = 1u;
-            for (int i = 0; i < 64; ++i) { P.Q[i] = I.Q[i]; if (I.Q[i] != 1u) { P.q_is_one = 0u; } }
+            for (int i = 0; i < 64; ++i) {
+                P.Q[i] = I.Q[i];
+                if (I.Q[i] != 1u) { P.q_is_one = 0u; }
+                div_magic(I.Q[i] != 0u ? I.Q[i] : 1u, &P.Qm[i], &P.Qsh[i]);
+            }
             const uint32_t pg = (uint32_t)planes.size();
             if (I.kind == TCG_PLANE_COLOR) {
                 cplanes.push_back(pg);
@@ -1564,8 +1724,14 @@ static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count
         TCG_CHECK(cudaEventRecord(C->ajoin, as));
     }
     if (nblk > 0) {
-        TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)cplanes.size(),
-                   (uint32_t)nblk, d_pix, d_coef, d_mask);
+        bool any_wide = false;
+        for (uint32_t pg : cplanes) { any_wide = any_wide || planes[pg].bd > 12u; }
+        TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + FB_BLOCKS - 1u) / FB_BLOCKS), 256, 0, d_pl, d_cp,
+                   (uint32_t)cplanes.size(), (uint32_t)nblk, d_pix, d_coef, d_mask);
+        if (any_wide) {
+            TCG_LAUNCH(C, K_FDCT, k_fdct_wide, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp,
+                       (uint32_t)cplanes.size(), (uint32_t)nblk, d_pix, d_coef, d_mask);
+        }
         const size_t tok_smem = H_BINS * 32u * 4u;
         static bool attr_set = false;
         if (!attr_set) {
@@ -1641,7 +1807,11 @@ static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t co
             P.blk0 = (uint32_t)nblk;
             P.fclamp = I.fclamp;
             P.q_is_one = 1u;
-            for (int i = 0; i < 64; ++i) { P.Q[i] = I.Q[i]; if (I.Q[i] != 1u) { P.q_is_one = 0u; } }
+            for (int i = 0; i < 64; ++i) {
+                P.Q[i] = I.Q[i];
+                if (I.Q[i] != 1u) { P.q_is_one = 0u; }
+                div_magic(I.Q[i] != 0u ? I.Q[i] : 1u, &P.Qm[i], &P.Qsh[i]);
+            }
             P.seg0 = (uint32_t)segs.size();
             P.sb_log2 = F.v8_sb_log2;
             const uint32_t pg = (uint32_t)planes.size();
@@ -1794,8 +1964,14 @@ static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t co
     uint32_t* d_ops = dptr<uint32_t>(C, B_OPS);
     uint8_t* d_stage = dptr<uint8_t>(C, B_STAGE);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_PKT);
-    TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)planes.size(),
-               (uint32_t)nblk, d_pix, d_coef, d_mask);
+    bool any_wide = false;
+    for (const EPlane& P : planes) { any_wide = any_wide || P.bd > 12u; }
+    TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + FB_BLOCKS - 1u) / FB_BLOCKS), 256, 0, d_pl, d_cp,
+               (uint32_t)planes.size(), (uint32_t)nblk, d_pix, d_coef, d_mask);
+    if (any_wide) {
+        TCG_LAUNCH(C, K_FDCT, k_fdct_wide, (uint32_t)((nblk + 127u) / 128u), 128, 0, d_pl, d_cp, (uint32_t)planes.size(),
+                   (uint32_t)nblk, d_pix, d_coef, d_mask);
+    }
     const size_t tok_smem = H_BINS * 32u * 4u;
     static bool attr_set = false;
     if (!attr_set) {
@@ -1817,7 +1993,7 @@ static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t co
     }
     TCG_LAUNCH(C, K_PACK_SIZES, k_v8_sizes, count, 1024, 0, d_fr, d_vp, d_sg, d_sres, d_tl, d_tres, d_fres, d_pkt, d_ex);
     TCG_LAUNCH(C, K_PACK_COPY, k_v8_copy, (nseg + 7u) / 8u, 256, 0, d_fr, d_vp, d_sg, nseg, d_sres, d_stage, d_pkt);
-    TCG_LAUNCH(C, K_PACK_CRC, k_v8_tiles, nt, 256, 0, d_fr, d_tl, d_tres, d_prefix, Tb.crc, d_pkt);
+    TCG_LAUNCH(C, K_PACK_CRC, k_v8_tiles, nt, 1024, 0, d_fr, d_tl, d_tres, d_prefix, Tb.crc, d_pkt);
     TCG_LAUNCH(C, K_PACK_HEADER, k_pack_header, (count + 127u) / 128u, 128, 0, d_fr, count, d_fres, Tb.crc, d_pkt);
     TCG_CHECK(cudaGetLastError());
     EFrameRes* hf = (EFrameRes*)C->h[1].p;

@@ -19,9 +19,10 @@ static DevTables g_tab;
 // buffer frees and allocates in the order of the context's own stream, so it
 // never synchronises the device (cudaMalloc / cudaFree do, and with several
 // calls in flight - the request server's workers - that stalls all of them).
-// The pool keeps what is freed (release threshold at the maximum) until
-// trim_idle returns idle contexts' memory.
+// At each synchronisation the pool gives memory freed this way back to the
+// device beyond POOL_KEEP bytes; trim_idle returns idle contexts' buffers.
 static cudaMemPool_t g_pool = nullptr;
+static constexpr uint64_t POOL_KEEP = 2ull << 30;
 static std::atomic<uint64_t> g_launches{0};
 static std::atomic<uint64_t> g_allocs{0};  // device and pinned host allocations made
 static std::atomic<int> g_prof_on{0};
@@ -293,7 +294,7 @@ static bool init_locked(int device)
             tcg_host_set_error(TCG_ERR_OUT_OF_MEMORY, "device memory pool creation failed");
             return false;
         }
-        uint64_t keep = UINT64_MAX;
+        uint64_t keep = POOL_KEEP;
         cudaMemPoolSetAttribute(g_pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     g_tab.div_m = (const uint32_t*)(d + om);

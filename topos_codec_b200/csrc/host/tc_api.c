@@ -781,6 +781,8 @@ TC_EXPORT int32_t tc_frame_decode_batch(const topos_batch_packet* packets, uint3
 
 TC_EXPORT int32_t tcg_device_init(int32_t device) { return tcg_init(device); }
 TC_EXPORT void tcg_device_release(void) { tcg_shutdown(); }
+
+TC_EXPORT void tcg_release_idle_memory(void) { tcg_trim_idle(); }
 TC_EXPORT uint64_t tcg_kernel_launches(void) { return tcg_launch_count(); }
 TC_EXPORT double tcg_last_device_ms(void) { return tcg_last_ms(); }
 TC_EXPORT uint32_t tcg_pipeline_plan(int32_t decode, const uint64_t* frame_bytes, uint32_t count, uint32_t* starts)

@@ -253,7 +253,8 @@ TC_EXPORT int32_t tc_frame_decode_reduced(const uint8_t* data, size_t size, tc_d
     if ((int32_t)scale < 0 || scale > TC_DECODE_SCALE_EIGHTH) {
         return tc_fail(TC_ERR_INVALID_ARGUMENT, "invalid decode scale dimensions");
     }
-    (void)info_reset(out_info);
+    /* out_info is written only once the packet's structure parses
+     * (codec.c:9602-9612); a V8 packet fails that parse */
     const fixed_plan f = {1u, 0u, 0u, 63u, (uint32_t)scale};
     return decode_one(data, size, planes_out, strides, out_info, reduced_resolve, &f);
 }

@@ -11,7 +11,10 @@
 // GPU instead of waiting for them. Admission: a batch takes requests while
 // the estimated device bytes of everything in flight fit the server's budget
 // and the device's free memory (the first request of a batch always goes, so
-// one large request cannot stall the queue). V8 decodes run through the
+// one large request cannot stall the queue). Call contexts keep the buffers
+// of their largest batch; when a batch leaves less than an eighth of the
+// device's memory free, the worker gives idle contexts' buffers back, so the
+// server leaves room for the process's other allocations. V8 decodes run through the
 // single-frame V8 decoder (the batched decode takes V7 packets only, as the
 // reference's does). Each request's latency is measured from submission to
 // completion.
@@ -27,6 +30,7 @@
 #include <vector>
 
 extern "C" {
+#include "../tcg_device.h"
 #include "tc_internal.h"
 }
 
@@ -78,22 +82,26 @@ struct tcg_server {
 
 namespace {
 
-// device bytes one frame of w x h luma samples needs while it is coded
-// (samples, coefficients, operation words, staging, packet for encode;
-// packet, coefficients, tables, planes for decode), rounded up
+// device bytes one frame of w x h luma samples needs while it is coded, with
+// the buffers' growth margin: per 8x8 block of a 4:2:2 frame (two blocks per
+// 64 luma samples) encode holds 128 B of samples, 256 B of coefficients,
+// 12 B of mask and DC, 1 KB of operation words, 512 B of staging and the
+// packet; decode the packet, 256 B of coefficients, 128 B of planes and the
+// slice tables
 uint64_t frame_bytes(uint32_t w, uint32_t h, bool encode)
 {
     const uint64_t px = (uint64_t)w * h;
-    return encode ? px * 40u + (1u << 20) : px * 20u + (1u << 20);
+    return encode ? px * 84u + (1u << 20) : px * 20u + (1u << 20);
 }
 
-uint64_t device_free()
+uint64_t device_free(uint64_t* total = nullptr)
 {
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
+    if (total != nullptr) { *total = tot; }
     return fr;
 }
 
@@ -203,6 +211,9 @@ void worker(tcg_server* s, bool encode)
             if (!q.empty()) { s->cv_work.notify_all(); }  // more for the next idle worker
         }
         run_batch(s, batch, encode);
+        uint64_t total = 0;
+        const uint64_t fr = device_free(&total);
+        if (total != 0u && fr < total / 8u) { tcg_trim_idle(); }
         std::lock_guard<std::mutex> g(s->mu);
         s->inflight -= used;
         if (!q.empty()) { s->cv_work.notify_all(); }

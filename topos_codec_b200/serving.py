@@ -11,7 +11,8 @@ The load generator is open-loop: arrivals follow their schedule whatever the
 server does. Input planes and packets are shared, read-only, per (resolution,
 tier); every request gets its own output buffer from a pool that is provisioned
 before the stream for half a second of arrivals and grows when all are in
-use, so a busy server never delays the next arrival. Latency runs
+use, so a busy server never delays the next arrival. Past saturation an
+arrival that finds 512 requests unfinished is shed and counted as dropped. Latency runs
 from a request's scheduled arrival to the moment its completion is seen
 (the generator's lag before submitting it plus the server's own
 submission-to-completion time, which is also reported alone). Percentiles are given for the whole stream and per resolution and
@@ -51,8 +52,10 @@ class _Kind:
         self.torch, self.dev = torch, dev
         planes = synth.make_frame(w, h, seed=seed, frame=0, device=dev)
         self.planes = [p.to(torch.uint16).contiguous() for p in planes]
-        self.cap = codec.packet_bound(self.cfg)
         pkt = codec.encode(self.cfg, [p.cpu().numpy() for p in self.planes])
+        # every request of this kind codes the same planes, so its packet has
+        # this size; the margin keeps the buffers far below the packet bound
+        self.cap = min(codec.packet_bound(self.cfg), len(pkt) + (1 << 20))
         self.pkt = torch.frombuffer(bytearray(pkt), dtype=torch.uint8).to(dev)
         self.free_out: List = []
         self.free_dec: List = []
@@ -89,9 +92,13 @@ def _kinds(codec, torch, dev, seed, generation):
 
 
 def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batch_frames: int = 32,
-              generation: str = "v7", workers: int = 4, kinds=None, resolutions=None) -> Dict:
+              generation: str = "v7", workers: int = 4, kinds=None, resolutions=None,
+              max_outstanding: int = 512) -> Dict:
     """Submit a Poisson request stream at rate_rps for duration_s; returns the
-    latency percentiles (whole stream, per resolution, per direction)."""
+    latency percentiles (whole stream, per resolution, per direction). An
+    arrival that finds max_outstanding requests unfinished is shed (counted
+    in "dropped", not submitted): past saturation the backlog would otherwise
+    grow without bound."""
     import torch
     dev = torch.device("cuda", torch.cuda.current_device())
     rng = random.Random(seed)
@@ -139,6 +146,7 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
     t0 = time.perf_counter()
     t_next = t0
     n = 0
+    dropped = 0
     try:
         while True:
             t_next += rng.expovariate(rate_rps)
@@ -152,6 +160,9 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
                 time.sleep(delay)
             k = kinds[key]
             with cv:
+                if len(pending) >= max_outstanding:
+                    dropped += 1
+                    continue
                 buf = k.out() if enc else k.dec()
             t_sub = time.perf_counter()
             if enc:
@@ -170,7 +181,7 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
         srv.close()
     wall = time.perf_counter() - t0
     out = {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
-           "errors": errors[0], "generation": generation}
+           "errors": errors[0], "dropped": dropped, "generation": generation}
     out.update(_summary([r[2] for r in records]))
     out["server_side"] = _summary([r[3] for r in records])
     out["by_resolution"] = {f"{w}x{h}": _summary([r[2] for r in records if r[0] == (w, h)]) for (w, h), _ in res_mix}
