@@ -737,13 +737,12 @@ constexpr uint32_t V8D_SMEM = V8D_CUM + DCH_CUM_BYTES;
 // width and height, output offset / 64, segment blocks log2, bit depth
 constexpr uint32_t V8_PINFO = 8u;
 
-// one 1024-thread block per tile (a frame has few tiles, ~1 MB each at
-// 3840x2160): CRC of the table and the member streams against the stored one
-__global__ void __launch_bounds__(1024) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
-                                                  const uint32_t* __restrict__ crctab, uint8_t* __restrict__ ok)
+// one block per tile: CRC of the table and the member streams against the stored one
+__global__ void __launch_bounds__(256) k_v8_tcrc(const tcg_v8_tile* __restrict__ tiles, const uint8_t* __restrict__ pkt,
+                                                 const uint32_t* __restrict__ crctab, uint8_t* __restrict__ ok)
 {
     __shared__ uint32_t t[8 * 256];
-    __shared__ uint32_t scratch[2 * 1024];
+    __shared__ uint32_t scratch[512];
     __shared__ uint32_t c_tab;
     for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
     __syncthreads();
@@ -2261,7 +2260,7 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
     TCG_CHECK(cudaMemsetAsync(d_coef, 0, nblk * 256u, st));
     const DevTables& T = tables();
     if (ntile > 0u) {
-        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, ntile, 1024, 0, d_tl, d_pkt, T.crc, d_ok);
+        TCG_LAUNCH(C, K_DCRC, k_v8_tcrc, ntile, 256, 0, d_tl, d_pkt, T.crc, d_ok);
         TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, ntile, 32, 0, d_tl, d_pkt, d_tab);
     }
     if (!wtile.empty()) {

@@ -501,9 +501,9 @@ __global__ void __launch_bounds__(1024) k_opscan(const ESlice* __restrict__ slic
     }
     if (threadIdx.x == 0) { sres[si].nops = carry; }
     // identity operations (word 0) from the count up to the next multiple of
-    // 64, so the chain reads whole 64-operation iterations without masking
+    // 32, so the chain reads whole 32-operation iterations without masking
     // (a slice window holds 256 words past its largest count)
-    if (threadIdx.x < 64u && carry + threadIdx.x < ((carry + 63u) & ~63u)) {
+    if (threadIdx.x < 32u && carry + threadIdx.x < ((carry + 31u) & ~31u)) {
         ops[S.op_base + carry + threadIdx.x] = 0u;
     }
 }
@@ -646,9 +646,9 @@ __device__ __forceinline__ void enc_step(uint32_t& x, uint8_t*& p, uint32_t o, c
 
 // Four consecutive operations of a slice or segment (group g). Its window
 // holds identity operations from its count to the next multiple of the
-// chain's iteration (64 operations for k_chain, 32 for k_v8_chain), and every
-// group a chain loads lies within the window (at most 127 words past the count;
-// a window has 256 words to spare).
+// chain's iteration (32 operations), and every group a chain loads lies
+// within the window (at most 63 words past the count; a window has 256 words
+// to spare).
 __device__ __forceinline__ uint4 op_group(const uint4* __restrict__ op4, uint32_t g, uint32_t)
 {
     return __ldg(op4 + g);
@@ -693,34 +693,24 @@ __global__ void __launch_bounds__(CHAIN_LANES) k_chain(const ESlice* __restrict_
     uint8_t* const end = stage + S.stage_base + S.stage_cap;  // emitted byte k lives at end[-1-k]
     uint8_t* p = end;
     uint32_t x = RANS_L;
-    // sixteen groups (64 operations) in registers, each reloaded sixteen groups
-    // ahead of its use, and an L1 prefetch 1 KB ahead
-    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops), q2 = op_group(op4, 2u, nops);
-    uint4 q3 = op_group(op4, 3u, nops), q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
-    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops), q8 = op_group(op4, 8u, nops);
-    uint4 q9 = op_group(op4, 9u, nops), q10 = op_group(op4, 10u, nops), q11 = op_group(op4, 11u, nops);
-    uint4 q12 = op_group(op4, 12u, nops), q13 = op_group(op4, 13u, nops), q14 = op_group(op4, 14u, nops);
-    uint4 q15 = op_group(op4, 15u, nops);
-    for (uint32_t g = 0; 4u * g < nops; g += 16u) {
-        const uint32_t pf = (uint32_t)(4u * (g + 64u) < nops);
+    // eight groups (32 operations) in registers, each reloaded eight groups ahead
+    // of its use, and an L1 prefetch 512 bytes ahead
+    uint4 q0 = op_group(op4, 0u, nops), q1 = op_group(op4, 1u, nops);
+    uint4 q2 = op_group(op4, 2u, nops), q3 = op_group(op4, 3u, nops);
+    uint4 q4 = op_group(op4, 4u, nops), q5 = op_group(op4, 5u, nops);
+    uint4 q6 = op_group(op4, 6u, nops), q7 = op_group(op4, 7u, nops);
+    for (uint32_t g = 0; 4u * g < nops; g += 8u) {
+        const uint32_t pf = (uint32_t)(4u * (g + 32u) < nops);
         asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %1, 0;\n\t@p prefetch.global.L1 [%0];\n\t}"
-                     :: "l"(op4 + g + 64u), "r"(pf));
-        ENC_GROUP(q0); q0 = op_group(op4, g + 16u, nops);
-        ENC_GROUP(q1); q1 = op_group(op4, g + 17u, nops);
-        ENC_GROUP(q2); q2 = op_group(op4, g + 18u, nops);
-        ENC_GROUP(q3); q3 = op_group(op4, g + 19u, nops);
-        ENC_GROUP(q4); q4 = op_group(op4, g + 20u, nops);
-        ENC_GROUP(q5); q5 = op_group(op4, g + 21u, nops);
-        ENC_GROUP(q6); q6 = op_group(op4, g + 22u, nops);
-        ENC_GROUP(q7); q7 = op_group(op4, g + 23u, nops);
-        ENC_GROUP(q8); q8 = op_group(op4, g + 24u, nops);
-        ENC_GROUP(q9); q9 = op_group(op4, g + 25u, nops);
-        ENC_GROUP(q10); q10 = op_group(op4, g + 26u, nops);
-        ENC_GROUP(q11); q11 = op_group(op4, g + 27u, nops);
-        ENC_GROUP(q12); q12 = op_group(op4, g + 28u, nops);
-        ENC_GROUP(q13); q13 = op_group(op4, g + 29u, nops);
-        ENC_GROUP(q14); q14 = op_group(op4, g + 30u, nops);
-        ENC_GROUP(q15); q15 = op_group(op4, g + 31u, nops);
+                     :: "l"(op4 + g + 32u), "r"(pf));
+        ENC_GROUP(q0); q0 = op_group(op4, g + 8u, nops);
+        ENC_GROUP(q1); q1 = op_group(op4, g + 9u, nops);
+        ENC_GROUP(q2); q2 = op_group(op4, g + 10u, nops);
+        ENC_GROUP(q3); q3 = op_group(op4, g + 11u, nops);
+        ENC_GROUP(q4); q4 = op_group(op4, g + 12u, nops);
+        ENC_GROUP(q5); q5 = op_group(op4, g + 13u, nops);
+        ENC_GROUP(q6); q6 = op_group(op4, g + 14u, nops);
+        ENC_GROUP(q7); q7 = op_group(op4, g + 15u, nops);
     }
     sres[si].nbytes = (uint32_t)(end - p);
     sres[si].xfin = x;
@@ -1487,15 +1477,15 @@ __global__ void __launch_bounds__(256) k_v8_copy(const EFrame* __restrict__ fram
     }
 }
 
-// One 1024-thread block per tile: the 350-byte table (flags, five DC rows, run row, five
+// One block per tile: the 350-byte table (flags, five DC rows, run row, five
 // level rows; rows past the model's contexts are the all-zero row {1, 0, ...},
 // codec.c:3949-3971), then the CRC of the table and the member streams.
-__global__ void __launch_bounds__(1024) k_v8_tiles(const EFrame* __restrict__ frames, const VTile* __restrict__ tiles,
-                                                   const ESliceRes* __restrict__ tres, const uint8_t* __restrict__ prefix,
-                                                   const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
+__global__ void __launch_bounds__(256) k_v8_tiles(const EFrame* __restrict__ frames, const VTile* __restrict__ tiles,
+                                                  const ESliceRes* __restrict__ tres, const uint8_t* __restrict__ prefix,
+                                                  const uint32_t* __restrict__ crctab, uint8_t* __restrict__ pkt)
 {
     __shared__ uint32_t t[8 * 256];
-    __shared__ uint32_t scratch[2 * 1024];
+    __shared__ uint32_t scratch[512];
     __shared__ uint32_t crc_tab;
     for (uint32_t i = threadIdx.x; i < 8u * 256u; i += blockDim.x) { t[i] = crctab[i]; }
     const uint32_t ti = blockIdx.x;
@@ -1993,7 +1983,7 @@ static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t co
     }
     TCG_LAUNCH(C, K_PACK_SIZES, k_v8_sizes, count, 1024, 0, d_fr, d_vp, d_sg, d_sres, d_tl, d_tres, d_fres, d_pkt, d_ex);
     TCG_LAUNCH(C, K_PACK_COPY, k_v8_copy, (nseg + 7u) / 8u, 256, 0, d_fr, d_vp, d_sg, nseg, d_sres, d_stage, d_pkt);
-    TCG_LAUNCH(C, K_PACK_CRC, k_v8_tiles, nt, 1024, 0, d_fr, d_tl, d_tres, d_prefix, Tb.crc, d_pkt);
+    TCG_LAUNCH(C, K_PACK_CRC, k_v8_tiles, nt, 256, 0, d_fr, d_tl, d_tres, d_prefix, Tb.crc, d_pkt);
     TCG_LAUNCH(C, K_PACK_HEADER, k_pack_header, (count + 127u) / 128u, 128, 0, d_fr, count, d_fres, Tb.crc, d_pkt);
     TCG_CHECK(cudaGetLastError());
     EFrameRes* hf = (EFrameRes*)C->h[1].p;
