@@ -677,6 +677,8 @@ def main():
                  "at_half_plain_saturation": serving.run_trace_plain(gpu, rate_rps=0.5 * psat, duration_s=plain_s,
                                                                      kinds=kinds)}
         del kinds
+        torch.cuda.empty_cache()
+        gpu._lib.tcg_release_idle_memory()
         # the same stream coded as V8 (segmented rANS): many short chains per frame
         k8 = serving._kinds(gpu, torch, dev, 0, "v8")
         sat8 = serving.saturation_rps(gpu, generation="v8", kinds=k8)

@@ -866,7 +866,7 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
 __global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
                                                   uint32_t nplanes, const uint32_t* __restrict__ q,
                                                   const int32_t* __restrict__ coef, uint32_t total,
-                                                  uint16_t* __restrict__ out)
+                                                  const uint32_t* __restrict__ umap, uint16_t* __restrict__ out)
 {
     __shared__ RShared sh;
     const uint32_t gb0 = blockIdx.x * RB_BLOCKS;
@@ -877,12 +877,7 @@ __global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__
         R.ok = 0u;
         const uint32_t gb = gb0 + threadIdx.x;
         if (gb < total) {
-            uint32_t lo = 0, hi = nplanes - 1u;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1u) >> 1;
-                if (pinfo[V8_PINFO * mid] <= gb) { lo = mid; } else { hi = mid - 1u; }
-            }
-            const uint32_t* I = pinfo + V8_PINFO * lo;
+            const uint32_t* I = pinfo + V8_PINFO * unit_of(pinfo, V8_PINFO, nplanes, umap[blockIdx.x], gb);
             const uint32_t lb = gb - I[0];
             const uint32_t cols = I[2], vis_w = I[3], vis_h = I[4], sb_log2 = I[6], bd = I[7];
             const tcg_v8_seg& S = segs[I[1] + (lb >> sb_log2)];
@@ -1195,6 +1190,7 @@ __global__ void __launch_bounds__(256) k_didct(const DSlice* __restrict__ slices
                                                const uint32_t* __restrict__ slice_tab, const DPlane* __restrict__ planes,
                                                const uint8_t* __restrict__ tabs, const int32_t* __restrict__ coef,
                                                const int32_t* __restrict__ status, uint32_t total,
+                                               const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ umap,
                                                uint16_t* __restrict__ out)
 {
     __shared__ RShared sh;
@@ -1206,12 +1202,7 @@ __global__ void __launch_bounds__(256) k_didct(const DSlice* __restrict__ slices
         R.ok = 0u;
         const uint32_t gb = gb0 + threadIdx.x;
         if (gb < total) {
-            uint32_t lo = 0, hi = ncs - 1u;
-            while (lo < hi) {
-                const uint32_t mid = (lo + hi + 1u) >> 1;
-                if (slices[cslices[mid]].blk0 <= gb) { lo = mid; } else { hi = mid - 1u; }
-            }
-            const uint32_t si = cslices[lo];
+            const uint32_t si = cslices[unit_of(cstart, 1u, ncs, umap[blockIdx.x], gb)];
             if (status[si] == 0) {
                 const DSlice& S = slices[si];
                 const DPlane& P = planes[S.plane];
@@ -1699,8 +1690,10 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const size_t desc = align_up(planes.size() * sizeof(DPlane), 256) + align_up(ns * sizeof(DSlice), 256) +
                         align_up((size_t)(nc + na) * 4u + 16, 256) + align_up((size_t)ns * 4u + 16, 256) +
                         align_up(dbp.size() * sizeof(DbPlane) + 16, 256) +
-                        align_up((size_t)nc * 4u + 16, 256) + align_up(decim.size() * sizeof(DecimPlane) + 16, 256);
+                        align_up((size_t)nc * 4u + 16, 256) + align_up(decim.size() * sizeof(DecimPlane) + 16, 256) +
+                        align_up((size_t)nc * 4u + 16, 256);
     if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_UMAP, (nblk + 31u) / 32u * 4u + 256) ||
         !dreserve(C, B_DEC_TAB, (size_t)nc * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
         !dreserve(C, B_DEC_RES, (size_t)ns * 4u + 256) || !dreserve(C, B_ALPHA, alpha_res * 4u + 256) ||
         !dreserve(C, B_DESC, desc + 256) || !hreserve(C, 0, desc + 256) || !hreserve(C, 1, (size_t)ns * 4u + 256)) {
@@ -1728,6 +1721,9 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const size_t o_db = put(dbp.data(), dbp.size() * sizeof(DbPlane));
     const size_t o_or = put(ord.data(), ord.size() * 4u);
     const size_t o_dm = put(decim.data(), decim.size() * sizeof(DecimPlane));
+    std::vector<uint32_t> cstart(nc);  // first block of each colour slice, for the reconstruction's unit lookup
+    for (uint32_t i = 0; i < nc; ++i) { cstart[i] = slices[cslices[i]].blk0; }
+    const size_t o_cb = put(cstart.data(), (size_t)nc * 4u);
     TCG_CHECK(cudaMemcpyAsync(dd, hd, o, cudaMemcpyHostToDevice, st));
     const DPlane* d_pl = (const DPlane*)(dd + o_pl);
     const DSlice* d_sl = (const DSlice*)(dd + o_sl);
@@ -1737,6 +1733,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
     const DbPlane* d_db = (const DbPlane*)(dd + o_db);
     const uint32_t* d_ord = (const uint32_t*)(dd + o_or);
     const DecimPlane* d_dm = (const DecimPlane*)(dd + o_dm);
+    const uint32_t* d_cb = (const uint32_t*)(dd + o_cb);
     uint8_t* d_pkt = dptr<uint8_t>(C, B_DEC_PKT);
     call_begin(C);
     if (after != nullptr) { TCG_CHECK(cudaStreamWaitEvent(st, after, 0)); }
@@ -1885,9 +1882,10 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
             std::lock_guard<std::mutex> g(g_tune_mu);
             g_tune[cls] = (int8_t)best;
         }
+        uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
+        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (nc + 255u) / 256u, 256, 0, d_cb, 1u, nc, (uint32_t)nblk, d_umap);
         TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sl, d_cs, nc, d_st, d_pl,
-                   d_tab, d_coef,
-                   d_status, (uint32_t)nblk, d_out);
+                   d_tab, d_coef, d_status, (uint32_t)nblk, d_cb, d_umap, d_out);
     }
     if (na > 0) {
         // the alpha planes have been on their own stream since the CRC check
@@ -2218,6 +2216,7 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
                         align_up(pinfo.size() * 4u + 16u, 256);
     const size_t resb = align_up((size_t)nseg + 16u, 256) + align_up((size_t)ntile + 16u, 256);
     if (!dreserve(C, B_DEC_PKT, pkt_bytes + 256) || !dreserve(C, B_DEC_COEF, nblk * 256u + 256) ||
+        !dreserve(C, B_UMAP, (nblk + 31u) / 32u * 4u + 256) ||
         !dreserve(C, B_DEC_TAB, (size_t)ntile * DTAB_BYTES + 256) || !dreserve(C, B_DEC_OUT, out_elems * 2u + 256) ||
         !dreserve(C, B_DEC_RES, resb) || !dreserve(C, B_DESC, desc) || !hreserve(C, 0, desc) || !hreserve(C, 1, resb)) {
         return TCG_ERR_OUT_OF_MEMORY;
@@ -2268,9 +2267,11 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
                    d_tab, d_coef, d_fail);
     }
     if (nblk > 0u) {
+        uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
+        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (nplanes + 255u) / 256u, 256, 0, d_pi, V8_PINFO, nplanes, (uint32_t)nblk,
+                   d_umap);
         TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sg, d_pi, nplanes,
-                   d_q, d_coef,
-                   (uint32_t)nblk, d_out);
+                   d_q, d_coef, (uint32_t)nblk, d_umap, d_out);
     }
     for (uint32_t f = 0; f < count; ++f) {
         for (uint32_t p = 0; p < 3u; ++p) {

@@ -32,7 +32,7 @@ static thread_local double t_last_ms = 0.0;
 static const char* k_names[K_COUNT] = {
     "k_fdct", "k_tokens", "k_select", "k_opscan", "k_opgen", "k_chain", "k_alpha", "k_pack_sizes", "k_pack_copy",
     "k_pack_crc", "k_pack_header", "k_dcrc", "k_dtables", "k_dchain", "k_dchain_w", "k_didct", "k_dalpha", "k_dalpha_med",
-    "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk", "k_decimate"};
+    "k_dconceal", "k_deblock_v", "k_deblock_h", "k_walk", "k_decimate", "k_unit_map"};
 
 void note_launch(uint32_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
@@ -195,7 +195,7 @@ int32_t cuda_fail(cudaError_t e, const char* what)
 
 // rANS division magic: q = umulhi(2x, m) >> l equals floor(x / f) for every
 // x < 2^31 and 1 <= f <= 4096, with l = ceil(log2 f), m = ceil(2^(31+l) / f)
-// (m < 2^32 for all such f; proof in the DESIGN notes and an exhaustive host test).
+// (m < 2^32 for all such f).
 static void build_div(uint32_t* m, uint8_t* l)
 {
     m[0] = 0; l[0] = 0;
@@ -355,8 +355,17 @@ void ctx_release(Ctx* c)
 // first run dry); the next call on such a context allocates again.
 void trim_idle()
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    for (Ctx* c = g_free; c != nullptr; c = c->next) {
+    // take the idle contexts off the free list, so that calls on other threads
+    // lease fresh contexts instead of waiting while these streams drain
+    Ctx* list = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        list = g_free;
+        g_free = nullptr;
+    }
+    if (list == nullptr) { return; }
+    Ctx* last = list;
+    for (Ctx* c = list; c != nullptr; c = c->next) {
         for (cudaStream_t s : {c->stream, c->side, c->aux}) {
             if (s != nullptr) { cudaStreamSynchronize(s); }
         }
@@ -366,7 +375,11 @@ void trim_idle()
             b.cap = 0;
         }
         cudaStreamSynchronize(c->stream);
+        last = c;
     }
+    std::lock_guard<std::mutex> lk(g_mu);
+    last->next = g_free;
+    g_free = list;
     if (g_pool != nullptr) { cudaMemPoolTrimTo(g_pool, 0); }
 }
 

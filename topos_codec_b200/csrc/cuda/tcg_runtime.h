@@ -38,14 +38,14 @@ struct HBuf {
 enum BufId {
     B_PIX, B_COEF, B_MASK, B_DCM, B_NOPS, B_OPOFF, B_HIST, B_STAB, B_OPS, B_STAGE,
     B_SRES, B_PKT, B_DESC, B_FRES, B_ALPHA, B_DEC_COEF, B_DEC_TAB, B_DEC_OUT, B_DEC_PKT,
-    B_DEC_RES, B_TMP0, B_TMP1, B_SIZED_PIX, B_SIZED_PKT, B_COUNT
+    B_DEC_RES, B_TMP0, B_TMP1, B_SIZED_PIX, B_SIZED_PKT, B_UMAP, B_COUNT
 };
 
 // Kernel identities for optional per-kernel event timing.
 enum KernelId {
     K_FDCT, K_TOKENS, K_SELECT, K_OPSCAN, K_OPGEN, K_CHAIN, K_ALPHA, K_PACK_SIZES, K_PACK_COPY, K_PACK_CRC,
     K_PACK_HEADER, K_DCRC, K_DTABLES, K_DCHAIN, K_DCHAIN_W, K_DIDCT, K_DALPHA, K_DALPHA_MED, K_DCONCEAL, K_DEBLOCK_V,
-    K_DEBLOCK_H, K_WALK, K_DECIMATE, K_COUNT
+    K_DEBLOCK_H, K_WALK, K_DECIMATE, K_UNIT_MAP, K_COUNT
 };
 
 constexpr int MAX_PROF = 64;

@@ -12,9 +12,10 @@
 // the estimated device bytes of everything in flight fit the server's budget
 // and the device's free memory (the first request of a batch always goes, so
 // one large request cannot stall the queue). Call contexts keep the buffers
-// of their largest batch; when a batch leaves less than an eighth of the
-// device's memory free, the worker gives idle contexts' buffers back, so the
-// server leaves room for the process's other allocations. V8 decodes run through the
+// of their largest batch; when a batch leaves less than a sixteenth of the
+// device's memory free, the worker gives idle contexts' buffers back (at most
+// once a second), so the server leaves room for the process's other
+// allocations. V8 decodes run through the
 // single-frame V8 decoder (the batched decode takes V7 packets only, as the
 // reference's does). Each request's latency is measured from submission to
 // completion.
@@ -75,6 +76,7 @@ struct tcg_server {
     uint64_t inflight = 0;       // estimated device bytes of the batches running
     uint32_t max_frames = 64;
     uint32_t idle[2] = {0, 0};   // idle workers per direction (0 decode, 1 encode)
+    Clock::time_point last_trim{};
     bool stop = false;
     std::vector<std::thread> workers;
     int device = 0;
@@ -213,7 +215,19 @@ void worker(tcg_server* s, bool encode)
         run_batch(s, batch, encode);
         uint64_t total = 0;
         const uint64_t fr = device_free(&total);
-        if (total != 0u && fr < total / 8u) { tcg_trim_idle(); }
+        if (total != 0u && fr < total / 16u) {
+            // at most once a second: the next calls reallocate what this frees
+            const Clock::time_point now = Clock::now();
+            bool go = false;
+            {
+                std::lock_guard<std::mutex> g(s->mu);
+                if (now - s->last_trim > std::chrono::seconds(1)) {
+                    s->last_trim = now;
+                    go = true;
+                }
+            }
+            if (go) { tcg_trim_idle(); }
+        }
         std::lock_guard<std::mutex> g(s->mu);
         s->inflight -= used;
         if (!q.empty()) { s->cv_work.notify_all(); }
