@@ -10,7 +10,7 @@ no deblocking or refined qp table, so those features are off).
 The load generator is open-loop: arrivals follow their schedule whatever the
 server does. Input planes and packets are shared, read-only, per (resolution,
 tier); every request gets its own output buffer from a pool that is provisioned
-before the stream for half a second of arrivals and grows when all are in
+before the stream for a second of arrivals and grows when all are in
 use, so a busy server never delays the next arrival. Past saturation an
 arrival that finds 512 requests unfinished is shed and counted as dropped. Latency runs
 from a request's scheduled arrival to the moment its completion is seen
@@ -108,7 +108,7 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
     for (wh, share) in res_mix:
         for t in TIERS:
             if (wh, t) in kinds:
-                n = int(rate_rps * share / len(TIERS) * 0.5 * 0.5) + 2
+                n = int(rate_rps * share / len(TIERS) * 0.5 * 1.0) + 2
                 kinds[(wh, t)].provision(n, n)
     torch.cuda.synchronize()
     srv = B.Server(codec, max_batch_frames=max_batch_frames, workers=workers)
@@ -130,8 +130,8 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
             with cv:
                 # scheduled arrival to completion: the generator's lag before
                 # submission plus the server's submission-to-completion time
-                # (completions are collected in submission order, so the time
-                # this thread sees one would add the wait for older requests)
+                # (collectors take requests in submission order, so the time
+                # one sees a completion could include the wait for older ones)
                 records.append((kind[0], enc, (t_sub - t_sched) * 1e3 + ms, ms))
                 if st not in (0, 1):
                     errors[0] += 1
@@ -140,8 +140,11 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
     def kind_obj(k):
         return kinds[k]
 
-    th = threading.Thread(target=waiter)
-    th.start()
+    # several collectors, so one slow request does not hold back the buffers
+    # of the faster ones submitted after it
+    ths = [threading.Thread(target=waiter) for _ in range(8)]
+    for th in ths:
+        th.start()
     weights = [w for _, w in res_mix]
     t0 = time.perf_counter()
     t_next = t0
@@ -177,7 +180,8 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
         closing.set()
         with cv:
             cv.notify_all()
-        th.join()
+        for th in ths:
+            th.join()
         srv.close()
     wall = time.perf_counter() - t0
     out = {"offered_rps": rate_rps, "requests": n, "duration_s": round(wall, 2), "throughput_rps": n / wall,
