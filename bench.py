@@ -660,7 +660,8 @@ def main():
         from topos_codec_b200 import serving
         floors = [serving.single_frame_floor(gpu, 1920, 1080, "422", g) for g in ("v7", "v8")]
         kinds = serving._kinds(gpu, torch, dev, 0, "v7")
-        sat = serving.saturation_rps(gpu, kinds=kinds)
+        pk = serving.peak_rps(gpu, kinds=kinds)
+        sat = pk["sustained_rps"]
         # a short discarded trace first: the decode-tiling tuner times the tilings
         # on the first batch of each batch-size class
         serving.run_trace(gpu, rate_rps=0.5 * sat, duration_s=3.0, seed=7, kinds=kinds)
@@ -681,7 +682,8 @@ def main():
         gpu._lib.tcg_release_idle_memory()
         # the same stream coded as V8 (segmented rANS): many short chains per frame
         k8 = serving._kinds(gpu, torch, dev, 0, "v8")
-        sat8 = serving.saturation_rps(gpu, generation="v8", kinds=k8)
+        pk8 = serving.peak_rps(gpu, generation="v8", kinds=k8)
+        sat8 = pk8["sustained_rps"]
         serving.run_trace(gpu, rate_rps=0.5 * sat8, duration_s=3.0, seed=7, generation="v8", kinds=k8)
         v8_half = serving.run_trace(gpu, rate_rps=0.5 * sat8, duration_s=args.serve_seconds, seed=50,
                                     generation="v8", kinds=k8)

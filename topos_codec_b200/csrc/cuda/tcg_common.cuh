@@ -256,15 +256,20 @@ __device__ inline void idct8x8(const int32_t c[64], int32_t xh[64])
 // from map[CTA], the unit holding the CTA's first block, and a short forward
 // step over the units' first blocks: units are in increasing order of their
 // first block and the first starts at block 0. k_unit_map fills map with one
-// thread per unit (unit i's first block at starts[i * stride]).
+// thread per 32-block chunk, each a binary search over the units' first blocks
+// (unit i's first block at starts[i * stride]).
 static __global__ void k_unit_map(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t n, uint32_t total,
                                   uint32_t* __restrict__ map)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) { return; }
-    const uint32_t b0 = starts[(size_t)i * stride];
-    const uint32_t b1 = i + 1u < n ? starts[(size_t)(i + 1u) * stride] : total;
-    for (uint32_t c = (b0 + 31u) / 32u; c * 32u < b1; ++c) { map[c] = i; }
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((uint64_t)c * 32u >= total) { return; }
+    const uint32_t gb = c * 32u;
+    uint32_t lo = 0, hi = n - 1u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (starts[(size_t)mid * stride] <= gb) { lo = mid; } else { hi = mid - 1u; }
+    }
+    map[c] = lo;
 }
 
 __device__ __forceinline__ uint32_t unit_of(const uint32_t* __restrict__ starts, uint32_t stride, uint32_t n,

@@ -1883,7 +1883,7 @@ static int32_t decode_launch(Ctx* C, const tcg_dec_frame* frames, uint32_t count
             g_tune[cls] = (int8_t)best;
         }
         uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
-        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (nc + 255u) / 256u, 256, 0, d_cb, 1u, nc, (uint32_t)nblk, d_umap);
+        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((nblk + 8191u) / 8192u), 256, 0, d_cb, 1u, nc, (uint32_t)nblk, d_umap);
         TCG_LAUNCH(C, K_DIDCT, k_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sl, d_cs, nc, d_st, d_pl,
                    d_tab, d_coef, d_status, (uint32_t)nblk, d_cb, d_umap, d_out);
     }
@@ -2268,7 +2268,7 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
     }
     if (nblk > 0u) {
         uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
-        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (nplanes + 255u) / 256u, 256, 0, d_pi, V8_PINFO, nplanes, (uint32_t)nblk,
+        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((nblk + 8191u) / 8192u), 256, 0, d_pi, V8_PINFO, nplanes, (uint32_t)nblk,
                    d_umap);
         TCG_LAUNCH(C, K_DIDCT, k_v8_didct, (uint32_t)((nblk + RB_BLOCKS - 1u) / RB_BLOCKS), 256, 0, d_sg, d_pi, nplanes,
                    d_q, d_coef, (uint32_t)nblk, d_umap, d_out);

@@ -1735,7 +1735,7 @@ static int32_t encode_launch(Ctx* C, const tcg_enc_frame* frames, uint32_t count
         bool any_wide = false;
         for (uint32_t pg : cplanes) { any_wide = any_wide || planes[pg].bd > 12u; }
         uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
-        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((cplanes.size() + 255u) / 256u), 256, 0, d_ps, 1u,
+        TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((nblk + 8191u) / 8192u), 256, 0, d_ps, 1u,
                    (uint32_t)cplanes.size(), (uint32_t)nblk, d_umap);
         TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + FB_BLOCKS - 1u) / FB_BLOCKS), 256, 0, d_pl, d_cp,
                    (uint32_t)cplanes.size(), (uint32_t)nblk, d_pix, d_coef, d_mask, d_ps, d_umap);
@@ -1984,7 +1984,7 @@ static int32_t encode_launch_v8(Ctx* C, const tcg_enc_frame* frames, uint32_t co
     bool any_wide = false;
     for (const EPlane& P : planes) { any_wide = any_wide || P.bd > 12u; }
     uint32_t* d_umap = dptr<uint32_t>(C, B_UMAP);
-    TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((planes.size() + 255u) / 256u), 256, 0, d_ps, 1u,
+    TCG_LAUNCH(C, K_UNIT_MAP, k_unit_map, (uint32_t)((nblk + 8191u) / 8192u), 256, 0, d_ps, 1u,
                (uint32_t)planes.size(), (uint32_t)nblk, d_umap);
     TCG_LAUNCH(C, K_FDCT, k_fdct, (uint32_t)((nblk + FB_BLOCKS - 1u) / FB_BLOCKS), 256, 0, d_pl, d_cp,
                (uint32_t)planes.size(), (uint32_t)nblk, d_pix, d_coef, d_mask, d_ps, d_umap);

@@ -104,7 +104,7 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
     rng = random.Random(seed)
     kinds = kinds or _kinds(codec, torch, dev, seed, generation)
     res_mix = resolutions or RESOLUTIONS
-    # output buffers for half a second of arrivals per (resolution, tier, direction)
+    # output buffers for a second of arrivals per (resolution, tier, direction)
     for (wh, share) in res_mix:
         for t in TIERS:
             if (wh, t) in kinds:
@@ -203,6 +203,18 @@ def saturation_rps(codec, n: int = 96, seed: int = 1, max_batch_frames: int = 32
     dev = torch.device("cuda", torch.cuda.current_device())
     kinds = kinds or _kinds(codec, torch, dev, seed, generation)
     return max(_saturation_pass(codec, n, seed, max_batch_frames, workers, kinds) for _ in range(2))
+
+
+def peak_rps(codec, generation: str = "v7", kinds=None, seconds: float = 6.0, workers: int = 4) -> Dict:
+    """The server's sustained peak: an open-loop stream offered at 1.5 times
+    the burst rate (saturation_rps) for `seconds`, with arrivals past 256
+    unfinished requests shed; the peak is the rate at which it completed
+    requests (a burst drains queues built before it, so it overstates what a
+    stream sustains)."""
+    burst = saturation_rps(codec, generation=generation, kinds=kinds, workers=workers)
+    r = run_trace(codec, rate_rps=1.5 * burst, duration_s=seconds, seed=3, generation=generation, kinds=kinds,
+                  workers=workers, max_outstanding=256)
+    return {"burst_rps": burst, "sustained_rps": min(burst, r["throughput_rps"]), "dropped": r["dropped"]}
 
 
 def _saturation_pass(codec, n, seed, max_batch_frames, workers, kinds) -> float:
