@@ -793,8 +793,13 @@ __global__ void __launch_bounds__(32) k_v8_dtab(const tcg_v8_tile* __restrict__ 
     }
 }
 
-// one lane per segment, up to 32 segments of one tile per warp
-__global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ wtile,
+// One thread per segment, up to V8DC_LANES segments of one tile per CTA: the
+// tile's tables are staged once per CTA, so four warps share 12.5 KB of shared
+// memory (one warp per CTA left the SMs at about 14 resident warps, too few to
+// hide the chains' latency).
+constexpr uint32_t V8DC_LANES = 128u;
+
+__global__ void __launch_bounds__(V8DC_LANES) k_v8_dchain(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ wtile,
                                                   const int32_t* __restrict__ wsegs, const uint32_t* __restrict__ pinfo,
                                                   const uint8_t* __restrict__ tile_ok, const uint8_t* __restrict__ pkt,
                                                   const uint8_t* __restrict__ tabs, int32_t* __restrict__ coef,
@@ -805,11 +810,11 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
     const uint32_t ti = wtile[blockIdx.x];
     if (tile_ok[ti] == 0u) { return; }  // concealed whole: coefficients stay zero
     const uint8_t* tb = tabs + (size_t)ti * DTAB_BYTES;
-    for (uint32_t k = lane; k < V8D_SMEM / 16u; k += 32u) {
+    for (uint32_t k = lane; k < V8D_SMEM / 16u; k += V8DC_LANES) {
         reinterpret_cast<uint4*>(vsm)[k] = reinterpret_cast<const uint4*>(tb)[k];
     }
-    __syncwarp();
-    const int32_t si = wsegs[blockIdx.x * 32u + lane];
+    __syncthreads();
+    const int32_t si = wsegs[blockIdx.x * V8DC_LANES + lane];
     if (si < 0) { return; }
     const tcg_v8_seg& S = segs[si];
     const uint32_t* hdr = reinterpret_cast<const uint32_t*>(tb + TAB_HDR);
@@ -860,9 +865,8 @@ __global__ void __launch_bounds__(32) k_v8_dchain(const tcg_v8_seg* __restrict__
 }
 
 // Reconstruction of every block of the batch's planes (k_didct's
-// arithmetic): the block's plane by a binary search over the planes' first
-// blocks, its segment by the plane's segment size, its quantiser steps by the
-// segment.
+// arithmetic): the block's plane from the unit map, its segment by the
+// plane's segment size, its quantiser steps by the segment.
 __global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__ segs, const uint32_t* __restrict__ pinfo,
                                                   uint32_t nplanes, const uint32_t* __restrict__ q,
                                                   const int32_t* __restrict__ coef, uint32_t total,
@@ -2205,9 +2209,11 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
     std::vector<uint32_t> wtile;
     std::vector<int32_t> wsegs;
     for (uint32_t t = 0; t < ntile; ++t) {
-        for (uint32_t k = 0; k < tiles[t].nseg; k += 32u) {
+        for (uint32_t k = 0; k < tiles[t].nseg; k += V8DC_LANES) {
             wtile.push_back(t);
-            for (uint32_t l = 0; l < 32u; ++l) { wsegs.push_back(k + l < tiles[t].nseg ? (int32_t)(tiles[t].seg0 + k + l) : -1); }
+            for (uint32_t l = 0; l < V8DC_LANES; ++l) {
+                wsegs.push_back(k + l < tiles[t].nseg ? (int32_t)(tiles[t].seg0 + k + l) : -1);
+            }
         }
     }
     const size_t desc = align_up((size_t)nseg * sizeof(tcg_v8_seg) + 16u, 256) +
@@ -2263,7 +2269,7 @@ static int32_t decode_v8_impl(Ctx* C, const tcg_v8_job* J, uint32_t count)
         TCG_LAUNCH(C, K_DTABLES, k_v8_dtab, ntile, 32, 0, d_tl, d_pkt, d_tab);
     }
     if (!wtile.empty()) {
-        TCG_LAUNCH(C, K_DCHAIN, k_v8_dchain, (uint32_t)wtile.size(), 32, V8D_SMEM, d_sg, d_wt, d_ws, d_pi, d_ok, d_pkt,
+        TCG_LAUNCH(C, K_DCHAIN, k_v8_dchain, (uint32_t)wtile.size(), V8DC_LANES, V8D_SMEM, d_sg, d_wt, d_ws, d_pi, d_ok, d_pkt,
                    d_tab, d_coef, d_fail);
     }
     if (nblk > 0u) {
