@@ -688,7 +688,8 @@ def main():
         v8_half = serving.run_trace(gpu, rate_rps=0.5 * sat8, duration_s=args.serve_seconds, seed=50,
                                     generation="v8", kinds=k8)
         del k8
-        keys = ("offered_rps", "throughput_rps", "p50_ms", "p99_ms", "p999_ms", "errors", "by_resolution")
+        keys = ("offered_rps", "throughput_rps", "p50_ms", "p99_ms", "p999_ms", "errors", "dropped", "by_resolution",
+                "server_side", "submit_lag")
         served.update({"load": 0.5, "saturation_rps": sat,
                        "mix": "50/50 encode/decode; 1080p 40 %, 2160p 40 %, 720p 20 %; 10-bit 4:2:2 tiers 422/HQ",
                        "latency": "client side, from each request's scheduled (open-loop Poisson) arrival to its "

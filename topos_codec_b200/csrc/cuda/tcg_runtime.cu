@@ -378,6 +378,8 @@ void trim_idle()
             b.cap = 0;
         }
         cudaStreamSynchronize(c->stream);
+        for (void* p : c->h_retired) { cudaFreeHost(p); }
+        c->h_retired.clear();
         last = c;
     }
     std::lock_guard<std::mutex> lk(g_mu);
@@ -427,8 +429,7 @@ bool hreserve(Ctx* c, int id, size_t bytes)
     HBuf& b = c->h[id];
     if (bytes <= b.cap) { return true; }
     if (b.p != nullptr) {
-        cudaStreamSynchronize(c->stream);
-        cudaFreeHost(b.p);
+        c->h_retired.push_back(b.p);
         b.p = nullptr;
         b.cap = 0;
     }
@@ -465,6 +466,7 @@ extern "C" void tcg_shutdown(void)
         for (auto& b : c->d) { if (b.p) { cudaFreeAsync(b.p, c->stream); } }
         if (c->stream != nullptr) { cudaStreamSynchronize(c->stream); }
         for (auto& b : c->h) { if (b.p) { cudaFreeHost(b.p); } }
+        for (void* p : c->h_retired) { cudaFreeHost(p); }
         for (cudaEvent_t e : {c->fork, c->join, c->afork, c->ajoin, c->gate, c->t0, c->t1}) {
             if (e != nullptr) { cudaEventDestroy(e); }
         }

@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <vector>
 
 #include "../tcg_device.h"
 
@@ -70,6 +71,10 @@ struct Ctx {
     bool prof = false;
     DBuf d[B_COUNT];
     HBuf h[4];
+    // pinned buffers outgrown by h[]: freeing pinned memory synchronises the
+    // whole device, so they are freed only where the device is idle for this
+    // context anyway (trim_idle, shutdown)
+    std::vector<void*> h_retired;
     Ctx* next = nullptr;
 };
 

@@ -196,10 +196,16 @@ void worker(tcg_server* s, bool encode)
             s->cv_work.wait(lk, [&] { return s->stop || !q.empty(); });
             idle--;
             if (s->stop && q.empty()) { return; }
+        }
+        // free memory is read without the lock: the driver call can wait behind
+        // another thread's allocation, and submissions must not wait for it
+        const uint64_t free_b = device_free();
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (q.empty()) { continue; }  // another worker took them meanwhile
             // an even share of what has arrived when other workers are idle too
             const size_t share = (q.size() + idle) / (idle + 1u);
             const size_t take = std::min<size_t>(std::max<size_t>(share, 1u), s->max_frames);
-            const uint64_t free_b = device_free();
             const uint64_t room = s->budget > s->inflight ? s->budget - s->inflight : 0u;
             const uint64_t cap = free_b == 0 ? room : std::min<uint64_t>(room, free_b - free_b / 8);
             while (!q.empty() && batch.size() < take) {

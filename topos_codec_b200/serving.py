@@ -132,7 +132,8 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
                 # submission plus the server's submission-to-completion time
                 # (collectors take requests in submission order, so the time
                 # one sees a completion could include the wait for older ones)
-                records.append((kind[0], enc, (t_sub - t_sched) * 1e3 + ms, ms))
+                records.append((kind[0], enc, (t_sub - t_sched) * 1e3 + ms, ms, (t_sub - t_sched) * 1e3,
+                                t_sched - t0))
                 if st not in (0, 1):
                     errors[0] += 1
                 (kind_obj(kind).free_out if enc else kind_obj(kind).free_dec).append(buf)
@@ -188,6 +189,11 @@ def run_trace(codec, rate_rps: float, duration_s: float, seed: int = 0, max_batc
            "errors": errors[0], "dropped": dropped, "generation": generation}
     out.update(_summary([r[2] for r in records]))
     out["server_side"] = _summary([r[3] for r in records])
+    out["submit_lag"] = _summary([r[4] for r in records])  # the generator's own delay
+    # when the worst client latencies arrived (seconds into the stream)
+    worst = sorted(records, key=lambda r: -r[2])[:8]
+    out["worst"] = [{"at_s": round(r[5], 3), "ms": round(r[2], 1), "server_ms": round(r[3], 1),
+                     "lag_ms": round(r[4], 1), "size": f"{r[0][0]}x{r[0][1]}", "encode": r[1]} for r in worst]
     out["by_resolution"] = {f"{w}x{h}": _summary([r[2] for r in records if r[0] == (w, h)]) for (w, h), _ in res_mix}
     out["by_direction"] = {"encode": _summary([r[2] for r in records if r[1]]),
                            "decode": _summary([r[2] for r in records if not r[1]])}
