@@ -433,7 +433,10 @@ bool hreserve(Ctx* c, int id, size_t bytes)
         b.p = nullptr;
         b.cap = 0;
     }
-    size_t want = bytes + bytes / 4 + 4096;
+    // pinning host memory takes tens of milliseconds and holds up other CUDA
+    // calls meanwhile, so these small staging buffers grow by doubling from
+    // 16 MB and rarely grow at all
+    size_t want = std::max<size_t>(bytes * 2u, 16u << 20);
     if (cudaMallocHost(&b.p, want) != cudaSuccess) {
         cudaGetLastError();
         b.p = nullptr;
@@ -521,6 +524,28 @@ extern "C" int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uin
 extern "C" void tcg_trim_idle(void)
 {
     if (tcg::ensure_init()) { tcg::trim_idle(); }
+}
+
+extern "C" int32_t tcg_pool_reserve(uint64_t bytes)
+{
+    if (!tcg::ensure_init()) { return TCG_ERR_NOT_IMPLEMENTED; }
+    if (bytes == 0u) { return 0; }
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return TCG_ERR_OUT_OF_MEMORY;
+    }
+    void* p = nullptr;
+    int32_t rc = 0;
+    if (cudaMallocFromPoolAsync(&p, bytes, tcg::g_pool, s) == cudaSuccess) {
+        cudaFreeAsync(p, s);
+    } else {
+        cudaGetLastError();
+        rc = TCG_ERR_OUT_OF_MEMORY;
+    }
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 extern "C" void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes)

@@ -21,6 +21,7 @@
 // completion.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -283,6 +284,15 @@ TC_EXPORT int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t ma
     s->budget = max_bytes_in_flight == 0u ? UINT64_MAX : max_bytes_in_flight;
     s->max_frames = max_batch_frames;
     s->device = dev;
+    {
+        // map memory for the workers' buffers now: a call that grows its
+        // buffers while others run would otherwise map new memory, and that
+        // stalled the device for up to 0.6 s under a V8 request stream
+        uint64_t fr = 0, tot = 0;
+        tcg_mem_info(&fr, &tot);
+        const uint64_t want = std::min<uint64_t>(fr / 2u, 64ull << 30);
+        if (want > (1ull << 30)) { (void)tcg_pool_reserve(want); }
+    }
     for (uint32_t i = 0; i < workers; ++i) {
         s->workers.emplace_back(worker, s, true);
         s->workers.emplace_back(worker, s, false);

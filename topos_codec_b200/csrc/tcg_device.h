@@ -145,6 +145,10 @@ int32_t tcg_read_device(void* dst, const void* src, size_t n);
 void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes);
 /* gives back the device buffers idle call contexts keep from earlier calls */
 void tcg_trim_idle(void);
+/* maps bytes of device memory into the library's memory pool ahead of use
+ * (allocated and freed at once; the pool keeps it), so that calls that grow
+ * their buffers later take it from the pool instead of mapping new memory */
+int32_t tcg_pool_reserve(uint64_t bytes);
 
 /* Structural walk of packets that live in device memory: per packet a record of
  * TCG_WALK_REC bytes = [64: packet bytes 0..60, zero beyond the packet]
