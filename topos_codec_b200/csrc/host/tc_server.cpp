@@ -78,6 +78,7 @@ struct tcg_server {
     uint32_t max_frames = 64;
     uint32_t idle[2] = {0, 0};   // idle workers per direction (0 decode, 1 encode)
     Clock::time_point last_trim{};
+    uint64_t batch_bytes = UINT64_MAX;  // estimated device bytes of one batch at most
     bool stop = false;
     std::vector<std::thread> workers;
     int device = 0;
@@ -211,7 +212,7 @@ void worker(tcg_server* s, bool encode)
             const uint64_t cap = free_b == 0 ? room : std::min<uint64_t>(room, free_b - free_b / 8);
             while (!q.empty() && batch.size() < take) {
                 const uint64_t b = q.front().bytes;
-                if (!batch.empty() && used + b > cap) { break; }
+                if (!batch.empty() && (used + b > cap || used + b > s->batch_bytes)) { break; }
                 used += b;
                 batch.push_back(q.front());
                 q.pop_front();
@@ -291,7 +292,12 @@ TC_EXPORT int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t ma
         uint64_t fr = 0, tot = 0;
         tcg_mem_info(&fr, &tot);
         const uint64_t want = std::min<uint64_t>(fr / 2u, 64ull << 30);
-        if (want > (1ull << 30)) { (void)tcg_pool_reserve(want); }
+        if (want > (1ull << 30) && tcg_pool_reserve(want) == 0) {
+            // every worker's context keeps its largest batch's buffers (and a
+            // context serves either direction), so batches are sized for all
+            // of them to fit in what was mapped
+            s->batch_bytes = want / (3u * workers);
+        }
     }
     for (uint32_t i = 0; i < workers; ++i) {
         s->workers.emplace_back(worker, s, true);
