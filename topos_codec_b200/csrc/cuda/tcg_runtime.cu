@@ -548,6 +548,8 @@ extern "C" int32_t tcg_pool_reserve(uint64_t bytes)
     return rc;
 }
 
+// Free device memory as the library can use it: the device's free memory plus
+// what the library's pool holds mapped but unused.
 extern "C" void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes)
 {
     size_t f = 0, t = 0;
@@ -555,6 +557,14 @@ extern "C" void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes)
         cudaGetLastError();
         f = t = 0;
     }
+    uint64_t reserved = 0, used = 0;
+    if (f != 0u && tcg::g_pool != nullptr &&
+        cudaMemPoolGetAttribute(tcg::g_pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+        cudaMemPoolGetAttribute(tcg::g_pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+        reserved > used) {
+        f += reserved - used;
+    }
+    cudaGetLastError();
     *free_bytes = f;
     *total_bytes = t;
 }

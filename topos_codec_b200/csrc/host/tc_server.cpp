@@ -98,13 +98,11 @@ uint64_t frame_bytes(uint32_t w, uint32_t h, bool encode)
     return encode ? px * 84u + (1u << 20) : px * 20u + (1u << 20);
 }
 
+// free device memory, counting what the library's pool holds mapped but unused
 uint64_t device_free(uint64_t* total = nullptr)
 {
-    size_t fr = 0, tot = 0;
-    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
+    uint64_t fr = 0, tot = 0;
+    tcg_mem_info(&fr, &tot);
     if (total != nullptr) { *total = tot; }
     return fr;
 }
