@@ -638,8 +638,8 @@ def main():
         target = len(gpu.encode(c24, sframes[0]))
         ref = B.ToposCodec(REF_LIB) if (rank == 0 and os.path.exists(REF_LIB)) else None
         r = WL.sized_vs_reference(gpu, ref, cfg, sframes, target, 0, 63, ref_threads=min(16, os.cpu_count() or 1))
-        r["workload"] = ("3840x2160 10-bit 4:2:2 HQ from host memory, tc_frame_encode_sized per frame in order, "
-                         "target = frame 0 at qp 24, qp 0..63")
+        r["workload"] = ("3840x2160 10-bit 4:2:2 HQ from host memory, tc_frame_encode_sized per frame in order "
+                         "after one untimed call, target = frame 0 at qp 24, qp 0..63")
         extra["sized_encode"] = r
         del sframes
         # preview decode: the batch's packets at half size (1920x1080, 24 zigzag coefficients kept)
