@@ -214,7 +214,7 @@ def sized_batch_vs_reference(product, reference, cfg: B.FrameConfig, frames, tar
     rcs = (ctypes.c_int32 * n)()
     # one untimed batch first, so that the searches' buffer growth stays out of
     # the time (the batch's searches carry no hint history)
-    for timed in (False, True):
+    for _ in range(2):
         t0 = time.perf_counter()
         rc = int(L.tcg_frame_encode_sized_batch(carr, iarr, ctypes.c_uint32(n), tarr, ctypes.c_uint8(qp_min),
                                                 ctypes.c_uint8(qp_max), qps, optr, ocap, st, rcs))
