@@ -8,7 +8,9 @@
 // workers are idle too, at most max_batch_frames - and codes them in one
 // batched call. Requests that arrive while batches run are picked up by the
 // next idle worker at once, so their work overlaps the batches already on the
-// GPU instead of waiting for them. Admission: a batch takes requests while
+// GPU instead of waiting for them. Half of each direction's workers take
+// frames up to 2560x1440 only, the others larger frames first, so small
+// requests always have a worker of their own. Admission: a batch takes requests while
 // the estimated device bytes of everything in flight fit the server's budget
 // and the device's free memory (the first request of a batch always goes, so
 // one large request cannot stall the queue). Call contexts keep the buffers
@@ -54,6 +56,7 @@ struct Request {
     uint16_t* planes[TC_FRAME_MAX_PLANES] = {nullptr, nullptr, nullptr, nullptr};
     size_t strides[TC_FRAME_MAX_PLANES] = {0, 0, 0, 0};
     uint64_t bytes = 0;  // estimated device footprint
+    bool big = false;    // above BIG_PIXELS luma samples
     bool v8 = false;     // decode of a V8 packet
     Clock::time_point t_submit;
 };
@@ -70,13 +73,13 @@ struct Result {
 struct tcg_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Request> q_enc, q_dec;
+    std::deque<Request> q[2][2];  // [encode][big]
     std::unordered_map<uint64_t, Result> done;
     uint64_t next_ticket = 1;
     uint64_t budget = 0;
     uint64_t inflight = 0;       // estimated device bytes of the batches running
     uint32_t max_frames = 64;
-    uint32_t idle[2] = {0, 0};   // idle workers per direction (0 decode, 1 encode)
+    uint32_t idle[2][2] = {{0, 0}, {0, 0}};  // idle workers [encode][lane: 0 small frames only, 1 any]
     Clock::time_point last_trim{};
     uint64_t batch_bytes = UINT64_MAX;  // estimated device bytes of one batch at most
     bool stop = false;
@@ -85,6 +88,10 @@ struct tcg_server {
 };
 
 namespace {
+
+// frames above this many luma samples (past 2560x1440) are served by the
+// general workers only
+constexpr uint64_t BIG_PIXELS = 2560ull * 1440ull;
 
 // device bytes one frame of w x h luma samples needs while it is coded, with
 // the buffers' growth margin: per 8x8 block of a 4:2:2 frame (two blocks per
@@ -182,29 +189,37 @@ void run_batch(tcg_server* s, std::vector<Request>& batch, bool encode)
     s->cv_done.notify_all();
 }
 
-void worker(tcg_server* s, bool encode)
+// A worker of lane 0 takes small frames only; a worker of lane 1 takes large
+// frames first and small ones when no large frame waits. So small requests
+// never queue behind a batch of large frames while a lane-0 worker is free.
+void worker(tcg_server* s, bool encode, int lane)
 {
     cudaSetDevice(s->device);
-    std::deque<Request>& q = encode ? s->q_enc : s->q_dec;
-    uint32_t& idle = s->idle[encode ? 1 : 0];
+    std::deque<Request>* qs = s->q[encode ? 1 : 0];
+    uint32_t* idle = s->idle[encode ? 1 : 0];
+    auto has_work = [&] { return !qs[0].empty() || (lane == 1 && !qs[1].empty()); };
     for (;;) {
         std::vector<Request> batch;
         uint64_t used = 0;
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            idle++;
-            s->cv_work.wait(lk, [&] { return s->stop || !q.empty(); });
-            idle--;
-            if (s->stop && q.empty()) { return; }
+            idle[lane]++;
+            s->cv_work.wait(lk, [&] { return s->stop || has_work(); });
+            idle[lane]--;
+            if (s->stop && !has_work()) { return; }
         }
         // free memory is read without the lock: the driver call can wait behind
         // another thread's allocation, and submissions must not wait for it
         const uint64_t free_b = device_free();
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (q.empty()) { continue; }  // another worker took them meanwhile
-            // an even share of what has arrived when other workers are idle too
-            const size_t share = (q.size() + idle) / (idle + 1u);
+            if (!has_work()) { continue; }  // another worker took them meanwhile
+            const bool big = lane == 1 && !qs[1].empty();
+            std::deque<Request>& q = qs[big ? 1 : 0];
+            // an even share of what has arrived when other workers that can
+            // take it are idle too
+            const uint32_t others = big ? idle[1] : idle[0] + idle[1];
+            const size_t share = (q.size() + others) / (others + 1u);
             const size_t take = std::min<size_t>(std::max<size_t>(share, 1u), s->max_frames);
             const uint64_t room = s->budget > s->inflight ? s->budget - s->inflight : 0u;
             const uint64_t cap = free_b == 0 ? room : std::min<uint64_t>(room, free_b - free_b / 8);
@@ -216,7 +231,7 @@ void worker(tcg_server* s, bool encode)
                 q.pop_front();
             }
             s->inflight += used;
-            if (!q.empty()) { s->cv_work.notify_all(); }  // more for the next idle worker
+            if (!qs[0].empty() || !qs[1].empty()) { s->cv_work.notify_all(); }  // more for the next idle worker
         }
         run_batch(s, batch, encode);
         uint64_t total = 0;
@@ -236,7 +251,7 @@ void worker(tcg_server* s, bool encode)
         }
         std::lock_guard<std::mutex> g(s->mu);
         s->inflight -= used;
-        if (!q.empty()) { s->cv_work.notify_all(); }
+        if (!qs[0].empty() || !qs[1].empty()) { s->cv_work.notify_all(); }
     }
 }
 
@@ -247,7 +262,7 @@ uint64_t submit(tcg_server* s, Request&& r, bool encode)
     r.encode = encode;
     r.t_submit = Clock::now();
     const uint64_t t = r.ticket;
-    (encode ? s->q_enc : s->q_dec).push_back(std::move(r));
+    s->q[encode ? 1 : 0][r.big ? 1 : 0].push_back(std::move(r));
     s->cv_work.notify_all();
     return t;
 }
@@ -297,9 +312,11 @@ TC_EXPORT int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t ma
             s->batch_bytes = want / (3u * workers);
         }
     }
+    // half of each direction's workers (rounded down) serve small frames only
     for (uint32_t i = 0; i < workers; ++i) {
-        s->workers.emplace_back(worker, s, true);
-        s->workers.emplace_back(worker, s, false);
+        const int lane = i < workers / 2u ? 0 : 1;
+        s->workers.emplace_back(worker, s, true, lane);
+        s->workers.emplace_back(worker, s, false, lane);
     }
     *out = s;
     return TC_OK;
@@ -329,6 +346,7 @@ TC_EXPORT int32_t tcg_server_submit_encode(tcg_server* s, const topos_frame_conf
     r.out = out;
     r.out_cap = out_cap;
     r.bytes = frame_bytes(cfg->visible_width, cfg->visible_height, true);
+    r.big = (uint64_t)cfg->visible_width * cfg->visible_height > BIG_PIXELS;
     *ticket = submit(s, std::move(r), true);
     return TC_OK;
 }
@@ -352,6 +370,7 @@ TC_EXPORT int32_t tcg_server_submit_decode(tcg_server* s, const uint8_t* packet,
         r.strides[p] = strides != NULL ? strides[p] : 0u;
     }
     r.bytes = frame_bytes(info.visible_width, info.visible_height, false);
+    r.big = (uint64_t)info.visible_width * info.visible_height > BIG_PIXELS;
     r.v8 = tc_packet_major(packet, size) == 8;
     *ticket = submit(s, std::move(r), false);
     return TC_OK;
