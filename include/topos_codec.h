@@ -311,8 +311,13 @@ int32_t tcg_frame_decode_v8_batch(const topos_batch_packet* packets, uint32_t co
  * other workers are idle too, at most max_batch_frames, 1..64) in one batched
  * call, and requests arriving while batches run are taken by the next idle
  * worker at once, so their work overlaps the batches already on the GPU.
- * A batch admits requests while the estimated device bytes of all batches in
- * flight fit max_bytes_in_flight (0 = no limit) and the device's free memory.
+ * Half of each direction's workers (rounded down) take frames up to
+ * 2560x1440 only. A batch admits requests while the estimated device bytes
+ * of all batches in flight fit max_bytes_in_flight (0 = no limit) and the
+ * device's free memory. Creating a server maps up to half of the free device
+ * memory (at most 64 GB) into the library's memory pool, so that workers'
+ * buffers do not map memory while other requests run; tcg_release_idle_memory
+ * gives back what idle contexts hold.
  * Every result equals the single-frame call's. tcg_server_wait blocks until
  * the ticket's request is done and returns its status (as tc_frame_encode /
  * tc_frame_decode would), its stats or frame information, and its latency
