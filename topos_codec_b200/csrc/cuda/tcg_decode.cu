@@ -598,7 +598,18 @@ __device__ __forceinline__ int64_t recon_clamp(uint32_t bd)
 
 // Phases 1-4 above; sh.blk is filled and visible (after a barrier) on entry.
 // coef points at block gb0 and holds nvalid blocks from there.
-__device__ __forceinline__ void recon_blocks(RShared& sh, const int32_t* __restrict__ coef, uint32_t nvalid)
+// The CTA's coefficients, loaded before the block facts are gathered so that
+// the loads overlap the lookups.
+__device__ __forceinline__ void recon_preload(const int32_t* __restrict__ coef, uint32_t nvalid, int4 pre[2])
+{
+#pragma unroll
+    for (uint32_t h = 0; h < 2u; ++h) {
+        const uint32_t idx = threadIdx.x + 256u * h;
+        pre[h] = (idx >> 4) < nvalid ? __ldg(reinterpret_cast<const int4*>(coef) + idx) : make_int4(0, 0, 0, 0);
+    }
+}
+
+__device__ __forceinline__ void recon_blocks(RShared& sh, const int4 pre[2], uint32_t nvalid)
 {
     const uint32_t t = threadIdx.x, w = t >> 5, lane = t & 31u;
     // dequantise into natural order
@@ -608,7 +619,7 @@ __device__ __forceinline__ void recon_blocks(RShared& sh, const int32_t* __restr
         const uint32_t b = idx >> 4, i0 = (idx & 15u) * 4u;
         const RBlock& R = sh.blk[b];
         if (b < nvalid && R.ok) {
-            const int4 v = __ldg(reinterpret_cast<const int4*>(coef) + idx);
+            const int4 v = pre[h];
             const int32_t vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
             for (uint32_t j = 0; j < 4u; ++j) {
@@ -875,6 +886,8 @@ __global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__
     __shared__ RShared sh;
     const uint32_t gb0 = blockIdx.x * RB_BLOCKS;
     const uint32_t nvalid = min(RB_BLOCKS, total - gb0);
+    int4 pre[2];
+    recon_preload(coef + (size_t)gb0 * 64u, nvalid, pre);
     if (threadIdx.x < 64u) { sh.zz[threadIdx.x] = k_zigzag[threadIdx.x]; }
     if (threadIdx.x < RB_BLOCKS) {
         RBlock R;
@@ -902,7 +915,7 @@ __global__ void __launch_bounds__(256) k_v8_didct(const tcg_v8_seg* __restrict__
         sh.blk[threadIdx.x] = R;
     }
     __syncthreads();
-    recon_blocks(sh, coef + (size_t)gb0 * 64u, nvalid);
+    recon_blocks(sh, pre, nvalid);
 }
 
 // ------------------------------------------------------------------ chain, warp tiling
@@ -1200,6 +1213,8 @@ __global__ void __launch_bounds__(256) k_didct(const DSlice* __restrict__ slices
     __shared__ RShared sh;
     const uint32_t gb0 = blockIdx.x * RB_BLOCKS;
     const uint32_t nvalid = min(RB_BLOCKS, total - gb0);
+    int4 pre[2];
+    recon_preload(coef + (size_t)gb0 * 64u, nvalid, pre);
     if (threadIdx.x < 64u) { sh.zz[threadIdx.x] = k_zigzag[threadIdx.x]; }
     if (threadIdx.x < RB_BLOCKS) {
         RBlock R;
@@ -1227,7 +1242,7 @@ __global__ void __launch_bounds__(256) k_didct(const DSlice* __restrict__ slices
         sh.blk[threadIdx.x] = R;
     }
     __syncthreads();
-    recon_blocks(sh, coef + (size_t)gb0 * 64u, nvalid);
+    recon_blocks(sh, pre, nvalid);
 }
 
 // Scaled delivery (reference color_store.h:223-313 scaled samples,
