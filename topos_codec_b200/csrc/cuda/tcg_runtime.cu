@@ -321,19 +321,41 @@ bool ensure_init()
 
 const DevTables& tables() { return g_tab; }
 
+// A thread with a lease class (the request server's workers: one class per
+// direction) takes an idle context of its class when there is one, so a
+// context keeps the buffers of one kind of work; other threads take the most
+// recently released context.
+static thread_local int t_lease_class = -1;
+
 Ctx* ctx_acquire()
 {
     if (!ensure_init()) { return nullptr; }
     {
         std::lock_guard<std::mutex> lk(g_mu);
-        if (g_free != nullptr) {
-            Ctx* c = g_free;
-            g_free = c->next;
+        Ctx** link = nullptr;
+        if (t_lease_class < 0) {
+            link = &g_free;
+        } else {
+            Ctx** unclassed = nullptr;
+            for (Ctx** l = &g_free; *l != nullptr; l = &(*l)->next) {
+                if ((*l)->cls == t_lease_class) {
+                    link = l;
+                    break;
+                }
+                if ((*l)->cls < 0 && unclassed == nullptr) { unclassed = l; }
+            }
+            if (link == nullptr) { link = unclassed; }
+        }
+        if (link != nullptr && *link != nullptr) {
+            Ctx* c = *link;
+            *link = c->next;
             c->next = nullptr;
+            c->cls = t_lease_class;
             return c;
         }
     }
     Ctx* c = new Ctx();
+    c->cls = t_lease_class;
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&c->gate, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
@@ -519,6 +541,11 @@ extern "C" int32_t tcg_prof_read(uint32_t id, const char** name, double* ms, uin
     if (ms) { *ms = tcg::g_prof_ms[id]; }
     if (launches) { *launches = tcg::g_prof_n[id]; }
     return 0;
+}
+
+extern "C" void tcg_set_lease_class(int32_t cls)
+{
+    tcg::t_lease_class = cls < 0 ? -1 : cls;
 }
 
 extern "C" void tcg_trim_idle(void)

@@ -76,6 +76,7 @@ struct Ctx {
     // context anyway (trim_idle, shutdown)
     std::vector<void*> h_retired;
     Ctx* next = nullptr;
+    int cls = -1;  // lease class of the thread that last used it (tcg_set_lease_class)
 };
 
 // Call bracketing: records the device start/end events and, with profiling

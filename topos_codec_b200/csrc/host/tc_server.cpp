@@ -17,7 +17,9 @@
 // of their largest batch; when a batch leaves less than a sixteenth of the
 // device's memory free, the worker gives idle contexts' buffers back (at most
 // once a second), so the server leaves room for the process's other
-// allocations. V8 decodes run through the
+// allocations. Each direction's workers lease their own contexts, so a
+// context holds one direction's buffers and all of them fit in the memory
+// mapped at start. V8 decodes run through the
 // single-frame V8 decoder (the batched decode takes V7 packets only, as the
 // reference's does). Each request's latency is measured from submission to
 // completion.
@@ -195,6 +197,7 @@ void run_batch(tcg_server* s, std::vector<Request>& batch, bool encode)
 void worker(tcg_server* s, bool encode, int lane)
 {
     cudaSetDevice(s->device);
+    tcg_set_lease_class(encode ? 1 : 0);  // a context keeps one direction's buffers
     std::deque<Request>* qs = s->q[encode ? 1 : 0];
     uint32_t* idle = s->idle[encode ? 1 : 0];
     auto has_work = [&] { return !qs[0].empty() || (lane == 1 && !qs[1].empty()); };

@@ -145,6 +145,9 @@ int32_t tcg_read_device(void* dst, const void* src, size_t n);
 void tcg_mem_info(uint64_t* free_bytes, uint64_t* total_bytes);
 /* gives back the device buffers idle call contexts keep from earlier calls */
 void tcg_trim_idle(void);
+/* the calling thread's lease class (-1: none): calls on a thread of class k
+ * reuse idle call contexts last used by class k, or unused ones */
+void tcg_set_lease_class(int32_t cls);
 /* maps bytes of device memory into the library's memory pool ahead of use
  * (allocated and freed at once; the pool keeps it), so that calls that grow
  * their buffers later take it from the pool instead of mapping new memory */
