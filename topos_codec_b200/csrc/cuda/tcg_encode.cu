@@ -172,14 +172,13 @@ __global__ void __launch_bounds__(256) k_fdct(const EPlane* __restrict__ planes,
 #pragma unroll
         for (int y = 0; y < 8; ++y) { col[y] = sa[b * FB_P + y * 8u + v]; }
         fwd8<int32_t>(col, F);
-        const int64_t fc = P.fclamp;
+        const int32_t fc = (int32_t)P.fclamp;  // 2^25 up to 12 bits
         const bool one = P.q_is_one != 0u;
 #pragma unroll
         for (int uu = 0; uu < 8; ++uu) {
             const uint32_t i = (uint32_t)uu * 8u + v;  // natural position
-            int64_t c = F[uu];
-            c = c > fc ? fc : (c < -fc ? -fc : c);
-            const uint32_t mag = (uint32_t)(c < 0 ? -c : c);
+            const int32_t c = min(max(F[uu], -fc), fc);
+            const uint32_t mag = (uint32_t)abs(c);
             uint32_t qm;
             if (one) {
                 qm = mag;
@@ -199,18 +198,20 @@ __global__ void __launch_bounds__(256) k_fdct(const EPlane* __restrict__ planes,
         const uint32_t idx = t + 256u * h;  // 16-byte piece of the CTA's coefficients
         const uint32_t bb = idx >> 4, i0 = (idx & 15u) * 4u;
         const bool live = s_pl[bb] != 0xFFFFFFFFu;
-        uint64_t m = 0;
+        uint32_t m = 0;
         if (live) {
             int4 q;
             q.x = sq[bb * FB_P + i0]; q.y = sq[bb * FB_P + i0 + 1u];
             q.z = sq[bb * FB_P + i0 + 2u]; q.w = sq[bb * FB_P + i0 + 3u];
             reinterpret_cast<int4*>(coef + (size_t)gb0 * 64u)[idx] = q;
-            m = (uint64_t)((q.x != 0) | ((q.y != 0) << 1) | ((q.z != 0) << 2) | ((q.w != 0) << 3)) << i0;
+            m = (uint32_t)((q.x != 0) | ((q.y != 0) << 1) | ((q.z != 0) << 2) | ((q.w != 0) << 3)) << (i0 & 31u);
         }
-        // the block's 16 pieces sit in 16 neighbouring lanes
+        // the block's 16 pieces sit in 16 neighbouring lanes: the first 8 hold
+        // positions 0..31, the next 8 positions 32..63
 #pragma unroll
-        for (uint32_t d = 1; d < 16u; d <<= 1) { m |= __shfl_xor_sync(0xFFFFFFFFu, m, d); }
-        if (live && (idx & 15u) == 0u) { mask[gb0 + bb] = m & ~(uint64_t)1; }
+        for (uint32_t d = 1; d < 8u; d <<= 1) { m |= __shfl_xor_sync(0xFFFFFFFFu, m, d); }
+        const uint32_t hi = __shfl_down_sync(0xFFFFFFFFu, m, 8);
+        if (live && (idx & 15u) == 0u) { mask[gb0 + bb] = ((uint64_t)hi << 32 | m) & ~(uint64_t)1; }
     }
 }
 
