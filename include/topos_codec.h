@@ -315,7 +315,9 @@ int32_t tcg_frame_decode_v8_batch(const topos_batch_packet* packets, uint32_t co
  * 2560x1440 only. A batch admits requests while the estimated device bytes
  * of all batches in flight fit max_bytes_in_flight (0 = no limit) and 7/8 of
  * the device memory that was free when the server was created (it is read
- * once: querying it while requests run stalled them). Creating a server maps up to half of the free device
+ * once: querying it while requests run stalled them). A worker that finds
+ * fewer than four V7-R2 requests waits up to 4 ms for more; V8 requests go at
+ * once. Creating a server maps up to half of the free device
  * memory (at most 64 GB) into the library's memory pool, so that workers'
  * buffers do not map memory while other requests run; tcg_release_idle_memory
  * gives back what idle contexts hold.

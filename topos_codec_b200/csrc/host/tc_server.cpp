@@ -18,7 +18,10 @@
 // the pool's counters) stalled calls in flight for up to a second, and with
 // the queries gone the V8 stream's p99 fell from 100-700 ms to under 5 ms.
 // Each direction's workers lease their own contexts, so a context holds one
-// direction's buffers and all of them fit in the memory mapped at start. V8 decodes run through the
+// direction's buffers and all of them fit in the memory mapped at start. A
+// worker that finds fewer than four V7-R2 requests waits up to 4 ms for
+// more (a V7-R2 batch costs its longest slice chain whatever its size); V8
+// requests go at once. V8 decodes run through the
 // single-frame V8 decoder (the batched decode takes V7 packets only, as the
 // reference's does). Each request's latency is measured from submission to
 // completion.
@@ -208,6 +211,18 @@ void worker(tcg_server* s, bool encode, int lane)
             if (!has_work()) { continue; }  // another worker took them meanwhile
             const bool big = lane == 1 && !qs[1].empty();
             std::deque<Request>& q = qs[big ? 1 : 0];
+            {
+                // a V7-R2 batch costs its longest slice chain whatever its
+                // size: give a lone V7-R2 request a few milliseconds of company
+                const Request& f = q.front();
+                const bool v7 = f.encode ? f.cfg.reserved[0] != 9u : !f.v8;
+                if (v7 && q.size() < 4u && !s->stop) {
+                    const size_t n0 = q.size();
+                    s->cv_work.wait_for(lk, std::chrono::milliseconds(4),
+                                        [&] { return s->stop || q.size() >= 4u || q.size() < n0; });
+                    if (q.empty()) { continue; }
+                }
+            }
             // an even share of what has arrived when other workers that can
             // take it are idle too
             const uint32_t others = big ? idle[1] : idle[0] + idle[1];
